@@ -1,0 +1,348 @@
+#!/usr/bin/env python
+"""Time to k eigenpairs at residual <= 1e-10 ||A||_1 on B200.
+
+A step is one complete solve of the workload: numeric factorization ('sm')
+plus thick-restart Lanczos to convergence, with the k eigenpairs left in
+device memory.  `value` times steps with the matrix and its symbolic
+analysis already resident on the GPU (speigs_plan_solve_device); `e2e` times
+the drop-in call speigs() from host CSC arrays to host results, so the host
+analysis and every host<->device copy are inside.  N GPUs run N independent
+replicas (the single-operator path does not shard), so scaling is weak.
+
+--impl reference times the reference's own CPU solver (compiled from its
+sources into oracle/_ref, CHOLMOD stand-in and OpenBLAS) on the same
+workload with every host thread, on rank 0 only.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(ROOT, "sparse-eigs-mex_b200")
+REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libspeigs_ref.so")
+METRIC = "time to k eigenpairs @ resid 1e-10: mixed/learned vs plain FP64, same B200"
+TOL = 1e-10
+
+
+def import_pkg():
+    import importlib.util
+    if "speigs_b200" in sys.modules:
+        return sys.modules["speigs_b200"]
+    spec = importlib.util.spec_from_file_location(
+        "speigs_b200", os.path.join(PKG_DIR, "__init__.py"), submodule_search_locations=[PKG_DIR])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["speigs_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def workloads(w, s):
+    return {
+        "lap46": dict(desc="3-D 7-point Dirichlet Laplacian 46^3 (n=97,336), k=6 smallest ('sm', "
+                           "shift-invert), FP64 CSR, tol 1e-10",
+                      build=lambda: w.lap3d(46), k=6, which=s.SM,
+                      exact=lambda: w.spectrum3d(46)[:6]),
+        "lap20": dict(desc="3-D 7-point Dirichlet Laplacian 20^3 (n=8,000), k=6 'sm', tol 1e-10",
+                      build=lambda: w.lap3d(20), k=6, which=s.SM,
+                      exact=lambda: w.spectrum3d(20)[:6]),
+        "lap2d1000": dict(desc="2-D 5-point Dirichlet Laplacian 1000^2 (n=1,000,000), k=6 largest "
+                               "('lm', direct Lanczos), tol 1e-10",
+                          build=lambda: w.lap2d(1000), k=6, which=s.LM,
+                          exact=lambda: w.spectrum2d_extreme(1000, 6, True)),
+        "varcoef64": dict(desc="3-D variable-coefficient FV diffusion 64^3 (n=262,144), log-normal "
+                               "conductivity (sigma=1, seed 3), k=20 'sm', plain FP64, tol 1e-10",
+                          build=lambda: w.varcoef3d(64, seed=3), k=20, which=s.SM, exact=None),
+    }
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self):
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self, gpu_index=None):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            if gpu_index is not None and p[0] != str(gpu_index):
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_reference_times(pkg, A, wl, steps, warmup, budget_s=None):
+    """Wall time of the reference's CPU solver (oracle/_ref) per full solve."""
+    s = pkg.speigs
+    ref = s.load(REF_LIB)
+    o = s.default_opts(ref, tol=TOL)
+    out = []
+    for i in range(warmup + steps):
+        t0 = time.perf_counter()
+        rc, lam, V, res, info = s.speigs(A, wl["k"], wl["which"], o, vectors=True, lib=ref)
+        dt = time.perf_counter() - t0
+        if rc != 0:
+            raise RuntimeError(f"reference solver rc={rc}")
+        if i >= warmup:
+            out.append(dt)
+        if budget_s is not None and sum(out) > budget_s and len(out) >= 1:
+            break
+    return out, lam, info
+
+
+def run_reference(args, pkg, wl, rank):
+    if rank != 0:
+        return 0
+    if not os.path.exists(REF_LIB):
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/libspeigs_ref.so not built (needs the reference tree)"}))
+        return 0
+    A = wl["build"]()
+    times, lam, info = cpu_reference_times(pkg, A, wl, args.steps, args.warmup)
+    v = statistics.mean(times)
+    cores = os.cpu_count()
+    line = {
+        "metric": METRIC, "value": v, "unit": "s", "n_gpus": args.gpus, "steps": len(times),
+        "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": wl["desc"], "n": int(A.shape[0]), "nnz": int(A.nnz), "k": wl["k"],
+                   "tol": TOL, "nops": int(info["nops"]), "restarts": int(info["restarts"])},
+        "cpu_baseline": {"value": v, "unit": "s", "cores": cores, "kind": "reference",
+                         "sample": "full solves of the same workload by the reference's "
+                                   "src/speigs_core.c (CHOLMOD stand-in + OpenBLAS, all host "
+                                   "threads)"},
+        "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="lap46")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pkg = import_pkg()
+    s, w = pkg.speigs, pkg.workloads
+    wl = workloads(w, s)[args.workload]
+
+    if args.impl == "reference":
+        return run_reference(args, pkg, wl, rank)
+
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    lib = s.load()
+
+    A = wl["build"]()
+    n, k = A.shape[0], wl["k"]
+    opts = s.default_opts(lib, tol=TOL)
+    plan = s.Plan(A, wl["which"], opts, lib=lib)
+    pstream = torch.cuda.ExternalStream(plan.stream(), device=dev)
+    lam = torch.zeros(k, dtype=torch.float64, device=dev)
+    V = torch.zeros((k, n), dtype=torch.float64, device=dev)    # column-major n x k
+    res = torch.zeros(k, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def solve():
+        rc, info = plan.solve_device(k, lam.data_ptr(), V.data_ptr(), res.data_ptr())
+        if rc != 0:
+            raise RuntimeError(f"solve rc={rc}: {s.last_error(lib)}")
+        return info
+
+    torch.cuda.synchronize()
+    for _ in range(args.warmup):
+        info = solve()
+    # ---- timed region: device time per solve, L2 flushed between steps
+    sampler = ClockSampler()
+    sampler.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = s.counters(lib)[0]
+    step_ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(pstream)
+        info = solve()
+        e1.record(pstream)
+        e1.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+    torch.cuda.synchronize()
+    launches = s.counters(lib)[0] - l0
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop(gpu_index=None)
+    ms = statistics.mean(step_ms)
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+
+    # ---- correctness of the timed result
+    lam_h = lam.cpu().numpy()
+    Vh = V.cpu().numpy().T
+    resid = np.linalg.norm(A @ Vh - Vh * lam_h, axis=0)
+    check = {"max_resid_over_anorm": float(resid.max() / info["anorm"]),
+             "nops": int(info["nops"]), "restarts": int(info["restarts"]),
+             "shift": info["shift"], "flag": int(info["flag"])}
+    if wl["exact"] is not None:
+        ex = wl["exact"]()
+        check["max_rel_err_vs_closed_form"] = float(np.max(np.abs(lam_h - ex) / np.abs(ex)))
+
+    # ---- roofline of the dominant kernel: the operator application
+    costs = plan.costs()
+    x = torch.randn(n, dtype=torch.float64, device=dev)
+    y = torch.empty_like(x)
+    torch.cuda.synchronize()
+    for _ in range(3):
+        plan.apply_device(x.data_ptr(), y.data_ptr())
+    op_ms = []
+    for _ in range(20):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(pstream)
+        plan.apply_device(x.data_ptr(), y.data_ptr())
+        e1.record(pstream)
+        e1.synchronize()
+        op_ms.append(e0.elapsed_time(e1))
+    op_s = statistics.mean(op_ms) * 1e-3
+    peak, peak_kind = measured_peaks()
+    achieved = costs["op_bytes"] / op_s / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get(args.workload)
+        except Exception:
+            traffic = None
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic,
+                "kernel": "shift-invert solve pair (forward+backward multifrontal GEMV levels)"
+                if wl["which"] == s.SM else "CSR SpMV",
+                "op_ms": op_s * 1e3, "op_bytes": costs["op_bytes"], "peak_source": peak_kind}
+
+    # ---- end to end through the drop-in API: host CSC in, host results out
+    e2e_t = []
+    c0 = s.counters(lib)
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rc, l2, V2, r2, inf2 = s.speigs(A, k, wl["which"], opts, vectors=True, lib=lib)
+        e2e_t.append(time.perf_counter() - t0)
+        if rc != 0:
+            raise RuntimeError(f"speigs rc={rc}")
+    c1 = s.counters(lib)
+    e2e = {"value": statistics.mean(e2e_t), "unit": "s",
+           "h2d_bytes_per_step": (c1[1] - c0[1]) // args.steps,
+           "d2h_bytes_per_step": (c1[2] - c0[2]) // args.steps}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_LIB):
+        times, _, _ = cpu_reference_times(pkg, A, wl, steps=3, warmup=1, budget_s=30.0)
+        cpu = {"value": statistics.median(times), "unit": "s", "cores": os.cpu_count(),
+               "kind": "reference",
+               "sample": f"{len(times)} full solve(s) of the same workload by the reference's "
+                         "src/speigs_core.c (CHOLMOD stand-in + OpenBLAS, all host threads), "
+                         "median"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": ms * 1e-3, "unit": "s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": wl["desc"], "n": int(n), "nnz": int(A.nnz), "k": k, "tol": TOL,
+                       "precision": "plain FP64", "parallelism": f"replicas x{world}",
+                       "l2": "256 MiB buffer written between timed steps",
+                       "value_scope": "numeric factor + Lanczos, matrix and analysis resident"},
+            "check": check, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": int(launches), "clocks": clocks,
+            "phase_s": {kk: info[kk] for kk in ("t_factor", "t_iter", "t_op", "t_ortho",
+                                                "t_resid", "t_ritz")},
+        }
+        print(json.dumps(line))
+    plan.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,1000 @@
+// Device engine: thick-restart Lanczos with full reorthogonalisation over a
+// pluggable operator, run on one GPU.
+//
+// The control flow is the reference's lanczos() (src/speigs_core.c:146-315)
+// step for step -- same ncv/maxit/tol defaults, same start-vector stream,
+// same breakdown threshold and re-injection, same convergence test and
+// thick-restart rule -- with every vector operation on the device.  The host
+// only reads back the scalars the reference branches on (a step's beta, the
+// number of converged pairs, a restart vector's norm).
+#include "engine.h"
+#include "../../include/speigs_b200.h"
+#include "kernels/krylov.cuh"
+#include "kernels/multifrontal.cuh"
+#include "counters.h"
+
+#include <cuda_runtime.h>
+#include <cub/device/device_radix_sort.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <vector>
+
+namespace spx {
+
+
+// cudaMemcpyAsync that feeds the transfer counters
+static cudaError_t copy_async(void *dst, const void *src, size_t bytes, cudaMemcpyKind kind,
+                              cudaStream_t st) {
+    if (kind == cudaMemcpyHostToDevice) note_h2d((long long)bytes);
+    else if (kind == cudaMemcpyDeviceToHost) note_d2h((long long)bytes);
+    return cudaMemcpyAsync(dst, src, bytes, kind, st);
+}
+
+static thread_local char g_err[256] = "";
+const char *last_cuda_error() { return g_err; }
+
+static int cuda_fail(cudaError_t e, const char *where) {
+    snprintf(g_err, sizeof g_err, "%s: %s", where, cudaGetErrorString(e));
+    cudaGetLastError();
+    return SPEIGS_ERR_INTERNAL;
+}
+
+// ------------------------------------------------------------- resources --
+// One memory pool per device with a high release threshold, so repeated calls
+// reuse device memory instead of returning it to the driver at every sync.
+static cudaMemPool_t device_pool(int dev) {
+    static std::mutex mu;
+    static std::vector<cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> lk(mu);
+    if ((int)pools.size() <= dev) pools.resize(dev + 1, nullptr);
+    if (!pools[dev]) {
+        cudaMemPoolProps props;
+        memset(&props, 0, sizeof props);
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t p = nullptr;
+        if (cudaMemPoolCreate(&p, &props) != cudaSuccess) { cudaGetLastError(); return nullptr; }
+        uint64_t thr = UINT64_MAX;
+        cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &thr);
+        pools[dev] = p;
+    }
+    return pools[dev];
+}
+
+struct Stream {
+    cudaStream_t s = nullptr;
+    cudaError_t err = cudaSuccess;
+    Stream() { err = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking); }
+    ~Stream() {
+        if (s) { cudaStreamSynchronize(s); cudaStreamDestroy(s); }
+    }
+};
+
+class Arena {
+public:
+    explicit Arena(cudaStream_t st) : st_(st) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        pool_ = device_pool(dev);
+    }
+    ~Arena() {
+        for (void *p : ptrs_) cudaFreeAsync(p, st_);
+    }
+    template <class T>
+    T *alloc(size_t cnt) {
+        void *p = nullptr;
+        size_t bytes = (cnt ? cnt : 1) * sizeof(T);
+        cudaError_t e = pool_ ? cudaMallocFromPoolAsync(&p, bytes, pool_, st_)
+                              : cudaMallocAsync(&p, bytes, st_);
+        if (e != cudaSuccess) { cudaGetLastError(); failed = true; return nullptr; }
+        ptrs_.push_back(p);
+        return (T *)p;
+    }
+    bool failed = false;
+
+private:
+    cudaStream_t st_;
+    cudaMemPool_t pool_ = nullptr;
+    std::vector<void *> ptrs_;
+};
+
+// Device-side phase timer: event pairs resolved at the next host sync.
+class PhaseTimer {
+public:
+    explicit PhaseTimer(cudaStream_t st) : st_(st) {}
+    ~PhaseTimer() {
+        for (auto &p : pend_) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
+        for (auto e : free_) cudaEventDestroy(e);
+    }
+    int begin() {
+        Pair p{ev(), nullptr, nullptr};
+        cudaEventRecord(p.a, st_);
+        pend_.push_back(p);
+        return (int)pend_.size() - 1;
+    }
+    void end(int id, double *acc) {
+        pend_[id].b = ev();
+        pend_[id].acc = acc;
+        cudaEventRecord(pend_[id].b, st_);
+    }
+    void resolve() {   // call after a stream sync
+        for (auto &p : pend_) {
+            if (p.b && p.acc) {
+                float ms = 0.f;
+                if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) *p.acc += ms;
+                else cudaGetLastError();
+            }
+            free_.push_back(p.a);
+            if (p.b) free_.push_back(p.b);
+        }
+        pend_.clear();
+    }
+
+private:
+    struct Pair { cudaEvent_t a, b; double *acc; };
+    cudaEvent_t ev() {
+        if (!free_.empty()) { cudaEvent_t e = free_.back(); free_.pop_back(); return e; }
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        return e;
+    }
+    cudaStream_t st_;
+    std::vector<Pair> pend_;
+    std::vector<cudaEvent_t> free_;
+};
+
+// ------------------------------------------------------------ operators --
+// The pluggable operator of the reference (speigs_op / op_apply,
+// src/speigs_core.c:57-116): mode 0 is y = A x, mode 1 the Cholesky solve.
+struct Operator {
+    virtual ~Operator() = default;
+    virtual void apply(const double *x, double *y, cudaStream_t st) = 0;
+    int64_t nops = 0;
+};
+
+struct DevA {
+    int n;
+    const int32_t *rp, *ci;
+    const double *va;
+};
+
+struct SpmvOperator : Operator {
+    DevA A;
+    explicit SpmvOperator(const DevA &a) : A(a) {}
+    void apply(const double *x, double *y, cudaStream_t st) override {
+        nops++;
+        launch_spmv(A.n, A.rp, A.ci, A.va, x, y, st);
+    }
+};
+
+struct CholOperator : Operator {
+    MultifrontalPlan *plan;
+    explicit CholOperator(MultifrontalPlan *p) : plan(p) {}
+    void apply(const double *x, double *y, cudaStream_t st) override {
+        nops++;
+        plan->solve(x, y, st);
+    }
+};
+
+// ------------------------------------------------------------- Lanczos --
+namespace {
+
+struct LanczosBufs {
+    int n = 0, ncv0 = 0, kk = 0;
+    int64_t ldv = 0;
+    double *V = nullptr, *Vn = nullptr, *H = nullptr, *S = nullptr, *theta = nullptr,
+           *thsave = nullptr, *w = nullptr, *X = nullptr, *AX = nullptr, *lam = nullptr,
+           *r2 = nullptr, *xn2 = nullptr, *h1 = nullptr, *h2 = nullptr, *nrm2 = nullptr,
+           *jwork = nullptr;
+    int *ord = nullptr, *jstat = nullptr;
+    ReduceScratch rs;
+};
+
+__global__ void thsave_kernel(const double *theta, const int *ord, int t, double *thsave,
+                              int nret) {
+    thsave[nret] = theta[ord[t]];
+}
+
+// dst = src * (1/sqrt(nrm2)) ; used for the normalisations the reference does
+// with dnrm2 + dscal
+inline void normalise(int n, const double *src, const double *nrm2, double *dst,
+                      cudaStream_t st) {
+    launch_scale_by_invnorm(n, src, nrm2, dst, st);
+}
+
+// w <- (I - B B^T) w twice (reference orth_block, src/speigs_core.c:122-132);
+// leaves ||w||^2 in nrm2[0].  hcol: optional projected-matrix column.
+inline void orth_block(const LanczosBufs &b, const double *B, int m, double *w, double *hcol,
+                       cudaStream_t st) {
+    if (m > 0) {
+        launch_ts_dot(B, b.ldv, b.n, m, w, b.h1, hcol, hcol ? 1 : 0, b.rs, st);
+        launch_ts_update_dot(B, b.ldv, b.n, m, w, b.h1, b.h2, hcol, hcol ? 2 : 0, b.rs, st);
+        launch_ts_update_norm(B, b.ldv, b.n, m, w, b.h2, b.nrm2, b.rs, st);
+    } else {
+        launch_ts_norm(b.n, w, b.nrm2, b.rs, st);
+    }
+}
+
+}  // namespace
+
+// Results: lambda/resid (host, the last Rayleigh-Ritz's nout pairs in Lanczos
+// order) and *Xdev (device, their Ritz vectors, leading dimension *ldx).
+static int lanczos_device(Operator &op, const DevA &A, int n, int64_t k, const speigs_opts &o,
+                          double anorm, double *lambda, double *resid, const double **Xdev,
+                          int64_t *ldx, int *nout, speigs_info *info, EngineStats *stats,
+                          Arena &ar, cudaStream_t st) {
+    int64_t ncv = o.ncv ? o.ncv : std::max<int64_t>(2 * k + 1, 20);
+    if (ncv > n) ncv = n;
+    if (ncv <= k) ncv = std::min<int64_t>(n, k + 1);
+    if (ncv < 2) ncv = std::min<int64_t>(n, 2);
+    const int64_t maxit = o.maxit ? o.maxit : 300;
+    const double tol = o.tol > 0 ? o.tol : 1e-14;
+    const double rtol = tol * std::max(anorm, 1.0);
+    const double bthr = 1e-13 * std::max(anorm, 1.0);
+
+    LanczosBufs b;
+    b.n = n;
+    b.ncv0 = (int)ncv;
+    b.kk = (int)std::min<int64_t>(k, ncv);
+    b.ldv = ((int64_t)n + 31) & ~(int64_t)31;
+    const int ldh = (int)ncv;     // H keeps the leading dimension it was allocated with
+    b.V = ar.alloc<double>((size_t)b.ldv * (ncv + 1));
+    b.Vn = ar.alloc<double>((size_t)b.ldv * (ncv + 1));
+    b.H = ar.alloc<double>((size_t)ncv * ncv);
+    b.S = ar.alloc<double>((size_t)ncv * ncv);
+    b.theta = ar.alloc<double>(ncv);
+    b.thsave = ar.alloc<double>(ncv);
+    b.w = ar.alloc<double>(b.ldv);
+    b.X = ar.alloc<double>((size_t)b.ldv * b.kk);
+    b.AX = ar.alloc<double>((size_t)b.ldv * b.kk);
+    b.lam = ar.alloc<double>(b.kk);
+    b.r2 = ar.alloc<double>(b.kk);
+    b.xn2 = ar.alloc<double>(std::max<int64_t>(b.kk, 1));
+    b.h1 = ar.alloc<double>(ncv + 1);
+    b.h2 = ar.alloc<double>(ncv + 1);
+    b.nrm2 = ar.alloc<double>(4);
+    b.ord = ar.alloc<int>(ncv);
+    b.jstat = ar.alloc<int>(2);
+    const int me = (int)((ncv + 1) & ~1);
+    b.jwork = ((int)ncv > syev_small_smem_limit()) ? ar.alloc<double>((size_t)2 * me * me) : nullptr;
+    const int nblk = (n + 511) / 512 + 1;
+    const int maxcols = (int)std::max<int64_t>(ncv + 1, b.kk) + 1;
+    b.rs.part = ar.alloc<double>((size_t)nblk * maxcols);
+    b.rs.counter = ar.alloc<unsigned>(1);
+    b.rs.max_blocks = nblk;
+    b.rs.max_cols = maxcols;
+    if (ar.failed) return SPEIGS_ERR_MEM;
+    cudaMemsetAsync(b.rs.counter, 0, sizeof(unsigned), st);
+    cudaMemsetAsync(b.H, 0, sizeof(double) * ncv * ncv, st);
+
+    double *hs = nullptr;   // pinned scalars
+    if (cudaMallocHost(&hs, sizeof(double) * (2 * b.kk + 8)) != cudaSuccess) {
+        cudaGetLastError();
+        return SPEIGS_ERR_MEM;
+    }
+    struct HostFree { double *p; ~HostFree() { if (p) cudaFreeHost(p); } } hf{hs};
+    double *h_lam = hs, *h_r2 = hs + b.kk, *h_nrm = hs + 2 * b.kk;
+
+    PhaseTimer tm(st);
+    double ms_op = 0, ms_ortho = 0, ms_resid = 0, ms_ritz = 0;
+    auto read_nrm = [&](double *out) -> int {
+        copy_async(h_nrm, b.nrm2, sizeof(double), cudaMemcpyDeviceToHost, st);
+        cudaError_t e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return cuda_fail(e, "lanczos sync");
+        tm.resolve();
+        *out = sqrt(h_nrm[0]);
+        return 0;
+    };
+
+    uint64_t seed = o.seed ? o.seed : 88172645463325252ULL;
+    auto rand_vec = [&](double *dst) {
+        launch_rand_vec(n, seed, dst, st);
+        seed = rng_advance(seed, (uint64_t)n);
+    };
+
+    // start vector (reference :187-191)
+    rand_vec(b.w);
+    launch_ts_norm(n, b.w, b.nrm2, b.rs, st);
+    double nr0 = 0;
+    if (int e = read_nrm(&nr0)) return e;
+    if (nr0 == 0.0) return SPEIGS_ERR_INTERNAL;
+    normalise(n, b.w, b.nrm2, b.V, st);
+
+    int64_t j = 0, restarts = 0, nconv = 0;
+    int rc = SPEIGS_OK;
+    int last_nwant = 0;   // Ritz vectors of the last Rayleigh-Ritz stay in X
+    for (;;) {
+        // ---- extend the basis from j to ncv (reference :197-229)
+        for (; j < ncv; j++) {
+            double *vj = b.V + (size_t)j * b.ldv;
+            int t0 = tm.begin();
+            op.apply(vj, b.w, st);
+            tm.end(t0, &ms_op);
+            int t1 = tm.begin();
+            double *hcol = b.H + (size_t)j * ldh;
+            orth_block(b, b.V, (int)(j + 1), b.w, hcol, st);
+            tm.end(t1, &ms_ortho);
+            double beta = 0;
+            if (int e = read_nrm(&beta)) return e;
+            int zero_rec = 0;
+            if (beta <= bthr) {
+                zero_rec = 1;
+                for (int att = 0; att < 3 && beta <= bthr; att++) {
+                    rand_vec(b.w);
+                    orth_block(b, b.V, (int)(j + 1), b.w, nullptr, st);
+                    if (int e = read_nrm(&beta)) return e;
+                }
+                if (beta <= bthr) { ncv = j + 1; break; }
+            }
+            normalise(n, b.w, b.nrm2, b.V + (size_t)(j + 1) * b.ldv, st);
+            if (j + 1 < ncv) launch_set_beta(b.H, ldh, (int)(j + 1), (int)j, b.nrm2, zero_rec, st);
+        }
+
+        // ---- projected eigenproblem (reference :231-240)
+        const int m = (int)ncv;
+        int tr = tm.begin();
+        launch_syev_small(m, b.H, ldh, b.theta, b.S, b.ord, b.jwork, b.jstat, st);
+
+        // ---- true residuals of the wanted Ritz pairs (reference :242-265)
+        const int nwant = (int)std::min<int64_t>(k, m);
+        launch_ritz_vectors(b.V, b.ldv, n, m, b.S, m, b.ord, 0, nwant, b.X, b.ldv, b.xn2, b.rs, st);
+        launch_scale_cols(n, nwant, b.X, b.ldv, b.xn2, st);
+        for (int t = 0; t < nwant; t++)
+            launch_spmv(A.n, A.rp, A.ci, A.va, b.X + (size_t)t * b.ldv, b.AX + (size_t)t * b.ldv, st);
+        launch_rayleigh_resid(n, nwant, b.X, b.ldv, b.AX, b.ldv, b.lam, b.r2, b.rs, st);
+        tm.end(tr, &ms_resid);
+        int jst[2] = {0, 0};
+        copy_async(h_lam, b.lam, sizeof(double) * nwant, cudaMemcpyDeviceToHost, st);
+        copy_async(h_r2, b.r2, sizeof(double) * nwant, cudaMemcpyDeviceToHost, st);
+        copy_async(jst, b.jstat, sizeof(int), cudaMemcpyDeviceToHost, st);
+        {
+            cudaError_t e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) return cuda_fail(e, "residual sync");
+            tm.resolve();
+        }
+        if (jst[0] < 0) { rc = SPEIGS_ERR_LAPACK; break; }
+        nconv = 0;
+        for (int t = 0; t < nwant; t++) {
+            const double r = sqrt(h_r2[t]);
+            lambda[t] = h_lam[t];
+            if (resid) resid[t] = r;
+            if (r <= rtol) nconv++;
+        }
+        last_nwant = nwant;
+
+        if (nconv >= std::min<int64_t>(k, m) || restarts >= maxit || m < ncv) break;
+        restarts++;
+
+        // ---- thick restart: keep the top-l Ritz vectors (reference :270-303)
+        int64_t l = std::min<int64_t>(k + 5, ncv - 1);
+        if (l < 1) l = 1;
+        int nret = 0;
+        int tk = tm.begin();
+        for (int t = 0; t < m && nret < l; t++) {
+            double *dst = b.Vn + (size_t)nret * b.ldv;
+            launch_ritz_vectors(b.V, b.ldv, n, m, b.S, m, b.ord, t, 1, dst, b.ldv, b.xn2, b.rs, st);
+            orth_block(b, b.Vn, nret, dst, nullptr, st);
+            double nr = 0;
+            if (int e = read_nrm(&nr)) return e;
+            if (nr < 1e-10) continue;
+            normalise(n, dst, b.nrm2, dst, st);
+            thsave_kernel<<<1, 1, 0, st>>>(b.theta, b.ord, t, b.thsave, nret);
+            note_launch();
+            nret++;
+        }
+        tm.end(tk, &ms_ritz);
+        // the (m+1)-th Lanczos vector continues the recurrence
+        launch_copy(n, b.V + (size_t)m * b.ldv, b.w, st);
+        orth_block(b, b.Vn, nret, b.w, nullptr, st);
+        double nr = 0;
+        if (int e = read_nrm(&nr)) return e;
+        if (nr < 1e-10) {
+            rand_vec(b.w);
+            orth_block(b, b.Vn, nret, b.w, nullptr, st);
+            if (int e = read_nrm(&nr)) return e;
+        }
+        if (nr < 1e-10) break;
+        normalise(n, b.w, b.nrm2, b.Vn + (size_t)nret * b.ldv, st);
+        std::swap(b.V, b.Vn);
+        launch_set_diag(ldh, nret, b.thsave, b.H, st);
+        j = nret;
+    }
+    if (rc) return rc;
+    *Xdev = b.X;
+    *ldx = b.ldv;
+    *nout = last_nwant;
+    {
+        cudaError_t e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return cuda_fail(e, "lanczos end");
+        tm.resolve();
+    }
+    info->nconv = nconv;
+    info->restarts = restarts;
+    info->nops = op.nops;
+    info->flag = (nconv >= std::min<int64_t>(k, ncv)) ? 0 : 1;
+    info->t_op += ms_op * 1e-3;
+    info->t_ortho += ms_ortho * 1e-3;
+    info->t_resid += ms_resid * 1e-3;
+    info->t_ritz += ms_ritz * 1e-3;
+    if (stats) {
+        stats->ms_op += ms_op; stats->ms_ortho += ms_ortho;
+        stats->ms_resid += ms_resid; stats->ms_ritz += ms_ritz;
+    }
+    return SPEIGS_OK;
+}
+
+// ----------------------------------------------------------- host CSR --
+int build_full_csr(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *Ax,
+                   HostCSR *out) {
+    if (n <= 0 || n > INT32_MAX) return SPEIGS_ERR_ARG;
+    int64_t *cnt = (int64_t *)calloc((size_t)n + 1, sizeof(int64_t));
+    if (!cnt) return SPEIGS_ERR_MEM;
+    for (int64_t c = 0; c < n; c++)
+        for (int64_t q = Ap[c]; q < Ap[c + 1]; q++) {
+            const int64_t r = Ai[q];
+            if (r > c) continue;
+            cnt[r + 1]++;
+            if (r != c) cnt[c + 1]++;
+        }
+    for (int64_t i = 0; i < n; i++) cnt[i + 1] += cnt[i];
+    const int64_t nnz = cnt[n];
+    if (nnz > INT32_MAX) { free(cnt); return SPEIGS_ERR_MEM; }
+    int32_t *ci = (int32_t *)malloc((size_t)(nnz ? nnz : 1) * sizeof(int32_t));
+    double *cx = (double *)malloc((size_t)(nnz ? nnz : 1) * sizeof(double));
+    int64_t *fill = (int64_t *)malloc((size_t)n * sizeof(int64_t));
+    if (!ci || !cx || !fill) { free(cnt); free(ci); free(cx); free(fill); return SPEIGS_ERR_MEM; }
+    memcpy(fill, cnt, (size_t)n * sizeof(int64_t));
+    // pass 1: entries (r, c) with r <= c go to row r in increasing c;
+    // pass 2: their mirrors (c, r), r < c, go to row c in increasing r.
+    // Row i then holds columns < i from pass 2 after columns >= i from pass 1.
+    for (int64_t c = 0; c < n; c++)
+        for (int64_t q = Ap[c]; q < Ap[c + 1]; q++) {
+            const int64_t r = Ai[q];
+            if (r > c) continue;
+            const int64_t d = fill[r]++;
+            ci[d] = (int32_t)c; cx[d] = Ax[q];
+        }
+    for (int64_t c = 0; c < n; c++)
+        for (int64_t q = Ap[c]; q < Ap[c + 1]; q++) {
+            const int64_t r = Ai[q];
+            if (r >= c) continue;
+            const int64_t d = fill[c]++;
+            ci[d] = (int32_t)r; cx[d] = Ax[q];
+        }
+    free(fill);
+    // rotate each row so its columns are ascending: [>= i part][< i part]
+    std::vector<int32_t> tc;
+    std::vector<double> tx;
+    for (int64_t i = 0; i < n; i++) {
+        const int64_t a = cnt[i], e = cnt[i + 1];
+        int64_t split = a;
+        while (split < e && ci[split] >= i) split++;
+        if (split == a || split == e) continue;
+        tc.assign(ci + split, ci + e);
+        tx.assign(cx + split, cx + e);
+        tc.insert(tc.end(), ci + a, ci + split);
+        tx.insert(tx.end(), cx + a, cx + split);
+        std::copy(tc.begin(), tc.end(), ci + a);
+        std::copy(tx.begin(), tx.end(), cx + a);
+    }
+    out->n = (int32_t)n;
+    out->rowptr = cnt;
+    out->col = ci;
+    out->val = cx;
+    return SPEIGS_OK;
+}
+
+void free_csr(HostCSR *A) {
+    free(A->rowptr); free(A->col); free(A->val);
+    A->rowptr = nullptr; A->col = nullptr; A->val = nullptr; A->n = 0;
+}
+
+static double wall() {
+    struct timespec t;
+    clock_gettime(CLOCK_MONOTONIC, &t);
+    return t.tv_sec + 1e-9 * t.tv_nsec;
+}
+
+// ------------------------------------------------------------- the plan --
+}  // namespace spx
+
+struct speigs_plan_s {
+    spx::Stream stream;
+    spx::HostCSR A;                  // full symmetric CSR (host copy of the pattern)
+    std::vector<int64_t> csc2csr;    // per CSC entry: CSR position(s) it feeds, or -1
+    int64_t csc_nnz = 0;
+    std::vector<int64_t> Ap_copy;    // CSC column pointers given at creation
+    std::vector<int64_t> Ai_copy;
+    speigs_which which = SPEIGS_SM;
+    speigs_opts opts;
+    double anorm = 1.0;
+    double shift = 0.0;
+    bool factored = false;
+    int32_t *d_rp = nullptr, *d_ci = nullptr;
+    double *d_va = nullptr;
+    spx::MultifrontalPlan mf;
+    double t_analyze = 0;
+    std::vector<void *> owned;
+};
+
+namespace spx {
+
+static int plan_upload_values(speigs_plan_s *p) {
+    const int64_t nnz = p->A.nnz();
+    cudaError_t e = copy_async(p->d_va, p->A.val, sizeof(double) * nnz,
+                                    cudaMemcpyHostToDevice, p->stream.s);
+    if (e != cudaSuccess) return cuda_fail(e, "upload values");
+    e = cudaStreamSynchronize(p->stream.s);
+    if (e != cudaSuccess) return cuda_fail(e, "upload values");
+    p->factored = false;
+    return 0;
+}
+
+static int plan_alloc(speigs_plan_s *p, void **ptr, size_t bytes) {
+    cudaError_t e = cudaMallocAsync(ptr, bytes ? bytes : 1, p->stream.s);
+    if (e != cudaSuccess) { cudaGetLastError(); return SPEIGS_ERR_MEM; }
+    p->owned.push_back(*ptr);
+    return 0;
+}
+
+// Build the plan from an already expanded full CSR (takes ownership of A).
+int plan_from_csr(HostCSR &A, speigs_which which, const speigs_opts &o, double anorm,
+                  speigs_plan_s **out) {
+    g_err[0] = 0;
+    int ndev = 0;
+    cudaError_t e0 = cudaGetDeviceCount(&ndev);
+    if (e0 != cudaSuccess || ndev == 0) {
+        cuda_fail(e0 != cudaSuccess ? e0 : cudaErrorNoDevice, "no CUDA device");
+        free_csr(&A);
+        return SPEIGS_ERR_INTERNAL;
+    }
+    speigs_plan_s *p = new (std::nothrow) speigs_plan_s;
+    if (!p) { free_csr(&A); return SPEIGS_ERR_MEM; }
+    p->A = A;
+    A = HostCSR();
+    p->which = which;
+    p->opts = o;
+    p->anorm = anorm;
+    if (p->stream.err != cudaSuccess) { int rc = cuda_fail(p->stream.err, "stream"); speigs_plan_destroy(p); return rc; }
+    cudaStream_t st = p->stream.s;
+    const int n = p->A.n;
+    const int64_t nnz = p->A.nnz();
+    int rc = 0;
+    rc = rc ? rc : plan_alloc(p, (void **)&p->d_rp, sizeof(int32_t) * (n + 1));
+    rc = rc ? rc : plan_alloc(p, (void **)&p->d_ci, sizeof(int32_t) * nnz);
+    rc = rc ? rc : plan_alloc(p, (void **)&p->d_va, sizeof(double) * nnz);
+    if (rc) { speigs_plan_destroy(p); return rc; }
+    std::vector<int32_t> rp32(n + 1);
+    for (int i = 0; i <= n; i++) rp32[i] = (int32_t)p->A.rowptr[i];
+    copy_async(p->d_rp, rp32.data(), sizeof(int32_t) * (n + 1), cudaMemcpyHostToDevice, st);
+    copy_async(p->d_ci, p->A.col, sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, st);
+    rc = plan_upload_values(p);
+    if (rc) { speigs_plan_destroy(p); return rc; }
+    if (which == SPEIGS_SM) {
+        const double ta = wall();
+        spx_symbolic S;
+        const int ord = o.ordering == 1 ? SPX_ORDER_MINDEG : o.ordering == 2 ? SPX_ORDER_ND
+                                                                            : SPX_ORDER_AUTO;
+        int arc = spx_analyze(n, p->A.rowptr, p->A.col, ord, &S);
+        if (arc) { speigs_plan_destroy(p); return arc == -2 ? SPEIGS_ERR_MEM : SPEIGS_ERR_FACTOR; }
+        rc = p->mf.init(S, p->A.rowptr, p->A.col, st);
+        spx_symbolic_free(&S);
+        p->t_analyze = wall() - ta;
+        if (rc) { speigs_plan_destroy(p); return rc; }
+    }
+    *out = p;
+    return 0;
+}
+
+// Numeric factorization with the reference's capped shift escalation
+// (src/speigs_core.c:938-970).  Returns 0, SPEIGS_ERR_FACTOR when A stays
+// indefinite, or another negative code.
+static int plan_factor(speigs_plan_s *p, EngineStats *stats) {
+    cudaStream_t st = p->stream.s;
+    const speigs_opts &o = p->opts;
+    double delta = 0.0;
+    // A pivot that is rounding noise on the scale of ||A||_1 is treated as
+    // not positive, so an exactly singular PSD matrix takes the shift route
+    // deterministically instead of by the sign of its last rounding error.
+    const double pivtol = 128.0 * 2.220446049250313e-16 * p->anorm;
+    int fr = p->mf.factorize(p->d_va, 0.0, pivtol, st);
+    int attempts = 1;
+    if (fr == 1) {
+        const double d0 = p->anorm * (o.shift0 > 0 ? o.shift0 : 1e-6);
+        double dcap = p->anorm * 1e-3;
+        if (d0 > dcap) dcap = d0;
+        for (delta = d0; delta <= dcap * 1.0000001; delta *= 10.0) {
+            fr = p->mf.factorize(p->d_va, delta, pivtol, st);
+            attempts++;
+            if (fr != 1) break;
+        }
+        if (fr == 1) delta = 0.0;
+    }
+    if (stats) {
+        stats->factor_attempts = attempts;
+        stats->factor_flops = p->mf.factor_flops();
+        stats->solve_bytes = p->mf.solve_bytes();
+    }
+    if (fr < 0) return fr;
+    if (fr == 1) {
+        // still indefinite: the reference switches to an LU here (:975-984),
+        // a route the device library does not provide
+        snprintf(g_err, sizeof g_err, "matrix is indefinite: LU route not available");
+        return SPEIGS_ERR_FACTOR;
+    }
+    p->shift = delta;
+    p->factored = true;
+    return 0;
+}
+
+struct Cand2 { double key; int idx; };
+
+// Factor (if 'sm') and iterate; results sorted by |lambda| into host or
+// device buffers.
+static int plan_solve(speigs_plan_s *p, int64_t k, double *lambda, double *V, double *resid,
+                      speigs_info *info, bool on_device, EngineStats *stats) {
+    g_err[0] = 0;
+    cudaStream_t st = p->stream.s;
+    const int n = p->A.n;
+    if (k <= 0 || k > n) return SPEIGS_ERR_ARG;
+    info->anorm = p->anorm;
+    info->ncomp = 0;
+    info->t_analyze = p->t_analyze;
+    DevA dA{n, p->d_rp, p->d_ci, p->d_va};
+    SpmvOperator spmv_op(dA);
+    CholOperator chol_op(&p->mf);
+    Operator *op = &spmv_op;
+    if (p->which == SPEIGS_LM) {
+        info->path = SPEIGS_PATH_DIRECT;
+    } else {
+        const double tf = wall();
+        int rc = plan_factor(p, stats);
+        info->t_factor = wall() - tf;
+        if (rc) return rc;
+        op = &chol_op;
+        info->shift = p->shift;
+        info->path = SPEIGS_PATH_SHIFTINV;
+    }
+    std::vector<double> lam_h(k, 0.0), res_h(k, 0.0);
+    int rc = 0;
+    {
+        Arena ar(st);
+        const double *X = nullptr;
+        int64_t ldx = 0;
+        int nout = 0;
+        const double ti = wall();
+        rc = lanczos_device(*op, dA, n, k, p->opts, p->anorm, lam_h.data(), res_h.data(), &X,
+                            &ldx, &nout, info, stats, ar, st);
+        if (rc == 0) {
+            // sort by |lambda|: ascending for 'sm', descending for 'lm'
+            // (reference :994-1012); entries past nout keep the caller's memory
+            std::vector<Cand2> ord(nout);
+            for (int i = 0; i < nout; i++) ord[i] = {fabs(lam_h[i]), i};
+            std::stable_sort(ord.begin(), ord.end(), [&](const Cand2 &a, const Cand2 &b) {
+                return p->which == SPEIGS_SM ? a.key < b.key : a.key > b.key;
+            });
+            std::vector<double> ls(nout), rs(nout);
+            for (int t = 0; t < nout; t++) { ls[t] = lam_h[ord[t].idx]; rs[t] = res_h[ord[t].idx]; }
+            const cudaMemcpyKind kv = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+            const cudaMemcpyKind ks = on_device ? cudaMemcpyHostToDevice : cudaMemcpyHostToHost;
+            if (V)
+                for (int t = 0; t < nout; t++)
+                    copy_async(V + (size_t)t * n, X + (size_t)ord[t].idx * ldx,
+                                    sizeof(double) * n, kv, st);
+            if (on_device) {
+                copy_async(lambda, ls.data(), sizeof(double) * nout, ks, st);
+                if (resid) copy_async(resid, rs.data(), sizeof(double) * nout, ks, st);
+            } else {
+                memcpy(lambda, ls.data(), sizeof(double) * nout);
+                if (resid) memcpy(resid, rs.data(), sizeof(double) * nout);
+            }
+            cudaError_t e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) rc = cuda_fail(e, "copy out");
+        }
+        info->t_iter = wall() - ti;
+    }
+    return rc;
+}
+
+int device_krylov(HostCSR &A, int64_t k, speigs_which which, const speigs_opts &o,
+                  double anorm, double *lambda, double *V, double *resid, speigs_info *info,
+                  EngineStats *stats) {
+    speigs_plan_s *p = nullptr;
+    int rc = plan_from_csr(A, which, o, anorm, &p);
+    if (rc) return rc;
+    rc = plan_solve(p, k, lambda, V, resid, info, false, stats);
+    speigs_plan_destroy(p);
+    return rc;
+}
+
+// ------------------------------------------------------------ diag path --
+__global__ void absbits_kernel(int n, const double *d, unsigned long long *key, int *idx) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        key[i] = (unsigned long long)__double_as_longlong(fabs(d[i]));
+        idx[i] = i;
+    }
+}
+
+int device_diag_path(int64_t n64, const double *diag, int64_t k, speigs_which which,
+                     double *lambda, double *V, double *resid, speigs_info *info) {
+    g_err[0] = 0;
+    if (n64 > INT32_MAX) return SPEIGS_ERR_ARG;
+    const int n = (int)n64;
+    Stream stream;
+    if (stream.err != cudaSuccess) return cuda_fail(stream.err, "stream");
+    cudaStream_t st = stream.s;
+    std::vector<int> ord(k);
+    {
+        Arena ar(st);
+        double *d = ar.alloc<double>(n);
+        unsigned long long *k0 = ar.alloc<unsigned long long>(n), *k1 = ar.alloc<unsigned long long>(n);
+        int *i0 = ar.alloc<int>(n), *i1 = ar.alloc<int>(n);
+        if (ar.failed) return SPEIGS_ERR_MEM;
+        copy_async(d, diag, sizeof(double) * n, cudaMemcpyHostToDevice, st);
+        absbits_kernel<<<std::min(1024, (n + 255) / 256), 256, 0, st>>>(n, d, k0, i0);
+        note_launch();
+        size_t tb = 0;
+        if (which == SPEIGS_SM)
+            cub::DeviceRadixSort::SortPairs(nullptr, tb, k0, k1, i0, i1, n, 0, 64, st);
+        else
+            cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, k0, k1, i0, i1, n, 0, 64, st);
+        void *tmp = ar.alloc<char>(tb);
+        if (ar.failed) return SPEIGS_ERR_MEM;
+        if (which == SPEIGS_SM)
+            cub::DeviceRadixSort::SortPairs(tmp, tb, k0, k1, i0, i1, n, 0, 64, st);
+        else
+            cub::DeviceRadixSort::SortPairsDescending(tmp, tb, k0, k1, i0, i1, n, 0, 64, st);
+        copy_async(ord.data(), i1, sizeof(int) * k, cudaMemcpyDeviceToHost, st);
+        cudaError_t e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return cuda_fail(e, "diag sort");
+    }
+    for (int64_t t = 0; t < k; t++) {
+        const int i = ord[t];
+        lambda[t] = diag[i];
+        if (V) { memset(V + (size_t)t * n, 0, (size_t)n * sizeof(double)); V[(size_t)t * n + i] = 1.0; }
+        if (resid) resid[t] = 0.0;
+    }
+    info->nconv = k;
+    info->flag = 0;
+    info->path = SPEIGS_PATH_DIAG;
+    return SPEIGS_OK;
+}
+
+// ----------------------------------------------------------- dense path --
+__global__ void densify_kernel(int n, const int32_t *rp, const int32_t *ci, const double *va,
+                               double *D) {
+    for (int r = blockIdx.x; r < n; r += gridDim.x)
+        for (int q = rp[r] + threadIdx.x; q < rp[r + 1]; q += blockDim.x)
+            D[(size_t)r + (size_t)ci[q] * n] = va[q];
+}
+
+int device_dense_path(const HostCSR &A, int64_t k, speigs_which which, double *lambda,
+                      double *V, double *resid, speigs_info *info) {
+    g_err[0] = 0;
+    const int n = A.n;
+    const int64_t nnz = A.nnz();
+    Stream stream;
+    if (stream.err != cudaSuccess) return cuda_fail(stream.err, "stream");
+    cudaStream_t st = stream.s;
+    std::vector<double> theta(n);
+    std::vector<int> ordd(n);
+    std::vector<int32_t> rp32(n + 1);
+    for (int i = 0; i <= n; i++) rp32[i] = (int32_t)A.rowptr[i];
+    {
+        Arena ar(st);
+        int32_t *d_rp = ar.alloc<int32_t>(n + 1);
+        int32_t *d_ci = ar.alloc<int32_t>(nnz);
+        double *d_va = ar.alloc<double>(nnz);
+        double *D = ar.alloc<double>((size_t)n * n);
+        double *th = ar.alloc<double>(n);
+        double *S = ar.alloc<double>((size_t)n * n);
+        int *od = ar.alloc<int>(n);
+        int *stt = ar.alloc<int>(2);
+        const int me = (n + 1) & ~1;
+        double *work = (n > syev_small_smem_limit()) ? ar.alloc<double>((size_t)2 * me * me) : nullptr;
+        if (ar.failed) return SPEIGS_ERR_MEM;
+        copy_async(d_rp, rp32.data(), sizeof(int32_t) * (n + 1), cudaMemcpyHostToDevice, st);
+        copy_async(d_ci, A.col, sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, st);
+        copy_async(d_va, A.val, sizeof(double) * nnz, cudaMemcpyHostToDevice, st);
+        cudaMemsetAsync(D, 0, sizeof(double) * n * n, st);
+        densify_kernel<<<std::min(n, 4096), 32, 0, st>>>(n, d_rp, d_ci, d_va, D);
+        note_launch();
+        launch_syev_small(n, D, n, th, S, od, work, stt, st);
+        int hst[2] = {0, 0};
+        copy_async(theta.data(), th, sizeof(double) * n, cudaMemcpyDeviceToHost, st);
+        copy_async(hst, stt, sizeof(int), cudaMemcpyDeviceToHost, st);
+        cudaError_t e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return cuda_fail(e, "dense path");
+        if (hst[0] < 0) return SPEIGS_ERR_LAPACK;
+        // order by |theta| ascending ('sm') or descending ('lm'), stable
+        for (int i = 0; i < n; i++) ordd[i] = i;
+        std::stable_sort(ordd.begin(), ordd.end(), [&](int a, int b) {
+            return which == SPEIGS_SM ? fabs(theta[a]) < fabs(theta[b])
+                                      : fabs(theta[a]) > fabs(theta[b]);
+        });
+        if (V)
+            for (int64_t t = 0; t < k; t++)
+                copy_async(V + (size_t)t * n, S + (size_t)ordd[t] * n, sizeof(double) * n,
+                                cudaMemcpyDeviceToHost, st);
+        e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return cuda_fail(e, "dense path copy");
+    }
+    for (int64_t t = 0; t < k; t++) {
+        lambda[t] = theta[ordd[t]];
+        if (resid) resid[t] = 0.0;
+    }
+    info->nconv = k;
+    info->flag = 0;
+    info->path = SPEIGS_PATH_DENSE;
+    return SPEIGS_OK;
+}
+
+}  // namespace spx
+
+// ================================================================ C API ==
+using spx::HostCSR;
+
+extern "C" {
+
+int speigs_plan_create(speigs_int n, const speigs_int *Ap, const speigs_int *Ai,
+                       const double *Ax, speigs_which which, const speigs_opts *opts,
+                       speigs_plan *plan) {
+    if (!plan) return SPEIGS_ERR_ARG;
+    *plan = nullptr;
+    speigs_opts defo;
+    if (!opts) { speigs_default_opts(&defo); opts = &defo; }
+    if (n <= 0 || !Ap || !Ai || !Ax) return SPEIGS_ERR_ARG;
+    if (opts->check_sym != 0 && spx::host_check_symmetry(n, Ap, Ai, Ax) == 0)
+        return SPEIGS_ERR_NOTSYM;
+    double anorm = spx::host_norm1_upper(n, Ap, Ai, Ax);
+    if (anorm <= 0) anorm = 1.0;
+    HostCSR A;
+    int rc = spx::build_full_csr(n, Ap, Ai, Ax, &A);
+    if (rc) return rc;
+    speigs_plan_s *p = nullptr;
+    rc = spx::plan_from_csr(A, which, *opts, anorm, &p);
+    if (rc) return rc;
+    p->Ap_copy.assign(Ap, Ap + n + 1);
+    p->Ai_copy.assign(Ai, Ai + Ap[n]);
+    *plan = p;
+    return SPEIGS_OK;
+}
+
+int speigs_plan_set_values(speigs_plan p, const double *Ax) {
+    if (!p || !Ax) return SPEIGS_ERR_ARG;
+    const int64_t n = p->A.n;
+    HostCSR B;
+    int rc = spx::build_full_csr(n, p->Ap_copy.data(), p->Ai_copy.data(), Ax, &B);
+    if (rc) return rc;
+    std::swap(p->A.val, B.val);
+    spx::free_csr(&B);
+    double anorm = spx::host_norm1_upper(n, p->Ap_copy.data(), p->Ai_copy.data(), Ax);
+    p->anorm = anorm > 0 ? anorm : 1.0;
+    return spx::plan_upload_values(p);
+}
+
+int speigs_plan_solve_device(speigs_plan p, speigs_int k, double *lambda, double *V,
+                             double *resid, speigs_info *info) {
+    if (!p || !lambda) return SPEIGS_ERR_ARG;
+    speigs_info li;
+    if (!info) info = &li;
+    memset(info, 0, sizeof *info);
+    return spx::plan_solve(p, k, lambda, V, resid, info, true, nullptr);
+}
+
+int speigs_plan_factor(speigs_plan p, double *shift) {
+    if (!p) return SPEIGS_ERR_ARG;
+    if (p->which != SPEIGS_SM) return SPEIGS_ERR_ARG;
+    int rc = spx::plan_factor(p, nullptr);
+    if (shift) *shift = p->shift;
+    return rc;
+}
+
+int speigs_plan_apply_device(speigs_plan p, const double *x, double *y) {
+    if (!p || !x || !y) return SPEIGS_ERR_ARG;
+    cudaStream_t st = p->stream.s;
+    if (p->which == SPEIGS_LM) {
+        spx::launch_spmv(p->A.n, p->d_rp, p->d_ci, p->d_va, x, y, st);
+    } else {
+        if (!p->factored) {
+            int rc = spx::plan_factor(p, nullptr);
+            if (rc) return rc;
+        }
+        p->mf.solve(x, y, st);
+    }
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return spx::cuda_fail(e, "apply");
+    return SPEIGS_OK;
+}
+
+void *speigs_plan_stream(speigs_plan p) { return p ? (void *)p->stream.s : nullptr; }
+
+int speigs_plan_costs(speigs_plan p, double *op_bytes, double *factor_flops, double *nnz_factor) {
+    if (!p) return SPEIGS_ERR_ARG;
+    const double n = p->A.n, nnz = (double)p->A.nnz();
+    if (p->which == SPEIGS_LM) {
+        if (op_bytes) *op_bytes = 12.0 * nnz + 4.0 * (n + 1) + 16.0 * n;
+        if (factor_flops) *factor_flops = 0;
+        if (nnz_factor) *nnz_factor = 0;
+    } else {
+        if (op_bytes) *op_bytes = (double)p->mf.solve_bytes();
+        if (factor_flops) *factor_flops = p->mf.factor_flops();
+        if (nnz_factor) *nnz_factor = (double)p->mf.panel_entries();
+    }
+    return SPEIGS_OK;
+}
+
+void speigs_plan_destroy(speigs_plan p) {
+    if (!p) return;
+    cudaStream_t st = p->stream.s;
+    p->mf.release(st);
+    for (void *q : p->owned) cudaFreeAsync(q, st);
+    p->owned.clear();
+    spx::free_csr(&p->A);
+    delete p;
+}
+
+int speigs_b200_rand_vec(speigs_int n, uint64_t seed, double *v) {
+    if (n <= 0 || n > INT32_MAX || !v) return SPEIGS_ERR_ARG;
+    spx::Stream s;
+    if (s.err != cudaSuccess) return spx::cuda_fail(s.err, "stream");
+    double *d = nullptr;
+    if (cudaMallocAsync(&d, sizeof(double) * n, s.s) != cudaSuccess) {
+        cudaGetLastError();
+        return SPEIGS_ERR_MEM;
+    }
+    spx::launch_rand_vec((int)n, seed, d, s.s);
+    spx::copy_async(v, d, sizeof(double) * n, cudaMemcpyDeviceToHost, s.s);
+    cudaFreeAsync(d, s.s);
+    cudaError_t e = cudaStreamSynchronize(s.s);
+    return e == cudaSuccess ? SPEIGS_OK : spx::cuda_fail(e, "rand_vec");
+}
+
+int speigs_b200_syev_small(int m, const double *H, double *theta, double *S, int *ord) {
+    if (m <= 0 || !H || !theta || !S || !ord) return SPEIGS_ERR_ARG;
+    spx::Stream s;
+    if (s.err != cudaSuccess) return spx::cuda_fail(s.err, "stream");
+    const size_t mm = (size_t)m * m, me = (size_t)((m + 1) & ~1);
+    double *dH = nullptr, *dth = nullptr, *dS = nullptr, *dw = nullptr;
+    int *dord = nullptr, *dst = nullptr;
+    int rc = 0;
+    if (cudaMallocAsync(&dH, sizeof(double) * mm, s.s) || cudaMallocAsync(&dth, sizeof(double) * m, s.s) ||
+        cudaMallocAsync(&dS, sizeof(double) * mm, s.s) || cudaMallocAsync(&dw, sizeof(double) * 2 * me * me, s.s) ||
+        cudaMallocAsync(&dord, sizeof(int) * m, s.s) || cudaMallocAsync(&dst, sizeof(int) * 2, s.s)) {
+        cudaGetLastError();
+        rc = SPEIGS_ERR_MEM;
+    }
+    int hst[2] = {0, 0};
+    if (!rc) {
+        spx::copy_async(dH, H, sizeof(double) * mm, cudaMemcpyHostToDevice, s.s);
+        spx::launch_syev_small(m, dH, m, dth, dS, dord, dw, dst, s.s);
+        spx::copy_async(theta, dth, sizeof(double) * m, cudaMemcpyDeviceToHost, s.s);
+        spx::copy_async(S, dS, sizeof(double) * mm, cudaMemcpyDeviceToHost, s.s);
+        spx::copy_async(ord, dord, sizeof(int) * m, cudaMemcpyDeviceToHost, s.s);
+        spx::copy_async(hst, dst, sizeof(int), cudaMemcpyDeviceToHost, s.s);
+    }
+    void *ptrs[] = {dH, dth, dS, dw, dord, dst};
+    for (void *q : ptrs) if (q) cudaFreeAsync(q, s.s);
+    cudaError_t e = cudaStreamSynchronize(s.s);
+    if (e != cudaSuccess) return spx::cuda_fail(e, "syev_small");
+    if (!rc && hst[0] < 0) rc = SPEIGS_ERR_LAPACK;
+    return rc;
+}
+
+const char *speigs_b200_last_error(void) { return spx::last_cuda_error(); }
+
+void speigs_b200_counters(long long *launches, long long *h2d_bytes, long long *d2h_bytes) {
+    spx::Counters &c = spx::counters();
+    if (launches) *launches = c.launches.load(std::memory_order_relaxed);
+    if (h2d_bytes) *h2d_bytes = c.h2d.load(std::memory_order_relaxed);
+    if (d2h_bytes) *d2h_bytes = c.d2h.load(std::memory_order_relaxed);
+}
+
+}  // extern "C"

@@ -1,0 +1,57 @@
+// Host-side interface between the C API driver (driver.cpp, plain C++) and
+// the device engine (engine.cu).  No CUDA types cross this header.
+#pragma once
+
+#include <stdint.h>
+
+#include "../../include/speigs.h"
+#include "host/symbolic.h"
+
+namespace spx {
+
+// Full symmetric CSR built on the host from the upper triangle of the
+// caller's CSC (the reference reads only the upper triangle: stype = 1 at
+// src/speigs_core.c:836).
+struct HostCSR {
+    int32_t  n = 0;
+    int64_t *rowptr = nullptr;   // n+1
+    int32_t *col = nullptr;      // nnz
+    double  *val = nullptr;      // nnz
+    int64_t  nnz() const { return rowptr ? rowptr[n] : 0; }
+};
+int  build_full_csr(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *Ax,
+                    HostCSR *out);
+void free_csr(HostCSR *A);
+
+// Extended results not in speigs_info (device-side phase times in ms).
+struct EngineStats {
+    double ms_factor = 0, ms_op = 0, ms_ortho = 0, ms_resid = 0, ms_ritz = 0;
+    int    factor_attempts = 0;
+    int64_t solve_bytes = 0;     // algorithmic bytes of one shift-invert solve
+    double factor_flops = 0;
+};
+
+// 'sm' (shift-invert) or 'lm' (direct) Lanczos on the device for a
+// connected matrix: the part of the reference's speigs() from the operator
+// set-up (:829-986) through lanczos() (:146-315).  lambda/V/resid are host
+// buffers; entries are written for the converged-or-final Ritz pairs, in the
+// Lanczos order (the caller sorts).  Returns 0 or SPEIGS_ERR_*.
+// A is consumed (its host arrays are freed by the call).
+int device_krylov(HostCSR &A, int64_t k, speigs_which which, const speigs_opts &o,
+                  double anorm, double *lambda, double *V, double *resid, speigs_info *info,
+                  EngineStats *stats);
+
+// Host set-up helpers shared by the C API entry points (driver.cpp).
+int    host_check_symmetry(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *Ax);
+double host_norm1_upper(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *Ax);
+
+// Structure fast paths on the device.
+int device_diag_path(int64_t n, const double *diag, int64_t k, speigs_which which,
+                     double *lambda, double *V, double *resid, speigs_info *info);
+int device_dense_path(const HostCSR &A, int64_t k, speigs_which which, double *lambda,
+                      double *V, double *resid, speigs_info *info);
+
+// Thread-local text of the last CUDA failure seen by the engine.
+const char *last_cuda_error();
+
+}  // namespace spx

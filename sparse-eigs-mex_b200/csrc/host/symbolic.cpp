@@ -1,0 +1,603 @@
+// Host symbolic analysis: ordering, elimination tree, column counts,
+// supernodes, row structures, relative maps, tree levels.
+//
+// This is the project's own replacement for the analysis that
+// cholmod_l_analyze performs in the reference (src/speigs_core.c:934, with
+// the ordering choice at :859-863).  The numeric work it prepares runs on the
+// device.
+#include "symbolic.h"
+
+#include <algorithm>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <vector>
+
+namespace {
+
+struct Graph {
+    int32_t n;
+    const int64_t *rp;
+    const int32_t *ci;
+};
+
+// ---------------------------------------------------------------- ordering --
+
+// Exact minimum degree on a region of at most 64 vertices, using bitset
+// adjacency of the elimination graph.  Appends the elimination order.
+void leaf_mindeg(const Graph &g, const std::vector<int32_t> &verts,
+                 std::vector<int32_t> &local, int32_t *out) {
+    const int m = (int)verts.size();
+    for (int a = 0; a < m; a++) local[verts[a]] = a;
+    uint64_t adj[64];
+    for (int a = 0; a < m; a++) {
+        uint64_t bits = 0;
+        int32_t v = verts[a];
+        for (int64_t p = g.rp[v]; p < g.rp[v + 1]; p++) {
+            int32_t u = g.ci[p];
+            int32_t b = local[u];
+            if (u != v && b >= 0 && b < m && verts[b] == u) bits |= (1ull << b);
+        }
+        adj[a] = bits;
+    }
+    uint64_t alive = (m == 64) ? ~0ull : ((1ull << m) - 1);
+    for (int t = 0; t < m; t++) {
+        int best = -1, bd = 1 << 30;
+        for (int a = 0; a < m; a++) {
+            if (!((alive >> a) & 1)) continue;
+            int d = __builtin_popcountll(adj[a] & alive);
+            if (d < bd) { bd = d; best = a; }
+        }
+        out[t] = verts[best];
+        uint64_t nb = adj[best] & alive & ~(1ull << best);
+        uint64_t it = nb;
+        while (it) {
+            int b = __builtin_ctzll(it);
+            it &= it - 1;
+            adj[b] |= nb & ~(1ull << b);
+        }
+        alive &= ~(1ull << best);
+    }
+    for (int a = 0; a < m; a++) local[verts[a]] = -1;
+}
+
+struct NDState {
+    const Graph &g;
+    std::vector<int32_t> part;   // region id of every vertex
+    std::vector<int32_t> level;  // BFS level scratch
+    std::vector<int32_t> queue;
+    std::vector<int32_t> local;  // leaf-local index scratch
+    int32_t next_id = 1;
+    int32_t *perm;
+    explicit NDState(const Graph &gg, int32_t *p)
+        : g(gg), part(gg.n, 0), level(gg.n, -1), queue(gg.n), local(gg.n, -1), perm(p) {}
+
+    // BFS inside region `id` from `src`; fills queue[0..cnt), level[]; returns
+    // the number reached and the eccentricity in *depth.
+    int32_t bfs(int32_t id, int32_t src, int32_t *depth) {
+        int32_t head = 0, tail = 0;
+        queue[tail++] = src;
+        level[src] = 0;
+        int32_t d = 0;
+        while (head < tail) {
+            int32_t v = queue[head++];
+            int32_t lv = level[v];
+            if (lv > d) d = lv;
+            for (int64_t p = g.rp[v]; p < g.rp[v + 1]; p++) {
+                int32_t u = g.ci[p];
+                if (part[u] == id && level[u] < 0) {
+                    level[u] = lv + 1;
+                    queue[tail++] = u;
+                }
+            }
+        }
+        *depth = d;
+        return tail;
+    }
+    void clear_levels(int32_t cnt) {
+        for (int32_t i = 0; i < cnt; i++) level[queue[i]] = -1;
+    }
+    int32_t degree_in(int32_t v, int32_t id) const {
+        int32_t d = 0;
+        for (int64_t p = g.rp[v]; p < g.rp[v + 1]; p++)
+            if (part[g.ci[p]] == id) d++;
+        return d;
+    }
+
+    // Order the vertices `verts` (all carrying region id `id`) into
+    // perm[lo .. lo+|verts|).
+    void order_region(std::vector<int32_t> verts, int32_t id, int32_t lo) {
+        const int32_t m = (int32_t)verts.size();
+        if (m == 0) return;
+        if (m <= 64) {
+            leaf_mindeg(g, verts, local, perm + lo);
+            return;
+        }
+        // pseudo-peripheral start: lowest degree vertex, then repeated BFS
+        int32_t src = verts[0], bestdeg = degree_in(verts[0], id);
+        for (int32_t v : verts) {
+            int32_t d = degree_in(v, id);
+            if (d < bestdeg) { bestdeg = d; src = v; }
+        }
+        int32_t depth = 0, cnt = bfs(id, src, &depth);
+        if (cnt < m) {
+            // disconnected region: order each connected piece on its own
+            std::vector<std::vector<int32_t>> pieces;
+            std::vector<int32_t> ids;
+            pieces.emplace_back(queue.begin(), queue.begin() + cnt);
+            clear_levels(cnt);
+            ids.push_back(next_id++);
+            for (int32_t v : pieces[0]) part[v] = ids[0];
+            for (int32_t v : verts) {
+                if (part[v] != id) continue;
+                int32_t d2 = 0, c2 = bfs(id, v, &d2);
+                pieces.emplace_back(queue.begin(), queue.begin() + c2);
+                clear_levels(c2);
+                ids.push_back(next_id++);
+                for (int32_t u : pieces.back()) part[u] = ids.back();
+            }
+            verts.clear();
+            verts.shrink_to_fit();
+            int32_t at = lo;
+            for (size_t i = 0; i < pieces.size(); i++) {
+                int32_t sz = (int32_t)pieces[i].size();
+                order_region(std::move(pieces[i]), ids[i], at);
+                at += sz;
+            }
+            return;
+        }
+        for (int it = 0; it < 6; it++) {
+            // candidate: min-degree vertex in the last level
+            int32_t cand = -1, cd = 1 << 30;
+            for (int32_t i = cnt - 1; i >= 0 && level[queue[i]] == depth; i--) {
+                int32_t d = degree_in(queue[i], id);
+                if (d < cd) { cd = d; cand = queue[i]; }
+            }
+            clear_levels(cnt);
+            int32_t d2 = 0;
+            bfs(id, cand, &d2);
+            if (d2 <= depth) {
+                // no improvement: redo the BFS from src to keep its levels
+                clear_levels(cnt);
+                bfs(id, src, &depth);
+                break;
+            }
+            src = cand;
+            depth = d2;
+        }
+        if (depth < 2) {
+            // too shallow to split (clique-like): order by degree, low first
+            std::vector<int32_t> vv(queue.begin(), queue.begin() + cnt);
+            clear_levels(cnt);
+            std::stable_sort(vv.begin(), vv.end(), [&](int32_t a, int32_t b) {
+                return degree_in(a, id) < degree_in(b, id);
+            });
+            for (int32_t i = 0; i < m; i++) perm[lo + i] = vv[i];
+            return;
+        }
+        // level sizes
+        std::vector<int32_t> lsz(depth + 1, 0);
+        for (int32_t i = 0; i < cnt; i++) lsz[level[queue[i]]]++;
+        std::vector<int64_t> cum(depth + 2, 0);
+        for (int32_t l = 0; l <= depth; l++) cum[l + 1] = cum[l] + lsz[l];
+        // choose separator level: smallest level subject to balance
+        int32_t best = -1;
+        double bestscore = 1e300;
+        for (int32_t l = 1; l < depth; l++) {
+            int64_t a = cum[l], b = (int64_t)m - cum[l + 1];
+            double bal = (double)std::min(a, b) / (double)(a + b);
+            if (bal < 0.30) continue;
+            double score = (double)lsz[l] * (1.0 + 0.5 * (0.5 - bal));
+            if (score < bestscore) { bestscore = score; best = l; }
+        }
+        if (best < 0) {
+            // take the median level
+            for (int32_t l = 1; l < depth; l++)
+                if (2 * cum[l + 1] >= m) { best = l; break; }
+            if (best < 0) best = depth / 2;
+        }
+        const int32_t ida = next_id++, idb = next_id++, ids = next_id++;
+        std::vector<int32_t> A, B, Sp;
+        for (int32_t i = 0; i < cnt; i++) {
+            int32_t v = queue[i], l = level[v];
+            if (l < best) { part[v] = ida; }
+            else if (l > best) { part[v] = idb; }
+            else { part[v] = ids; }
+        }
+        clear_levels(cnt);
+        // thin the separator: a separator vertex with no neighbour on one side
+        // can join the other side.
+        for (int32_t v : verts) {
+            if (part[v] != ids) continue;
+            bool hasA = false, hasB = false;
+            for (int64_t p = g.rp[v]; p < g.rp[v + 1]; p++) {
+                int32_t u = g.ci[p];
+                if (part[u] == ida) hasA = true;
+                else if (part[u] == idb) hasB = true;
+            }
+            if (!hasB) part[v] = ida;
+            else if (!hasA) part[v] = idb;
+        }
+        for (int32_t v : verts) {
+            if (part[v] == ida) A.push_back(v);
+            else if (part[v] == idb) B.push_back(v);
+            else Sp.push_back(v);
+        }
+        const int32_t na = (int32_t)A.size(), nb = (int32_t)B.size();
+        // separator last, ordered by minimum degree when small
+        if ((int32_t)Sp.size() <= 64) {
+            leaf_mindeg(g, Sp, local, perm + lo + na + nb);
+        } else {
+            for (int32_t i = 0; i < (int32_t)Sp.size(); i++) perm[lo + na + nb + i] = Sp[i];
+        }
+        verts.clear();
+        verts.shrink_to_fit();
+        order_region(std::move(A), ida, lo);
+        order_region(std::move(B), idb, lo + na);
+    }
+};
+
+}  // namespace
+
+extern "C" int spx_order(int32_t n, const int64_t *rowptr, const int32_t *col,
+                         int ordering, int32_t *perm) {
+    (void)ordering;  // nested dissection for every size; leaves by minimum degree
+    if (n <= 0 || !rowptr || !col || !perm) return -1;
+    try {
+        Graph g{n, rowptr, col};
+        NDState st(g, perm);
+        std::vector<int32_t> all(n);
+        for (int32_t i = 0; i < n; i++) all[i] = i;
+        st.order_region(std::move(all), 0, 0);
+    } catch (const std::bad_alloc &) {
+        return -2;
+    }
+    return 0;
+}
+
+namespace {
+
+// cs-style leaf test of Gilbert, Ng and Peyton's column-count algorithm.
+inline int32_t gnp_leaf(int32_t i, int32_t j, const int32_t *first, int32_t *maxfirst,
+                        int32_t *prevleaf, int32_t *ancestor, int *jleaf) {
+    *jleaf = 0;
+    if (i <= j || first[j] <= maxfirst[i]) return -1;
+    maxfirst[i] = first[j];
+    int32_t jprev = prevleaf[i];
+    prevleaf[i] = j;
+    *jleaf = (jprev == -1) ? 1 : 2;
+    if (*jleaf == 1) return i;
+    int32_t q = jprev;
+    while (q != ancestor[q]) q = ancestor[q];
+    for (int32_t s = jprev, sp; s != q; s = sp) {
+        sp = ancestor[s];
+        ancestor[s] = q;
+    }
+    return q;
+}
+
+}  // namespace
+
+extern "C" void spx_symbolic_free(spx_symbolic *S) {
+    if (!S) return;
+    free(S->perm); free(S->iperm); free(S->sfirst); free(S->sparent);
+    free(S->rowptr); free(S->rows); free(S->relmap); free(S->frontptr);
+    free(S->col2sup); free(S->level_ptr); free(S->level_sup);
+    free(S->child_ptr); free(S->child_list);
+    memset(S, 0, sizeof *S);
+}
+
+template <class T>
+static T *xalloc(size_t cnt) {
+    T *p = (T *)malloc((cnt ? cnt : 1) * sizeof(T));
+    if (!p) throw std::bad_alloc();
+    return p;
+}
+
+extern "C" int spx_analyze(int32_t n, const int64_t *rowptr, const int32_t *col,
+                           int ordering, spx_symbolic *S) {
+    if (!S || n <= 0 || !rowptr || !col) return -1;
+    memset(S, 0, sizeof *S);
+    try {
+        S->n = n;
+        // ---- 1. ordering
+        std::vector<int32_t> perm0(n);
+        int rc = spx_order(n, rowptr, col, ordering, perm0.data());
+        if (rc) return rc;
+        std::vector<int32_t> ip0(n);
+        for (int32_t i = 0; i < n; i++) ip0[perm0[i]] = i;
+
+        // ---- 2. permuted adjacency (new numbering), without the diagonal
+        std::vector<int64_t> prp(n + 1, 0);
+        for (int32_t j = 0; j < n; j++) {
+            int32_t o = perm0[j];
+            int64_t c = 0;
+            for (int64_t p = rowptr[o]; p < rowptr[o + 1]; p++) c += (col[p] != o);
+            prp[j + 1] = prp[j] + c;
+        }
+        std::vector<int32_t> pci(prp[n]);
+        for (int32_t j = 0; j < n; j++) {
+            int32_t o = perm0[j];
+            int64_t q = prp[j];
+            for (int64_t p = rowptr[o]; p < rowptr[o + 1]; p++)
+                if (col[p] != o) pci[q++] = ip0[col[p]];
+        }
+
+        // ---- 3. elimination tree (Liu, with path compression)
+        std::vector<int32_t> parent(n, -1), anc(n, -1);
+        for (int32_t k = 0; k < n; k++) {
+            for (int64_t p = prp[k]; p < prp[k + 1]; p++) {
+                int32_t i = pci[p];
+                while (i != -1 && i < k) {
+                    int32_t inext = anc[i];
+                    anc[i] = k;
+                    if (inext == -1) parent[i] = k;
+                    i = inext;
+                }
+            }
+        }
+
+        // ---- 4. postorder, children in increasing order
+        std::vector<int32_t> head(n, -1), next(n, -1), post(n), stack(n);
+        for (int32_t j = n - 1; j >= 0; j--) {
+            if (parent[j] == -1) continue;
+            next[j] = head[parent[j]];
+            head[parent[j]] = j;
+        }
+        {
+            int32_t k = 0;
+            for (int32_t r = 0; r < n; r++) {
+                if (parent[r] != -1) continue;
+                int32_t top = 0;
+                stack[0] = r;
+                while (top >= 0) {
+                    int32_t p = stack[top];
+                    int32_t c = head[p];
+                    if (c == -1) {
+                        top--;
+                        post[k++] = p;
+                    } else {
+                        head[p] = next[c];
+                        stack[++top] = c;
+                    }
+                }
+            }
+        }
+        // relabel: final perm = perm0[post[.]]
+        std::vector<int32_t> ipost(n);
+        for (int32_t k = 0; k < n; k++) ipost[post[k]] = k;
+        S->perm = xalloc<int32_t>(n);
+        S->iperm = xalloc<int32_t>(n);
+        for (int32_t k = 0; k < n; k++) S->perm[k] = perm0[post[k]];
+        for (int32_t k = 0; k < n; k++) S->iperm[S->perm[k]] = k;
+        std::vector<int32_t> par(n);
+        for (int32_t k = 0; k < n; k++) {
+            int32_t p = parent[post[k]];
+            par[k] = (p == -1) ? -1 : ipost[p];
+        }
+        // adjacency in final numbering
+        {
+            std::vector<int64_t> rp2(n + 1, 0);
+            for (int32_t k = 0; k < n; k++) rp2[k + 1] = rp2[k] + (prp[post[k] + 1] - prp[post[k]]);
+            std::vector<int32_t> ci2(rp2[n]);
+            for (int32_t k = 0; k < n; k++) {
+                int64_t q = rp2[k];
+                for (int64_t p = prp[post[k]]; p < prp[post[k] + 1]; p++) ci2[q++] = ipost[pci[p]];
+            }
+            prp.swap(rp2);
+            pci.swap(ci2);
+        }
+
+        // ---- 5. column counts (Gilbert, Ng and Peyton)
+        std::vector<int32_t> first(n, -1), maxfirst(n, -1), prevleaf(n, -1), ancestor(n);
+        std::vector<int64_t> delta(n, 0);
+        for (int32_t k = 0; k < n; k++) {
+            int32_t j = k;
+            delta[j] = (first[j] == -1) ? 1 : 0;
+            for (; j != -1 && first[j] == -1; j = par[j]) first[j] = k;
+        }
+        for (int32_t i = 0; i < n; i++) ancestor[i] = i;
+        for (int32_t j = 0; j < n; j++) {
+            if (par[j] != -1) delta[par[j]]--;
+            for (int64_t p = prp[j]; p < prp[j + 1]; p++) {
+                int32_t i = pci[p];
+                int jleaf;
+                int32_t q = gnp_leaf(i, j, first.data(), maxfirst.data(), prevleaf.data(),
+                                     ancestor.data(), &jleaf);
+                if (jleaf >= 1) delta[j]++;
+                if (jleaf == 2) delta[q]--;
+            }
+            if (par[j] != -1) ancestor[j] = par[j];
+        }
+        std::vector<int64_t> cc(delta);
+        for (int32_t j = 0; j < n; j++)
+            if (par[j] != -1) cc[par[j]] += cc[j];
+
+        // ---- 6. fundamental supernodes
+        std::vector<int32_t> nchild(n, 0);
+        for (int32_t j = 0; j < n; j++)
+            if (par[j] != -1) nchild[par[j]]++;
+        std::vector<int32_t> fs_first;
+        fs_first.reserve(n / 2 + 1);
+        for (int32_t j = 0; j < n; j++) {
+            bool join = j > 0 && par[j - 1] == j && cc[j - 1] == cc[j] + 1 && nchild[j] == 1;
+            if (!join) fs_first.push_back(j);
+        }
+        int32_t nfs = (int32_t)fs_first.size();
+        fs_first.push_back(n);
+        std::vector<int32_t> fs_of(n);
+        for (int32_t s = 0; s < nfs; s++)
+            for (int32_t j = fs_first[s]; j < fs_first[s + 1]; j++) fs_of[j] = s;
+        std::vector<int32_t> fs_par(nfs);
+        for (int32_t s = 0; s < nfs; s++) {
+            int32_t last = fs_first[s + 1] - 1;
+            fs_par[s] = (par[last] == -1) ? -1 : fs_of[par[last]];
+        }
+
+        // ---- 7. relaxed amalgamation (bottom-up; merge a child into its
+        // parent when the child's columns immediately precede the parent's)
+        std::vector<int32_t> mfirst(fs_first.begin(), fs_first.end() - 1);  // current first col
+        std::vector<int32_t> mcols(nfs), mrows(nfs), rep(nfs);
+        std::vector<double> mzeros(nfs, 0.0);
+        for (int32_t s = 0; s < nfs; s++) {
+            mcols[s] = fs_first[s + 1] - fs_first[s];
+            mrows[s] = (int32_t)cc[fs_first[s]];
+            rep[s] = s;
+        }
+        // rep[s]: the fundamental supernode that now heads s's merged group
+        // (groups are merged upward; the parent's record stays the live one)
+        std::vector<char> absorbed(nfs, 0);
+        for (int32_t s = 0; s < nfs; s++) {
+            int32_t p = fs_par[s];
+            if (p < 0) continue;
+            // live group of p is p itself (p has not been absorbed yet, since
+            // p > s in postorder and merging only goes upward)
+            int32_t cs = mcols[s], cp = mcols[p];
+            if (mfirst[s] + cs != mfirst[p]) continue;  // not contiguous
+            int32_t rs = mrows[s], rp = mrows[p];
+            int32_t ns = cs + cp;
+            int32_t rnew = cs + rp;
+            double newz = (double)cs * (double)(cs + rp - rs);
+            double totz = mzeros[s] + mzeros[p] + newz;
+            double denom = (double)ns * (ns + 1) / 2.0 + (double)ns * (double)(rnew - ns);
+            double z = denom > 0 ? totz / denom : 0.0;
+            bool merge = (ns <= 4) || (ns <= 16 && z < 0.8) || (ns <= 48 && z < 0.1) ||
+                         (z < 0.05);
+            if (!merge) continue;
+            mfirst[p] = mfirst[s];
+            mcols[p] = ns;
+            mrows[p] = rnew;
+            mzeros[p] = totz;
+            absorbed[s] = 1;
+        }
+        // final supernodes: the non-absorbed fundamental ones, in column order
+        std::vector<int32_t> fin_of_fs(nfs, -1);
+        std::vector<int32_t> sf;
+        for (int32_t s = 0; s < nfs; s++) {
+            if (absorbed[s]) continue;
+            fin_of_fs[s] = (int32_t)sf.size();
+            sf.push_back(mfirst[s]);
+        }
+        const int32_t ns = (int32_t)sf.size();
+        // sort by first column (postorder guarantees increasing already, but be safe)
+        std::vector<int32_t> order(ns);
+        for (int32_t i = 0; i < ns; i++) order[i] = i;
+        std::sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return sf[a] < sf[b]; });
+        std::vector<int32_t> rank(ns);
+        for (int32_t i = 0; i < ns; i++) rank[order[i]] = i;
+        S->nsuper = ns;
+        S->sfirst = xalloc<int32_t>(ns + 1);
+        for (int32_t i = 0; i < ns; i++) S->sfirst[i] = sf[order[i]];
+        S->sfirst[ns] = n;
+        S->col2sup = xalloc<int32_t>(n);
+        for (int32_t s = 0; s < ns; s++)
+            for (int32_t j = S->sfirst[s]; j < S->sfirst[s + 1]; j++) S->col2sup[j] = s;
+        S->sparent = xalloc<int32_t>(ns);
+        for (int32_t s = 0; s < ns; s++) {
+            int32_t last = S->sfirst[s + 1] - 1;
+            S->sparent[s] = (par[last] == -1) ? -1 : S->col2sup[par[last]];
+        }
+
+        // ---- 8. row structure of every supernode
+        std::vector<int32_t> cptr(ns + 1, 0), clist(ns);
+        for (int32_t s = 0; s < ns; s++)
+            if (S->sparent[s] >= 0) cptr[S->sparent[s] + 1]++;
+        for (int32_t s = 0; s < ns; s++) cptr[s + 1] += cptr[s];
+        {
+            std::vector<int32_t> fill(cptr.begin(), cptr.end() - 1);
+            for (int32_t s = 0; s < ns; s++)
+                if (S->sparent[s] >= 0) clist[fill[S->sparent[s]]++] = s;
+        }
+        std::vector<int64_t> rptr(ns + 1, 0);
+        std::vector<int32_t> rows;
+        rows.reserve((size_t)n * 8);
+        std::vector<int32_t> mark(n, -1);
+        std::vector<int32_t> tmp;
+        for (int32_t s = 0; s < ns; s++) {
+            int32_t f = S->sfirst[s], l = S->sfirst[s + 1];
+            tmp.clear();
+            for (int32_t j = f; j < l; j++) {
+                for (int64_t p = prp[j]; p < prp[j + 1]; p++) {
+                    int32_t i = pci[p];
+                    if (i >= l && mark[i] != s) { mark[i] = s; tmp.push_back(i); }
+                }
+            }
+            for (int32_t q = cptr[s]; q < cptr[s + 1]; q++) {
+                int32_t c = clist[q];
+                int32_t cc0 = S->sfirst[c + 1] - S->sfirst[c];
+                for (int64_t p = rptr[c] + cc0; p < rptr[c + 1]; p++) {
+                    int32_t i = rows[p];
+                    if (i >= l && mark[i] != s) { mark[i] = s; tmp.push_back(i); }
+                }
+            }
+            std::sort(tmp.begin(), tmp.end());
+            for (int32_t j = f; j < l; j++) rows.push_back(j);
+            rows.insert(rows.end(), tmp.begin(), tmp.end());
+            rptr[s + 1] = (int64_t)rows.size();
+        }
+        const int64_t nrows_total = rptr[ns];
+        S->rowptr = xalloc<int64_t>(ns + 1);
+        memcpy(S->rowptr, rptr.data(), (ns + 1) * sizeof(int64_t));
+        S->rows = xalloc<int32_t>(nrows_total);
+        memcpy(S->rows, rows.data(), nrows_total * sizeof(int32_t));
+
+        // ---- 9. relative maps into the parent's row list
+        S->relmap = xalloc<int32_t>(nrows_total);
+        std::vector<int32_t> pos(n, -1);
+        for (int64_t t = 0; t < nrows_total; t++) S->relmap[t] = -1;
+        for (int32_t p = 0; p < ns; p++) {
+            if (cptr[p] == cptr[p + 1]) continue;
+            for (int64_t t = rptr[p]; t < rptr[p + 1]; t++) pos[rows[t]] = (int32_t)(t - rptr[p]);
+            for (int32_t q = cptr[p]; q < cptr[p + 1]; q++) {
+                int32_t c = clist[q];
+                int32_t cc0 = S->sfirst[c + 1] - S->sfirst[c];
+                for (int64_t t = rptr[c] + cc0; t < rptr[c + 1]; t++) S->relmap[t] = pos[rows[t]];
+            }
+            for (int64_t t = rptr[p]; t < rptr[p + 1]; t++) pos[rows[t]] = -1;
+        }
+
+        // ---- 10. levels, fronts, statistics
+        std::vector<int32_t> lev(ns, 0);
+        int32_t maxlev = 0;
+        for (int32_t s = 0; s < ns; s++) {  // children precede parents
+            int32_t p = S->sparent[s];
+            if (p >= 0 && lev[p] < lev[s] + 1) lev[p] = lev[s] + 1;
+            if (lev[s] > maxlev) maxlev = lev[s];
+        }
+        S->nlevels = maxlev + 1;
+        S->level_ptr = xalloc<int32_t>(S->nlevels + 1);
+        S->level_sup = xalloc<int32_t>(ns);
+        for (int32_t l = 0; l <= S->nlevels; l++) S->level_ptr[l] = 0;
+        for (int32_t s = 0; s < ns; s++) S->level_ptr[lev[s] + 1]++;
+        for (int32_t l = 0; l < S->nlevels; l++) S->level_ptr[l + 1] += S->level_ptr[l];
+        {
+            std::vector<int32_t> fill(S->level_ptr, S->level_ptr + S->nlevels);
+            for (int32_t s = 0; s < ns; s++) S->level_sup[fill[lev[s]]++] = s;
+        }
+        S->child_ptr = xalloc<int32_t>(ns + 1);
+        S->child_list = xalloc<int32_t>(ns);
+        memcpy(S->child_ptr, cptr.data(), (ns + 1) * sizeof(int32_t));
+        memcpy(S->child_list, clist.data(), ns * sizeof(int32_t));
+        S->frontptr = xalloc<int64_t>(ns + 1);
+        S->frontptr[0] = 0;
+        S->nnzL = 0;
+        S->flops = 0;
+        S->max_rows = 0;
+        S->max_cols = 0;
+        for (int32_t s = 0; s < ns; s++) {
+            int64_t r = rptr[s + 1] - rptr[s];
+            int64_t c = S->sfirst[s + 1] - S->sfirst[s];
+            S->frontptr[s + 1] = S->frontptr[s] + r * r;
+            S->nnzL += c * (c + 1) / 2 + (r - c) * c;
+            double cd = (double)c, bd = (double)(r - c);
+            S->flops += cd * cd * cd / 3.0 + bd * cd * cd + bd * (bd + 1) * cd;
+            if (r > S->max_rows) S->max_rows = (int32_t)r;
+            if (c > S->max_cols) S->max_cols = (int32_t)c;
+        }
+        S->front_total = S->frontptr[ns];
+    } catch (const std::bad_alloc &) {
+        spx_symbolic_free(S);
+        return -2;
+    }
+    return 0;
+}

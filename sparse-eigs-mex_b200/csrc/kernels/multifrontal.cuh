@@ -1,0 +1,93 @@
+// Device multifrontal supernodal Cholesky and the shift-invert solve.
+//
+// Replaces cholmod_l_factorize_p (reference src/speigs_core.c:940, :966) and
+// cholmod_l_solve2 (:96) for the 'sm' operator.  The host symbolic analysis
+// (host/symbolic.h) fixes the supernodes and tree levels; this file owns the
+// device copy of that structure, the tile task lists, and the kernels.
+//
+// Storage.  Every supernode s has a dense front of r x r doubles (column
+// major, rows in the supernode's row-list order) that lives only during the
+// factorization, and a persistent r x c panel
+//     G_s = [ inv(L11) ; L21 * inv(L11) ]
+// that replaces the usual [L11 ; L21].  With G, both triangular solves are a
+// single dense (transposed) product per supernode, so every supernode of a
+// tree level is solved in parallel with no sequential substitution.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "../host/symbolic.h"
+
+namespace spx {
+
+constexpr int kTile = 32;
+
+enum MfTaskKind { MF_ASSEMBLE = 0, MF_POTRF, MF_TRSM, MF_UPDATE, MF_INVERT, MF_WMUL, MF_NKIND };
+
+struct MfLaunch {
+    int     kind;
+    int64_t off;     // first task
+    int64_t count;   // tasks
+};
+
+struct MfSolveLaunch {
+    int64_t off, count;
+};
+
+class MultifrontalPlan {
+public:
+    MultifrontalPlan() = default;
+    ~MultifrontalPlan();
+    MultifrontalPlan(const MultifrontalPlan &) = delete;
+    MultifrontalPlan &operator=(const MultifrontalPlan &) = delete;
+
+    // Upload the symbolic structure and build the task lists.  rowptr/col
+    // are the host copy of the full symmetric CSR (original numbering) whose
+    // values live on the device at the same positions.  Returns 0 or a
+    // negative SPEIGS_ERR_* code.
+    int init(const spx_symbolic &S, const int64_t *rowptr, const int32_t *col,
+             cudaStream_t st);
+
+    // Numeric factorization of A + shift*I from the device CSR values.
+    // A pivot <= pivtol counts as not positive.  Returns 0, 1 when a pivot
+    // was not positive (A + shift*I not PD), or a negative error code.
+    int factorize(const double *d_val, double shift, double pivtol, cudaStream_t st);
+
+    // x = (A + shift I)^{-1} b  (b, x device vectors in the original order)
+    void solve(const double *b, double *x, cudaStream_t st);
+
+    void release(cudaStream_t st);
+
+    int64_t n() const { return n_; }
+    double factor_flops() const { return flops_; }
+    int64_t panel_entries() const { return g_total_; }
+    int64_t solve_bytes() const;      // algorithmic bytes of one solve pair
+    int levels() const { return nlevels_; }
+
+private:
+    int32_t n_ = 0, ns_ = 0, nlevels_ = 0;
+    double flops_ = 0.0;
+    int64_t front_total_ = 0, g_total_ = 0, u_total_ = 0, nrows_total_ = 0;
+    // device symbolic
+    int32_t *d_perm_ = nullptr, *d_sfirst_ = nullptr, *d_rows_ = nullptr, *d_relmap_ = nullptr;
+    int32_t *d_child_ptr_ = nullptr, *d_child_list_ = nullptr;
+    int64_t *d_rowptr_ = nullptr, *d_frontptr_ = nullptr, *d_gptr_ = nullptr, *d_uptr_ = nullptr;
+    int32_t *d_acolptr_ = nullptr;   // [n+1] assembly entries per new column
+    int32_t *d_atpos_ = nullptr;     // row position within the front
+    int32_t *d_asrc_ = nullptr;      // index into the CSR values
+    int4 *d_tasks_ = nullptr;
+    int4 *d_stasks_ = nullptr;       // solve tasks (s, chunk, 0, 0)
+    std::vector<MfLaunch> launches_;
+    std::vector<MfSolveLaunch> fwd_, bwd_;
+    // numeric
+    double *d_front_ = nullptr;
+    double *d_G_ = nullptr;
+    double *d_u_ = nullptr, *d_yf_ = nullptr, *d_x_ = nullptr;
+    int *d_status_ = nullptr;
+    int max_rows_ = 0;
+};
+
+}  // namespace spx

@@ -1,0 +1,240 @@
+"""ctypes binding of the speigs C ABI (include/speigs.h, include/speigs_b200.h).
+
+The same binding drives any library that exports the reference interface,
+so a test can call the B200 library and a CPU build of the reference through
+identical code.  Loading the B200 library fails loudly when it has not been
+built: there is no Python or CPU stand-in behind these calls.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, c_char_p, c_double, c_int, c_int64, c_uint64, c_void_p
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libspeigs.so")
+
+SM, LM = 0, 1
+PATH_DIAG, PATH_DENSE, PATH_SHIFTINV, PATH_DIRECT, PATH_BLOCKS, PATH_LU, PATH_BANDED = range(7)
+OK, ERR_ARG, ERR_MEM, ERR_FACTOR, ERR_LAPACK, ERR_INTERNAL, ERR_NOTSYM = 0, -1, -2, -3, -4, -5, -6
+
+
+class Opts(ctypes.Structure):
+    """speigs_opts (reference include/speigs.h:40-55)."""
+    _fields_ = [("tol", c_double), ("maxit", c_int64), ("ncv", c_int64), ("dense_max", c_int),
+                ("detect", c_int), ("seed", c_uint64), ("check_sym", c_int), ("band_max", c_int),
+                ("ordering", c_int), ("shift0", c_double)]
+
+
+class Info(ctypes.Structure):
+    """speigs_info (reference include/speigs.h:57-68)."""
+    _fields_ = [("flag", c_int), ("nconv", c_int64), ("restarts", c_int64), ("nops", c_int64),
+                ("shift", c_double), ("anorm", c_double), ("path", c_int), ("ncomp", c_int64),
+                ("t_analyze", c_double), ("t_factor", c_double), ("t_iter", c_double),
+                ("t_op", c_double), ("t_ortho", c_double), ("t_resid", c_double),
+                ("t_ritz", c_double)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+_I64P = POINTER(c_int64)
+_DP = POINTER(c_double)
+
+_SIGNATURES = {
+    "speigs_default_opts": (None, [POINTER(Opts)]),
+    "speigs": (c_int, [c_int64, _I64P, _I64P, _DP, c_int64, c_int, POINTER(Opts), _DP, _DP, _DP,
+                       POINTER(Info)]),
+    "speigs_z": (c_int, [c_int64, _I64P, _I64P, _DP, _DP, c_int64, c_int, POINTER(Opts), _DP, _DP,
+                         _DP, _DP, POINTER(Info)]),
+    "speigs_errmsg": (c_char_p, [c_int]),
+}
+_EXT_SIGNATURES = {
+    "speigs_plan_create": (c_int, [c_int64, _I64P, _I64P, _DP, c_int, POINTER(Opts),
+                                   POINTER(c_void_p)]),
+    "speigs_plan_set_values": (c_int, [c_void_p, _DP]),
+    "speigs_plan_solve_device": (c_int, [c_void_p, c_int64, c_void_p, c_void_p, c_void_p,
+                                         POINTER(Info)]),
+    "speigs_plan_apply_device": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "speigs_plan_factor": (c_int, [c_void_p, _DP]),
+    "speigs_plan_stream": (c_void_p, [c_void_p]),
+    "speigs_plan_costs": (c_int, [c_void_p, _DP, _DP, _DP]),
+    "speigs_plan_destroy": (None, [c_void_p]),
+    "speigs_b200_rand_vec": (c_int, [c_int64, c_uint64, _DP]),
+    "speigs_b200_syev_small": (c_int, [c_int, _DP, _DP, _DP, POINTER(c_int)]),
+    "speigs_b200_last_error": (c_char_p, []),
+    "speigs_b200_counters": (None, [POINTER(ctypes.c_longlong)] * 3),
+}
+
+_cache: dict[str, ctypes.CDLL] = {}
+
+
+def load(path: str | None = None) -> ctypes.CDLL:
+    """Load a library exporting the speigs ABI (default: the B200 build)."""
+    path = os.path.abspath(path or LIB_PATH)
+    if path in _cache:
+        return _cache[path]
+    if not os.path.exists(path):
+        raise RuntimeError(f"speigs library not built: {path} (run __graft_entry__.build())")
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in _SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype, fn.argtypes = res, args
+    for name, (res, args) in _EXT_SIGNATURES.items():
+        fn = getattr(lib, name, None)
+        if fn is not None:
+            fn.restype, fn.argtypes = res, args
+    _cache[path] = lib
+    return lib
+
+
+def default_opts(lib=None, **kw) -> Opts:
+    lib = lib or load()
+    o = Opts()
+    lib.speigs_default_opts(ctypes.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def _csc_arrays(A):
+    """(n, Ap, Ai, Ax) int64/float64 contiguous from a scipy sparse matrix or a tuple."""
+    if isinstance(A, tuple):
+        n, Ap, Ai, Ax = A
+    else:
+        A = A.tocsc()
+        A.sort_indices()
+        n, Ap, Ai, Ax = A.shape[0], A.indptr, A.indices, A.data
+    return (int(n), np.ascontiguousarray(Ap, dtype=np.int64),
+            np.ascontiguousarray(Ai, dtype=np.int64), np.ascontiguousarray(Ax, dtype=np.float64))
+
+
+def _p(a, t=c_double):
+    return a.ctypes.data_as(POINTER(t))
+
+
+def speigs(A, k, which=SM, opts: Opts | None = None, vectors=True, lib=None):
+    """Call speigs() through the C ABI.
+
+    Returns (rc, lam[k], V[n, k] or None, resid[k], info dict).
+    """
+    lib = lib or load()
+    n, Ap, Ai, Ax = _csc_arrays(A)
+    lam = np.zeros(k)
+    res = np.zeros(k)
+    V = np.zeros((k, n)) if vectors else None   # column-major n x k == row-major k x n
+    info = Info()
+    o = opts if opts is not None else default_opts(lib)
+    rc = lib.speigs(n, _p(Ap, c_int64), _p(Ai, c_int64), _p(Ax), k, which, ctypes.byref(o),
+                    _p(lam), _p(V) if vectors else None, _p(res), ctypes.byref(info))
+    return rc, lam, (V.T.copy() if vectors else None), res, info.as_dict()
+
+
+def speigs_z(A_re, A_im, k, which=SM, opts: Opts | None = None, lib=None):
+    """Complex Hermitian through the C ABI: A_re/A_im share one CSC pattern."""
+    lib = lib or load()
+    n, Ap, Ai, Axr = _csc_arrays(A_re)
+    Axi = np.ascontiguousarray(A_im, dtype=np.float64)
+    lam = np.zeros(k)
+    res = np.zeros(k)
+    Vr = np.zeros((k, n))
+    Vi = np.zeros((k, n))
+    info = Info()
+    o = opts if opts is not None else default_opts(lib)
+    rc = lib.speigs_z(n, _p(Ap, c_int64), _p(Ai, c_int64), _p(Axr), _p(Axi), k, which,
+                      ctypes.byref(o), _p(lam), _p(Vr), _p(Vi), _p(res), ctypes.byref(info))
+    return rc, lam, (Vr.T + 1j * Vi.T), res, info.as_dict()
+
+
+def errmsg(rc, lib=None) -> str:
+    return (lib or load()).speigs_errmsg(rc).decode()
+
+
+def last_error(lib=None) -> str:
+    return (lib or load()).speigs_b200_last_error().decode()
+
+
+class Plan:
+    """speigs_plan: a matrix kept on the GPU across solves (speigs_b200.h)."""
+
+    def __init__(self, A, which=SM, opts: Opts | None = None, lib=None):
+        self.lib = lib or load()
+        self.n, self._Ap, self._Ai, Ax = _csc_arrays(A)
+        self.which = which
+        h = c_void_p()
+        o = opts if opts is not None else default_opts(self.lib)
+        rc = self.lib.speigs_plan_create(self.n, _p(self._Ap, c_int64), _p(self._Ai, c_int64),
+                                         _p(Ax), which, ctypes.byref(o), ctypes.byref(h))
+        if rc != 0:
+            raise RuntimeError(f"speigs_plan_create: {errmsg(rc, self.lib)} ({last_error(self.lib)})")
+        self.h = h
+
+    def set_values(self, Ax):
+        Ax = np.ascontiguousarray(Ax, dtype=np.float64)
+        return self.lib.speigs_plan_set_values(self.h, _p(Ax))
+
+    def solve_device(self, k, lam_ptr, V_ptr, resid_ptr):
+        info = Info()
+        rc = self.lib.speigs_plan_solve_device(self.h, k, lam_ptr, V_ptr, resid_ptr,
+                                               ctypes.byref(info))
+        return rc, info.as_dict()
+
+    def apply_device(self, x_ptr, y_ptr):
+        return self.lib.speigs_plan_apply_device(self.h, x_ptr, y_ptr)
+
+    def factor(self):
+        s = c_double()
+        rc = self.lib.speigs_plan_factor(self.h, ctypes.byref(s))
+        return rc, s.value
+
+    def stream(self) -> int:
+        return self.lib.speigs_plan_stream(self.h) or 0
+
+    def costs(self):
+        b, f, z = c_double(), c_double(), c_double()
+        self.lib.speigs_plan_costs(self.h, ctypes.byref(b), ctypes.byref(f), ctypes.byref(z))
+        return {"op_bytes": b.value, "factor_flops": f.value, "nnz_factor": z.value}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.speigs_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def counters(lib=None):
+    """(kernel launches, H2D bytes, D2H bytes) issued by the library so far."""
+    lib = lib or load()
+    a, b, c = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+    lib.speigs_b200_counters(ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
+    return a.value, b.value, c.value
+
+
+def rand_vec(n, seed, lib=None):
+    lib = lib or load()
+    v = np.zeros(n)
+    rc = lib.speigs_b200_rand_vec(n, seed, _p(v))
+    if rc:
+        raise RuntimeError(f"rand_vec: {errmsg(rc, lib)} ({last_error(lib)})")
+    return v
+
+
+def syev_small(H, lib=None):
+    lib = lib or load()
+    H = np.asfortranarray(H, dtype=np.float64)
+    m = H.shape[0]
+    th = np.zeros(m)
+    S = np.zeros((m, m), order="F")
+    ordv = np.zeros(m, dtype=np.int32)
+    rc = lib.speigs_b200_syev_small(m, H.ctypes.data_as(_DP), _p(th),
+                                    S.ctypes.data_as(_DP), ordv.ctypes.data_as(POINTER(c_int)))
+    if rc:
+        raise RuntimeError(f"syev_small: {errmsg(rc, lib)} ({last_error(lib)})")
+    return th, S, ordv

@@ -1,0 +1,126 @@
+"""Seeded synthetic operators for the solver's workloads and tests.
+
+The Laplacians follow the reference's own builders (test/test_speigs.c:31-47
+lap3d: 7-point stencil, x fastest, Dirichlet diagonal 6 or Neumann diagonal
+= degree) and closed-form spectra (:53-62).  The variable-coefficient
+finite-volume operator is the one named for the mixed-precision workload:
+cell conductivities log-normal, face transmissibility the harmonic mean
+2 k_i k_j / (k_i + k_j), Dirichlet boundary faces 2 k_i.
+All matrices are returned as scipy CSC with both triangles and sorted rows.
+"""
+from __future__ import annotations
+
+import numpy as np
+import scipy.sparse as sp
+
+
+def _lap1d(N: int, dirichlet: bool) -> sp.csr_matrix:
+    main = np.full(N, 2.0)
+    if not dirichlet:
+        main[0] = main[-1] = 1.0
+        if N == 1:
+            main[0] = 0.0
+    off = -np.ones(N - 1)
+    return sp.diags([off, main, off], [-1, 0, 1], format="csr")
+
+
+def lap3d(N: int, dirichlet: bool = True) -> sp.csc_matrix:
+    """3-D 7-point Laplacian on an N^3 grid (Dirichlet: diag 6; Neumann: degree)."""
+    L = _lap1d(N, dirichlet)
+    I = sp.identity(N, format="csr")
+    A = sp.kron(I, sp.kron(I, L)) + sp.kron(I, sp.kron(L, I)) + sp.kron(L, sp.kron(I, I))
+    A = A.tocsc()
+    A.sort_indices()
+    A.eliminate_zeros()
+    return A
+
+
+def lap2d(N: int) -> sp.csc_matrix:
+    """2-D 5-point Dirichlet Laplacian (diag 4) on an N^2 grid."""
+    L = _lap1d(N, True)
+    I = sp.identity(N, format="csr")
+    A = (sp.kron(I, L) + sp.kron(L, I)).tocsc()
+    A.sort_indices()
+    return A
+
+
+def lap1d(n: int) -> sp.csc_matrix:
+    A = _lap1d(n, True).tocsc()
+    A.sort_indices()
+    return A
+
+
+def spectrum3d(N: int, dirichlet: bool = True) -> np.ndarray:
+    """All eigenvalues of lap3d(N), ascending (reference exact_spectrum)."""
+    p = np.arange(N)
+    e1 = 2.0 - 2.0 * np.cos((p + 1) * np.pi / (N + 1)) if dirichlet else \
+        2.0 - 2.0 * np.cos(p * np.pi / N)
+    return np.sort((e1[:, None, None] + e1[None, :, None] + e1[None, None, :]).ravel())
+
+
+def spectrum2d_extreme(N: int, k: int, largest: bool) -> np.ndarray:
+    """k smallest (or largest) eigenvalues of lap2d(N) from the closed form."""
+    p = np.arange(1, N + 1)
+    e1 = 2.0 - 2.0 * np.cos(p * np.pi / (N + 1))
+    e1 = np.sort(e1)
+    m = min(N, k + 2)
+    cand = (e1[-m:][:, None] + e1[-m:][None, :]).ravel() if largest else \
+        (e1[:m][:, None] + e1[:m][None, :]).ravel()
+    cand = np.sort(cand)
+    return cand[::-1][:k] if largest else cand[:k]
+
+
+def varcoef3d(N: int, seed: int = 3, sigma: float = 1.0) -> sp.csc_matrix:
+    """3-D finite-volume diffusion operator with log-normal cell conductivity."""
+    rng = np.random.default_rng(seed)
+    kap = np.exp(sigma * rng.standard_normal((N, N, N)))   # index [z, y, x]
+    return _fv_operator(kap)
+
+
+def _fv_operator(kap: np.ndarray) -> sp.csc_matrix:
+    N = kap.shape[0]
+    n = N ** 3
+    idx = np.arange(n).reshape(N, N, N)
+    diag = np.zeros((N, N, N))
+    rows, cols, vals = [], [], []
+    for ax in range(3):
+        a = [slice(None)] * 3
+        b = [slice(None)] * 3
+        a[ax] = slice(0, N - 1)
+        b[ax] = slice(1, N)
+        ka, kb = kap[tuple(a)], kap[tuple(b)]
+        t = 2.0 * ka * kb / (ka + kb)
+        diag[tuple(a)] += t
+        diag[tuple(b)] += t
+        ia, ib = idx[tuple(a)].ravel(), idx[tuple(b)].ravel()
+        rows += [ia, ib]
+        cols += [ib, ia]
+        vals += [-t.ravel(), -t.ravel()]
+        # Dirichlet boundary faces on both ends of this axis
+        lo = [slice(None)] * 3
+        hi = [slice(None)] * 3
+        lo[ax] = 0
+        hi[ax] = N - 1
+        diag[tuple(lo)] += 2.0 * kap[tuple(lo)]
+        diag[tuple(hi)] += 2.0 * kap[tuple(hi)]
+    rows.append(idx.ravel())
+    cols.append(idx.ravel())
+    vals.append(diag.ravel())
+    A = sp.csc_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                      shape=(n, n))
+    A.sum_duplicates()
+    A.sort_indices()
+    return A
+
+
+def upper(A: sp.spmatrix) -> sp.csc_matrix:
+    """Upper triangle (with diagonal) in CSC, the other storage speigs accepts."""
+    U = sp.triu(A, format="csc")
+    U.sort_indices()
+    return U
+
+
+def block_diag(*blocks) -> sp.csc_matrix:
+    A = sp.block_diag(blocks, format="csc")
+    A.sort_indices()
+    return A
