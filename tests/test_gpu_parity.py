@@ -221,6 +221,8 @@ def test_parity_varcoef_sm(pkg, lib, ref_lib):
     assert abs(info["nops"] - rinfo["nops"]) <= info["nops"] // 4
 
 
-def test_parity_lap3d_lm(pkg, lib, ref_lib):
-    A = pkg.workloads.lap3d(20)
+def test_parity_varcoef_lm(pkg, lib, ref_lib):
+    """'lm' on an operator without repeated eigenvalues (the Laplacian's top
+    eigenvalues come in triples, whose discovery depends on rounding)."""
+    A = pkg.workloads.varcoef3d(20, seed=5)
     _parity(pkg, lib, ref_lib, A, 6, 1)
