@@ -105,49 +105,50 @@ private:
     std::vector<void *> ptrs_;
 };
 
-// Device-side phase timer: event pairs resolved at the next host sync.
+// Device-side phase timer: event pairs resolved at host syncs.  A pair keeps
+// its slot until the timer dies, so a phase may span several syncs.
 class PhaseTimer {
 public:
     explicit PhaseTimer(cudaStream_t st) : st_(st) {}
     ~PhaseTimer() {
-        for (auto &p : pend_) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
-        for (auto e : free_) cudaEventDestroy(e);
+        for (auto &p : pairs_) {
+            cudaEventDestroy(p.a);
+            if (p.b) cudaEventDestroy(p.b);
+        }
     }
     int begin() {
-        Pair p{ev(), nullptr, nullptr};
+        Pair p{mk(), nullptr, nullptr, false};
         cudaEventRecord(p.a, st_);
-        pend_.push_back(p);
-        return (int)pend_.size() - 1;
+        pairs_.push_back(p);
+        return (int)pairs_.size() - 1;
     }
     void end(int id, double *acc) {
-        pend_[id].b = ev();
-        pend_[id].acc = acc;
-        cudaEventRecord(pend_[id].b, st_);
+        pairs_[id].b = mk();
+        pairs_[id].acc = acc;
+        cudaEventRecord(pairs_[id].b, st_);
     }
-    void resolve() {   // call after a stream sync
-        for (auto &p : pend_) {
-            if (p.b && p.acc) {
-                float ms = 0.f;
-                if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) *p.acc += ms;
-                else cudaGetLastError();
-            }
-            free_.push_back(p.a);
-            if (p.b) free_.push_back(p.b);
+    void resolve() {   // after a stream sync: every ended pair is complete
+        for (size_t i = first_open_; i < pairs_.size(); i++) {
+            Pair &p = pairs_[i];
+            if (!p.b || p.done) continue;
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) *p.acc += ms;
+            else cudaGetLastError();
+            p.done = true;
         }
-        pend_.clear();
+        while (first_open_ < pairs_.size() && pairs_[first_open_].done) first_open_++;
     }
 
 private:
-    struct Pair { cudaEvent_t a, b; double *acc; };
-    cudaEvent_t ev() {
-        if (!free_.empty()) { cudaEvent_t e = free_.back(); free_.pop_back(); return e; }
+    struct Pair { cudaEvent_t a, b; double *acc; bool done; };
+    cudaEvent_t mk() {
         cudaEvent_t e;
         cudaEventCreate(&e);
         return e;
     }
     cudaStream_t st_;
-    std::vector<Pair> pend_;
-    std::vector<cudaEvent_t> free_;
+    std::vector<Pair> pairs_;
+    size_t first_open_ = 0;
 };
 
 // ------------------------------------------------------------ operators --

@@ -126,12 +126,14 @@ def test_ref9_banded_1d(pkg, lib):
 def test_ref10_isolated(pkg, lib):
     m = 2000
     L = pkg.workloads.lap1d(m)
-    iso = sp.diags([1e-7, -5e-8, 3e-7, 0.0], format="csc")
-    A = sp.block_diag([L, iso], format="csc")
-    A.sort_indices()
-    # keep the stored zero explicitly, as the reference test does
-    A = sp.csc_matrix((A.data, A.indices, A.indptr), shape=A.shape)
-    assert A.nnz == L.nnz + 4
+    # chain + 3 isolated diagonals + one row whose only entry is a stored zero
+    # (reference test_isolated, test/test_speigs.c:299-325)
+    n = m + 4
+    Ap = np.concatenate([L.indptr, L.nnz + np.arange(1, 5)]).astype(np.int64)
+    Ai = np.concatenate([L.indices, np.arange(m, n)]).astype(np.int64)
+    Ax = np.concatenate([L.data, [1e-7, -5e-8, 3e-7, 0.0]])
+    A = (n, Ap, Ai, Ax)
+    assert Ap[-1] == L.nnz + 4
     rc, lam, V, res, info = call(pkg, lib, A, 4, vectors=False)
     assert rc == 0 and info["ncomp"] == 5
     assert abs(lam[0]) < 1e-14
