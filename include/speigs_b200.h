@@ -70,6 +70,23 @@ int speigs_b200_rand_vec(speigs_int n, uint64_t seed, double *v);
  * ascending, S[m*m] eigenvectors, ord[m] indices by |theta| descending. */
 int speigs_b200_syev_small(int m, const double *H, double *theta, double *S, int *ord);
 
+/* Allocation-free variant of speigs_b200_syev_small.  No counterpart in the
+ * reference interface.  For callers that cannot call cudaMalloc where they
+ * need the solve -- code running under CUDA stream capture, real-time loops
+ * that must not touch the allocator, hosts whose device memory belongs to
+ * another allocator.  All pointers are DEVICE memory owned by the caller: H
+ * (m x m column-major, upper triangle read), theta[m], S[m*m], ord[m];
+ * status (optional, may be NULL) receives the sweep count, negative if the
+ * sweeps did not converge.  The work is enqueued on `stream` (a
+ * cudaStream_t; NULL = the legacy default stream) and the call returns
+ * without waiting.  m must be 1..256: larger sizes return SPEIGS_ERR_ARG.
+ * The workspace is a 1 MiB array compiled into the library, held by every
+ * GPU that loads it until the process exits and shared by all calls: calls
+ * that overlap on the GPU race.  The first call on each device looks up the
+ * array's device address; make that first call before any stream capture. */
+int speigs_b200_syev_small_noalloc(int m, const double *H, double *theta, double *S, int *ord,
+                                   int *status, void *stream);
+
 /* Process-wide counts since the library was loaded: kernels this library
  * launched, and bytes it copied host->device and device->host. */
 void speigs_b200_counters(long long *launches, long long *h2d_bytes, long long *d2h_bytes);

@@ -38,6 +38,10 @@ static cudaError_t copy_async(void *dst, const void *src, size_t bytes, cudaMemc
 
 static thread_local char g_err[256] = "";
 const char *last_cuda_error() { return g_err; }
+const char *set_last_error_text(const char *msg) {
+    snprintf(g_err, sizeof g_err, "%s", msg);
+    return g_err;
+}
 
 static int cuda_fail(cudaError_t e, const char *where) {
     snprintf(g_err, sizeof g_err, "%s: %s", where, cudaGetErrorString(e));

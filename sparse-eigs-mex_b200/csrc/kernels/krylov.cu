@@ -638,6 +638,15 @@ void launch_syev_small(int m, const double *H, int ldh, double *theta, double *S
     note_launch();
 }
 
+void launch_syev_small_workspace(int m, const double *H, int ldh, double *theta, double *S,
+                                 int *ord, double *work, int *status, cudaStream_t st) {
+    if (m <= 0) return;
+    const size_t me = (size_t)((m + 1) & ~1);
+    const size_t smem = sizeof(double) * me + sizeof(int) * (me + 2);
+    jacobi_kernel<<<1, kJacThreads, smem, st>>>(m, H, ldh, theta, S, ord, work, status, 0);
+    note_launch();
+}
+
 // ------------------------------------------------------------- helpers --
 __global__ void set_diag_kernel(int ldh, int nd, const double *d, double *H) {
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ldh * ldh; t += gridDim.x * blockDim.x) {

@@ -67,6 +67,11 @@ uint64_t rng_advance(uint64_t seed, uint64_t steps);
 void launch_syev_small(int m, const double *H, int ldh, double *theta, double *S, int *ord,
                        double *work, int *status, cudaStream_t st);
 int syev_small_smem_limit();
+// Same eigensolver, always keeping its two m x m matrices in the caller's
+// global workspace `work` (>= 2*m_even^2 doubles); shared memory holds only
+// the rotation parameters.
+void launch_syev_small_workspace(int m, const double *H, int ldh, double *theta, double *S,
+                                 int *ord, double *work, int *status, cudaStream_t st);
 
 // H (ldh x ldh) = diag(d[0..nd)) with zeros elsewhere in the leading m x m part
 void launch_set_diag(int ldh, int nd, const double *d, double *H, cudaStream_t st);
