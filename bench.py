@@ -311,7 +311,8 @@ def main():
     c1 = s.counters(lib)
     e2e = {"value": statistics.mean(e2e_t), "unit": "s",
            "h2d_bytes_per_step": (c1[1] - c0[1]) // args.steps,
-           "d2h_bytes_per_step": (c1[2] - c0[2]) // args.steps}
+           "d2h_bytes_per_step": (c1[2] - c0[2]) // args.steps,
+           "phase_s": {kk: inf2[kk] for kk in ("t_analyze", "t_factor", "t_iter")}}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_LIB):
@@ -334,6 +335,7 @@ def main():
                        "value_scope": "numeric factor + Lanczos, matrix and analysis resident"},
             "check": check, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(launches), "clocks": clocks,
+            "step_ms": [round(x, 3) for x in step_ms],
             "phase_s": {kk: info[kk] for kk in ("t_factor", "t_iter", "t_op", "t_ortho",
                                                 "t_resid", "t_ritz")},
         }

@@ -52,7 +52,7 @@ static int cuda_fail(cudaError_t e, const char *where) {
 // ------------------------------------------------------------- resources --
 // One memory pool per device with a high release threshold, so repeated calls
 // reuse device memory instead of returning it to the driver at every sync.
-static cudaMemPool_t device_pool(int dev) {
+cudaMemPool_t device_pool(int dev) {
     static std::mutex mu;
     static std::vector<cudaMemPool_t> pools;
     std::lock_guard<std::mutex> lk(mu);
@@ -109,22 +109,30 @@ private:
     std::vector<void *> ptrs_;
 };
 
-// Device-side phase timer: event pairs resolved at host syncs.  A pair keeps
-// its slot until the timer dies, so a phase may span several syncs.
+// Device-side phase timer: event pairs resolved at host syncs.  Events come
+// from a pool that is recycled as pairs are resolved, so a long iteration
+// creates only as many events as are in flight between two syncs.
 class PhaseTimer {
 public:
     explicit PhaseTimer(cudaStream_t st) : st_(st) {}
     ~PhaseTimer() {
         for (auto &p : pairs_) {
-            cudaEventDestroy(p.a);
+            if (p.a) cudaEventDestroy(p.a);
             if (p.b) cudaEventDestroy(p.b);
         }
+        for (auto e : free_) cudaEventDestroy(e);
     }
     int begin() {
-        Pair p{mk(), nullptr, nullptr, false};
+        int id;
+        if (!free_ids_.empty()) { id = free_ids_.back(); free_ids_.pop_back(); }
+        else { id = (int)pairs_.size(); pairs_.push_back({}); }
+        Pair &p = pairs_[id];
+        p.a = mk();
+        p.b = nullptr;
+        p.acc = nullptr;
+        p.live = true;
         cudaEventRecord(p.a, st_);
-        pairs_.push_back(p);
-        return (int)pairs_.size() - 1;
+        return id;
     }
     void end(int id, double *acc) {
         pairs_[id].b = mk();
@@ -132,27 +140,32 @@ public:
         cudaEventRecord(pairs_[id].b, st_);
     }
     void resolve() {   // after a stream sync: every ended pair is complete
-        for (size_t i = first_open_; i < pairs_.size(); i++) {
-            Pair &p = pairs_[i];
-            if (!p.b || p.done) continue;
+        for (int id = 0; id < (int)pairs_.size(); id++) {
+            Pair &p = pairs_[id];
+            if (!p.live || !p.b) continue;
             float ms = 0.f;
             if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) *p.acc += ms;
             else cudaGetLastError();
-            p.done = true;
+            free_.push_back(p.a);
+            free_.push_back(p.b);
+            p.a = p.b = nullptr;
+            p.live = false;
+            free_ids_.push_back(id);
         }
-        while (first_open_ < pairs_.size() && pairs_[first_open_].done) first_open_++;
     }
 
 private:
-    struct Pair { cudaEvent_t a, b; double *acc; bool done; };
+    struct Pair { cudaEvent_t a = nullptr, b = nullptr; double *acc = nullptr; bool live = false; };
     cudaEvent_t mk() {
+        if (!free_.empty()) { cudaEvent_t e = free_.back(); free_.pop_back(); return e; }
         cudaEvent_t e;
         cudaEventCreate(&e);
         return e;
     }
     cudaStream_t st_;
     std::vector<Pair> pairs_;
-    size_t first_open_ = 0;
+    std::vector<int> free_ids_;
+    std::vector<cudaEvent_t> free_;
 };
 
 // ------------------------------------------------------------ operators --
@@ -161,6 +174,8 @@ private:
 struct Operator {
     virtual ~Operator() = default;
     virtual void apply(const double *x, double *y, cudaStream_t st) = 0;
+    // device word that becomes nonzero if an application failed (or null)
+    virtual const int *error_word() const { return nullptr; }
     int64_t nops = 0;
 };
 
@@ -186,6 +201,7 @@ struct CholOperator : Operator {
         nops++;
         plan->solve(x, y, st);
     }
+    const int *error_word() const override { return plan->error_word(); }
 };
 
 // ------------------------------------------------------------- Lanczos --
@@ -234,7 +250,7 @@ inline void orth_block(const LanczosBufs &b, const double *B, int m, double *w, 
 static int lanczos_device(Operator &op, const DevA &A, int n, int64_t k, const speigs_opts &o,
                           double anorm, double *lambda, double *resid, const double **Xdev,
                           int64_t *ldx, int *nout, speigs_info *info, EngineStats *stats,
-                          Arena &ar, cudaStream_t st) {
+                          Arena &ar, double *pinned, cudaStream_t st) {
     int64_t ncv = o.ncv ? o.ncv : std::max<int64_t>(2 * k + 1, 20);
     if (ncv > n) ncv = n;
     if (ncv <= k) ncv = std::min<int64_t>(n, k + 1);
@@ -279,21 +295,24 @@ static int lanczos_device(Operator &op, const DevA &A, int n, int64_t k, const s
     cudaMemsetAsync(b.rs.counter, 0, sizeof(unsigned), st);
     cudaMemsetAsync(b.H, 0, sizeof(double) * ncv * ncv, st);
 
-    double *hs = nullptr;   // pinned scalars
-    if (cudaMallocHost(&hs, sizeof(double) * (2 * b.kk + 8)) != cudaSuccess) {
-        cudaGetLastError();
-        return SPEIGS_ERR_MEM;
-    }
-    struct HostFree { double *p; ~HostFree() { if (p) cudaFreeHost(p); } } hf{hs};
+    // pinned scalars read back by the host (the caller's buffer holds >= 2k+8)
+    double *hs = pinned;
     double *h_lam = hs, *h_r2 = hs + b.kk, *h_nrm = hs + 2 * b.kk;
 
     PhaseTimer tm(st);
     double ms_op = 0, ms_ortho = 0, ms_resid = 0, ms_ritz = 0;
+    const int *op_err = op.error_word();
+    int *h_operr = reinterpret_cast<int *>(h_nrm + 2);
     auto read_nrm = [&](double *out) -> int {
         copy_async(h_nrm, b.nrm2, sizeof(double), cudaMemcpyDeviceToHost, st);
+        if (op_err) copy_async(h_operr, op_err, sizeof(int), cudaMemcpyDeviceToHost, st);
         cudaError_t e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) return cuda_fail(e, "lanczos sync");
         tm.resolve();
+        if (op_err && *h_operr) {
+            set_last_error_text("operator application failed: a solve dependency wait ran out");
+            return SPEIGS_ERR_INTERNAL;
+        }
         *out = sqrt(h_nrm[0]);
         return 0;
     };
@@ -527,6 +546,8 @@ struct speigs_plan_s {
     spx::MultifrontalPlan mf;
     double t_analyze = 0;
     std::vector<void *> owned;
+    double *pinned = nullptr;        // host scalars read back during a solve
+    size_t pinned_n = 0;
 };
 
 namespace spx {
@@ -669,6 +690,18 @@ static int plan_solve(speigs_plan_s *p, int64_t k, double *lambda, double *V, do
     }
     std::vector<double> lam_h(k, 0.0), res_h(k, 0.0);
     int rc = 0;
+    const size_t need = 2 * (size_t)k + 8;
+    if (p->pinned_n < need) {
+        if (p->pinned) cudaFreeHost(p->pinned);
+        p->pinned = nullptr;
+        p->pinned_n = 0;
+        if (cudaMallocHost(&p->pinned, sizeof(double) * need) != cudaSuccess) {
+            cudaGetLastError();
+            p->pinned = nullptr;
+            return SPEIGS_ERR_MEM;
+        }
+        p->pinned_n = need;
+    }
     {
         Arena ar(st);
         const double *X = nullptr;
@@ -676,7 +709,7 @@ static int plan_solve(speigs_plan_s *p, int64_t k, double *lambda, double *V, do
         int nout = 0;
         const double ti = wall();
         rc = lanczos_device(*op, dA, n, k, p->opts, p->anorm, lam_h.data(), res_h.data(), &X,
-                            &ldx, &nout, info, stats, ar, st);
+                            &ldx, &nout, info, stats, ar, p->pinned, st);
         if (rc == 0) {
             // sort by |lambda|: ascending for 'sm', descending for 'lm'
             // (reference :994-1012); entries past nout keep the caller's memory
@@ -914,8 +947,15 @@ int speigs_plan_apply_device(speigs_plan p, const double *x, double *y) {
         }
         p->mf.solve(x, y, st);
     }
+    int herr = 0;
+    if (p->which == SPEIGS_SM && p->mf.error_word())
+        cudaMemcpyAsync(&herr, p->mf.error_word(), sizeof(int), cudaMemcpyDeviceToHost, st);
     cudaError_t e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return spx::cuda_fail(e, "apply");
+    if (herr) {
+        spx::set_last_error_text("solve failed: a dependency wait ran out");
+        return SPEIGS_ERR_INTERNAL;
+    }
     return SPEIGS_OK;
 }
 
@@ -942,6 +982,9 @@ void speigs_plan_destroy(speigs_plan p) {
     p->mf.release(st);
     for (void *q : p->owned) cudaFreeAsync(q, st);
     p->owned.clear();
+    cudaStreamSynchronize(st);
+    if (p->pinned) cudaFreeHost(p->pinned);
+    p->pinned = nullptr;
     spx::free_csr(&p->A);
     delete p;
 }

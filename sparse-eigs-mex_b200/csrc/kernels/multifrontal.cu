@@ -16,6 +16,9 @@
 #include "../common.cuh"
 #include "../counters.h"
 
+#include <cooperative_groups.h>
+namespace cg = cooperative_groups;
+
 #include <algorithm>
 #include <cstring>
 #include <new>
@@ -23,6 +26,9 @@
 #include "../../../include/speigs.h"
 
 namespace spx {
+
+// memory pool of the device (engine.cu): allocations are cached across calls
+cudaMemPool_t device_pool(int dev);
 
 namespace {
 
@@ -37,6 +43,7 @@ struct Sym {
 struct Front {
     int64_t fptr, gptr;
     int r, c, nkb, nt, first;
+    int ldg;          // leading dimension of the G panel: r rounded up to even
 };
 
 SPX_DEV Front front_of(const Sym &y, int s) {
@@ -48,6 +55,7 @@ SPX_DEV Front front_of(const Sym &y, int s) {
     f.nt = f.nkb + (f.r - f.c + T - 1) / T;
     f.fptr = y.frontptr[s];
     f.gptr = y.gptr[s];
+    f.ldg = (f.r + 1) & ~1;
     return f;
 }
 
@@ -187,7 +195,7 @@ mf_potrf(const int4 *__restrict__ tasks, Sym y, double *__restrict__ F, double *
     double *Gs = G + f.gptr;
     for (int t = threadIdx.x; t < T * T; t += blockDim.x) {
         const int i = t & (T - 1), j = t >> 5;
-        if (i < w && j < w && j <= i) Gs[(int64_t)(a + i) + (int64_t)(a + j) * f.r] = X[i][j];
+        if (i < w && j < w && j <= i) Gs[(int64_t)(a + i) + (int64_t)(a + j) * f.ldg] = X[i][j];
     }
 }
 
@@ -226,7 +234,7 @@ mf_trsm(const int4 *__restrict__ tasks, Sym y, double *__restrict__ F,
     const int h = rb - ra, w = kbb - ka;
     double *Fs = F + f.fptr;
     load_tile(A, Fs, f.r, ra, h, ka, w);
-    load_tile(X, G + f.gptr, f.r, ka, w, ka, w);
+    load_tile(X, G + f.gptr, f.ldg, ka, w, ka, w);
     __syncthreads();
     double acc[4] = {0, 0, 0, 0};
     mm_abt(acc, A, X, w);
@@ -291,7 +299,7 @@ mf_invert(const int4 *__restrict__ tasks, Sym y, const double *__restrict__ F,
         tile_range(f, k, ka, kbb);
         const int kw = kbb - ka;
         load_tile(A, Fs, f.r, ra, h, ka, kw);
-        load_tile(B, Gs, f.r, ka, kw, ca, w);
+        load_tile(B, Gs, f.ldg, ka, kw, ca, w);
         __syncthreads();
         mm_ab(acc, A, B, kw);
         __syncthreads();
@@ -299,14 +307,14 @@ mf_invert(const int4 *__restrict__ tasks, Sym y, const double *__restrict__ F,
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
 #pragma unroll
     for (int q = 0; q < 4; q++) B[tx][ty + 8 * q] = acc[q];
-    load_tile(A, Gs, f.r, ra, h, ra, h);   // X_ib,ib
+    load_tile(A, Gs, f.ldg, ra, h, ra, h);   // X_ib,ib
     __syncthreads();
     double out[4] = {0, 0, 0, 0};
     mm_ab(out, A, B, h);
 #pragma unroll
     for (int q = 0; q < 4; q++) {
         const int j = ty + 8 * q;
-        if (tx < h && j < w) Gs[(int64_t)(ra + tx) + (int64_t)(ca + j) * f.r] = -out[q];
+        if (tx < h && j < w) Gs[(int64_t)(ra + tx) + (int64_t)(ca + j) * f.ldg] = -out[q];
     }
 }
 
@@ -332,7 +340,7 @@ mf_wmul(const int4 *__restrict__ tasks, Sym y, const double *__restrict__ F,
         tile_range(f, k, ka, kbb);
         const int kw = kbb - ka;
         load_tile(A, Fs, f.r, ra, h, ka, kw);
-        load_tile(B, Gs, f.r, ka, kw, ca, w);
+        load_tile(B, Gs, f.ldg, ka, kw, ca, w);
         __syncthreads();
         mm_ab(acc, A, B, kw);
         __syncthreads();
@@ -341,88 +349,603 @@ mf_wmul(const int4 *__restrict__ tasks, Sym y, const double *__restrict__ F,
 #pragma unroll
     for (int q = 0; q < 4; q++) {
         const int j = ty + 8 * q;
-        if (tx < h && j < w) Gs[(int64_t)(ra + tx) + (int64_t)(ca + j) * f.r] = acc[q];
+        if (tx < h && j < w) Gs[(int64_t)(ra + tx) + (int64_t)(ca + j) * f.ldg] = acc[q];
     }
 }
 
 // ---------------------------------------------------------------- solve --
-constexpr int kFwdRows = 64;     // rows of G per forward block
-constexpr int kBwdCols = 8;      // columns of G per backward block (one warp each)
+// The whole solve pair is one persistent kernel that pulls tasks from an
+// atomic queue in a topological order (forward tasks leaves -> root, then
+// backward tasks root -> leaves) and waits only for the tasks it depends on:
+// a forward task for supernode s waits until all children of s are done, a
+// backward task until its parent is done.  There is no grid-wide barrier, so
+// independent subtrees overlap.  Every task first loads what does not depend
+// on other tasks (its panel tile, index lists, b) and only then waits.
+// Waits are bounded: a wait that runs out records an error word and returns.
+// Deadlock cannot occur: a task waits only on tasks earlier in the queue,
+// which are held by running blocks.
+//
+// Tasks: up to 8 small supernodes (c <= 32, r <= 128) as a bundle, one per
+// warp; a larger supernode as 64 x 64 tiles of its panel G, one block task
+// per tile that can hold a nonzero.  A tile writes its partial products to
+// scratch; the last tile of a row chunk (forward) or column chunk
+// (backward), found with an atomic counter, adds the partials in a fixed
+// order, so results are the same on every run.
+//
+// Forward, supernode s:  f = b(pivots) + children's update vectors (host-built
+// gather list per front row, children in a fixed order);
+// [x1; r2] = G f(0:c);  yf(pivots) = x1;  u_s = f(c:r) - r2.
+// Backward:  x1 = G^T [yf(pivots); -x(rows below)].
 constexpr int kSThreads = 256;
+constexpr int kSWarps = kSThreads / 32;
+constexpr int kST = 64;          // rows per forward task, columns per backward task
+constexpr int kStrip = 128;      // columns per forward task, rows per backward task
+constexpr int kWarpMaxC = 32;    // warp tasks: c <= 32 ...
+constexpr int kWarpMaxR = 128;   // ... and r <= 128
+constexpr int kGW = 6;           // gather entries per row staged in shared memory
+constexpr int kTinyR = 24;       // thread tasks: leaves with r <= 24 ...
+constexpr int kTinyC = 6;        // ... and c <= 6
+constexpr long kSpinLimit = 1L << 22;
 
-struct SolveArgs {
-    Sym y;
-    const int32_t *perm;
-    const int64_t *uptr;
-    const double *G;
-    double *u, *yf, *x;
+enum { ST_FWD_BUNDLE = 0, ST_FWD_TILE = 1, ST_BWD_BUNDLE = 2, ST_BWD_TILE = 3, ST_FWD_THREADS = 4,
+       ST_BWD_THREADS = 5 };
+
+struct SNode {          // per-supernode solve metadata (64 bytes)
+    int4 a;             // first, c, r, ldg
+    int4 b;             // parent, completions expected from the children
+                        // (forward), row chunks, column chunks
+    longlong2 p;        // panel offset, row-list offset
+    long long uptr;
+    int bwd_expect;     // completions of the parent's backward (of its own
+                        // forward, for a root) that the backward waits for
+    int nchild;
 };
 
-// forward: f = b(pivots) + children's update vectors; [x1; r2] = G f(0:c);
-// yf(pivots) = x1, u_s = f(c:r) - r2
-__global__ void __launch_bounds__(kSThreads)
-mf_forward(const int4 *__restrict__ tasks, SolveArgs a, const double *__restrict__ bvec) {
-    extern __shared__ double fsh[];
-    __shared__ double part[4][kFwdRows];
-    const int4 tk = tasks[blockIdx.x];
-    const int s = tk.x, chunk = tk.y;
-    const Front f = front_of(a.y, s);
-    for (int t = threadIdx.x; t < f.r; t += blockDim.x)
-        fsh[t] = (t < f.c) ? bvec[a.perm[f.first + t]] : 0.0;
-    __syncthreads();
-    for (int q = a.y.child_ptr[s]; q < a.y.child_ptr[s + 1]; q++) {
-        const int ch = a.y.child_list[q];
-        const int rch = (int)(a.y.rowptr[ch + 1] - a.y.rowptr[ch]);
-        const int cch = a.y.sfirst[ch + 1] - a.y.sfirst[ch];
-        const int32_t *rm = a.y.relmap + a.y.rowptr[ch] + cch;
-        const double *uc = a.u + a.uptr[ch];
-        for (int i = threadIdx.x; i < rch - cch; i += blockDim.x) fsh[rm[i]] += uc[i];
-        __syncthreads();
+struct STask {
+    int4 a;             // kind, s, I, J
+    int4 b;             // chunk, bundle offset, bundle size, 0
+};
+
+struct SolveArgs {
+    const SNode *meta;
+    const STask *tasks;
+    int ntasks, ns;
+    const int32_t *bundle, *perm, *rows, *cptr, *cidx;
+    const double *G;
+    double *u, *yf, *x;
+    const int32_t *fc_base, *fc_n, *bc_base, *bc_n;
+    double *fpart, *bpart;
+    int *fcnt, *bcnt;
+    int *sync;          // queue | forward arrivals per parent [ns] | (unused) [ns] |
+                        // backward arrivals [ns] | root forward arrivals [ns] | [ns] | err
+    const double *b;
+    double *out;
+};
+
+SPX_DEV int ld_acquire(const int *p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Bounded wait for *p >= target; gives up (and flags *err) after about a
+// second, or at once when another wait has already given up.
+SPX_DEV void wait_at_least(const int *p, int target, int *err) {
+    if (ld_acquire(p) >= target) return;
+    for (long it = 0; it < kSpinLimit; it++) {
+        __nanosleep(100);
+        if (ld_acquire(p) >= target) return;
+        if ((it & 255) == 0 && *(volatile int *)err) return;
     }
-    const int ri = threadIdx.x % kFwdRows, g = threadIdx.x / kFwdRows;
-    const int i = chunk * kFwdRows + ri;
-    const double *Gs = a.G + f.gptr;
+    atomicExch(err, 1);
+}
+
+// Stage the gather list of front row g: count in *n, first kGW indices in
+// idx[0..), the list start in *e0 (for entries past kGW).
+SPX_DEV void stage_list(const SolveArgs &a, int64_t g, int *idx, int *n, int *e0) {
+    const int b0 = a.cptr[g], b1 = a.cptr[g + 1];
+    *n = b1 - b0;
+    *e0 = b0;
+    const int m = min(b1 - b0, kGW);
+    for (int e = 0; e < m; e++) idx[e] = a.cidx[b0 + e];
+}
+SPX_DEV double sum_list(const SolveArgs &a, const int *idx, int n, int e0) {
     double acc = 0.0;
-    if (i < f.r) {
-        const int jend = (i < f.c) ? i + 1 : f.c;
-        for (int j = g; j < jend; j += 4) acc += Gs[(int64_t)i + (int64_t)j * f.r] * fsh[j];
-    }
-    part[g][ri] = acc;
+    const int m = min(n, kGW);
+    for (int e = 0; e < m; e++) acc += __ldcg(a.u + idx[e]);
+    for (int e = kGW; e < n; e++) acc += __ldcg(a.u + a.cidx[e0 + e]);
+    return acc;
+}
+
+// true in every thread of the block that holds the chunk's last arrival
+SPX_DEV bool last_arrival(int *cnt, int n, int *flag) {
+    __threadfence();
     __syncthreads();
-    if (g == 0 && i < f.r) {
-        const double r = (part[0][ri] + part[1][ri]) + (part[2][ri] + part[3][ri]);
-        if (i < f.c) a.yf[f.first + i] = r;
-        else a.u[a.uptr[s] + (i - f.c)] = fsh[i] - r;
+    if (threadIdx.x == 0) {
+        const int old = atomicAdd(cnt, 1);
+        *flag = (old == n - 1);
+        if (*flag) *cnt = 0;          // every arrival for this solve is in
+    }
+    __syncthreads();
+    const bool last = *flag;
+    if (last) __threadfence();
+    return last;
+}
+
+// shared memory of one solve block.  gbuf holds one panel strip, staged by
+// bulk asynchronous copies (one per panel column) that complete on `bar`.
+struct SolveShared {
+    double gbuf[kStrip * kST];        // forward: 128 cols x 64 rows; backward: 64 x 128
+    double part[4][kST];
+    double vec[kStrip];               // f segment (forward) or v segment (backward)
+    double colsum[kST];
+    int idx[kStrip][kGW];             // gather lists of the strip's pivot columns
+    int cnt[kStrip], e0[kStrip];
+    int idx2[kST][kGW];               // gather lists of the chunk's rows below the pivots
+    int cnt2[kST], e02[kST];
+    int rowv[kStrip];
+    int permv[kST];
+    double bsum[kST];
+};
+struct WarpShared {           // per warp in a bundle: gather lists of <= 128 rows
+    int idx[kWarpMaxR][kGW];
+    int cnt[kWarpMaxR], e0[kWarpMaxR];
+};
+
+// ---- bulk asynchronous copies into shared memory, tracked by an mbarrier
+SPX_DEV uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+SPX_DEV void mbar_init(unsigned long long *bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+SPX_DEV void mbar_expect(unsigned long long *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+                 "r"(bytes) : "memory");
+}
+// copy `bytes` (a multiple of 16, both addresses 16-byte aligned) global -> shared
+SPX_DEV void bulk_load(void *dst, const void *src, uint32_t bytes, unsigned long long *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+        ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar)) : "memory");
+}
+SPX_DEV bool mbar_test(unsigned long long *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                 " selp.u32 %0, 1, 0, p;\n}" : "=r"(ok) : "r"(smem_addr(bar)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+// bounded wait for the copies of the current phase; a wait that runs out
+// flags *err and then waits again (bounded) for the copies still in flight
+SPX_DEV void mbar_wait(unsigned long long *bar, uint32_t parity, int *err) {
+    for (long it = 0; it < kSpinLimit; it++)
+        if (mbar_test(bar, parity)) return;
+    atomicExch(err, 1);
+    for (long it = 0; it < kSpinLimit; it++)
+        if (mbar_test(bar, parity)) return;
+}
+SPX_DEV void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// Stage columns [j0, j0+ncols) x rows [i0, i0+nrows) of a panel (leading
+// dimension ldg, column-major) into buf (column stride `stride` doubles):
+// one bulk copy per column, issued by the lanes of warp 0.  nrows is even.
+SPX_DEV void stage_panel(double *buf, int stride, const double *panel, int ldg, int i0, int nrows,
+                         int j0, int ncols, unsigned long long *bar) {
+    if (threadIdx.x >= 32) return;
+    if (threadIdx.x == 0) mbar_expect(bar, (uint32_t)(ncols * nrows * 8));
+    __syncwarp();
+    for (int jj = threadIdx.x; jj < ncols; jj += 32)
+        bulk_load(buf + (size_t)jj * stride, panel + (int64_t)i0 + (int64_t)(j0 + jj) * ldg,
+                  (uint32_t)(nrows * 8), bar);
+}
+
+// ---- forward, one tiny leaf supernode (r <= 24, c <= 6) per thread.  A
+// leaf has no children, so f is b(pivots); the row and column loops are
+// unrolled with predication so all of the thread's loads are in flight at once.
+SPX_DEV void fwd_thread(const SolveArgs &a, int s) {
+    int *const fcd = a.sync + 1, *const fchk = fcd + 3 * a.ns;
+    const SNode m = a.meta[s];
+    const int first = m.a.x, c = m.a.y, r = m.a.z, ldg = m.a.w, parent = m.b.x;
+    const double *Gs = a.G + m.p.x;
+    double f[kTinyC];
+#pragma unroll
+    for (int j = 0; j < kTinyC; j++) f[j] = (j < c) ? a.b[a.perm[first + j]] : 0.0;
+#pragma unroll
+    for (int i = 0; i < kTinyR; i++) {
+        if (i < r) {
+            double acc = 0.0;
+#pragma unroll
+            for (int j = 0; j < kTinyC; j++)
+                if (j < c) acc += Gs[(int64_t)i + (int64_t)j * ldg] * f[j];
+            if (i < c) a.yf[first + i] = acc;
+            else a.u[m.uptr + (i - c)] = -acc;
+        }
+    }
+    __threadfence();
+    atomicAdd(parent >= 0 ? fcd + parent : fchk + s, 1);
+}
+
+// ---- backward, one tiny leaf supernode per thread
+SPX_DEV void bwd_thread(const SolveArgs &a, int s) {
+    int *const bdone = a.sync + 1 + 2 * a.ns, *const fchk = bdone + a.ns,
+              *const err = a.sync + 1 + 5 * a.ns;
+    const SNode m = a.meta[s];
+    const int first = m.a.x, c = m.a.y, r = m.a.z, ldg = m.a.w, parent = m.b.x;
+    const int32_t *rows = a.rows + m.p.y;
+    const double *Gs = a.G + m.p.x;
+    int ri[kTinyR];
+#pragma unroll
+    for (int i = 0; i < kTinyR; i++) ri[i] = (i >= c && i < r) ? rows[i] : 0;
+    wait_at_least(parent >= 0 ? bdone + parent : fchk + s, m.bwd_expect, err);
+    double v[kTinyR];
+#pragma unroll
+    for (int i = 0; i < kTinyR; i++)
+        v[i] = (i < r) ? ((i < c) ? __ldcg(a.yf + first + i) : -__ldcg(a.x + ri[i])) : 0.0;
+#pragma unroll
+    for (int j = 0; j < kTinyC; j++) {
+        if (j < c) {
+            double acc = 0.0;
+#pragma unroll
+            for (int i = 0; i < kTinyR; i++)
+                if (i < r) acc += Gs[(int64_t)i + (int64_t)j * ldg] * v[i];
+            a.x[first + j] = acc;
+            a.out[a.perm[first + j]] = acc;
+        }
+    }
+    __threadfence();
+    atomicAdd(bdone + s, 1);
+}
+
+// ---- forward, one small supernode per warp.  Row i lives in lane i % 32
+// (q = i / 32); the panel values of a lane's rows are read in blocks of 4
+// columns before they are used, so loads are not serialised behind the
+// column loop.
+SPX_DEV void fwd_warp(const SolveArgs &a, int s, WarpShared &w) {
+    int *const fcd = a.sync + 1, *const fchk = fcd + 3 * a.ns, *const err = a.sync + 1 + 5 * a.ns;
+    const SNode m = a.meta[s];
+    const int first = m.a.x, c = m.a.y, r = m.a.z, ldg = m.a.w;
+    const int parent = m.b.x, nchild = m.nchild, expect = m.b.y;
+    const int64_t g0 = m.p.y;
+    const double *Gs = a.G + m.p.x;
+    const int lane = threadIdx.x & 31;
+    const int nq = (r + 31) >> 5;
+    double bv = 0.0;
+    if (lane < c) bv = a.b[a.perm[first + lane]];
+    // tiny panels (r <= 32, c <= 8) are read completely before the wait
+    double gt[8];
+    const bool tiny = (r <= 32 && c <= 8);
+    if (tiny) {
+#pragma unroll
+        for (int j = 0; j < 8; j++)
+            gt[j] = (j < c && lane < r) ? Gs[(int64_t)lane + (int64_t)j * ldg] : 0.0;
+    }
+    if (nchild > 0)
+        for (int i = lane; i < r; i += 32) stage_list(a, g0 + i, w.idx[i], &w.cnt[i], &w.e0[i]);
+    __syncwarp();
+    if (nchild > 0) {
+        if (lane == 0) wait_at_least(fcd + s, expect, err);
+        __syncwarp();
+    }
+    double fj = 0.0;
+    if (lane < c) fj = bv + (nchild > 0 ? sum_list(a, w.idx[lane], w.cnt[lane], w.e0[lane]) : 0.0);
+    double acc[kWarpMaxR / 32];
+#pragma unroll
+    for (int q = 0; q < kWarpMaxR / 32; q++) acc[q] = 0.0;
+    if (tiny) {
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc[0] += gt[j] * __shfl_sync(0xffffffffu, fj, j);
+    } else {
+        for (int j0 = 0; j0 < c; j0 += 4) {
+            double gv[4][kWarpMaxR / 32];
+#pragma unroll
+            for (int jj = 0; jj < 4; jj++)
+#pragma unroll
+                for (int q = 0; q < kWarpMaxR / 32; q++) {
+                    const int i = lane + 32 * q, j = j0 + jj;
+                    gv[jj][q] = (q < nq && i < r && j < c) ? Gs[(int64_t)i + (int64_t)j * ldg] : 0.0;
+                }
+#pragma unroll
+            for (int jj = 0; jj < 4; jj++) {
+                const double fb = __shfl_sync(0xffffffffu, fj, (j0 + jj) & 31);
+#pragma unroll
+                for (int q = 0; q < kWarpMaxR / 32; q++) acc[q] += gv[jj][q] * fb;
+            }
+        }
+    }
+    // (the panel is zero above the diagonal of its pivot block, so the
+    // products above need no masking)
+#pragma unroll
+    for (int q = 0; q < kWarpMaxR / 32; q++) {
+        const int i = lane + 32 * q;
+        if (i >= r) continue;
+        if (i < c) a.yf[first + i] = acc[q];
+        else a.u[m.uptr + (i - c)] =
+            (nchild > 0 ? sum_list(a, w.idx[i], w.cnt[i], w.e0[i]) : 0.0) - acc[q];
+    }
+    __threadfence();
+    __syncwarp();
+    if (lane == 0) atomicAdd(parent >= 0 ? fcd + parent : fchk + s, 1);
+}
+
+// ---- forward, rows [64 I, 64 I + 64) x a 128-column strip S of a large
+// supernode's panel.  The strip is staged into shared memory before the
+// dependency wait.
+SPX_DEV void fwd_tile(const SolveArgs &a, int s, int I, int S, int chunk, SolveShared &sh,
+                      unsigned long long *bar, uint32_t &phase, int *flag) {
+    int *const fcd = a.sync + 1, *const fchk = fcd + 3 * a.ns, *const err = a.sync + 1 + 5 * a.ns;
+    const SNode m = a.meta[s];
+    const int first = m.a.x, c = m.a.y, r = m.a.z, ldg = m.a.w;
+    const int parent = m.b.x, nchild = m.nchild, expect = m.b.y;
+    const int64_t g0 = m.p.y;
+    const int i0 = I * kST, j0 = S * kStrip;
+    const int jn = min(kStrip, c - j0);
+    const int hcopy = min(kST, ldg - i0);          // even: ldg is even, i0 is a multiple of 64
+    stage_panel(sh.gbuf, kST, a.G + m.p.x, ldg, i0, hcopy, j0, jn, bar);
+    const int t = threadIdx.x;
+    double bv = 0.0;
+    if (t < jn) {
+        bv = a.b[a.perm[first + j0 + t]];
+        if (nchild > 0) stage_list(a, g0 + j0 + t, sh.idx[t], &sh.cnt[t], &sh.e0[t]);
+    }
+    if (t >= kStrip && t < kStrip + kST) {
+        const int tt = t - kStrip, ii = i0 + tt;
+        if (nchild > 0 && ii >= c && ii < r) stage_list(a, g0 + ii, sh.idx2[tt], &sh.cnt2[tt], &sh.e02[tt]);
+    }
+    if (nchild > 0 && t == 0) wait_at_least(fcd + s, expect, err);
+    __syncthreads();
+    if (t < kStrip) {
+        sh.vec[t] = (t < jn) ? bv + (nchild > 0 ? sum_list(a, sh.idx[t], sh.cnt[t], sh.e0[t]) : 0.0)
+                             : 0.0;
+    } else if (t < kStrip + kST) {
+        // the children's contributions to the chunk's rows below the pivots,
+        // needed by whichever strip finishes the chunk
+        const int tt = t - kStrip, ii = i0 + tt;
+        sh.bsum[tt] = (nchild > 0 && ii >= c && ii < r)
+                          ? sum_list(a, sh.idx2[tt], sh.cnt2[tt], sh.e02[tt]) : 0.0;
+    }
+    mbar_wait(bar, phase, err);
+    phase ^= 1u;
+    __syncthreads();
+    const int row = t & (kST - 1), grp = t >> 6;
+    double acc = 0.0;
+    if (row < hcopy)
+        for (int jj = grp; jj < jn; jj += 4) acc += sh.gbuf[jj * kST + row] * sh.vec[jj];
+    sh.part[grp][row] = acc;
+    __syncthreads();
+    const int nt = a.fc_n[chunk];
+    double own = 0.0;
+    if (t < kST) {
+        own = (sh.part[0][t] + sh.part[1][t]) + (sh.part[2][t] + sh.part[3][t]);
+        if (nt > 1) a.fpart[(int64_t)(a.fc_base[chunk] + S) * kST + t] = own;
+    }
+    // a row chunk held by one strip needs no cross-block sum
+    if (nt == 1 || last_arrival(a.fcnt + chunk, nt, flag)) {
+        const int ii = i0 + t;
+        if (t < kST && ii < r) {
+            double rr = own;
+            if (nt > 1) {
+                const double *p0 = a.fpart + (int64_t)a.fc_base[chunk] * kST + t;
+                rr = 0.0;
+                for (int q = 0; q < nt; q++) rr += __ldcg(p0 + (int64_t)q * kST);
+            }
+            if (ii < c) a.yf[first + ii] = rr;
+            else a.u[m.uptr + (ii - c)] = sh.bsum[t] - rr;
+            __threadfence();
+        }
+        __syncthreads();
+        // one completed row chunk: the parent counts every chunk of every child
+        if (t == 0) atomicAdd(parent >= 0 ? fcd + parent : fchk + s, 1);
+    }
+    __syncthreads();
+}
+
+// ---- backward, one small supernode per warp: column sums x1_j = sum_i
+// G(i, j) v_i, with the panel values of blocks of 4 columns loaded before
+// their reductions.
+SPX_DEV void bwd_warp(const SolveArgs &a, int s) {
+    int *const bdone = a.sync + 1 + 2 * a.ns, *const fchk = bdone + a.ns,
+              *const err = a.sync + 1 + 5 * a.ns;
+    const SNode m = a.meta[s];
+    const int first = m.a.x, c = m.a.y, r = m.a.z, ldg = m.a.w, parent = m.b.x;
+    const int32_t *rows = a.rows + m.p.y;
+    const double *Gs = a.G + m.p.x;
+    const int lane = threadIdx.x & 31;
+    const int nq = (r + 31) >> 5;
+    int rv[kWarpMaxR / 32];
+#pragma unroll
+    for (int q = 0; q < kWarpMaxR / 32; q++) {
+        const int i = lane + 32 * q;
+        rv[q] = (i >= c && i < r) ? rows[i] : 0;
+    }
+    const int pj = (lane < c) ? a.perm[first + lane] : 0;
+    double gt[8];
+    const bool tiny = (r <= 32 && c <= 8);
+    if (tiny) {
+#pragma unroll
+        for (int j = 0; j < 8; j++)
+            gt[j] = (j < c && lane < r) ? Gs[(int64_t)lane + (int64_t)j * ldg] : 0.0;
+    }
+    if (lane == 0) wait_at_least(parent >= 0 ? bdone + parent : fchk + s, m.bwd_expect, err);
+    __syncwarp();
+    double v[kWarpMaxR / 32];
+#pragma unroll
+    for (int q = 0; q < kWarpMaxR / 32; q++) {
+        const int i = lane + 32 * q;
+        v[q] = (i < r) ? ((i < c) ? __ldcg(a.yf + first + i) : -__ldcg(a.x + rv[q])) : 0.0;
+    }
+    double mine = 0.0;
+    if (tiny) {
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            const double p = warp_sum(gt[j] * v[0]);
+            if (lane == j) mine = p;
+        }
+    } else {
+        for (int j0 = 0; j0 < c; j0 += 4) {
+            double p[4];
+#pragma unroll
+            for (int jj = 0; jj < 4; jj++) {
+                p[jj] = 0.0;
+#pragma unroll
+                for (int q = 0; q < kWarpMaxR / 32; q++) {
+                    const int i = lane + 32 * q, j = j0 + jj;
+                    if (q < nq && i < r && j < c) p[jj] += Gs[(int64_t)i + (int64_t)j * ldg] * v[q];
+                }
+            }
+#pragma unroll
+            for (int jj = 0; jj < 4; jj++) {
+                const double t = warp_sum(p[jj]);
+                if (lane == j0 + jj) mine = t;
+            }
+        }
+    }
+    if (lane < c) {
+        a.x[first + lane] = mine;
+        a.out[pj] = mine;
+    }
+    __threadfence();
+    __syncwarp();
+    if (lane == 0) atomicAdd(bdone + s, 1);
+}
+
+// ---- backward, columns [64 J, 64 J + 64) x a 128-row strip S of a large
+// supernode's panel, staged into shared memory before the dependency wait.
+SPX_DEV void bwd_tile(const SolveArgs &a, int s, int J, int S, int chunk, SolveShared &sh,
+                      unsigned long long *bar, uint32_t &phase, int *flag) {
+    int *const bdone = a.sync + 1 + 2 * a.ns, *const fchk = bdone + a.ns,
+              *const err = a.sync + 1 + 5 * a.ns;
+    const SNode m = a.meta[s];
+    const int first = m.a.x, c = m.a.y, r = m.a.z, ldg = m.a.w, parent = m.b.x;
+    const int32_t *rows = a.rows + m.p.y;
+    const int i0 = S * kStrip, j0 = J * kST;
+    const int in = min(kStrip, r - i0), jn = min(kST, c - j0);
+    const int hcopy = min(kStrip, ldg - i0);
+    stage_panel(sh.gbuf, kStrip, a.G + m.p.x, ldg, i0, hcopy, j0, jn, bar);
+    const int t = threadIdx.x;
+    if (t < kStrip) {
+        const int ii = i0 + t;
+        sh.rowv[t] = (t < in && ii >= c) ? rows[ii] : 0;
+    } else if (t < kStrip + kST) {
+        const int tt = t - kStrip;
+        sh.permv[tt] = (tt < jn) ? a.perm[first + j0 + tt] : 0;
+    }
+    if (t == 0) wait_at_least(parent >= 0 ? bdone + parent : fchk + s, m.bwd_expect, err);
+    __syncthreads();
+    if (t < kStrip) {
+        const int ii = i0 + t;
+        sh.vec[t] = (t < in) ? ((ii < c) ? __ldcg(a.yf + first + ii) : -__ldcg(a.x + sh.rowv[t]))
+                             : 0.0;
+    }
+    mbar_wait(bar, phase, err);
+    phase ^= 1u;
+    __syncthreads();
+    const int lane = t & 31, wid = t >> 5;
+    const int nt = a.bc_n[chunk];
+    for (int k = 0; k < kST / kSWarps; k++) {
+        const int jj = wid + kSWarps * k;
+        double p = 0.0;
+        if (jj < jn) {
+#pragma unroll
+            for (int q = 0; q < kStrip / 32; q++) {
+                const int ii = lane + 32 * q;
+                if (ii < hcopy) p += sh.gbuf[jj * kStrip + ii] * sh.vec[ii];
+            }
+        }
+        p = warp_sum(p);
+        if (lane == 0) {
+            if (nt > 1) a.bpart[(int64_t)(a.bc_base[chunk] + (S - (j0 / kStrip))) * kST + jj] = p;
+            else sh.colsum[jj] = p;
+        }
+    }
+    if (nt == 1) __syncthreads();
+    // a column chunk held by one strip needs no cross-block sum
+    if (nt == 1 || last_arrival(a.bcnt + chunk, nt, flag)) {
+        const int jj = t;
+        if (jj < jn) {
+            double rr = sh.colsum[jj];
+            if (nt > 1) {
+                const double *p0 = a.bpart + (int64_t)a.bc_base[chunk] * kST + jj;
+                rr = 0.0;
+                for (int q = 0; q < nt; q++) rr += __ldcg(p0 + (int64_t)q * kST);
+            }
+            a.x[first + j0 + jj] = rr;
+            a.out[sh.permv[jj]] = rr;
+            __threadfence();
+        }
+        __syncthreads();
+        // one completed column chunk: the children count every chunk
+        if (t == 0) atomicAdd(bdone + s, 1);
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kSThreads, 2) mf_solve_sf(SolveArgs a) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ int s_task, s_flag;
+    __shared__ __align__(8) unsigned long long s_bar;
+    SolveShared &sh = *reinterpret_cast<SolveShared *>(smem_raw);
+    WarpShared *ws = reinterpret_cast<WarpShared *>(smem_raw);
+    const int wid = threadIdx.x >> 5;
+    uint32_t phase = 0;
+    if (threadIdx.x == 0) mbar_init(&s_bar);
+    __syncthreads();
+    for (;;) {
+        if (threadIdx.x == 0) s_task = atomicAdd(a.sync, 1);
+        __syncthreads();
+        const int t = s_task;
+        __syncthreads();
+        if (t >= a.ntasks) break;
+        const STask tk = a.tasks[t];
+        switch (tk.a.x) {
+            case ST_FWD_BUNDLE:
+                if (wid < tk.b.z) fwd_warp(a, a.bundle[tk.b.y + wid], ws[wid]);
+                break;
+            case ST_FWD_TILE:
+                fwd_tile(a, tk.a.y, tk.a.z, tk.a.w, tk.b.x, sh, &s_bar, phase, &s_flag);
+                break;
+            case ST_BWD_BUNDLE:
+                if (wid < tk.b.z) bwd_warp(a, a.bundle[tk.b.y + wid]);
+                break;
+            case ST_FWD_THREADS:
+                if ((int)threadIdx.x < tk.b.z) fwd_thread(a, a.bundle[tk.b.y + threadIdx.x]);
+                break;
+            case ST_BWD_THREADS:
+                if ((int)threadIdx.x < tk.b.z) bwd_thread(a, a.bundle[tk.b.y + threadIdx.x]);
+                break;
+            default:
+                bwd_tile(a, tk.a.y, tk.a.z, tk.a.w, tk.b.x, sh, &s_bar, phase, &s_flag);
+                break;
+        }
+        __syncthreads();
+        // shared memory read by this task may be refilled by the async
+        // proxy in the next one
+        fence_proxy_async();
     }
 }
 
-// backward: x1 = G^T [yf(pivots); -x(rows below)]
-__global__ void __launch_bounds__(kSThreads)
-mf_backward(const int4 *__restrict__ tasks, SolveArgs a, double *__restrict__ out) {
-    extern __shared__ double vsh[];
-    const int4 tk = tasks[blockIdx.x];
-    const int s = tk.x, chunk = tk.y;
-    const Front f = front_of(a.y, s);
-    const int32_t *rows = a.y.rows + a.y.rowptr[s];
-    for (int t = threadIdx.x; t < f.r; t += blockDim.x)
-        vsh[t] = (t < f.c) ? a.yf[f.first + t] : -a.x[rows[t]];
-    __syncthreads();
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int j = chunk * kBwdCols + wid;
-    if (j >= f.c) return;
-    const double *gc = a.G + f.gptr + (int64_t)j * f.r;
-    double acc = 0.0;
-    for (int i = j + lane; i < f.r; i += 32) acc += gc[i] * vsh[i];
-    acc = warp_sum(acc);
-    if (lane == 0) {
-        a.x[f.first + j] = acc;
-        out[a.perm[f.first + j]] = acc;
-    }
+static size_t solve_smem_bytes() {
+    return std::max(sizeof(SolveShared), sizeof(WarpShared) * kSWarps);
 }
+
+// host mirrors of SNode / STask
+struct SNodeH {
+    int first, c, r, ldg, parent, fwd_expect, nrc, ncc;
+    long long gptr, g0, uptr;
+    int bwd_expect, nchild;
+};
+struct STaskH {
+    int kind, s, I, J, chunk, boff, bn, pad;
+};
 
 template <class Tp>
 static int dmalloc(Tp **p, size_t cnt, cudaStream_t st) {
-    if (cudaMallocAsync((void **)p, (cnt ? cnt : 1) * sizeof(Tp), st) != cudaSuccess) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaMemPool_t pool = device_pool(dev);
+    const size_t bytes = (cnt ? cnt : 1) * sizeof(Tp);
+    cudaError_t e = pool ? cudaMallocFromPoolAsync((void **)p, bytes, pool, st)
+                         : cudaMallocAsync((void **)p, bytes, st);
+    if (e != cudaSuccess) {
         *p = nullptr;
         cudaGetLastError();
         return SPEIGS_ERR_MEM;
@@ -447,13 +970,20 @@ MultifrontalPlan::~MultifrontalPlan() { release(0); }
 void MultifrontalPlan::release(cudaStream_t st) {
     void *ptrs[] = {d_perm_, d_sfirst_, d_rows_, d_relmap_, d_child_ptr_, d_child_list_,
                     d_rowptr_, d_frontptr_, d_gptr_, d_uptr_, d_acolptr_, d_atpos_, d_asrc_,
-                    d_tasks_, d_stasks_, d_front_, d_G_, d_u_, d_yf_, d_x_, d_status_};
+                    d_tasks_, d_front_, d_G_, d_u_, d_yf_, d_x_, d_status_, d_meta_,
+                    d_stask_, d_bundle_, d_cptr_, d_cidx_, d_chunks_, d_fpart_, d_bpart_,
+                    d_cnt_, d_sync_};
     for (void *p : ptrs)
         if (p) cudaFreeAsync(p, st);
     d_perm_ = d_sfirst_ = d_rows_ = d_relmap_ = d_child_ptr_ = d_child_list_ = nullptr;
     d_rowptr_ = d_frontptr_ = d_gptr_ = d_uptr_ = nullptr;
     d_acolptr_ = d_atpos_ = d_asrc_ = nullptr;
-    d_tasks_ = d_stasks_ = nullptr;
+    d_tasks_ = nullptr;
+    d_bundle_ = d_cptr_ = d_cidx_ = d_chunks_ = nullptr;
+    d_meta_ = nullptr;
+    d_stask_ = nullptr;
+    d_fpart_ = d_bpart_ = nullptr;
+    d_cnt_ = d_sync_ = nullptr;
     d_front_ = d_G_ = d_u_ = d_yf_ = d_x_ = nullptr;
     d_status_ = nullptr;
 }
@@ -480,7 +1010,7 @@ int MultifrontalPlan::init(const spx_symbolic &S, const int64_t *rowptr, const i
         int64_t gtri = 0;
         for (int32_t s = 0; s < ns; s++) {
             int64_t r = S.rowptr[s + 1] - S.rowptr[s], c = S.sfirst[s + 1] - S.sfirst[s];
-            gptr[s + 1] = gptr[s] + r * c;
+            gptr[s + 1] = gptr[s] + ((r + 1) & ~(int64_t)1) * c;
             uptr[s + 1] = uptr[s] + (r - c);
             gtri += c * (c + 1) / 2 + (r - c) * c;
         }
@@ -519,9 +1049,6 @@ int MultifrontalPlan::init(const spx_symbolic &S, const int64_t *rowptr, const i
             if (tasks.size() > before)
                 launches_.push_back({kind, (int64_t)before, (int64_t)(tasks.size() - before)});
         };
-        std::vector<int4> stasks;
-        fwd_.clear();
-        bwd_.clear();
         for (int l = 0; l < S.nlevels; l++) {
             const int32_t q0 = S.level_ptr[l], q1 = S.level_ptr[l + 1];
             int nkbmax = 0;
@@ -586,23 +1113,143 @@ int MultifrontalPlan::init(const spx_symbolic &S, const int64_t *rowptr, const i
                     for (int J = 0; J < nkb; J++) tasks.push_back(make_int4(s, I, J, 0));
             }
             emit(MF_WMUL, bw);
-            // solve tasks
-            size_t f0 = stasks.size();
-            for (int32_t q = q0; q < q1; q++) {
-                const int s = S.level_sup[q];
-                const int r = (int)(S.rowptr[s + 1] - S.rowptr[s]);
-                for (int ch = 0; ch * kFwdRows < r; ch++) stasks.push_back(make_int4(s, ch, 0, 0));
+        }
+        // solve: per-supernode metadata and the task queue.  Forward tasks
+        // level by level from the leaves (tiles of large supernodes first,
+        // then bundles of up to 8 small ones), then backward tasks level by
+        // level from the roots.  Every task depends only on earlier tasks.
+        std::vector<SNodeH> meta(ns);
+        auto small = [&](int r, int c) { return c <= kWarpMaxC && r <= kWarpMaxR; };
+        std::vector<STaskH> tasks_s;
+        std::vector<int32_t> bundle, fc_base, fc_n, bc_base, bc_n;
+        int32_t fslots = 0, bslots = 0;
+        // one thread per tiny leaf; everything else small goes to a warp
+        auto tiny_leaf = [&](int s2) {
+            return meta[s2].c <= kTinyC && meta[s2].r <= kTinyR && meta[s2].nchild == 0;
+        };
+        for (int32_t s2 = 0; s2 < ns; s2++) {
+            const int r = (int)(S.rowptr[s2 + 1] - S.rowptr[s2]);
+            const int c = S.sfirst[s2 + 1] - S.sfirst[s2];
+            SNodeH &m = meta[s2];
+            m.first = S.sfirst[s2]; m.c = c; m.r = r; m.ldg = (r + 1) & ~1;
+            m.parent = S.sparent[s2];
+            m.nchild = S.child_ptr[s2 + 1] - S.child_ptr[s2];
+            m.nrc = (r + kST - 1) / kST;
+            m.ncc = (c + kST - 1) / kST;
+            m.gptr = gptr[s2]; m.g0 = S.rowptr[s2]; m.uptr = uptr[s2];
+            m.fwd_expect = 0;
+            m.bwd_expect = 0;
+        }
+        // completions a supernode reports: one per row chunk (forward) or
+        // column chunk (backward) when it is cut into tiles, else one
+        auto fwd_done_count = [&](int s2) {
+            return small(meta[s2].r, meta[s2].c) ? 1 : meta[s2].nrc;
+        };
+        auto bwd_done_count = [&](int s2) {
+            return small(meta[s2].r, meta[s2].c) ? 1 : meta[s2].ncc;
+        };
+        for (int32_t s2 = 0; s2 < ns; s2++) {
+            const int p2 = meta[s2].parent;
+            if (p2 >= 0) {
+                meta[p2].fwd_expect += fwd_done_count(s2);
+                meta[s2].bwd_expect = bwd_done_count(p2);
+            } else {
+                meta[s2].bwd_expect = fwd_done_count(s2);
             }
-            fwd_.push_back({(int64_t)f0, (int64_t)(stasks.size() - f0)});
+        }
+        for (int l = 0; l < S.nlevels; l++) {
+            for (int32_t q = S.level_ptr[l]; q < S.level_ptr[l + 1]; q++) {
+                const int s2 = S.level_sup[q];
+                const int r = meta[s2].r, c = meta[s2].c;
+                if (small(r, c)) continue;
+                const int nI = meta[s2].nrc, nS = (c + kStrip - 1) / kStrip;
+                for (int I = 0; I < nI; I++) {
+                    // strip S can hold a nonzero of row chunk I iff the chunk's
+                    // last row >= the strip's first column
+                    const int smax = std::min(nS - 1, (std::min(r, (I + 1) * kST) - 1) / kStrip);
+                    const int chunk = (int)fc_base.size();
+                    fc_base.push_back(fslots);
+                    fc_n.push_back(smax + 1);
+                    fslots += smax + 1;
+                    for (int S2 = 0; S2 <= smax; S2++)
+                        tasks_s.push_back({ST_FWD_TILE, s2, I, S2, chunk, 0, 0, 0});
+                }
+            }
+            std::vector<int32_t> sm, ti;
+            for (int32_t q = S.level_ptr[l]; q < S.level_ptr[l + 1]; q++) {
+                const int s2 = S.level_sup[q];
+                if (tiny_leaf(s2)) ti.push_back(s2);
+                else if (small(meta[s2].r, meta[s2].c)) sm.push_back(s2);
+            }
+            for (size_t b0 = 0; b0 < sm.size(); b0 += kSWarps) {
+                const int nb = (int)std::min<size_t>(kSWarps, sm.size() - b0);
+                tasks_s.push_back({ST_FWD_BUNDLE, 0, 0, 0, 0, (int)bundle.size(), nb, 0});
+                bundle.insert(bundle.end(), sm.begin() + b0, sm.begin() + b0 + nb);
+            }
+            for (size_t b0 = 0; b0 < ti.size(); b0 += kSThreads) {
+                const int nb = (int)std::min<size_t>(kSThreads, ti.size() - b0);
+                tasks_s.push_back({ST_FWD_THREADS, 0, 0, 0, 0, (int)bundle.size(), nb, 0});
+                bundle.insert(bundle.end(), ti.begin() + b0, ti.begin() + b0 + nb);
+            }
         }
         for (int l = S.nlevels - 1; l >= 0; l--) {
-            size_t b0 = stasks.size();
             for (int32_t q = S.level_ptr[l]; q < S.level_ptr[l + 1]; q++) {
-                const int s = S.level_sup[q];
-                const int c = S.sfirst[s + 1] - S.sfirst[s];
-                for (int ch = 0; ch * kBwdCols < c; ch++) stasks.push_back(make_int4(s, ch, 0, 0));
+                const int s2 = S.level_sup[q];
+                const int r = meta[s2].r, c = meta[s2].c;
+                if (small(r, c)) continue;
+                const int nJ = meta[s2].ncc, nS = (r + kStrip - 1) / kStrip;
+                for (int J = 0; J < nJ; J++) {
+                    // row strips from the one holding the chunk's first column
+                    const int smin = (J * kST) / kStrip;
+                    const int chunk = (int)bc_base.size();
+                    bc_base.push_back(bslots);
+                    bc_n.push_back(nS - smin);
+                    bslots += nS - smin;
+                    for (int S2 = smin; S2 < nS; S2++)
+                        tasks_s.push_back({ST_BWD_TILE, s2, J, S2, chunk, 0, 0, 0});
+                }
             }
-            bwd_.push_back({(int64_t)b0, (int64_t)(stasks.size() - b0)});
+            std::vector<int32_t> sm, ti;
+            for (int32_t q = S.level_ptr[l]; q < S.level_ptr[l + 1]; q++) {
+                const int s2 = S.level_sup[q];
+                if (tiny_leaf(s2)) ti.push_back(s2);
+                else if (small(meta[s2].r, meta[s2].c)) sm.push_back(s2);
+            }
+            for (size_t b0 = 0; b0 < sm.size(); b0 += kSWarps) {
+                const int nb = (int)std::min<size_t>(kSWarps, sm.size() - b0);
+                tasks_s.push_back({ST_BWD_BUNDLE, 0, 0, 0, 0, (int)bundle.size(), nb, 0});
+                bundle.insert(bundle.end(), sm.begin() + b0, sm.begin() + b0 + nb);
+            }
+            for (size_t b0 = 0; b0 < ti.size(); b0 += kSThreads) {
+                const int nb = (int)std::min<size_t>(kSThreads, ti.size() - b0);
+                tasks_s.push_back({ST_BWD_THREADS, 0, 0, 0, 0, (int)bundle.size(), nb, 0});
+                bundle.insert(bundle.end(), ti.begin() + b0, ti.begin() + b0 + nb);
+            }
+        }
+        ntasks_ = (int)tasks_s.size();
+        // gather lists: for every front row (global row-list index g) the
+        // update-vector entries of the children that land on it, children in
+        // their fixed order
+        std::vector<int32_t> cptr(nrows_total_ + 1, 0), cidx;
+        for (int32_t par = 0; par < ns; par++)
+            for (int32_t q = S.child_ptr[par]; q < S.child_ptr[par + 1]; q++) {
+                const int ch = S.child_list[q];
+                const int cc = S.sfirst[ch + 1] - S.sfirst[ch];
+                for (int64_t t = S.rowptr[ch] + cc; t < S.rowptr[ch + 1]; t++)
+                    cptr[S.rowptr[par] + S.relmap[t] + 1]++;
+            }
+        for (int64_t g = 0; g < nrows_total_; g++) cptr[g + 1] += cptr[g];
+        cidx.assign(cptr[nrows_total_], 0);
+        {
+            std::vector<int32_t> fill(cptr.begin(), cptr.end() - 1);
+            for (int32_t par = 0; par < ns; par++)
+                for (int32_t q = S.child_ptr[par]; q < S.child_ptr[par + 1]; q++) {
+                    const int ch = S.child_list[q];
+                    const int cc = S.sfirst[ch + 1] - S.sfirst[ch];
+                    for (int64_t t = S.rowptr[ch] + cc; t < S.rowptr[ch + 1]; t++)
+                        cidx[fill[S.rowptr[par] + S.relmap[t]]++] =
+                            (int32_t)(uptr[ch] + (t - S.rowptr[ch] - cc));
+                }
         }
         int rc = 0;
         rc = rc ? rc : dupload(&d_perm_, S.perm, n, st);
@@ -619,8 +1266,34 @@ int MultifrontalPlan::init(const spx_symbolic &S, const int64_t *rowptr, const i
         rc = rc ? rc : dupload(&d_atpos_, atpos.data(), atpos.size(), st);
         rc = rc ? rc : dupload(&d_asrc_, asrc.data(), asrc.size(), st);
         rc = rc ? rc : dupload(&d_tasks_, tasks.data(), tasks.size(), st);
-        rc = rc ? rc : dupload(&d_stasks_, stasks.data(), stasks.size(), st);
+        {
+            std::vector<int32_t> ch;
+            ch.insert(ch.end(), fc_base.begin(), fc_base.end());
+            ch.insert(ch.end(), fc_n.begin(), fc_n.end());
+            ch.insert(ch.end(), bc_base.begin(), bc_base.end());
+            ch.insert(ch.end(), bc_n.begin(), bc_n.end());
+            rc = rc ? rc : dupload(&d_chunks_, ch.data(), ch.size(), st);
+            nfc_ = (int32_t)fc_base.size();
+            nbc_ = (int32_t)bc_base.size();
+        }
+        static_assert(sizeof(SNodeH) == sizeof(SNode), "metadata layout");
+        static_assert(sizeof(STaskH) == sizeof(STask), "task layout");
+        rc = rc ? rc : dupload((SNodeH **)&d_meta_, meta.data(), meta.size(), st);
+        rc = rc ? rc : dupload((STaskH **)&d_stask_, tasks_s.data(), tasks_s.size(), st);
+        rc = rc ? rc : dupload(&d_bundle_, bundle.data(), bundle.size(), st);
+        rc = rc ? rc : dmalloc(&d_fpart_, (size_t)fslots * kST, st);
+        rc = rc ? rc : dmalloc(&d_bpart_, (size_t)bslots * kST, st);
+        rc = rc ? rc : dmalloc(&d_cnt_, (size_t)(nfc_ + nbc_), st);
+        if (!rc) cudaMemsetAsync(d_cnt_, 0, sizeof(int) * (size_t)(nfc_ + nbc_), st);
+        sync_ints_ = 2 + 5 * (size_t)ns;
+        rc = rc ? rc : dmalloc(&d_sync_, sync_ints_, st);
+        if (!rc) cudaMemsetAsync(d_sync_, 0, sizeof(int) * sync_ints_, st);
+        rc = rc ? rc : dupload(&d_cptr_, cptr.data(), cptr.size(), st);
+        rc = rc ? rc : dupload(&d_cidx_, cidx.data(), cidx.size(), st);
         rc = rc ? rc : dmalloc(&d_G_, (size_t)gptr[ns], st);
+        // the solve reads whole tiles: the strictly upper part of every
+        // inv(L11) block and the padding row stay zero for the plan's life
+        if (!rc) cudaMemsetAsync(d_G_, 0, sizeof(double) * (size_t)gptr[ns], st);
         rc = rc ? rc : dmalloc(&d_u_, (size_t)u_total_, st);
         rc = rc ? rc : dmalloc(&d_yf_, (size_t)n, st);
         rc = rc ? rc : dmalloc(&d_x_, (size_t)n, st);
@@ -628,12 +1301,17 @@ int MultifrontalPlan::init(const spx_symbolic &S, const int64_t *rowptr, const i
         if (rc) return rc;
         // everything uploaded above comes from host vectors that die here
         if (cudaStreamSynchronize(st) != cudaSuccess) return SPEIGS_ERR_INTERNAL;
-        const size_t need = (size_t)max_rows_ * sizeof(double);
-        if (need > 48 * 1024) {
-            if (need > 227 * 1024) return SPEIGS_ERR_MEM;
-            cudaFuncSetAttribute(mf_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need);
-            cudaFuncSetAttribute(mf_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need);
-        }
+        // persistent grid for the task-queue solve
+        solve_smem_ = solve_smem_bytes();
+        if (solve_smem_ > 48 * 1024)
+            cudaFuncSetAttribute(mf_solve_sf, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)solve_smem_);
+        int dev = 0, nsm = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mf_solve_sf, kSThreads, solve_smem_);
+        if (per_sm <= 0 || nsm <= 0) return SPEIGS_ERR_INTERNAL;
+        solve_grid_ = nsm * std::min(per_sm, 4);
     } catch (const std::bad_alloc &) {
         return SPEIGS_ERR_MEM;
     }
@@ -688,17 +1366,38 @@ int MultifrontalPlan::factorize(const double *d_val, double shift, double pivtol
 }
 
 void MultifrontalPlan::solve(const double *b, double *x, cudaStream_t st) {
-    Sym y{d_sfirst_, d_rows_, d_relmap_, d_child_ptr_, d_child_list_, d_rowptr_, d_frontptr_, d_gptr_};
-    SolveArgs a{y, d_perm_, d_uptr_, d_G_, d_u_, d_yf_, d_x_};
-    const size_t smem = (size_t)max_rows_ * sizeof(double);
-    for (const MfSolveLaunch &L : fwd_)
-        if (L.count)
-            mf_forward<<<(unsigned)L.count, kSThreads, smem, st>>>(d_stasks_ + L.off, a, b);
-            note_launch();
-    for (const MfSolveLaunch &L : bwd_)
-        if (L.count)
-            mf_backward<<<(unsigned)L.count, kSThreads, smem, st>>>(d_stasks_ + L.off, a, x);
-            note_launch();
+    SolveArgs a;
+    a.meta = (const SNode *)d_meta_;
+    a.tasks = (const STask *)d_stask_;
+    a.ntasks = ntasks_;
+    a.ns = ns_;
+    a.bundle = d_bundle_;
+    a.perm = d_perm_;
+    a.rows = d_rows_;
+    a.cptr = d_cptr_;
+    a.cidx = d_cidx_;
+    a.G = d_G_;
+    a.u = d_u_;
+    a.yf = d_yf_;
+    a.x = d_x_;
+    a.fc_base = d_chunks_;
+    a.fc_n = d_chunks_ + nfc_;
+    a.bc_base = d_chunks_ + 2 * nfc_;
+    a.bc_n = d_chunks_ + 2 * nfc_ + nbc_;
+    a.fpart = d_fpart_;
+    a.bpart = d_bpart_;
+    a.fcnt = d_cnt_;
+    a.bcnt = d_cnt_ + nfc_;
+    a.sync = d_sync_;
+    a.b = b;
+    a.out = x;
+    // queue, dependency counters and flags start at zero; the error word at
+    // the end keeps its value so a failed solve stays visible until read
+    cudaMemsetAsync(d_sync_, 0, sizeof(int) * (sync_ints_ - 1), st);
+    mf_solve_sf<<<solve_grid_, kSThreads, solve_smem_, st>>>(a);
+    note_launch();
 }
+
+int *MultifrontalPlan::error_word() const { return d_sync_ ? d_sync_ + (sync_ints_ - 1) : nullptr; }
 
 }  // namespace spx

@@ -33,10 +33,6 @@ struct MfLaunch {
     int64_t count;   // tasks
 };
 
-struct MfSolveLaunch {
-    int64_t off, count;
-};
-
 class MultifrontalPlan {
 public:
     MultifrontalPlan() = default;
@@ -61,6 +57,9 @@ public:
 
     void release(cudaStream_t st);
 
+    // device word set when a solve's dependency wait gave up (0 otherwise)
+    int *error_word() const;
+
     int64_t n() const { return n_; }
     double factor_flops() const { return flops_; }
     int64_t panel_entries() const { return g_total_; }
@@ -79,9 +78,19 @@ private:
     int32_t *d_atpos_ = nullptr;     // row position within the front
     int32_t *d_asrc_ = nullptr;      // index into the CSR values
     int4 *d_tasks_ = nullptr;
-    int4 *d_stasks_ = nullptr;       // solve tasks (s, chunk, 0, 0)
     std::vector<MfLaunch> launches_;
-    std::vector<MfSolveLaunch> fwd_, bwd_;
+    // solve: per-level task offsets (4 lists), tasks, gather lists
+    void *d_meta_ = nullptr;         // per-supernode solve metadata
+    void *d_stask_ = nullptr;        // solve task queue
+    int32_t *d_bundle_ = nullptr;
+    int32_t *d_cptr_ = nullptr, *d_cidx_ = nullptr, *d_chunks_ = nullptr;
+    double *d_fpart_ = nullptr, *d_bpart_ = nullptr;
+    int *d_cnt_ = nullptr, *d_sync_ = nullptr;
+    int32_t nfc_ = 0, nbc_ = 0;
+    int ntasks_ = 0;
+    size_t sync_ints_ = 0;
+    int solve_grid_ = 0;
+    size_t solve_smem_ = 0;
     // numeric
     double *d_front_ = nullptr;
     double *d_G_ = nullptr;
