@@ -380,7 +380,7 @@ constexpr int kSThreads = 256;
 constexpr int kSWarps = kSThreads / 32;
 constexpr int kST = 64;          // rows per forward task, columns per backward task
 constexpr int kStrip = 128;      // columns per forward task, rows per backward task
-constexpr int kWarpMaxC = 32;    // warp tasks: c <= 32 ...
+constexpr int kWarpMaxC = 16;    // warp tasks: c <= 16 ...
 constexpr int kWarpMaxR = 128;   // ... and r <= 128
 constexpr int kGW = 6;           // gather entries per row staged in shared memory
 constexpr int kTinyR = 24;       // thread tasks: leaves with r <= 24 ...
@@ -422,6 +422,13 @@ struct SolveArgs {
     double *out;
 };
 
+// relaxed-free publish: a release atomic orders every write that precedes it
+// in causality order -- the caller's own, and those of threads that reached a
+// block or warp barrier before it -- ahead of the increment
+SPX_DEV void add_release(int *p, int v) {
+    asm volatile("red.release.gpu.global.add.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 SPX_DEV int ld_acquire(const int *p) {
     int v;
     asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -459,17 +466,15 @@ SPX_DEV double sum_list(const SolveArgs &a, const int *idx, int n, int e0) {
 
 // true in every thread of the block that holds the chunk's last arrival
 SPX_DEV bool last_arrival(int *cnt, int n, int *flag) {
-    __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) {
-        const int old = atomicAdd(cnt, 1);
+        int old;
+        asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], 1;" : "=r"(old) : "l"(cnt) : "memory");
         *flag = (old == n - 1);
         if (*flag) *cnt = 0;          // every arrival for this solve is in
     }
     __syncthreads();
-    const bool last = *flag;
-    if (last) __threadfence();
-    return last;
+    return *flag;
 }
 
 // shared memory of one solve block.  gbuf holds one panel strip, staged by
@@ -491,6 +496,40 @@ struct WarpShared {           // per warp in a bundle: gather lists of <= 128 ro
     int idx[kWarpMaxR][kGW];
     int cnt[kWarpMaxR], e0[kWarpMaxR];
 };
+
+// Sum p[j] over the 32 lanes for every j < 16 at once: four exchange steps
+// (8 + 4 + 2 + 1 shuffles) leave lanes L and L ^ 16 each holding the half
+// sum for j = L & 15; one more exchange completes it.
+SPX_DEV double transpose_reduce16(double (&p)[16], int lane) {
+#pragma unroll
+    for (int m = 0; m < 8; m++) {
+        const bool hi = lane & 8;
+        const double send = hi ? p[m] : p[m + 8];
+        const double keep = hi ? p[m + 8] : p[m];
+        p[m] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+        const bool hi = lane & 4;
+        const double send = hi ? p[m] : p[m + 4];
+        const double keep = hi ? p[m + 4] : p[m];
+        p[m] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+    }
+#pragma unroll
+    for (int m = 0; m < 2; m++) {
+        const bool hi = lane & 2;
+        const double send = hi ? p[m] : p[m + 2];
+        const double keep = hi ? p[m + 2] : p[m];
+        p[m] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
+    }
+    {
+        const bool hi = lane & 1;
+        const double send = hi ? p[0] : p[1];
+        const double keep = hi ? p[1] : p[0];
+        p[0] = keep + __shfl_xor_sync(0xffffffffu, send, 1);
+    }
+    return p[0] + __shfl_xor_sync(0xffffffffu, p[0], 16);
+}
 
 // ---- bulk asynchronous copies into shared memory, tracked by an mbarrier
 SPX_DEV uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -561,8 +600,7 @@ SPX_DEV void fwd_thread(const SolveArgs &a, int s) {
             else a.u[m.uptr + (i - c)] = -acc;
         }
     }
-    __threadfence();
-    atomicAdd(parent >= 0 ? fcd + parent : fchk + s, 1);
+    add_release(parent >= 0 ? fcd + parent : fchk + s, 1);
 }
 
 // ---- backward, one tiny leaf supernode per thread
@@ -592,8 +630,7 @@ SPX_DEV void bwd_thread(const SolveArgs &a, int s) {
             a.out[a.perm[first + j]] = acc;
         }
     }
-    __threadfence();
-    atomicAdd(bdone + s, 1);
+    add_release(bdone + s, 1);
 }
 
 // ---- forward, one small supernode per warp.  Row i lives in lane i % 32
@@ -635,20 +672,13 @@ SPX_DEV void fwd_warp(const SolveArgs &a, int s, WarpShared &w) {
 #pragma unroll
         for (int j = 0; j < 8; j++) acc[0] += gt[j] * __shfl_sync(0xffffffffu, fj, j);
     } else {
-        for (int j0 = 0; j0 < c; j0 += 4) {
-            double gv[4][kWarpMaxR / 32];
 #pragma unroll
-            for (int jj = 0; jj < 4; jj++)
+        for (int j = 0; j < kWarpMaxC; j++) {
+            const double fb = __shfl_sync(0xffffffffu, fj, j);
 #pragma unroll
-                for (int q = 0; q < kWarpMaxR / 32; q++) {
-                    const int i = lane + 32 * q, j = j0 + jj;
-                    gv[jj][q] = (q < nq && i < r && j < c) ? Gs[(int64_t)i + (int64_t)j * ldg] : 0.0;
-                }
-#pragma unroll
-            for (int jj = 0; jj < 4; jj++) {
-                const double fb = __shfl_sync(0xffffffffu, fj, (j0 + jj) & 31);
-#pragma unroll
-                for (int q = 0; q < kWarpMaxR / 32; q++) acc[q] += gv[jj][q] * fb;
+            for (int q = 0; q < kWarpMaxR / 32; q++) {
+                const int i = lane + 32 * q;
+                if (j < c && q < nq && i < r) acc[q] += Gs[(int64_t)i + (int64_t)j * ldg] * fb;
             }
         }
     }
@@ -662,9 +692,8 @@ SPX_DEV void fwd_warp(const SolveArgs &a, int s, WarpShared &w) {
         else a.u[m.uptr + (i - c)] =
             (nchild > 0 ? sum_list(a, w.idx[i], w.cnt[i], w.e0[i]) : 0.0) - acc[q];
     }
-    __threadfence();
     __syncwarp();
-    if (lane == 0) atomicAdd(parent >= 0 ? fcd + parent : fchk + s, 1);
+    if (lane == 0) add_release(parent >= 0 ? fcd + parent : fchk + s, 1);
 }
 
 // ---- forward, rows [64 I, 64 I + 64) x a 128-column strip S of a large
@@ -730,11 +759,10 @@ SPX_DEV void fwd_tile(const SolveArgs &a, int s, int I, int S, int chunk, SolveS
             }
             if (ii < c) a.yf[first + ii] = rr;
             else a.u[m.uptr + (ii - c)] = sh.bsum[t] - rr;
-            __threadfence();
         }
         __syncthreads();
         // one completed row chunk: the parent counts every chunk of every child
-        if (t == 0) atomicAdd(parent >= 0 ? fcd + parent : fchk + s, 1);
+        if (t == 0) add_release(parent >= 0 ? fcd + parent : fchk + s, 1);
     }
     __syncthreads();
 }
@@ -773,39 +801,32 @@ SPX_DEV void bwd_warp(const SolveArgs &a, int s) {
         const int i = lane + 32 * q;
         v[q] = (i < r) ? ((i < c) ? __ldcg(a.yf + first + i) : -__ldcg(a.x + rv[q])) : 0.0;
     }
-    double mine = 0.0;
+    // every lane accumulates its rows' products for all 16 columns, then one
+    // transposing reduction leaves column j's sum in lanes j and j + 16
+    double p[kWarpMaxC];
+#pragma unroll
+    for (int j = 0; j < kWarpMaxC; j++) p[j] = 0.0;
     if (tiny) {
 #pragma unroll
-        for (int j = 0; j < 8; j++) {
-            const double p = warp_sum(gt[j] * v[0]);
-            if (lane == j) mine = p;
-        }
+        for (int j = 0; j < 8; j++) p[j] = gt[j] * v[0];
     } else {
-        for (int j0 = 0; j0 < c; j0 += 4) {
-            double p[4];
 #pragma unroll
-            for (int jj = 0; jj < 4; jj++) {
-                p[jj] = 0.0;
+        for (int q = 0; q < kWarpMaxR / 32; q++) {
+            const int i = lane + 32 * q;
+            if (q < nq && i < r) {
 #pragma unroll
-                for (int q = 0; q < kWarpMaxR / 32; q++) {
-                    const int i = lane + 32 * q, j = j0 + jj;
-                    if (q < nq && i < r && j < c) p[jj] += Gs[(int64_t)i + (int64_t)j * ldg] * v[q];
-                }
-            }
-#pragma unroll
-            for (int jj = 0; jj < 4; jj++) {
-                const double t = warp_sum(p[jj]);
-                if (lane == j0 + jj) mine = t;
+                for (int j = 0; j < kWarpMaxC; j++)
+                    if (j < c) p[j] += Gs[(int64_t)i + (int64_t)j * ldg] * v[q];
             }
         }
     }
+    const double mine = transpose_reduce16(p, lane);
     if (lane < c) {
         a.x[first + lane] = mine;
         a.out[pj] = mine;
     }
-    __threadfence();
     __syncwarp();
-    if (lane == 0) atomicAdd(bdone + s, 1);
+    if (lane == 0) add_release(bdone + s, 1);
 }
 
 // ---- backward, columns [64 J, 64 J + 64) x a 128-row strip S of a large
@@ -841,20 +862,50 @@ SPX_DEV void bwd_tile(const SolveArgs &a, int s, int J, int S, int chunk, SolveS
     __syncthreads();
     const int lane = t & 31, wid = t >> 5;
     const int nt = a.bc_n[chunk];
-    for (int k = 0; k < kST / kSWarps; k++) {
-        const int jj = wid + kSWarps * k;
-        double p = 0.0;
-        if (jj < jn) {
+    {
+        // warp wid owns columns wid + 8k, k < 8; lanes own rows lane + 32q
+        double p[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const int jj = wid + kSWarps * k;
+            double acc = 0.0;
 #pragma unroll
             for (int q = 0; q < kStrip / 32; q++) {
                 const int ii = lane + 32 * q;
-                if (ii < hcopy) p += sh.gbuf[jj * kStrip + ii] * sh.vec[ii];
+                if (jj < jn && ii < hcopy) acc += sh.gbuf[jj * kStrip + ii] * sh.vec[ii];
             }
+            p[k] = acc;
         }
-        p = warp_sum(p);
-        if (lane == 0) {
-            if (nt > 1) a.bpart[(int64_t)(a.bc_base[chunk] + (S - (j0 / kStrip))) * kST + jj] = p;
-            else sh.colsum[jj] = p;
+        // halve the 8 partial columns across lane bits 2, 1, 0, then finish
+        // the sums over lane bits 3 and 4: lane L ends with column k = L & 7
+#pragma unroll
+        for (int m = 0; m < 4; m++) {
+            const bool hi = lane & 4;
+            const double send = hi ? p[m] : p[m + 4];
+            const double keep = hi ? p[m + 4] : p[m];
+            p[m] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+        }
+#pragma unroll
+        for (int m = 0; m < 2; m++) {
+            const bool hi = lane & 2;
+            const double send = hi ? p[m] : p[m + 2];
+            const double keep = hi ? p[m + 2] : p[m];
+            p[m] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
+        }
+        {
+            const bool hi = lane & 1;
+            const double send = hi ? p[0] : p[1];
+            const double keep = hi ? p[1] : p[0];
+            p[0] = keep + __shfl_xor_sync(0xffffffffu, send, 1);
+        }
+        double col = p[0] + __shfl_xor_sync(0xffffffffu, p[0], 8);
+        col += __shfl_xor_sync(0xffffffffu, col, 16);
+        if (lane < 8) {
+            const int jj = wid + kSWarps * lane;
+            if (jj < jn) {
+                if (nt > 1) a.bpart[(int64_t)(a.bc_base[chunk] + (S - (j0 / kStrip))) * kST + jj] = col;
+                else sh.colsum[jj] = col;
+            }
         }
     }
     if (nt == 1) __syncthreads();
@@ -870,11 +921,10 @@ SPX_DEV void bwd_tile(const SolveArgs &a, int s, int J, int S, int chunk, SolveS
             }
             a.x[first + j0 + jj] = rr;
             a.out[sh.permv[jj]] = rr;
-            __threadfence();
         }
         __syncthreads();
         // one completed column chunk: the children count every chunk
-        if (t == 0) atomicAdd(bdone + s, 1);
+        if (t == 0) add_release(bdone + s, 1);
     }
     __syncthreads();
 }
