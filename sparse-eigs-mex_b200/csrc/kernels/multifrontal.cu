@@ -86,10 +86,11 @@ SPX_DEV int lower_bound_i32(const int32_t *a, int n, int key) {
 __global__ void __launch_bounds__(kFThreads)
 mf_assemble(const int4 *__restrict__ tasks, Sym y, double *__restrict__ F,
             const int32_t *__restrict__ acolptr, const int32_t *__restrict__ atpos,
-            const int32_t *__restrict__ asrc, const double *__restrict__ val, double shift,
-            const int *status) {
+            const int32_t *__restrict__ asrc, const double *__restrict__ val,
+            const double *__restrict__ params, const int *status) {
     __shared__ double S[T][T + 1];
     if (*(volatile const int *)status) return;
+    const double shift = params[0];
     const int4 tk = tasks[blockIdx.x];
     const int s = tk.x, I = tk.y, J = tk.z;
     const Front f = front_of(y, s);
@@ -137,65 +138,156 @@ mf_assemble(const int4 *__restrict__ tasks, Sym y, double *__restrict__ F,
     }
 }
 
+// ------------------------------------------------------ warp Cholesky --
+// Shared by the diagonal-tile POTRF and the tiny-front kernel: one warp,
+// lane i owns row i of M (n <= 32 rows in shared memory).  The scaled column
+// j is published in its own array `col`, so the rank-1 updates read it
+// without aliasing the rows being updated.  Factors the first c columns of
+// the n x n lower matrix M in place (rows >= c receive L21 and the Schur
+// complement) and sets dinv[j] = 1 / L(j, j); a pivot <= pivtol records its
+// column in *status and is replaced by 1 so the sweep stays finite.
+SPX_DEV void warp_cholesky(double (*M)[T + 1], double *col, double *dinv, int n, int c,
+                           double pivtol, int *status, int colbase) {
+    const int lane = threadIdx.x & 31;
+    for (int j = 0; j < c; j++) {
+        if (lane == j) {
+            double d = M[j][j];
+            if (!(d > pivtol)) {
+                atomicCAS(status, 0, colbase + j + 1);
+                d = 1.0;
+            }
+            d = sqrt(d);
+            M[j][j] = d;
+            dinv[j] = 1.0 / d;
+        }
+        __syncwarp();
+        double lij = 0.0;
+        if (lane > j && lane < n) {
+            lij = M[lane][j] * dinv[j];
+            M[lane][j] = lij;
+            col[lane] = lij;
+        }
+        __syncwarp();
+        if (lane > j && lane < n)
+            for (int k = j + 1; k <= lane; k++) M[lane][k] -= lij * col[k];
+        __syncwarp();
+    }
+}
+
+// X = inv(L11) for the leading c x c block of M, kept in M's strictly upper
+// part: X(i, j) for i > j sits at M[j][i] (lane j computes column j), and
+// X(j, j) = dinv[j].  The lower part (L) is left as it is.
+SPX_DEV void warp_tri_inverse(double (*M)[T + 1], const double *dinv, int c) {
+    const int j = threadIdx.x & 31;
+    if (j < c) {
+        for (int i = j + 1; i < c; i++) {
+            double acc = M[i][j] * dinv[j];
+            for (int t2 = j + 1; t2 < i; t2++) acc += M[i][t2] * M[j][t2];
+            M[j][i] = -acc * dinv[i];
+        }
+    }
+    __syncwarp();
+}
+
 // --------------------------------------------------------------- potrf --
-__global__ void __launch_bounds__(kFThreads)
-mf_potrf(const int4 *__restrict__ tasks, Sym y, double *__restrict__ F, double *__restrict__ G,
-         double pivtol, int *status) {
-    __shared__ double L[T][T + 1];
-    __shared__ double X[T][T + 1];
+// One warp factors one 32 x 32 diagonal tile and writes its inverse into G.
+constexpr int kPotrfWarps = 4;
+
+__global__ void __launch_bounds__(32 * kPotrfWarps)
+mf_potrf(const int4 *__restrict__ tasks, int ntasks, Sym y, double *__restrict__ F,
+         double *__restrict__ G, const double *__restrict__ params, int *status) {
+    __shared__ double Ms[kPotrfWarps][T][T + 1];
+    __shared__ double cols[kPotrfWarps][T], dinvs[kPotrfWarps][T];
     if (*(volatile int *)status) return;
-    const int4 tk = tasks[blockIdx.x];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int task = blockIdx.x * kPotrfWarps + wid;
+    if (task >= ntasks) return;
+    const int4 tk = tasks[task];
     const int s = tk.x, kb = tk.w;
     const Front f = front_of(y, s);
     int a, b;
     tile_range(f, kb, a, b);
     const int w = b - a;
     double *Fs = F + f.fptr;
-    for (int t = threadIdx.x; t < T * T; t += blockDim.x) {
-        const int i = t & (T - 1), j = t >> 5;
-        L[i][j] = (i < w && j < w && j <= i) ? Fs[(int64_t)(a + i) + (int64_t)(a + j) * f.r] : 0.0;
-        X[i][j] = 0.0;
-    }
-    __syncthreads();
-    for (int j = 0; j < w; j++) {
-        if (threadIdx.x == 0) {
-            double d = L[j][j];
-            if (!(d > pivtol)) {
-                atomicCAS(status, 0, f.first + a + j + 1);
-                d = 1.0;
-            }
-            L[j][j] = sqrt(d);
-        }
-        __syncthreads();
-        const double djj = L[j][j];
-        if ((int)threadIdx.x > j && (int)threadIdx.x < w) L[threadIdx.x][j] /= djj;
-        __syncthreads();
-        const int m = w - j - 1;
-        for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
-            const int i = j + 1 + t % m, k = j + 1 + t / m;
-            if (k <= i) L[i][k] -= L[i][j] * L[k][j];
-        }
-        __syncthreads();
-    }
-    for (int t = threadIdx.x; t < T * T; t += blockDim.x) {
-        const int i = t & (T - 1), j = t >> 5;
-        if (i < w && j < w && j <= i) Fs[(int64_t)(a + i) + (int64_t)(a + j) * f.r] = L[i][j];
-    }
-    // X = inv(L): column j by thread j
-    if ((int)threadIdx.x < w) {
-        const int j = threadIdx.x;
-        X[j][j] = 1.0 / L[j][j];
-        for (int i = j + 1; i < w; i++) {
-            double acc = 0.0;
-            for (int t = j; t < i; t++) acc += L[i][t] * X[t][j];
-            X[i][j] = -acc / L[i][i];
-        }
-    }
-    __syncthreads();
+    double (*M)[T + 1] = Ms[wid];
+    // lanes walk a column (coalesced): M[i][j] = F(a+i, a+j), lower part
+    for (int j = 0; j < T; j++)
+        M[lane][j] = (lane < w && j < w && j <= lane) ? Fs[(int64_t)(a + lane) + (int64_t)(a + j) * f.r]
+                                                      : 0.0;
+    __syncwarp();
+    warp_cholesky(M, cols[wid], dinvs[wid], w, w, params[1], status, f.first + a);
+    for (int j = 0; j < w; j++)
+        if (lane < w && j <= lane) Fs[(int64_t)(a + lane) + (int64_t)(a + j) * f.r] = M[lane][j];
+    warp_tri_inverse(M, dinvs[wid], w);
     double *Gs = G + f.gptr;
-    for (int t = threadIdx.x; t < T * T; t += blockDim.x) {
-        const int i = t & (T - 1), j = t >> 5;
-        if (i < w && j < w && j <= i) Gs[(int64_t)(a + i) + (int64_t)(a + j) * f.ldg] = X[i][j];
+    for (int j = 0; j < w; j++)
+        if (lane < w && lane >= j)
+            Gs[(int64_t)(a + lane) + (int64_t)(a + j) * f.ldg] = lane == j ? dinvs[wid][j] : M[j][lane];
+}
+
+// ---------------------------------------------------------- tiny front --
+// A front with at most 32 rows is done by one warp end to end: assembly
+// (children's update matrices, then A and the shift), partial Cholesky of its
+// c pivots with the Schur complement left in the rows below, the update
+// matrix written back for the parent, then X = inv(L11) and W = L21 X into G.
+constexpr int kTinyWarps = 4;
+
+__global__ void __launch_bounds__(32 * kTinyWarps)
+mf_tiny_front(const int4 *__restrict__ tasks, int ntasks, Sym y, double *__restrict__ F,
+              double *__restrict__ G, const int32_t *__restrict__ acolptr,
+              const int32_t *__restrict__ atpos, const int32_t *__restrict__ asrc,
+              const double *__restrict__ val, const double *__restrict__ params, int *status) {
+    __shared__ double Ms[kTinyWarps][T][T + 1];
+    __shared__ double cols[kTinyWarps][T], dinvs[kTinyWarps][T];
+    if (*(volatile int *)status) return;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int task = blockIdx.x * kTinyWarps + wid;
+    if (task >= ntasks) return;
+    const double shift = params[0];
+    const int s = tasks[task].x;
+    const Front f = front_of(y, s);
+    const int r = f.r, c = f.c;
+    double (*M)[T + 1] = Ms[wid];
+    for (int k = 0; k < T; k++) M[lane][k] = 0.0;
+    __syncwarp();
+    for (int q = y.child_ptr[s]; q < y.child_ptr[s + 1]; q++) {
+        const int ch = y.child_list[q];
+        const int rch = (int)(y.rowptr[ch + 1] - y.rowptr[ch]);
+        const int cch = y.sfirst[ch + 1] - y.sfirst[ch];
+        const int nb = rch - cch;
+        const int32_t *rm = y.relmap + y.rowptr[ch] + cch;
+        const double *U = F + y.frontptr[ch];
+        for (int e = lane; e < nb * nb; e += 32) {
+            const int a2 = e % nb, b2 = e / nb;
+            if (a2 >= b2) M[rm[a2]][rm[b2]] += U[(int64_t)(cch + a2) + (int64_t)(cch + b2) * rch];
+        }
+        __syncwarp();
+    }
+    if (lane < c) {
+        const int col = f.first + lane;
+        for (int e = acolptr[col]; e < acolptr[col + 1]; e++) M[atpos[e]][lane] += val[asrc[e]];
+        M[lane][lane] += shift;
+    }
+    __syncwarp();
+    warp_cholesky(M, cols[wid], dinvs[wid], r, c, params[1], status, f.first);
+    // update matrix (rows and columns c..r-1) for the parent's assembly
+    double *Fs = F + f.fptr;
+    if (lane >= c && lane < r)
+        for (int k = c; k <= lane; k++) Fs[(int64_t)lane + (int64_t)k * r] = M[lane][k];
+    const double *dinv = dinvs[wid];
+    warp_tri_inverse(M, dinv, c);
+    double *Gs = G + f.gptr;
+    if (lane < c) {
+        Gs[(int64_t)lane + (int64_t)lane * f.ldg] = dinv[lane];
+        for (int i = lane + 1; i < c; i++) Gs[(int64_t)i + (int64_t)lane * f.ldg] = M[lane][i];
+    }
+    // W = L21 X: lane i >= c owns row i
+    if (lane >= c && lane < r) {
+        for (int j = 0; j < c; j++) {
+            double acc = M[lane][j] * dinv[j];
+            for (int t2 = j + 1; t2 < c; t2++) acc += M[lane][t2] * M[j][t2];
+            Gs[(int64_t)lane + (int64_t)j * f.ldg] = acc;
+        }
     }
 }
 
@@ -277,24 +369,30 @@ mf_update(const int4 *__restrict__ tasks, Sym y, double *__restrict__ F, const i
     }
 }
 
-// X_ib,jb = -X_ib,ib * sum_{k=jb}^{ib-1} L_ib,k X_k,jb
+// inv(L11) by recursive doubling over tile blocks.  After step l every
+// diagonal block of 2^l tiles is inverted; step l joins blocks A = [A0, C0)
+// and C = [C0, C1) (C0 = A0 + 2^l) through
+//   T = L_CA X_A          (mf_inv_t: T lands in the unused upper part of F)
+//   X_CA = -X_C T         (mf_inv_x)
+// task = (s, i, j, l): output tile (i, j), i in C, j in A.
 __global__ void __launch_bounds__(kFThreads)
-mf_invert(const int4 *__restrict__ tasks, Sym y, const double *__restrict__ F,
-          double *__restrict__ G, const int *status) {
+mf_inv_t(const int4 *__restrict__ tasks, Sym y, double *__restrict__ F,
+         const double *__restrict__ G, const int *status) {
     __shared__ double A[T][T + 1];
     __shared__ double B[T][T + 1];
     if (*(volatile const int *)status) return;
     const int4 tk = tasks[blockIdx.x];
-    const int s = tk.x, ib = tk.y, jb = tk.z;
+    const int s = tk.x, i = tk.y, j = tk.z, l = tk.w;
     const Front f = front_of(y, s);
+    const int C0 = (j >> (l + 1) << (l + 1)) + (1 << l);
     int ra, rb, ca, cb;
-    tile_range(f, ib, ra, rb);
-    tile_range(f, jb, ca, cb);
+    tile_range(f, i, ra, rb);
+    tile_range(f, j, ca, cb);
     const int h = rb - ra, w = cb - ca;
-    const double *Fs = F + f.fptr;
-    double *Gs = G + f.gptr;
+    double *Fs = F + f.fptr;
+    const double *Gs = G + f.gptr;
     double acc[4] = {0, 0, 0, 0};
-    for (int k = jb; k < ib; k++) {
+    for (int k = j; k < C0; k++) {
         int ka, kbb;
         tile_range(f, k, ka, kbb);
         const int kw = kbb - ka;
@@ -304,17 +402,51 @@ mf_invert(const int4 *__restrict__ tasks, Sym y, const double *__restrict__ F,
         mm_ab(acc, A, B, kw);
         __syncthreads();
     }
+    // T_ij is kept at tile (j, i) of F: strictly upper, never used otherwise
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
 #pragma unroll
-    for (int q = 0; q < 4; q++) B[tx][ty + 8 * q] = acc[q];
-    load_tile(A, Gs, f.ldg, ra, h, ra, h);   // X_ib,ib
-    __syncthreads();
-    double out[4] = {0, 0, 0, 0};
-    mm_ab(out, A, B, h);
+    for (int q = 0; q < 4; q++) {
+        const int jj = ty + 8 * q;
+        if (tx < h && jj < w) Fs[(int64_t)(ca + jj) + (int64_t)(ra + tx) * f.r] = acc[q];
+    }
+}
+
+__global__ void __launch_bounds__(kFThreads)
+mf_inv_x(const int4 *__restrict__ tasks, Sym y, const double *__restrict__ F,
+         double *__restrict__ G, const int *status) {
+    __shared__ double A[T][T + 1];
+    __shared__ double B[T][T + 1];
+    if (*(volatile const int *)status) return;
+    const int4 tk = tasks[blockIdx.x];
+    const int s = tk.x, i = tk.y, j = tk.z, l = tk.w;
+    const Front f = front_of(y, s);
+    const int C0 = (j >> (l + 1) << (l + 1)) + (1 << l);
+    int ra, rb, ca, cb;
+    tile_range(f, i, ra, rb);
+    tile_range(f, j, ca, cb);
+    const int h = rb - ra, w = cb - ca;
+    const double *Fs = F + f.fptr;
+    double *Gs = G + f.gptr;
+    double acc[4] = {0, 0, 0, 0};
+    for (int k = C0; k <= i; k++) {
+        int ka, kbb;
+        tile_range(f, k, ka, kbb);
+        const int kw = kbb - ka;
+        load_tile(A, Gs, f.ldg, ra, h, ka, kw);          // X_ik
+        // T_kj, stored transposed at tile (j, k) of F
+        for (int t2 = threadIdx.x; t2 < T * T; t2 += blockDim.x) {
+            const int r2 = t2 & (T - 1), c2 = t2 >> 5;   // B[r2][c2] = T_kj(r2, c2)
+            B[r2][c2] = (r2 < kw && c2 < w) ? Fs[(int64_t)(ca + c2) + (int64_t)(ka + r2) * f.r] : 0.0;
+        }
+        __syncthreads();
+        mm_ab(acc, A, B, kw);
+        __syncthreads();
+    }
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
 #pragma unroll
     for (int q = 0; q < 4; q++) {
-        const int j = ty + 8 * q;
-        if (tx < h && j < w) Gs[(int64_t)(ra + tx) + (int64_t)(ca + j) * f.ldg] = -out[q];
+        const int jj = ty + 8 * q;
+        if (tx < h && jj < w) Gs[(int64_t)(ra + tx) + (int64_t)(ca + jj) * f.ldg] = -acc[q];
     }
 }
 
@@ -1018,6 +1150,9 @@ static int dupload(Tp **p, const Tp *h, size_t cnt, cudaStream_t st) {
 MultifrontalPlan::~MultifrontalPlan() { release(0); }
 
 void MultifrontalPlan::release(cudaStream_t st) {
+    if (fgraph_) { cudaGraphExecDestroy(fgraph_); fgraph_ = nullptr; }
+    fgraph_val_ = nullptr;
+    if (d_params_) { cudaFreeAsync(d_params_, st); d_params_ = nullptr; }
     void *ptrs[] = {d_perm_, d_sfirst_, d_rows_, d_relmap_, d_child_ptr_, d_child_list_,
                     d_rowptr_, d_frontptr_, d_gptr_, d_uptr_, d_acolptr_, d_atpos_, d_asrc_,
                     d_tasks_, d_front_, d_G_, d_u_, d_yf_, d_x_, d_status_, d_meta_,
@@ -1099,12 +1234,20 @@ int MultifrontalPlan::init(const spx_symbolic &S, const int64_t *rowptr, const i
             if (tasks.size() > before)
                 launches_.push_back({kind, (int64_t)before, (int64_t)(tasks.size() - before)});
         };
+        auto is_tiny = [&](int s) { return S.rowptr[s + 1] - S.rowptr[s] <= T; };
         for (int l = 0; l < S.nlevels; l++) {
             const int32_t q0 = S.level_ptr[l], q1 = S.level_ptr[l + 1];
             int nkbmax = 0;
+            {
+                size_t bt = tasks.size();
+                for (int32_t q = q0; q < q1; q++)
+                    if (is_tiny(S.level_sup[q])) tasks.push_back(make_int4(S.level_sup[q], 0, 0, 0));
+                emit(MF_TINY, bt);
+            }
             size_t b = tasks.size();
             for (int32_t q = q0; q < q1; q++) {
                 const int s = S.level_sup[q];
+                if (is_tiny(s)) continue;
                 const int r = (int)(S.rowptr[s + 1] - S.rowptr[s]);
                 const int c = S.sfirst[s + 1] - S.sfirst[s];
                 const int nkb = (c + T - 1) / T, nt = nkb + (r - c + T - 1) / T;
@@ -1117,6 +1260,7 @@ int MultifrontalPlan::init(const spx_symbolic &S, const int64_t *rowptr, const i
                 size_t b0 = tasks.size();
                 for (int32_t q = q0; q < q1; q++) {
                     const int s = S.level_sup[q];
+                    if (is_tiny(s)) continue;
                     const int c = S.sfirst[s + 1] - S.sfirst[s];
                     if ((c + T - 1) / T > kb) tasks.push_back(make_int4(s, kb, kb, kb));
                 }
@@ -1126,6 +1270,7 @@ int MultifrontalPlan::init(const spx_symbolic &S, const int64_t *rowptr, const i
                     const int s = S.level_sup[q];
                     const int r = (int)(S.rowptr[s + 1] - S.rowptr[s]);
                     const int c = S.sfirst[s + 1] - S.sfirst[s];
+                    if (is_tiny(s)) continue;
                     const int nkb = (c + T - 1) / T, nt = nkb + (r - c + T - 1) / T;
                     if (nkb <= kb) continue;
                     for (int I = kb + 1; I < nt; I++) tasks.push_back(make_int4(s, I, kb, kb));
@@ -1136,6 +1281,7 @@ int MultifrontalPlan::init(const spx_symbolic &S, const int64_t *rowptr, const i
                     const int s = S.level_sup[q];
                     const int r = (int)(S.rowptr[s + 1] - S.rowptr[s]);
                     const int c = S.sfirst[s + 1] - S.sfirst[s];
+                    if (is_tiny(s)) continue;
                     const int nkb = (c + T - 1) / T, nt = nkb + (r - c + T - 1) / T;
                     if (nkb <= kb) continue;
                     for (int I = kb + 1; I < nt; I++)
@@ -1143,21 +1289,30 @@ int MultifrontalPlan::init(const spx_symbolic &S, const int64_t *rowptr, const i
                 }
                 emit(MF_UPDATE, b2);
             }
-            for (int ib = 1; ib < nkbmax; ib++) {
-                size_t b0 = tasks.size();
-                for (int32_t q = q0; q < q1; q++) {
-                    const int s = S.level_sup[q];
-                    const int c = S.sfirst[s + 1] - S.sfirst[s];
-                    if ((c + T - 1) / T <= ib) continue;
-                    for (int jb = 0; jb < ib; jb++) tasks.push_back(make_int4(s, ib, jb, 0));
+            for (int l = 0; (1 << l) < nkbmax; l++) {
+                const int half = 1 << l;
+                for (int phase = 0; phase < 2; phase++) {
+                    size_t b0 = tasks.size();
+                    for (int32_t q = q0; q < q1; q++) {
+                        const int s = S.level_sup[q];
+                        if (is_tiny(s)) continue;
+                        const int c = S.sfirst[s + 1] - S.sfirst[s];
+                        const int nkb = (c + T - 1) / T;
+                        for (int A0 = 0; A0 + half < nkb; A0 += 2 * half) {
+                            const int C0 = A0 + half, C1 = std::min(A0 + 2 * half, nkb);
+                            for (int i = C0; i < C1; i++)
+                                for (int j = A0; j < C0; j++) tasks.push_back(make_int4(s, i, j, l));
+                        }
+                    }
+                    emit(phase == 0 ? MF_INV_T : MF_INV_X, b0);
                 }
-                emit(MF_INVERT, b0);
             }
             size_t bw = tasks.size();
             for (int32_t q = q0; q < q1; q++) {
                 const int s = S.level_sup[q];
                 const int r = (int)(S.rowptr[s + 1] - S.rowptr[s]);
                 const int c = S.sfirst[s + 1] - S.sfirst[s];
+                if (is_tiny(s)) continue;
                 const int nkb = (c + T - 1) / T, nt = nkb + (r - c + T - 1) / T;
                 for (int I = nkb; I < nt; I++)
                     for (int J = 0; J < nkb; J++) tasks.push_back(make_int4(s, I, J, 0));
@@ -1368,45 +1523,76 @@ int MultifrontalPlan::init(const spx_symbolic &S, const int64_t *rowptr, const i
     return 0;
 }
 
-int MultifrontalPlan::factorize(const double *d_val, double shift, double pivtol,
-                                cudaStream_t st) {
-    if (!d_front_) {
-        if (dmalloc(&d_front_, (size_t)front_total_, st)) return SPEIGS_ERR_MEM;
-    }
+void MultifrontalPlan::launch_factor(const double *d_val, cudaStream_t st) {
     Sym y{d_sfirst_, d_rows_, d_relmap_, d_child_ptr_, d_child_list_, d_rowptr_, d_frontptr_, d_gptr_};
-    // (G's strictly upper pivot part is never written or read)
-    cudaMemsetAsync(d_status_, 0, sizeof(int), st);
     for (const MfLaunch &L : launches_) {
         const int4 *tk = d_tasks_ + L.off;
         const unsigned nb = (unsigned)L.count;
         switch (L.kind) {
             case MF_ASSEMBLE:
                 mf_assemble<<<nb, kFThreads, 0, st>>>(tk, y, d_front_, d_acolptr_, d_atpos_,
-                                                      d_asrc_, d_val, shift, d_status_);
-                note_launch();
+                                                      d_asrc_, d_val, d_params_, d_status_);
+                break;
+            case MF_TINY:
+                mf_tiny_front<<<(nb + kTinyWarps - 1) / kTinyWarps, 32 * kTinyWarps, 0, st>>>(
+                    tk, (int)nb, y, d_front_, d_G_, d_acolptr_, d_atpos_, d_asrc_, d_val, d_params_,
+                    d_status_);
                 break;
             case MF_POTRF:
-                mf_potrf<<<nb, kFThreads, 0, st>>>(tk, y, d_front_, d_G_, pivtol, d_status_);
-                note_launch();
+                mf_potrf<<<(nb + kPotrfWarps - 1) / kPotrfWarps, 32 * kPotrfWarps, 0, st>>>(
+                    tk, (int)nb, y, d_front_, d_G_, d_params_, d_status_);
                 break;
             case MF_TRSM:
                 mf_trsm<<<nb, kFThreads, 0, st>>>(tk, y, d_front_, d_G_, d_status_);
-                note_launch();
                 break;
             case MF_UPDATE:
                 mf_update<<<nb, kFThreads, 0, st>>>(tk, y, d_front_, d_status_);
-                note_launch();
                 break;
-            case MF_INVERT:
-                mf_invert<<<nb, kFThreads, 0, st>>>(tk, y, d_front_, d_G_, d_status_);
-                note_launch();
+            case MF_INV_T:
+                mf_inv_t<<<nb, kFThreads, 0, st>>>(tk, y, d_front_, d_G_, d_status_);
+                break;
+            case MF_INV_X:
+                mf_inv_x<<<nb, kFThreads, 0, st>>>(tk, y, d_front_, d_G_, d_status_);
                 break;
             case MF_WMUL:
                 mf_wmul<<<nb, kFThreads, 0, st>>>(tk, y, d_front_, d_G_, d_status_);
-                note_launch();
                 break;
         }
     }
+}
+
+// The launch sequence is fixed by the symbolic analysis, so it is captured
+// once into a CUDA graph and replayed; the shift and the pivot tolerance are
+// read from device memory by the kernels.
+int MultifrontalPlan::factorize(const double *d_val, double shift, double pivtol,
+                                cudaStream_t st) {
+    if (!d_front_) {
+        if (dmalloc(&d_front_, (size_t)front_total_, st)) return SPEIGS_ERR_MEM;
+    }
+    if (!d_params_) {
+        if (dmalloc(&d_params_, 2, st)) return SPEIGS_ERR_MEM;
+    }
+    const double hp[2] = {shift, pivtol};
+    cudaMemcpyAsync(d_params_, hp, sizeof hp, cudaMemcpyHostToDevice, st);
+    note_h2d(sizeof hp);
+    cudaMemsetAsync(d_status_, 0, sizeof(int), st);
+    if (!fgraph_ || fgraph_val_ != d_val) {
+        if (fgraph_) { cudaGraphExecDestroy(fgraph_); fgraph_ = nullptr; }
+        cudaGraph_t g = nullptr;
+        if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+            return SPEIGS_ERR_INTERNAL;
+        launch_factor(d_val, st);
+        if (cudaStreamEndCapture(st, &g) != cudaSuccess || !g) {
+            cudaGetLastError();
+            return SPEIGS_ERR_INTERNAL;
+        }
+        cudaError_t e = cudaGraphInstantiate(&fgraph_, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) { cudaGetLastError(); fgraph_ = nullptr; return SPEIGS_ERR_INTERNAL; }
+        fgraph_val_ = d_val;
+    }
+    if (cudaGraphLaunch(fgraph_, st) != cudaSuccess) { cudaGetLastError(); return SPEIGS_ERR_INTERNAL; }
+    note_launch((long long)launches_.size());
     int h_status = 0;
     cudaMemcpyAsync(&h_status, d_status_, sizeof(int), cudaMemcpyDeviceToHost, st);
     note_d2h(sizeof(int));

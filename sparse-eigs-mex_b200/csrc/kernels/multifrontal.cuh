@@ -25,7 +25,8 @@ namespace spx {
 
 constexpr int kTile = 32;
 
-enum MfTaskKind { MF_ASSEMBLE = 0, MF_POTRF, MF_TRSM, MF_UPDATE, MF_INVERT, MF_WMUL, MF_NKIND };
+enum MfTaskKind { MF_ASSEMBLE = 0, MF_POTRF, MF_TRSM, MF_UPDATE, MF_INV_T, MF_INV_X, MF_WMUL,
+                  MF_TINY, MF_NKIND };
 
 struct MfLaunch {
     int     kind;
@@ -67,6 +68,7 @@ public:
     int levels() const { return nlevels_; }
 
 private:
+    void launch_factor(const double *d_val, cudaStream_t st);
     int32_t n_ = 0, ns_ = 0, nlevels_ = 0;
     double flops_ = 0.0;
     int64_t front_total_ = 0, g_total_ = 0, u_total_ = 0, nrows_total_ = 0;
@@ -96,6 +98,9 @@ private:
     double *d_G_ = nullptr;
     double *d_u_ = nullptr, *d_yf_ = nullptr, *d_x_ = nullptr;
     int *d_status_ = nullptr;
+    double *d_params_ = nullptr;     // shift, pivot tolerance (read by the graph)
+    cudaGraphExec_t fgraph_ = nullptr;
+    const double *fgraph_val_ = nullptr;
     int max_rows_ = 0;
 };
 
