@@ -8,9 +8,11 @@
 #include "symbolic.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cstdlib>
 #include <cstring>
 #include <new>
+#include <thread>
 #include <vector>
 
 namespace {
@@ -61,20 +63,27 @@ void leaf_mindeg(const Graph &g, const std::vector<int32_t> &verts,
     for (int a = 0; a < m; a++) local[verts[a]] = -1;
 }
 
+// Regions are ordered recursively; the two halves of a split touch disjoint
+// vertex sets (a separator leaves no edge between them), so large halves are
+// ordered on separate threads.  The per-vertex arrays are shared: a region
+// only writes the entries of its own vertices and reads those of its
+// neighbours, which lie in the region itself or in separators that are
+// already final.
 struct NDState {
     const Graph &g;
     std::vector<int32_t> part;   // region id of every vertex
     std::vector<int32_t> level;  // BFS level scratch
-    std::vector<int32_t> queue;
     std::vector<int32_t> local;  // leaf-local index scratch
-    int32_t next_id = 1;
+    std::atomic<int32_t> next_id{1};
+    std::atomic<int> spare_threads{0};
     int32_t *perm;
     explicit NDState(const Graph &gg, int32_t *p)
-        : g(gg), part(gg.n, 0), level(gg.n, -1), queue(gg.n), local(gg.n, -1), perm(p) {}
+        : g(gg), part(gg.n, 0), level(gg.n, -1), local(gg.n, -1), perm(p) {}
 
     // BFS inside region `id` from `src`; fills queue[0..cnt), level[]; returns
-    // the number reached and the eccentricity in *depth.
-    int32_t bfs(int32_t id, int32_t src, int32_t *depth) {
+    // the number reached and the eccentricity in *depth.  `queue` holds at
+    // least as many entries as the region has vertices.
+    int32_t bfs(int32_t id, int32_t src, int32_t *depth, std::vector<int32_t> &queue) {
         int32_t head = 0, tail = 0;
         queue[tail++] = src;
         level[src] = 0;
@@ -94,7 +103,7 @@ struct NDState {
         *depth = d;
         return tail;
     }
-    void clear_levels(int32_t cnt) {
+    void clear_levels(const std::vector<int32_t> &queue, int32_t cnt) {
         for (int32_t i = 0; i < cnt; i++) level[queue[i]] = -1;
     }
     int32_t degree_in(int32_t v, int32_t id) const {
@@ -113,26 +122,27 @@ struct NDState {
             leaf_mindeg(g, verts, local, perm + lo);
             return;
         }
+        std::vector<int32_t> queue(m);
         // pseudo-peripheral start: lowest degree vertex, then repeated BFS
         int32_t src = verts[0], bestdeg = degree_in(verts[0], id);
         for (int32_t v : verts) {
             int32_t d = degree_in(v, id);
             if (d < bestdeg) { bestdeg = d; src = v; }
         }
-        int32_t depth = 0, cnt = bfs(id, src, &depth);
+        int32_t depth = 0, cnt = bfs(id, src, &depth, queue);
         if (cnt < m) {
             // disconnected region: order each connected piece on its own
             std::vector<std::vector<int32_t>> pieces;
             std::vector<int32_t> ids;
             pieces.emplace_back(queue.begin(), queue.begin() + cnt);
-            clear_levels(cnt);
+            clear_levels(queue, cnt);
             ids.push_back(next_id++);
             for (int32_t v : pieces[0]) part[v] = ids[0];
             for (int32_t v : verts) {
                 if (part[v] != id) continue;
-                int32_t d2 = 0, c2 = bfs(id, v, &d2);
+                int32_t d2 = 0, c2 = bfs(id, v, &d2, queue);
                 pieces.emplace_back(queue.begin(), queue.begin() + c2);
-                clear_levels(c2);
+                clear_levels(queue, c2);
                 ids.push_back(next_id++);
                 for (int32_t u : pieces.back()) part[u] = ids.back();
             }
@@ -153,13 +163,13 @@ struct NDState {
                 int32_t d = degree_in(queue[i], id);
                 if (d < cd) { cd = d; cand = queue[i]; }
             }
-            clear_levels(cnt);
+            clear_levels(queue, cnt);
             int32_t d2 = 0;
-            bfs(id, cand, &d2);
+            bfs(id, cand, &d2, queue);
             if (d2 <= depth) {
                 // no improvement: redo the BFS from src to keep its levels
-                clear_levels(cnt);
-                bfs(id, src, &depth);
+                clear_levels(queue, cnt);
+                bfs(id, src, &depth, queue);
                 break;
             }
             src = cand;
@@ -168,7 +178,7 @@ struct NDState {
         if (depth < 2) {
             // too shallow to split (clique-like): order by degree, low first
             std::vector<int32_t> vv(queue.begin(), queue.begin() + cnt);
-            clear_levels(cnt);
+            clear_levels(queue, cnt);
             std::stable_sort(vv.begin(), vv.end(), [&](int32_t a, int32_t b) {
                 return degree_in(a, id) < degree_in(b, id);
             });
@@ -204,7 +214,7 @@ struct NDState {
             else if (l > best) { part[v] = idb; }
             else { part[v] = ids; }
         }
-        clear_levels(cnt);
+        clear_levels(queue, cnt);
         // thin the separator: a separator vertex with no neighbour on one side
         // can join the other side.
         for (int32_t v : verts) {
@@ -232,9 +242,20 @@ struct NDState {
         }
         verts.clear();
         verts.shrink_to_fit();
-        order_region(std::move(A), ida, lo);
-        order_region(std::move(B), idb, lo + na);
+        queue.clear();
+        queue.shrink_to_fit();
+        if (na > kParallelMin && nb > kParallelMin && spare_threads.fetch_sub(1) > 0) {
+            std::thread t([this, &A, ida, lo] { order_region(std::move(A), ida, lo); });
+            order_region(std::move(B), idb, lo + na);
+            t.join();
+            spare_threads.fetch_add(1);
+        } else {
+            if (na > kParallelMin && nb > kParallelMin) spare_threads.fetch_add(1);
+            order_region(std::move(A), ida, lo);
+            order_region(std::move(B), idb, lo + na);
+        }
     }
+    static constexpr int32_t kParallelMin = 4096;
 };
 
 }  // namespace
@@ -246,6 +267,8 @@ extern "C" int spx_order(int32_t n, const int64_t *rowptr, const int32_t *col,
     try {
         Graph g{n, rowptr, col};
         NDState st(g, perm);
+        const unsigned hw = std::thread::hardware_concurrency();
+        st.spare_threads = (int)std::min(hw > 1 ? hw - 1 : 0u, 31u);
         std::vector<int32_t> all(n);
         for (int32_t i = 0; i < n; i++) all[i] = i;
         st.order_region(std::move(all), 0, 0);
@@ -508,12 +531,14 @@ extern "C" int spx_analyze(int32_t n, const int64_t *rowptr, const int32_t *col,
             for (int32_t s = 0; s < ns; s++)
                 if (S->sparent[s] >= 0) clist[fill[S->sparent[s]]++] = s;
         }
-        std::vector<int64_t> rptr(ns + 1, 0);
-        std::vector<int32_t> rows;
-        rows.reserve((size_t)n * 8);
-        std::vector<int32_t> mark(n, -1);
-        std::vector<int32_t> tmp;
-        for (int32_t s = 0; s < ns; s++) {
+        // Rows of supernode s: its own columns, then every row >= its last
+        // column that appears in A's pivot columns or in a child's rows,
+        // ascending.  Supernodes are in postorder, so a subtree is a
+        // contiguous range ending at its root; disjoint subtrees are built
+        // on separate threads (each with its own mark array), then the
+        // supernodes above them in order.
+        std::vector<std::vector<int32_t>> rs(ns);
+        auto build_rows = [&](int32_t s, std::vector<int32_t> &mark, std::vector<int32_t> &tmp) {
             int32_t f = S->sfirst[s], l = S->sfirst[s + 1];
             tmp.clear();
             for (int32_t j = f; j < l; j++) {
@@ -525,15 +550,67 @@ extern "C" int spx_analyze(int32_t n, const int64_t *rowptr, const int32_t *col,
             for (int32_t q = cptr[s]; q < cptr[s + 1]; q++) {
                 int32_t c = clist[q];
                 int32_t cc0 = S->sfirst[c + 1] - S->sfirst[c];
-                for (int64_t p = rptr[c] + cc0; p < rptr[c + 1]; p++) {
-                    int32_t i = rows[p];
+                const std::vector<int32_t> &rc = rs[c];
+                for (size_t p = (size_t)cc0; p < rc.size(); p++) {
+                    int32_t i = rc[p];
                     if (i >= l && mark[i] != s) { mark[i] = s; tmp.push_back(i); }
                 }
             }
             std::sort(tmp.begin(), tmp.end());
-            for (int32_t j = f; j < l; j++) rows.push_back(j);
-            rows.insert(rows.end(), tmp.begin(), tmp.end());
-            rptr[s + 1] = (int64_t)rows.size();
+            std::vector<int32_t> &out = rs[s];
+            out.reserve((size_t)(l - f) + tmp.size());
+            for (int32_t j = f; j < l; j++) out.push_back(j);
+            out.insert(out.end(), tmp.begin(), tmp.end());
+        };
+        {
+            // subtree sizes and first descendants (postorder)
+            std::vector<int32_t> fdesc(ns);
+            for (int32_t s = 0; s < ns; s++) fdesc[s] = s;
+            for (int32_t s = 0; s < ns; s++) {
+                const int32_t p = S->sparent[s];
+                if (p >= 0 && fdesc[s] < fdesc[p]) fdesc[p] = fdesc[s];
+            }
+            const unsigned hw = std::max(1u, std::min(std::thread::hardware_concurrency(), 32u));
+            const int32_t target = std::max<int32_t>(256, ns / (int32_t)(4 * hw));
+            std::vector<char> in_task(ns, 0);
+            std::vector<int32_t> task_root;
+            std::vector<int32_t> stack;
+            for (int32_t s = 0; s < ns; s++)
+                if (S->sparent[s] < 0) stack.push_back(s);
+            while (!stack.empty()) {
+                const int32_t s = stack.back();
+                stack.pop_back();
+                if (s - fdesc[s] + 1 <= target) {
+                    task_root.push_back(s);
+                    continue;
+                }
+                for (int32_t q = cptr[s]; q < cptr[s + 1]; q++) stack.push_back(clist[q]);
+            }
+            for (int32_t r : task_root)
+                for (int32_t s = fdesc[r]; s <= r; s++) in_task[s] = 1;
+            const unsigned nth = (hw > 1 && ns > 2048) ? hw : 1u;
+            std::atomic<size_t> next{0};
+            auto worker = [&] {
+                std::vector<int32_t> mark(n, -1), tmp;
+                for (size_t t; (t = next.fetch_add(1)) < task_root.size();) {
+                    const int32_t r = task_root[t];
+                    for (int32_t s = fdesc[r]; s <= r; s++) build_rows(s, mark, tmp);
+                }
+            };
+            std::vector<std::thread> th;
+            for (unsigned i = 1; i < nth; i++) th.emplace_back(worker);
+            worker();
+            for (auto &t : th) t.join();
+            std::vector<int32_t> mark(n, -1), tmp;
+            for (int32_t s = 0; s < ns; s++)
+                if (!in_task[s]) build_rows(s, mark, tmp);
+        }
+        std::vector<int64_t> rptr(ns + 1, 0);
+        for (int32_t s = 0; s < ns; s++) rptr[s + 1] = rptr[s] + (int64_t)rs[s].size();
+        std::vector<int32_t> rows(rptr[ns]);
+        for (int32_t s = 0; s < ns; s++) {
+            std::copy(rs[s].begin(), rs[s].end(), rows.begin() + rptr[s]);
+            std::vector<int32_t>().swap(rs[s]);
         }
         const int64_t nrows_total = rptr[ns];
         S->rowptr = xalloc<int64_t>(ns + 1);
