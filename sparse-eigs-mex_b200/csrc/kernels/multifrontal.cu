@@ -1,14 +1,16 @@
-// Device multifrontal supernodal Cholesky (FP64) and the level-scheduled
+// Device multifrontal supernodal Cholesky (FP64) and the task-queue
 // shift-invert solve.  See multifrontal.cuh for the storage scheme.
 //
-// Factorization of one tree level, with T = 32 tiles over each front
-// (pivot tiles first, then the tiles of the rows below the pivots):
+// Factorization of one tree level.  Fronts of at most 32 rows are done by
+// one warp each (mf_tiny_front).  Larger fronts are assembled on 32 x 32
+// tiles and factored on 64 x 64 tiles (pivot tiles first, then the tiles of
+// the rows below the pivots), every tile product on the FP64 tensor cores:
 //   assemble  F = A(pivot columns) + shift*I + extend-add of the children's
 //             update matrices (pulled per tile, children in a fixed order)
-//   for kb:   potrf of the diagonal tile kb (+ its inverse into G),
-//             trsm of the tiles below it (as a product with that inverse),
+//   for kb:   panel: Cholesky + inverse of the diagonal tile kb (inv into
+//             G), the tiles below it as L_Ik = F_Ik inv(L_kk)^T;
 //             update of the trailing tiles, update matrix included
-//   invert    the off-diagonal tiles of inv(L11), row block by row block
+//   invert    the off-diagonal tiles of inv(L11) by recursive doubling
 //   wmul      G's lower part = L21 * inv(L11)
 // A pivot that is not positive records the failing column in a device status
 // word (never a trap); later kernels of the same factorization return early.
@@ -38,6 +40,10 @@ constexpr int kFThreads = 256;
 struct Sym {
     const int32_t *sfirst, *rows, *relmap, *child_ptr, *child_list;
     const int64_t *rowptr, *frontptr, *gptr;
+    // per child: for each 32-row tile boundary of its parent, the first
+    // entry of the child's update rows that maps at or below it
+    const int32_t *cbnd;
+    const int64_t *cbnd_ptr;
 };
 
 struct Front {
@@ -46,40 +52,26 @@ struct Front {
     int ldg;          // leading dimension of the G panel: r rounded up to even
 };
 
+// Front geometry with tiles of TS rows/columns: pivot tiles first, then the
+// tiles of the rows below the pivots.
+template <int TS>
 SPX_DEV Front front_of(const Sym &y, int s) {
     Front f;
     f.first = y.sfirst[s];
     f.c = y.sfirst[s + 1] - f.first;
     f.r = (int)(y.rowptr[s + 1] - y.rowptr[s]);
-    f.nkb = (f.c + T - 1) / T;
-    f.nt = f.nkb + (f.r - f.c + T - 1) / T;
+    f.nkb = (f.c + TS - 1) / TS;
+    f.nt = f.nkb + (f.r - f.c + TS - 1) / TS;
     f.fptr = y.frontptr[s];
     f.gptr = y.gptr[s];
     f.ldg = (f.r + 1) & ~1;
     return f;
 }
 
+template <int TS>
 SPX_DEV void tile_range(const Front &f, int I, int &a, int &b) {
-    if (I < f.nkb) { a = I * T; b = min(a + T, f.c); }
-    else { a = f.c + (I - f.nkb) * T; b = min(a + T, f.r); }
-}
-
-// load an h x w tile of a column-major matrix into S[i][j] (zero padded)
-SPX_DEV void load_tile(double (*S)[T + 1], const double *M, int64_t ld, int ra, int h, int ca,
-                       int w) {
-    for (int t = threadIdx.x; t < T * T; t += blockDim.x) {
-        int i = t & (T - 1), j = t >> 5;
-        S[i][j] = (i < h && j < w) ? M[(int64_t)(ra + i) + (int64_t)(ca + j) * ld] : 0.0;
-    }
-}
-
-SPX_DEV int lower_bound_i32(const int32_t *a, int n, int key) {
-    int lo = 0, hi = n;
-    while (lo < hi) {
-        int mid = (lo + hi) >> 1;
-        if (a[mid] < key) lo = mid + 1; else hi = mid;
-    }
-    return lo;
+    if (I < f.nkb) { a = I * TS; b = min(a + TS, f.c); }
+    else { a = f.c + (I - f.nkb) * TS; b = min(a + TS, f.r); }
 }
 
 // ------------------------------------------------------------ assemble --
@@ -93,10 +85,10 @@ mf_assemble(const int4 *__restrict__ tasks, Sym y, double *__restrict__ F,
     const double shift = params[0];
     const int4 tk = tasks[blockIdx.x];
     const int s = tk.x, I = tk.y, J = tk.z;
-    const Front f = front_of(y, s);
+    const Front f = front_of<T>(y, s);
     int ra, rb, ca, cb;
-    tile_range(f, I, ra, rb);
-    tile_range(f, J, ca, cb);
+    tile_range<T>(f, I, ra, rb);
+    tile_range<T>(f, J, ca, cb);
     const int h = rb - ra, w = cb - ca;
     for (int t = threadIdx.x; t < T * T; t += blockDim.x) S[t & (T - 1)][t >> 5] = 0.0;
     __syncthreads();
@@ -106,9 +98,10 @@ mf_assemble(const int4 *__restrict__ tasks, Sym y, double *__restrict__ F,
         const int cch = y.sfirst[ch + 1] - y.sfirst[ch];
         const int nb = rch - cch;
         const int32_t *rm = y.relmap + y.rowptr[ch] + cch;
-        const int ia = lower_bound_i32(rm, nb, ra), ib = lower_bound_i32(rm, nb, rb);
-        const int ja = lower_bound_i32(rm, nb, ca), jb = lower_bound_i32(rm, nb, cb);
+        const int32_t *bd = y.cbnd + y.cbnd_ptr[ch];
+        const int ia = bd[I], ib = bd[I + 1], ja = bd[J], jb = bd[J + 1];
         const int hi = ib - ia, wj = jb - ja;
+        (void)nb;
         if (hi > 0 && wj > 0) {
             const double *U = F + y.frontptr[ch];
             for (int t = threadIdx.x; t < hi * wj; t += blockDim.x) {
@@ -189,42 +182,6 @@ SPX_DEV void warp_tri_inverse(double (*M)[T + 1], const double *dinv, int c) {
     __syncwarp();
 }
 
-// --------------------------------------------------------------- potrf --
-// One warp factors one 32 x 32 diagonal tile and writes its inverse into G.
-constexpr int kPotrfWarps = 4;
-
-__global__ void __launch_bounds__(32 * kPotrfWarps)
-mf_potrf(const int4 *__restrict__ tasks, int ntasks, Sym y, double *__restrict__ F,
-         double *__restrict__ G, const double *__restrict__ params, int *status) {
-    __shared__ double Ms[kPotrfWarps][T][T + 1];
-    __shared__ double cols[kPotrfWarps][T], dinvs[kPotrfWarps][T];
-    if (*(volatile int *)status) return;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int task = blockIdx.x * kPotrfWarps + wid;
-    if (task >= ntasks) return;
-    const int4 tk = tasks[task];
-    const int s = tk.x, kb = tk.w;
-    const Front f = front_of(y, s);
-    int a, b;
-    tile_range(f, kb, a, b);
-    const int w = b - a;
-    double *Fs = F + f.fptr;
-    double (*M)[T + 1] = Ms[wid];
-    // lanes walk a column (coalesced): M[i][j] = F(a+i, a+j), lower part
-    for (int j = 0; j < T; j++)
-        M[lane][j] = (lane < w && j < w && j <= lane) ? Fs[(int64_t)(a + lane) + (int64_t)(a + j) * f.r]
-                                                      : 0.0;
-    __syncwarp();
-    warp_cholesky(M, cols[wid], dinvs[wid], w, w, params[1], status, f.first + a);
-    for (int j = 0; j < w; j++)
-        if (lane < w && j <= lane) Fs[(int64_t)(a + lane) + (int64_t)(a + j) * f.r] = M[lane][j];
-    warp_tri_inverse(M, dinvs[wid], w);
-    double *Gs = G + f.gptr;
-    for (int j = 0; j < w; j++)
-        if (lane < w && lane >= j)
-            Gs[(int64_t)(a + lane) + (int64_t)(a + j) * f.ldg] = lane == j ? dinvs[wid][j] : M[j][lane];
-}
-
 // ---------------------------------------------------------- tiny front --
 // A front with at most 32 rows is done by one warp end to end: assembly
 // (children's update matrices, then A and the shift), partial Cholesky of its
@@ -245,7 +202,7 @@ mf_tiny_front(const int4 *__restrict__ tasks, int ntasks, Sym y, double *__restr
     if (task >= ntasks) return;
     const double shift = params[0];
     const int s = tasks[task].x;
-    const Front f = front_of(y, s);
+    const Front f = front_of<T>(y, s);
     const int r = f.r, c = f.c;
     double (*M)[T + 1] = Ms[wid];
     for (int k = 0; k < T; k++) M[lane][k] = 0.0;
@@ -291,199 +248,420 @@ mf_tiny_front(const int4 *__restrict__ tasks, int ntasks, Sym y, double *__restr
     }
 }
 
-// ---------------------------------------------------------- tile products --
-// thread (tx, ty) owns C[tx][ty + 8q], q = 0..3
-SPX_DEV void mm_abt(double acc[4], const double (*A)[T + 1], const double (*B)[T + 1], int kw) {
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-    for (int t = 0; t < kw; t++) {
-        const double av = A[tx][t];
-#pragma unroll
-        for (int q = 0; q < 4; q++) acc[q] += av * B[ty + 8 * q][t];
-    }
-}
-SPX_DEV void mm_ab(double acc[4], const double (*A)[T + 1], const double (*B)[T + 1], int kw) {
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-    for (int t = 0; t < kw; t++) {
-        const double av = A[tx][t];
-#pragma unroll
-        for (int q = 0; q < 4; q++) acc[q] += av * B[t][ty + 8 * q];
-    }
+// ------------------------------------------------------- factor tiles --
+// Fronts with more than 32 rows are factored on 64 x 64 tiles.  Every tile
+// product runs on the FP64 tensor cores (mma.sync m8n8k4 f64): a CTA of four
+// warps owns one 64 x 64 output tile, each warp a 32 x 32 quarter held as
+// 4 x 4 accumulator fragments.  Operand tiles are staged in shared memory
+// column-major with a leading dimension of 68 doubles, which makes both the
+// fragment reads (8 rows x 4 columns per warp) and the coalesced column
+// loads free of bank conflicts.
+constexpr int FT = 64;
+constexpr int FLD = 68;
+constexpr int kGThreads = 128;
+constexpr int kFTileDoubles = FT * FLD;
+constexpr int kPanelGroup = 4;   // panel tiles of a small front share one block
+constexpr size_t kPanelSmem = 4 * sizeof(double) * kFTileDoubles;
+constexpr size_t kPairSmem = 2 * sizeof(double) * kFTileDoubles;
+
+SPX_DEV void dmma(double &d0, double &d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(d0), "+d"(d1) : "d"(a), "d"(b));
 }
 
-// L_Ik = F_Ik * inv(L_kk)^T
-__global__ void __launch_bounds__(kFThreads)
-mf_trsm(const int4 *__restrict__ tasks, Sym y, double *__restrict__ F,
-        const double *__restrict__ G, const int *status) {
-    __shared__ double A[T][T + 1];
-    __shared__ double X[T][T + 1];
-    if (*(volatile const int *)status) return;
-    const int4 tk = tasks[blockIdx.x];
-    const int s = tk.x, I = tk.y, kb = tk.w;
-    const Front f = front_of(y, s);
-    int ra, rb, ka, kbb;
-    tile_range(f, I, ra, rb);
-    tile_range(f, kb, ka, kbb);
-    const int h = rb - ra, w = kbb - ka;
-    double *Fs = F + f.fptr;
-    load_tile(A, Fs, f.r, ra, h, ka, w);
-    load_tile(X, G + f.gptr, f.ldg, ka, w, ka, w);
+// Tile loads go through cp.async (8 bytes per element, zero-filled outside
+// the h x w block), so all of a thread's 32 element copies are in flight at
+// once; cp_wait() completes them and makes them visible to the block.
+SPX_DEV void cp_async8(double *dst, const double *src, bool valid) {
+    const unsigned saddr = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(saddr), "l"(src),
+                 "r"(valid ? 8 : 0) : "memory");
+}
+SPX_DEV void cp_wait() {
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
     __syncthreads();
-    double acc[4] = {0, 0, 0, 0};
-    mm_abt(acc, A, X, w);
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-        const int j = ty + 8 * q;
-        if (tx < h && j < w) Fs[(int64_t)(ra + tx) + (int64_t)(ka + j) * f.r] = acc[q];
+}
+
+// s(i, j) = M(ra + i, ca + j) for i < h, j < w; zero elsewhere in the tile
+SPX_DEV void ftile_load(double *s, const double *M, int64_t ld, int ra, int h, int ca, int w) {
+#pragma unroll 8
+    for (int q = 0; q < FT * FT / kGThreads; q++) {
+        const int t = threadIdx.x + q * kGThreads;
+        const int i = t & (FT - 1), j = t >> 6;
+        const bool v = (i < h && j < w);
+        cp_async8(s + j * FLD + i, v ? M + (int64_t)(ra + i) + (int64_t)(ca + j) * ld : M, v);
+    }
+}
+// s(i, j) = M(ca + j, ra + i): the transpose of the stored block
+SPX_DEV void ftile_load_t(double *s, const double *M, int64_t ld, int ra, int h, int ca, int w) {
+#pragma unroll 8
+    for (int q = 0; q < FT * FT / kGThreads; q++) {
+        const int t = threadIdx.x + q * kGThreads;
+        const int j = t & (FT - 1), i = t >> 6;
+        const bool v = (i < h && j < w);
+        cp_async8(s + j * FLD + i, v ? M + (int64_t)(ca + j) + (int64_t)(ra + i) * ld : M, v);
+    }
+}
+// lower triangle of the w x w block at (a, a); zero elsewhere
+SPX_DEV void ftile_load_lower(double *s, const double *M, int64_t ld, int a, int w) {
+#pragma unroll 8
+    for (int q = 0; q < FT * FT / kGThreads; q++) {
+        const int t = threadIdx.x + q * kGThreads;
+        const int i = t & (FT - 1), j = t >> 6;
+        const bool v = (i < w && j <= i);
+        cp_async8(s + j * FLD + i, v ? M + (int64_t)(a + i) + (int64_t)(a + j) * ld : M, v);
     }
 }
 
-// F_IJ -= L_Ik L_Jk^T
-__global__ void __launch_bounds__(kFThreads)
-mf_update(const int4 *__restrict__ tasks, Sym y, double *__restrict__ F, const int *status) {
-    __shared__ double A[T][T + 1];
-    __shared__ double B[T][T + 1];
+using Acc = double[4][4][2];
+
+SPX_DEV void acc_zero(Acc &acc) {
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
+}
+
+// acc += A B^T (BT) or A B, with A a 64 x kw tile (s(i, k) at k*FLD + i) and
+// B given as 64 x kw (BT: B(n, k) at k*FLD + n) or kw x 64 (B(k, n) at n*FLD + k).
+// Only the fragments that touch the first mh rows / nw columns of the
+// output are computed (the rest of the accumulator stays zero).
+template <bool BT>
+SPX_DEV void warp_mma(Acc &acc, const double *As, const double *Bs, int kw, int mh = FT,
+                      int nw = FT) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    const int wid = threadIdx.x >> 5, m0 = (wid & 1) * 32, n0 = (wid >> 1) * 32;
+    if (m0 >= mh || n0 >= nw) return;
+    const int mi = min(4, (mh - m0 + 7) >> 3), nj = min(4, (nw - n0 + 7) >> 3);
+    for (int k = 0; k < kw; k += 4) {
+        double a[4], b[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) a[i] = As[(k + t) * FLD + m0 + 8 * i + g];
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            b[j] = BT ? Bs[(k + t) * FLD + n0 + 8 * j + g] : Bs[(n0 + 8 * j + g) * FLD + k + t];
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                if (i < mi && j < nj) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+    }
+}
+
+// M(ra + m, ca + n) = alpha * acc(m, n) (+ M when add), for m < h, n < w.
+// TRANS stores acc(m, n) at M(ca + n, ra + m) instead.
+template <bool TRANS>
+SPX_DEV void acc_store(const Acc &acc, double *M, int64_t ld, int ra, int h, int ca, int w,
+                       double alpha, bool add) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    const int wid = threadIdx.x >> 5, m0 = (wid & 1) * 32, n0 = (wid >> 1) * 32;
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                const int m = m0 + 8 * i + g, n = n0 + 8 * j + 2 * t + e;
+                if (m < h && n < w) {
+                    double *p = TRANS ? M + (int64_t)(ca + n) + (int64_t)(ra + m) * ld
+                                      : M + (int64_t)(ra + m) + (int64_t)(ca + n) * ld;
+                    *p = add ? *p + alpha * acc[i][j][e] : alpha * acc[i][j][e];
+                }
+            }
+}
+
+// ---- recursive Cholesky + inverse of a diagonal tile (w <= 64) --------
+// chol_inv_rec<N>: L (lower) and X = inv(L) of the leading w x w part of the
+// N x N lower matrix D (all column-major, leading dimension FLD), by the 128
+// threads of the block, 2 x 2 blocked down to 8 x 8:
+//   L00, X00 (recursive); L10 = A10 X00^T; A11 -= L10 L10^T and
+//   T = L10 X00 (one phase); L11, X11 (recursive); X10 = -X11 T.
+// The sequential chain is one 8 x 8 base case per 8 pivots; everything else
+// is small products spread over the block.  Rows/columns >= w of L and X are
+// zero except for ones on the diagonal (identity padding), so the products
+// need no edge tests.  D is destroyed; `tmp` is a scratch tile (64 x FLD).
+
+// 8 x 8 base case by warp 0, lanes 0..7 holding rows in registers
+SPX_DEV void chol_inv8(double *D, double *L, double *X, int w, double pivtol, int *status,
+                       int colbase, bool record) {
+    if (threadIdx.x >= 32) return;
+    const unsigned full = 0xffffffffu;
+    const int i = threadIdx.x & 7;
+    const bool act = threadIdx.x < 8;
+    double a[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) a[k] = (i < w && k <= i) ? D[k * FLD + i] : (k == i ? 1.0 : 0.0);
+    double myr = 1.0;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        double d = __shfl_sync(full, a[j], j);
+        if (!(d > pivtol)) {
+            if (record && act && i == 0 && j < w) atomicCAS(status, 0, colbase + j + 1);
+            d = 1.0;
+        }
+        const double rl = rsqrt(d);
+        const double lij = (i > j) ? a[j] * rl : (i == j ? d * rl : 0.0);
+        a[j] = lij;
+        if (i == j) myr = rl;
+#pragma unroll
+        for (int k = j + 1; k < 8; k++) {
+            const double lkj = __shfl_sync(full, lij, k);
+            if (k <= i) a[k] -= lij * lkj;
+        }
+    }
+    double x[8];
+#pragma unroll
+    for (int c = 0; c < 8; c++) x[c] = (c == i) ? myr : 0.0;
+#pragma unroll
+    for (int t = 0; t < 7; t++) {
+#pragma unroll
+        for (int c = 0; c <= t; c++) {
+            const double xtc = __shfl_sync(full, x[c], t);
+            if (i > t) x[c] -= a[t] * xtc;
+        }
+        if (i == t + 1)
+#pragma unroll
+            for (int c = 0; c <= t; c++) x[c] *= myr;
+    }
+    if (act)
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            L[k * FLD + i] = a[k];
+            X[k * FLD + i] = x[k];
+        }
+}
+
+// C (h x h) = sum_k A(i, k) B'(k, j) over k < h, for the four small products
+// of the recursion; each thread computes h*h/128 (or one) outputs.
+// mode 0: C = A B^T (A, B both stored row-index-first, i.e. B(j, k))
+// mode 1: C = A B   (B(k, j))
+template <int H, int MODE>
+SPX_DEV void small_mm(const double *A, const double *B, double *C, double alpha, bool accumulate) {
+    constexpr int NOUT = H * H;
+    for (int o = threadIdx.x; o < NOUT; o += blockDim.x) {
+        const int i = o % H, j = o / H;
+        double acc = 0.0;
+#pragma unroll
+        for (int k = 0; k < H; k++)
+            acc += A[k * FLD + i] * (MODE == 0 ? B[k * FLD + j] : B[j * FLD + k]);
+        C[j * FLD + i] = accumulate ? C[j * FLD + i] + alpha * acc : alpha * acc;
+    }
+}
+
+template <int N>
+SPX_DEV void chol_inv_rec(double *D, double *L, double *X, double *tmp, int w, double pivtol,
+                          int *status, int colbase, bool record) {
+    if constexpr (N == 8) {
+        chol_inv8(D, L, X, w, pivtol, status, colbase, record);
+        __syncthreads();
+    } else {
+        constexpr int H = N / 2;
+        const int w0 = min(w, H), w1 = max(w - H, 0);
+        chol_inv_rec<H>(D, L, X, tmp, w0, pivtol, status, colbase, record);
+        if (w1 == 0) {
+            // nothing left to factor: identity padding for the second half
+            for (int t = threadIdx.x; t < H * H; t += blockDim.x) {
+                const int i = t % H, j = t / H;
+                L[(H + j) * FLD + i] = 0.0;
+                X[(H + j) * FLD + i] = 0.0;
+                L[j * FLD + H + i] = 0.0;
+                X[j * FLD + H + i] = 0.0;
+                L[(H + j) * FLD + H + i] = (i == j) ? 1.0 : 0.0;
+                X[(H + j) * FLD + H + i] = (i == j) ? 1.0 : 0.0;
+            }
+            __syncthreads();
+            return;
+        }
+        // off-diagonal blocks of L and X above the diagonal stay zero
+        for (int t = threadIdx.x; t < H * H; t += blockDim.x) {
+            const int i = t % H, j = t / H;
+            L[(H + j) * FLD + i] = 0.0;
+            X[(H + j) * FLD + i] = 0.0;
+        }
+        small_mm<H, 0>(D + H, X, L + H, 1.0, false);               // L10 = A10 X00^T
+        __syncthreads();
+        small_mm<H, 0>(L + H, L + H, D + H * FLD + H, -1.0, true); // A11 -= L10 L10^T
+        small_mm<H, 1>(L + H, X, tmp, 1.0, false);                 // T = L10 X00
+        __syncthreads();
+        chol_inv_rec<H>(D + H * FLD + H, L + H * FLD + H, X + H * FLD + H, tmp + H * FLD, w1,
+                        pivtol, status, colbase + H, record);
+        small_mm<H, 1>(X + H * FLD + H, tmp, X + H, -1.0, false);  // X10 = -X11 T
+        __syncthreads();
+    }
+}
+
+// Panel step kb of a front: Cholesky and inverse of the (updated) diagonal
+// tile kb, then the block's own tiles I0 .. I0+nI-1 of column block kb: the
+// diagonal (inv(L_kk) into G) or a tile below it, L_Ik = F_Ik inv(L_kk)^T.
+// The diagonal factorization is redone by every block of the step, so the
+// tiles of a large front proceed in parallel; a small front's tiles share
+// one block.  task = (s, I0, nI, kb).
+__global__ void __launch_bounds__(kGThreads)
+mf_panel64(const int4 *__restrict__ tasks, Sym y, double *__restrict__ F,
+           double *__restrict__ G, const double *__restrict__ params, int *status) {
+    extern __shared__ double fsm[];
+    double *Ds = fsm, *Ls = fsm + kFTileDoubles, *Xs = fsm + 2 * kFTileDoubles;
+    double *Ts = fsm + 3 * kFTileDoubles;
+    if (*(volatile int *)status) return;
+    const int4 tk = tasks[blockIdx.x];
+    const int s = tk.x, I0 = tk.y, nI = tk.z, kb = tk.w;
+    const Front f = front_of<FT>(y, s);
+    int ka, kz;
+    tile_range<FT>(f, kb, ka, kz);
+    const int w = kz - ka;
+    double *Fs = F + f.fptr;
+    ftile_load_lower(Ds, Fs, f.r, ka, w);
+    cp_wait();
+    chol_inv_rec<64>(Ds, Ls, Xs, Ts, w, params[1], status, f.first + ka, I0 == kb);
+    for (int I = I0; I < I0 + nI; I++) {
+        if (I == kb) {
+            // only inv(L_kk) is kept: nothing later reads a diagonal tile of
+            // L, and the diagonal tile of F must stay as it is while the
+            // other blocks of this step are still reading it
+            double *Gs = G + f.gptr;
+            for (int t = threadIdx.x; t < FT * FT; t += blockDim.x) {
+                const int i = t & (FT - 1), j = t >> 6;
+                if (i < w && j <= i) Gs[(int64_t)(ka + i) + (int64_t)(ka + j) * f.ldg] = Xs[j * FLD + i];
+            }
+            continue;
+        }
+        int ra, rb;
+        tile_range<FT>(f, I, ra, rb);
+        const int h = rb - ra;
+        ftile_load(Ds, Fs, f.r, ra, h, ka, w);
+        cp_wait();
+        Acc acc;
+        acc_zero(acc);
+        warp_mma<true>(acc, Ds, Xs, (w + 3) & ~3, h, w);
+        acc_store<false>(acc, Fs, f.r, ra, h, ka, w, 1.0, false);
+        __syncthreads();
+    }
+}
+
+// F_IJ -= L_Ik L_Jk^T    task = (s, I, J, kb)
+__global__ void __launch_bounds__(kGThreads)
+mf_update64(const int4 *__restrict__ tasks, Sym y, double *__restrict__ F, const int *status) {
+    extern __shared__ double fsm[];
+    double *As = fsm, *Bs = fsm + kFTileDoubles;
     if (*(volatile const int *)status) return;
     const int4 tk = tasks[blockIdx.x];
     const int s = tk.x, I = tk.y, J = tk.z, kb = tk.w;
-    const Front f = front_of(y, s);
-    int ra, rb, ca, cb, ka, kbb;
-    tile_range(f, I, ra, rb);
-    tile_range(f, J, ca, cb);
-    tile_range(f, kb, ka, kbb);
-    const int h = rb - ra, w = cb - ca, kw = kbb - ka;
+    const Front f = front_of<FT>(y, s);
+    int ra, rb, ca, cb, ka, kz;
+    tile_range<FT>(f, I, ra, rb);
+    tile_range<FT>(f, J, ca, cb);
+    tile_range<FT>(f, kb, ka, kz);
+    const int h = rb - ra, w = cb - ca, kw = kz - ka;
     double *Fs = F + f.fptr;
-    load_tile(A, Fs, f.r, ra, h, ka, kw);
-    load_tile(B, Fs, f.r, ca, w, ka, kw);
-    __syncthreads();
-    double acc[4] = {0, 0, 0, 0};
-    mm_abt(acc, A, B, kw);
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-        const int j = ty + 8 * q;
-        if (tx < h && j < w) {
-            double *p = Fs + (int64_t)(ra + tx) + (int64_t)(ca + j) * f.r;
-            *p -= acc[q];
-        }
-    }
+    ftile_load(As, Fs, f.r, ra, h, ka, kw);
+    ftile_load(Bs, Fs, f.r, ca, w, ka, kw);
+    cp_wait();
+    Acc acc;
+    acc_zero(acc);
+    warp_mma<true>(acc, As, Bs, (kw + 3) & ~3, h, w);
+    acc_store<false>(acc, Fs, f.r, ra, h, ca, w, -1.0, true);
 }
 
 // inv(L11) by recursive doubling over tile blocks.  After step l every
 // diagonal block of 2^l tiles is inverted; step l joins blocks A = [A0, C0)
 // and C = [C0, C1) (C0 = A0 + 2^l) through
-//   T = L_CA X_A          (mf_inv_t: T lands in the unused upper part of F)
-//   X_CA = -X_C T         (mf_inv_x)
+//   T = L_CA X_A          (mf_inv_t64: T lands in the unused upper part of F)
+//   X_CA = -X_C T         (mf_inv_x64)
 // task = (s, i, j, l): output tile (i, j), i in C, j in A.
-__global__ void __launch_bounds__(kFThreads)
-mf_inv_t(const int4 *__restrict__ tasks, Sym y, double *__restrict__ F,
-         const double *__restrict__ G, const int *status) {
-    __shared__ double A[T][T + 1];
-    __shared__ double B[T][T + 1];
+__global__ void __launch_bounds__(kGThreads)
+mf_inv_t64(const int4 *__restrict__ tasks, Sym y, double *__restrict__ F,
+           const double *__restrict__ G, const int *status) {
+    extern __shared__ double fsm[];
+    double *As = fsm, *Bs = fsm + kFTileDoubles;
     if (*(volatile const int *)status) return;
     const int4 tk = tasks[blockIdx.x];
     const int s = tk.x, i = tk.y, j = tk.z, l = tk.w;
-    const Front f = front_of(y, s);
+    const Front f = front_of<FT>(y, s);
     const int C0 = (j >> (l + 1) << (l + 1)) + (1 << l);
     int ra, rb, ca, cb;
-    tile_range(f, i, ra, rb);
-    tile_range(f, j, ca, cb);
+    tile_range<FT>(f, i, ra, rb);
+    tile_range<FT>(f, j, ca, cb);
     const int h = rb - ra, w = cb - ca;
     double *Fs = F + f.fptr;
     const double *Gs = G + f.gptr;
-    double acc[4] = {0, 0, 0, 0};
+    Acc acc;
+    acc_zero(acc);
     for (int k = j; k < C0; k++) {
-        int ka, kbb;
-        tile_range(f, k, ka, kbb);
-        const int kw = kbb - ka;
-        load_tile(A, Fs, f.r, ra, h, ka, kw);
-        load_tile(B, Gs, f.ldg, ka, kw, ca, w);
-        __syncthreads();
-        mm_ab(acc, A, B, kw);
+        int ka, kz;
+        tile_range<FT>(f, k, ka, kz);
+        const int kw = kz - ka;
+        ftile_load(As, Fs, f.r, ra, h, ka, kw);      // L_ik
+        ftile_load(Bs, Gs, f.ldg, ka, kw, ca, w);    // X_kj
+        cp_wait();
+        warp_mma<false>(acc, As, Bs, (kw + 3) & ~3, h, w);
         __syncthreads();
     }
     // T_ij is kept at tile (j, i) of F: strictly upper, never used otherwise
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-        const int jj = ty + 8 * q;
-        if (tx < h && jj < w) Fs[(int64_t)(ca + jj) + (int64_t)(ra + tx) * f.r] = acc[q];
-    }
+    acc_store<true>(acc, Fs, f.r, ra, h, ca, w, 1.0, false);
 }
 
-__global__ void __launch_bounds__(kFThreads)
-mf_inv_x(const int4 *__restrict__ tasks, Sym y, const double *__restrict__ F,
-         double *__restrict__ G, const int *status) {
-    __shared__ double A[T][T + 1];
-    __shared__ double B[T][T + 1];
+__global__ void __launch_bounds__(kGThreads)
+mf_inv_x64(const int4 *__restrict__ tasks, Sym y, const double *__restrict__ F,
+           double *__restrict__ G, const int *status) {
+    extern __shared__ double fsm[];
+    double *As = fsm, *Bs = fsm + kFTileDoubles;
     if (*(volatile const int *)status) return;
     const int4 tk = tasks[blockIdx.x];
     const int s = tk.x, i = tk.y, j = tk.z, l = tk.w;
-    const Front f = front_of(y, s);
+    const Front f = front_of<FT>(y, s);
     const int C0 = (j >> (l + 1) << (l + 1)) + (1 << l);
     int ra, rb, ca, cb;
-    tile_range(f, i, ra, rb);
-    tile_range(f, j, ca, cb);
+    tile_range<FT>(f, i, ra, rb);
+    tile_range<FT>(f, j, ca, cb);
     const int h = rb - ra, w = cb - ca;
     const double *Fs = F + f.fptr;
     double *Gs = G + f.gptr;
-    double acc[4] = {0, 0, 0, 0};
+    Acc acc;
+    acc_zero(acc);
     for (int k = C0; k <= i; k++) {
-        int ka, kbb;
-        tile_range(f, k, ka, kbb);
-        const int kw = kbb - ka;
-        load_tile(A, Gs, f.ldg, ra, h, ka, kw);          // X_ik
-        // T_kj, stored transposed at tile (j, k) of F
-        for (int t2 = threadIdx.x; t2 < T * T; t2 += blockDim.x) {
-            const int r2 = t2 & (T - 1), c2 = t2 >> 5;   // B[r2][c2] = T_kj(r2, c2)
-            B[r2][c2] = (r2 < kw && c2 < w) ? Fs[(int64_t)(ca + c2) + (int64_t)(ka + r2) * f.r] : 0.0;
-        }
-        __syncthreads();
-        mm_ab(acc, A, B, kw);
+        int ka, kz;
+        tile_range<FT>(f, k, ka, kz);
+        const int kw = kz - ka;
+        ftile_load(As, Gs, f.ldg, ra, h, ka, kw);    // X_ik
+        ftile_load_t(Bs, Fs, f.r, ka, kw, ca, w);    // T_kj, stored transposed at tile (j, k)
+        cp_wait();
+        warp_mma<false>(acc, As, Bs, (kw + 3) & ~3, h, w);
         __syncthreads();
     }
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-        const int jj = ty + 8 * q;
-        if (tx < h && jj < w) Gs[(int64_t)(ra + tx) + (int64_t)(ca + jj) * f.ldg] = -acc[q];
-    }
+    acc_store<false>(acc, Gs, f.ldg, ra, h, ca, w, -1.0, false);
 }
 
 // W_IJ = sum_{K=J}^{nkb-1} L_IK X_KJ   (I a tile of the rows below the pivots)
-__global__ void __launch_bounds__(kFThreads)
-mf_wmul(const int4 *__restrict__ tasks, Sym y, const double *__restrict__ F,
-        double *__restrict__ G, const int *status) {
-    __shared__ double A[T][T + 1];
-    __shared__ double B[T][T + 1];
+__global__ void __launch_bounds__(kGThreads)
+mf_wmul64(const int4 *__restrict__ tasks, Sym y, const double *__restrict__ F,
+          double *__restrict__ G, const int *status) {
+    extern __shared__ double fsm[];
+    double *As = fsm, *Bs = fsm + kFTileDoubles;
     if (*(volatile const int *)status) return;
     const int4 tk = tasks[blockIdx.x];
     const int s = tk.x, I = tk.y, J = tk.z;
-    const Front f = front_of(y, s);
+    const Front f = front_of<FT>(y, s);
     int ra, rb, ca, cb;
-    tile_range(f, I, ra, rb);
-    tile_range(f, J, ca, cb);
+    tile_range<FT>(f, I, ra, rb);
+    tile_range<FT>(f, J, ca, cb);
     const int h = rb - ra, w = cb - ca;
     const double *Fs = F + f.fptr;
     double *Gs = G + f.gptr;
-    double acc[4] = {0, 0, 0, 0};
+    Acc acc;
+    acc_zero(acc);
     for (int k = J; k < f.nkb; k++) {
-        int ka, kbb;
-        tile_range(f, k, ka, kbb);
-        const int kw = kbb - ka;
-        load_tile(A, Fs, f.r, ra, h, ka, kw);
-        load_tile(B, Gs, f.ldg, ka, kw, ca, w);
-        __syncthreads();
-        mm_ab(acc, A, B, kw);
+        int ka, kz;
+        tile_range<FT>(f, k, ka, kz);
+        const int kw = kz - ka;
+        ftile_load(As, Fs, f.r, ra, h, ka, kw);
+        ftile_load(Bs, Gs, f.ldg, ka, kw, ca, w);
+        cp_wait();
+        warp_mma<false>(acc, As, Bs, (kw + 3) & ~3, h, w);
         __syncthreads();
     }
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-        const int j = ty + 8 * q;
-        if (tx < h && j < w) Gs[(int64_t)(ra + tx) + (int64_t)(ca + j) * f.ldg] = acc[q];
-    }
+    acc_store<false>(acc, Gs, f.ldg, ra, h, ca, w, 1.0, false);
 }
+
 
 // ---------------------------------------------------------------- solve --
 // The whole solve pair is one persistent kernel that pulls tasks from an
@@ -1153,7 +1331,7 @@ void MultifrontalPlan::release(cudaStream_t st) {
     if (fgraph_) { cudaGraphExecDestroy(fgraph_); fgraph_ = nullptr; }
     fgraph_val_ = nullptr;
     if (d_params_) { cudaFreeAsync(d_params_, st); d_params_ = nullptr; }
-    void *ptrs[] = {d_perm_, d_sfirst_, d_rows_, d_relmap_, d_child_ptr_, d_child_list_,
+    void *ptrs[] = {d_cbnd_, d_cbnd_ptr_, d_perm_, d_sfirst_, d_rows_, d_relmap_, d_child_ptr_, d_child_list_,
                     d_rowptr_, d_frontptr_, d_gptr_, d_uptr_, d_acolptr_, d_atpos_, d_asrc_,
                     d_tasks_, d_front_, d_G_, d_u_, d_yf_, d_x_, d_status_, d_meta_,
                     d_stask_, d_bundle_, d_cptr_, d_cidx_, d_chunks_, d_fpart_, d_bpart_,
@@ -1161,6 +1339,8 @@ void MultifrontalPlan::release(cudaStream_t st) {
     for (void *p : ptrs)
         if (p) cudaFreeAsync(p, st);
     d_perm_ = d_sfirst_ = d_rows_ = d_relmap_ = d_child_ptr_ = d_child_list_ = nullptr;
+    d_cbnd_ = nullptr;
+    d_cbnd_ptr_ = nullptr;
     d_rowptr_ = d_frontptr_ = d_gptr_ = d_uptr_ = nullptr;
     d_acolptr_ = d_atpos_ = d_asrc_ = nullptr;
     d_tasks_ = nullptr;
@@ -1256,33 +1436,43 @@ int MultifrontalPlan::init(const spx_symbolic &S, const int64_t *rowptr, const i
                     for (int J = 0; J <= I; J++) tasks.push_back(make_int4(s, I, J, 0));
             }
             emit(MF_ASSEMBLE, b);
+            // factor steps on 64-tiles: panel kb (diagonal Cholesky + the
+            // tiles below it), then the right-looking update of the trailing
+            // tiles, Schur complement included
+            auto geo = [&](int s, int &r, int &c, int &nkb, int &nt) {
+                r = (int)(S.rowptr[s + 1] - S.rowptr[s]);
+                c = S.sfirst[s + 1] - S.sfirst[s];
+                nkb = (c + FT - 1) / FT;
+                nt = nkb + (r - c + FT - 1) / FT;
+            };
+            nkbmax = 0;
+            for (int32_t q = q0; q < q1; q++) {
+                const int s = S.level_sup[q];
+                if (is_tiny(s)) continue;
+                int r, c, nkb, nt;
+                geo(s, r, c, nkb, nt);
+                nkbmax = std::max(nkbmax, nkb);
+            }
             for (int kb = 0; kb < nkbmax; kb++) {
                 size_t b0 = tasks.size();
                 for (int32_t q = q0; q < q1; q++) {
                     const int s = S.level_sup[q];
                     if (is_tiny(s)) continue;
-                    const int c = S.sfirst[s + 1] - S.sfirst[s];
-                    if ((c + T - 1) / T > kb) tasks.push_back(make_int4(s, kb, kb, kb));
-                }
-                emit(MF_POTRF, b0);
-                size_t b1 = tasks.size();
-                for (int32_t q = q0; q < q1; q++) {
-                    const int s = S.level_sup[q];
-                    const int r = (int)(S.rowptr[s + 1] - S.rowptr[s]);
-                    const int c = S.sfirst[s + 1] - S.sfirst[s];
-                    if (is_tiny(s)) continue;
-                    const int nkb = (c + T - 1) / T, nt = nkb + (r - c + T - 1) / T;
+                    int r, c, nkb, nt;
+                    geo(s, r, c, nkb, nt);
                     if (nkb <= kb) continue;
-                    for (int I = kb + 1; I < nt; I++) tasks.push_back(make_int4(s, I, kb, kb));
+                    // a front with few tiles left: one block; else one per tile
+                    if (nt - kb <= kPanelGroup) tasks.push_back(make_int4(s, kb, nt - kb, kb));
+                    else
+                        for (int I = kb; I < nt; I++) tasks.push_back(make_int4(s, I, 1, kb));
                 }
-                emit(MF_TRSM, b1);
+                emit(MF_PANEL, b0);
                 size_t b2 = tasks.size();
                 for (int32_t q = q0; q < q1; q++) {
                     const int s = S.level_sup[q];
-                    const int r = (int)(S.rowptr[s + 1] - S.rowptr[s]);
-                    const int c = S.sfirst[s + 1] - S.sfirst[s];
                     if (is_tiny(s)) continue;
-                    const int nkb = (c + T - 1) / T, nt = nkb + (r - c + T - 1) / T;
+                    int r, c, nkb, nt;
+                    geo(s, r, c, nkb, nt);
                     if (nkb <= kb) continue;
                     for (int I = kb + 1; I < nt; I++)
                         for (int J = kb + 1; J <= I; J++) tasks.push_back(make_int4(s, I, J, kb));
@@ -1296,8 +1486,8 @@ int MultifrontalPlan::init(const spx_symbolic &S, const int64_t *rowptr, const i
                     for (int32_t q = q0; q < q1; q++) {
                         const int s = S.level_sup[q];
                         if (is_tiny(s)) continue;
-                        const int c = S.sfirst[s + 1] - S.sfirst[s];
-                        const int nkb = (c + T - 1) / T;
+                        int r, c, nkb, nt;
+                        geo(s, r, c, nkb, nt);
                         for (int A0 = 0; A0 + half < nkb; A0 += 2 * half) {
                             const int C0 = A0 + half, C1 = std::min(A0 + 2 * half, nkb);
                             for (int i = C0; i < C1; i++)
@@ -1310,10 +1500,9 @@ int MultifrontalPlan::init(const spx_symbolic &S, const int64_t *rowptr, const i
             size_t bw = tasks.size();
             for (int32_t q = q0; q < q1; q++) {
                 const int s = S.level_sup[q];
-                const int r = (int)(S.rowptr[s + 1] - S.rowptr[s]);
-                const int c = S.sfirst[s + 1] - S.sfirst[s];
                 if (is_tiny(s)) continue;
-                const int nkb = (c + T - 1) / T, nt = nkb + (r - c + T - 1) / T;
+                int r, c, nkb, nt;
+                geo(s, r, c, nkb, nt);
                 for (int I = nkb; I < nt; I++)
                     for (int J = 0; J < nkb; J++) tasks.push_back(make_int4(s, I, J, 0));
             }
@@ -1456,7 +1645,28 @@ int MultifrontalPlan::init(const spx_symbolic &S, const int64_t *rowptr, const i
                             (int32_t)(uptr[ch] + (t - S.rowptr[ch] - cc));
                 }
         }
+        // child tile bounds for the assembly (32-row tiles of the parent)
+        std::vector<int64_t> cbnd_ptr(ns + 1, 0);
+        std::vector<int32_t> cbnd;
+        for (int32_t ch = 0; ch < ns; ch++) {
+            const int p = S.sparent[ch];
+            cbnd_ptr[ch] = (int64_t)cbnd.size();
+            if (p < 0) continue;
+            const int rp = (int)(S.rowptr[p + 1] - S.rowptr[p]);
+            const int cp = S.sfirst[p + 1] - S.sfirst[p];
+            const int nkb = (cp + T - 1) / T, ntp = nkb + (rp - cp + T - 1) / T;
+            const int cch = S.sfirst[ch + 1] - S.sfirst[ch];
+            const int32_t *rm = S.relmap + S.rowptr[ch] + cch;
+            const int nb = (int)(S.rowptr[ch + 1] - S.rowptr[ch]) - cch;
+            for (int I = 0; I <= ntp; I++) {
+                const int start = (I == ntp) ? rp : (I < nkb ? I * T : cp + (I - nkb) * T);
+                cbnd.push_back((int32_t)(std::lower_bound(rm, rm + nb, start) - rm));
+            }
+        }
+        cbnd_ptr[ns] = (int64_t)cbnd.size();
         int rc = 0;
+        rc = rc ? rc : dupload(&d_cbnd_, cbnd.data(), cbnd.size(), st);
+        rc = rc ? rc : dupload(&d_cbnd_ptr_, cbnd_ptr.data(), cbnd_ptr.size(), st);
         rc = rc ? rc : dupload(&d_perm_, S.perm, n, st);
         rc = rc ? rc : dupload(&d_sfirst_, S.sfirst, ns + 1, st);
         rc = rc ? rc : dupload(&d_rows_, S.rows, (size_t)nrows_total_, st);
@@ -1507,6 +1717,12 @@ int MultifrontalPlan::init(const spx_symbolic &S, const int64_t *rowptr, const i
         // everything uploaded above comes from host vectors that die here
         if (cudaStreamSynchronize(st) != cudaSuccess) return SPEIGS_ERR_INTERNAL;
         // persistent grid for the task-queue solve
+        // factor tile kernels stage two or three 64 x 64 tiles
+        cudaFuncSetAttribute(mf_panel64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelSmem);
+        cudaFuncSetAttribute(mf_update64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPairSmem);
+        cudaFuncSetAttribute(mf_inv_t64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPairSmem);
+        cudaFuncSetAttribute(mf_inv_x64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPairSmem);
+        cudaFuncSetAttribute(mf_wmul64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPairSmem);
         solve_smem_ = solve_smem_bytes();
         if (solve_smem_ > 48 * 1024)
             cudaFuncSetAttribute(mf_solve_sf, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1524,7 +1740,8 @@ int MultifrontalPlan::init(const spx_symbolic &S, const int64_t *rowptr, const i
 }
 
 void MultifrontalPlan::launch_factor(const double *d_val, cudaStream_t st) {
-    Sym y{d_sfirst_, d_rows_, d_relmap_, d_child_ptr_, d_child_list_, d_rowptr_, d_frontptr_, d_gptr_};
+    Sym y{d_sfirst_, d_rows_, d_relmap_, d_child_ptr_, d_child_list_, d_rowptr_, d_frontptr_,
+          d_gptr_, d_cbnd_, d_cbnd_ptr_};
     for (const MfLaunch &L : launches_) {
         const int4 *tk = d_tasks_ + L.off;
         const unsigned nb = (unsigned)L.count;
@@ -1538,24 +1755,21 @@ void MultifrontalPlan::launch_factor(const double *d_val, cudaStream_t st) {
                     tk, (int)nb, y, d_front_, d_G_, d_acolptr_, d_atpos_, d_asrc_, d_val, d_params_,
                     d_status_);
                 break;
-            case MF_POTRF:
-                mf_potrf<<<(nb + kPotrfWarps - 1) / kPotrfWarps, 32 * kPotrfWarps, 0, st>>>(
-                    tk, (int)nb, y, d_front_, d_G_, d_params_, d_status_);
-                break;
-            case MF_TRSM:
-                mf_trsm<<<nb, kFThreads, 0, st>>>(tk, y, d_front_, d_G_, d_status_);
+            case MF_PANEL:
+                mf_panel64<<<nb, kGThreads, kPanelSmem, st>>>(tk, y, d_front_, d_G_, d_params_,
+                                                               d_status_);
                 break;
             case MF_UPDATE:
-                mf_update<<<nb, kFThreads, 0, st>>>(tk, y, d_front_, d_status_);
+                mf_update64<<<nb, kGThreads, kPairSmem, st>>>(tk, y, d_front_, d_status_);
                 break;
             case MF_INV_T:
-                mf_inv_t<<<nb, kFThreads, 0, st>>>(tk, y, d_front_, d_G_, d_status_);
+                mf_inv_t64<<<nb, kGThreads, kPairSmem, st>>>(tk, y, d_front_, d_G_, d_status_);
                 break;
             case MF_INV_X:
-                mf_inv_x<<<nb, kFThreads, 0, st>>>(tk, y, d_front_, d_G_, d_status_);
+                mf_inv_x64<<<nb, kGThreads, kPairSmem, st>>>(tk, y, d_front_, d_G_, d_status_);
                 break;
             case MF_WMUL:
-                mf_wmul<<<nb, kFThreads, 0, st>>>(tk, y, d_front_, d_G_, d_status_);
+                mf_wmul64<<<nb, kGThreads, kPairSmem, st>>>(tk, y, d_front_, d_G_, d_status_);
                 break;
         }
     }

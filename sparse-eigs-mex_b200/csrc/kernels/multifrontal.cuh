@@ -25,7 +25,7 @@ namespace spx {
 
 constexpr int kTile = 32;
 
-enum MfTaskKind { MF_ASSEMBLE = 0, MF_POTRF, MF_TRSM, MF_UPDATE, MF_INV_T, MF_INV_X, MF_WMUL,
+enum MfTaskKind { MF_ASSEMBLE = 0, MF_PANEL, MF_UPDATE, MF_INV_T, MF_INV_X, MF_WMUL,
                   MF_TINY, MF_NKIND };
 
 struct MfLaunch {
@@ -79,6 +79,8 @@ private:
     int32_t *d_acolptr_ = nullptr;   // [n+1] assembly entries per new column
     int32_t *d_atpos_ = nullptr;     // row position within the front
     int32_t *d_asrc_ = nullptr;      // index into the CSR values
+    int32_t *d_cbnd_ = nullptr;      // child bounds per parent 32-row tile
+    int64_t *d_cbnd_ptr_ = nullptr;
     int4 *d_tasks_ = nullptr;
     std::vector<MfLaunch> launches_;
     // solve: per-level task offsets (4 lists), tasks, gather lists

@@ -88,6 +88,46 @@ def test_cholesky_solve_operator(lib, pkg, N, coef):
     P.close()
 
 
+@pytest.mark.parametrize("n", [65, 333, 1000])
+def test_cholesky_solve_dense_front(lib, pkg, n):
+    """A dense SPD matrix is one front with n pivots: many 64-column panel
+    steps, ragged edge tiles, and the tile-level inversion of L11."""
+    torch = pytest.importorskip("torch")
+    import scipy.sparse as sp
+    rng = np.random.default_rng(n)
+    B = rng.standard_normal((n, n))
+    Ad = B @ B.T / n + np.eye(n)
+    A = sp.csc_matrix(Ad)
+    P = pkg.Plan(A, which=pkg.speigs.SM, lib=lib)
+    rc, shift = P.factor()
+    assert rc == 0 and shift == 0.0
+    b = torch.randn(n, dtype=torch.float64, device="cuda")
+    x = torch.empty_like(b)
+    torch.cuda.synchronize()
+    assert P.apply_device(b.data_ptr(), x.data_ptr()) == 0
+    bh, xh = b.cpu().numpy(), x.cpu().numpy()
+    ref = np.linalg.solve(Ad, bh)
+    assert np.linalg.norm(xh - ref) / np.linalg.norm(ref) < 1e-11
+    P.close()
+
+
+def test_cholesky_solve_large_separators(lib, pkg):
+    """3-D Laplacian 40^3: separators of ~1,600 columns (25 panel steps)."""
+    torch = pytest.importorskip("torch")
+    import scipy.sparse.linalg as spla
+    A = pkg.workloads.lap3d(40)
+    P = pkg.Plan(A, which=pkg.speigs.SM, lib=lib)
+    rc, shift = P.factor()
+    assert rc == 0 and shift == 0.0
+    b = torch.randn(A.shape[0], dtype=torch.float64, device="cuda")
+    x = torch.empty_like(b)
+    torch.cuda.synchronize()
+    assert P.apply_device(b.data_ptr(), x.data_ptr()) == 0
+    bh, xh = b.cpu().numpy(), x.cpu().numpy()
+    assert np.linalg.norm(A @ xh - bh) / np.linalg.norm(bh) < 1e-12
+    P.close()
+
+
 def test_cholesky_not_pd_escalates(lib, pkg):
     """Singular PSD (Neumann) input: the first factorization fails on device,
     the capped escalation finds delta = 1e-6 ||A||_1 (reference :953-970)."""
