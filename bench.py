@@ -57,7 +57,7 @@ def workloads(w, s):
                           build=lambda: w.lap2d(1000), k=6, which=s.LM,
                           exact=lambda: w.spectrum2d_extreme(1000, 6, True)),
         "varcoef64": dict(desc="3-D variable-coefficient FV diffusion 64^3 (n=262,144), log-normal "
-                               "conductivity (sigma=1, seed 3), k=20 'sm', plain FP64, tol 1e-10",
+                               "conductivity (sigma=1, seed 3), k=20 'sm', tol 1e-10",
                           build=lambda: w.varcoef3d(64, seed=3), k=20, which=s.SM, exact=None),
     }
 
@@ -180,6 +180,11 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="lap46")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                    help="operator of the timed line: plain FP64 factor, or FP32 factor on the "
+                         "tensor cores with FP64 refinement")
+    ap.add_argument("--no-compare", action="store_true",
+                    help="skip the side-by-side measurement of the other precision")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -208,111 +213,154 @@ def main():
     A = wl["build"]()
     n, k = A.shape[0], wl["k"]
     opts = s.default_opts(lib, tol=TOL)
-    plan = s.Plan(A, wl["which"], opts, lib=lib)
-    pstream = torch.cuda.ExternalStream(plan.stream(), device=dev)
-    lam = torch.zeros(k, dtype=torch.float64, device=dev)
-    V = torch.zeros((k, n), dtype=torch.float64, device=dev)    # column-major n x k
-    res = torch.zeros(k, dtype=torch.float64, device=dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    peak, peak_kind = measured_peaks()
 
-    def solve():
-        rc, info = plan.solve_device(k, lam.data_ptr(), V.data_ptr(), res.data_ptr())
-        if rc != 0:
-            raise RuntimeError(f"solve rc={rc}: {s.last_error(lib)}")
-        return info
+    def measure(precision, steps, with_clocks):
+        """Time `steps` full solves of one form on the device, then its operator,
+        then the drop-in call end to end."""
+        prec = s.MIXED if precision == "mixed" else s.FP64
+        ext = s.ext_opts(lib, precision=prec)
+        plan = s.Plan(A, wl["which"], opts, lib=lib, ext=ext)
+        pstream = torch.cuda.ExternalStream(plan.stream(), device=dev)
+        lam = torch.zeros(k, dtype=torch.float64, device=dev)
+        V = torch.zeros((k, n), dtype=torch.float64, device=dev)    # column-major n x k
+        res = torch.zeros(k, dtype=torch.float64, device=dev)
 
-    torch.cuda.synchronize()
-    for _ in range(args.warmup):
-        info = solve()
-    # ---- timed region: device time per solve, L2 flushed between steps
-    sampler = ClockSampler()
-    sampler.start()
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    l0 = s.counters(lib)[0]
-    step_ms = []
-    for _ in range(args.steps):
-        flush.zero_()
+        def solve():
+            rc, info = plan.solve_device(k, lam.data_ptr(), V.data_ptr(), res.data_ptr())
+            if rc != 0:
+                raise RuntimeError(f"solve rc={rc}: {s.last_error(lib)}")
+            return info
+
         torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(pstream)
-        info = solve()
-        e1.record(pstream)
-        e1.synchronize()
-        step_ms.append(e0.elapsed_time(e1))
-    torch.cuda.synchronize()
-    launches = s.counters(lib)[0] - l0
-    if world > 1:
-        dist.barrier()
-    clocks = sampler.stop(gpu_index=None)
-    ms = statistics.mean(step_ms)
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        for _ in range(args.warmup):
+            info = solve()
+        # ---- timed region: device time per solve, L2 flushed between steps
+        sampler = ClockSampler()
+        if with_clocks:
+            sampler.start()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        l0 = s.counters(lib)[0]
+        step_ms = []
+        for _ in range(steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(pstream)
+            info = solve()
+            e1.record(pstream)
+            e1.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+        torch.cuda.synchronize()
+        launches = (s.counters(lib)[0] - l0) // max(steps, 1)
+        if world > 1:
+            dist.barrier()
+        clocks = sampler.stop(gpu_index=None) if with_clocks else None
+        einfo = plan.ext_info()
+        ms = statistics.mean(step_ms)
+        lam_h = lam.cpu().numpy()
+        Vh = V.cpu().numpy().T
+
+        # ---- the operator (the dominant kernel: the solve pair, or the SpMV)
+        costs = plan.costs()
+        x = torch.randn(n, dtype=torch.float64, device=dev)
+        y = torch.empty_like(x)
+        torch.cuda.synchronize()
+        for _ in range(3):
+            plan.apply_device(x.data_ptr(), y.data_ptr())
+        op_ms = []
+        for _ in range(20):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(pstream)
+            plan.apply_device(x.data_ptr(), y.data_ptr())
+            e1.record(pstream)
+            e1.synchronize()
+            op_ms.append(e0.elapsed_time(e1))
+        plan.close()
+
+        # ---- end to end through the drop-in API: host CSC in, host results out
+        e2e_t = []
+        c0 = s.counters(lib)
+        for _ in range(steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            rc, l2, V2, r2, inf2, ei2 = s.speigs_ex(A, k, wl["which"], opts, ext, vectors=True,
+                                                    lib=lib)
+            e2e_t.append(time.perf_counter() - t0)
+            if rc != 0:
+                raise RuntimeError(f"speigs rc={rc}")
+        c1 = s.counters(lib)
+        e2e = {"value": statistics.mean(e2e_t), "unit": "s",
+               "h2d_bytes_per_step": (c1[1] - c0[1]) // steps,
+               "d2h_bytes_per_step": (c1[2] - c0[2]) // steps,
+               "phase_s": {kk: inf2[kk] for kk in ("t_analyze", "t_factor", "t_iter")}}
+        return dict(ms=ms, step_ms=step_ms, info=info, einfo=einfo, lam=lam_h, V=Vh,
+                    launches=launches, clocks=clocks, costs=costs,
+                    op_s=statistics.mean(op_ms) * 1e-3, e2e=e2e)
+
+    main_m = measure(args.precision, args.steps, True)
+    t = torch.tensor([main_m["ms"]], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms = float(t.item())
+    info = main_m["info"]
 
     # ---- correctness of the timed result
-    lam_h = lam.cpu().numpy()
-    Vh = V.cpu().numpy().T
+    lam_h, Vh = main_m["lam"], main_m["V"]
     resid = np.linalg.norm(A @ Vh - Vh * lam_h, axis=0)
     check = {"max_resid_over_anorm": float(resid.max() / info["anorm"]),
              "nops": int(info["nops"]), "restarts": int(info["restarts"]),
-             "shift": info["shift"], "flag": int(info["flag"])}
+             "shift": info["shift"], "flag": int(info["flag"]),
+             "refine_steps": int(main_m["einfo"]["refine_steps"])}
     if wl["exact"] is not None:
         ex = wl["exact"]()
         check["max_rel_err_vs_closed_form"] = float(np.max(np.abs(lam_h - ex) / np.abs(ex)))
 
-    # ---- roofline of the dominant kernel: the operator application
-    costs = plan.costs()
-    x = torch.randn(n, dtype=torch.float64, device=dev)
-    y = torch.empty_like(x)
-    torch.cuda.synchronize()
-    for _ in range(3):
-        plan.apply_device(x.data_ptr(), y.data_ptr())
-    op_ms = []
-    for _ in range(20):
-        flush.zero_()
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(pstream)
-        plan.apply_device(x.data_ptr(), y.data_ptr())
-        e1.record(pstream)
-        e1.synchronize()
-        op_ms.append(e0.elapsed_time(e1))
-    op_s = statistics.mean(op_ms) * 1e-3
-    peak, peak_kind = measured_peaks()
-    achieved = costs["op_bytes"] / op_s / 1e9
+    # ---- roofline of the dominant kernel: the operator application.  For
+    # the mixed form the algorithmic bytes are those of every FP32 solve pair
+    # and FP64 residual the refined application performs.
+    costs = main_m["costs"]
+    op_bytes = costs["op_bytes"]
+    if args.precision == "mixed" and info["nops"] > 0:
+        per_app = 1.0 + main_m["einfo"]["refine_steps"] / info["nops"]
+        nnz = float(A.nnz)
+        op_bytes = costs["op_bytes"] * per_app + per_app * (12.0 * nnz + 40.0 * n)
+    achieved = op_bytes / main_m["op_s"] / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         try:
-            traffic = json.load(open(tpath)).get(args.workload)
+            traffic = json.load(open(tpath)).get(f"{args.workload}:{args.precision}")
         except Exception:
             traffic = None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic,
-                "kernel": "shift-invert solve pair (forward+backward multifrontal GEMV levels)"
+                "kernel": ("shift-invert solve pair (task-queue multifrontal solve)"
+                           + (", FP32 panels + FP64 refinement" if args.precision == "mixed" else ""))
                 if wl["which"] == s.SM else "CSR SpMV",
-                "op_ms": op_s * 1e3, "op_bytes": costs["op_bytes"], "peak_source": peak_kind}
+                "op_ms": main_m["op_s"] * 1e3, "op_bytes": op_bytes, "peak_source": peak_kind}
 
-    # ---- end to end through the drop-in API: host CSC in, host results out
-    e2e_t = []
-    c0 = s.counters(lib)
-    for _ in range(args.steps):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        rc, l2, V2, r2, inf2 = s.speigs(A, k, wl["which"], opts, vectors=True, lib=lib)
-        e2e_t.append(time.perf_counter() - t0)
-        if rc != 0:
-            raise RuntimeError(f"speigs rc={rc}")
-    c1 = s.counters(lib)
-    e2e = {"value": statistics.mean(e2e_t), "unit": "s",
-           "h2d_bytes_per_step": (c1[1] - c0[1]) // args.steps,
-           "d2h_bytes_per_step": (c1[2] - c0[2]) // args.steps,
-           "phase_s": {kk: inf2[kk] for kk in ("t_analyze", "t_factor", "t_iter")}}
+    # ---- the other precision on the same workload, same B200 (the metric's
+    # comparison), with the per-eigenpair error between the two forms
+    compare = None
+    if wl["which"] == s.SM and not args.no_compare and world == 1:
+        other = "mixed" if args.precision == "fp64" else "fp64"
+        om = measure(other, max(2, min(args.steps, 3)), False)
+        fp64_lam = om["lam"] if other == "fp64" else lam_h
+        mixed_lam = lam_h if other == "fp64" else om["lam"]
+        compare = {"precision": other, "value": om["ms"] * 1e-3, "unit": "s",
+                   "e2e": om["e2e"]["value"], "nops": int(om["info"]["nops"]),
+                   "refine_steps": int(om["einfo"]["refine_steps"]),
+                   "mixed_over_fp64_value": (om["ms"] / ms) if other == "mixed" else (ms / om["ms"]),
+                   "eig_rel_err_mixed_vs_fp64": [float(abs(a - b) / abs(b))
+                                                 for a, b in zip(mixed_lam, fp64_lam)]}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_LIB):
@@ -330,17 +378,19 @@ def main():
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
             "config": {"workload": wl["desc"], "n": int(n), "nnz": int(A.nnz), "k": k, "tol": TOL,
-                       "precision": "plain FP64", "parallelism": f"replicas x{world}",
+                       "precision": "plain FP64" if args.precision == "fp64" else
+                       "mixed: FP32 factor (TF32 tensor-core updates) + FP64 refinement",
+                       "parallelism": f"replicas x{world}",
                        "l2": "256 MiB buffer written between timed steps",
                        "value_scope": "numeric factor + Lanczos, matrix and analysis resident"},
-            "check": check, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": int(launches), "clocks": clocks,
-            "step_ms": [round(x, 3) for x in step_ms],
+            "check": check, "roofline": roofline, "cpu_baseline": cpu, "e2e": main_m["e2e"],
+            "gpu_launches": int(main_m["launches"]), "clocks": main_m["clocks"],
+            "step_ms": [round(x, 3) for x in main_m["step_ms"]],
             "phase_s": {kk: info[kk] for kk in ("t_factor", "t_iter", "t_op", "t_ortho",
                                                 "t_resid", "t_ritz")},
+            "compare": compare,
         }
         print(json.dumps(line))
-    plan.close()
     if world > 1:
         dist.destroy_process_group()
     return 0

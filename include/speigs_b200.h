@@ -17,6 +17,44 @@
 extern "C" {
 #endif
 
+/* ---- extension options: precision of the shift-invert operator ------------
+ * SPEIGS_B200_FP64: the drop-in path, an FP64 supernodal factor.
+ * SPEIGS_B200_MIXED ('sm' only): the factor is stored in FP32 and its
+ * trailing updates run on the TF32 tensor cores with an FP32-accurate
+ * three-term split; every solve is refined in FP64 (r = b - (A+dI)y,
+ * y += M^{-1} r) until ||r|| <= refine_tol * (||A||_1 ||y|| + ||b||) or
+ * refine_max corrections were made.  The Lanczos recurrence, the
+ * reorthogonalisation, the Ritz problem and the residuals stay FP64.
+ * No counterpart in the reference interface. */
+#define SPEIGS_B200_FP64  0
+#define SPEIGS_B200_MIXED 1
+
+typedef struct {
+    int          precision;    /* SPEIGS_B200_FP64 (default) or SPEIGS_B200_MIXED     */
+    int          refine_max;   /* corrections per solve (mixed); 0 => 10               */
+    double       refine_tol;   /* backward-error target (mixed); 0 => 1e-14            */
+    const double *warm;        /* optional start subspace, n x warm_cols, column-major,
+                                  host memory; NULL => the reference's random start   */
+    speigs_int   warm_cols;
+} speigs_ext_opts;
+
+typedef struct {
+    int          precision;      /* precision actually used                         */
+    speigs_int   refine_steps;   /* FP64 refinement corrections made (mixed)        */
+    speigs_int   factor_solves;  /* solves with the factor: applications + corrections */
+    speigs_int   warm_cols;      /* start-subspace columns used (0: random start)   */
+} speigs_ext_info;
+
+/* Fill *e with the defaults (FP64, no start subspace). */
+void speigs_default_ext_opts(speigs_ext_opts *e);
+
+/* speigs() with extension options; ext == NULL is speigs() itself.  einfo
+ * (may be NULL) receives the extension diagnostics of the Krylov route. */
+int speigs_ex(speigs_int n, const speigs_int *Ap, const speigs_int *Ai, const double *Ax,
+              speigs_int k, speigs_which which, const speigs_opts *opts,
+              const speigs_ext_opts *ext, double *lambda, double *V, double *resid,
+              speigs_info *info, speigs_ext_info *einfo);
+
 /* Opaque solver plan: one connected symmetric matrix on one GPU, with its
  * operator ('sm': symbolic analysis done, numeric factor per solve; 'lm':
  * the matrix itself) and every device buffer the Lanczos iteration needs.
@@ -31,6 +69,15 @@ typedef struct speigs_plan_s *speigs_plan;
 int speigs_plan_create(speigs_int n, const speigs_int *Ap, const speigs_int *Ai,
                        const double *Ax, speigs_which which, const speigs_opts *opts,
                        speigs_plan *plan);
+
+/* speigs_plan_create with extension options (precision; the start subspace
+ * is taken per solve from ext->warm when given here). */
+int speigs_plan_create_ex(speigs_int n, const speigs_int *Ap, const speigs_int *Ai,
+                          const double *Ax, speigs_which which, const speigs_opts *opts,
+                          const speigs_ext_opts *ext, speigs_plan *plan);
+
+/* Extension diagnostics of the plan's last solve. */
+int speigs_plan_ext_info(speigs_plan plan, speigs_ext_info *einfo);
 
 /* New values for the same pattern.  Ax follows the CSC given at creation
  * (host pointer); only the upper triangle is read. */

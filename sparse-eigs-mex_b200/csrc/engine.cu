@@ -185,6 +185,38 @@ struct DevA {
     const double *va;
 };
 
+// The numeric factor in the storage precision the plan was created with:
+// FP64 (the drop-in operator) or FP32 (mixed precision, refined in FP64).
+struct Factor {
+    MultifrontalPlan f64;
+    MultifrontalPlan32 f32;
+    bool mixed = false;
+    int init(const spx_symbolic &S, const int64_t *rp, const int32_t *ci, cudaStream_t st) {
+        return mixed ? f32.init(S, rp, ci, st) : f64.init(S, rp, ci, st);
+    }
+    int factorize(const double *val, double shift, double pivtol, cudaStream_t st) {
+        return mixed ? f32.factorize(val, shift, pivtol, st) : f64.factorize(val, shift, pivtol, st);
+    }
+    void solve(const double *b, double *x, cudaStream_t st, const int *skip = nullptr) {
+        if (mixed) f32.solve(b, x, st, skip);
+        else f64.solve(b, x, st, skip);
+    }
+    int *error_word() const { return mixed ? f32.error_word() : f64.error_word(); }
+    double factor_flops() const { return mixed ? f32.factor_flops() : f64.factor_flops(); }
+    int64_t solve_bytes() const { return mixed ? f32.solve_bytes() : f64.solve_bytes(); }
+    int64_t panel_entries() const { return mixed ? f32.panel_entries() : f64.panel_entries(); }
+    void release(cudaStream_t st) { f64.release(st); f32.release(st); }
+};
+
+// Device state of the FP64 refinement of a mixed-precision solve.
+struct RefineState {
+    double *r = nullptr, *d = nullptr;
+    int *flag = nullptr, *count = nullptr;
+    ReduceScratch rs;
+    int max_steps = 10;
+    double tol = 1e-14;
+};
+
 struct SpmvOperator : Operator {
     DevA A;
     explicit SpmvOperator(const DevA &a) : A(a) {}
@@ -195,11 +227,38 @@ struct SpmvOperator : Operator {
 };
 
 struct CholOperator : Operator {
-    MultifrontalPlan *plan;
-    explicit CholOperator(MultifrontalPlan *p) : plan(p) {}
+    Factor *plan;
+    explicit CholOperator(Factor *p) : plan(p) {}
     void apply(const double *x, double *y, cudaStream_t st) override {
         nops++;
         plan->solve(x, y, st);
+    }
+    const int *error_word() const override { return plan->error_word(); }
+};
+
+// Mixed precision: y = (A + shift I)^{-1} x with the FP32 factor, refined
+// in FP64 -- r = x - (A + shift I) y, y += M^{-1} r -- until the backward
+// error test of launch_refine_residual holds or max_steps corrections were
+// made.  The loop is launched in full every time; steps after convergence
+// return at once on the device flag, so the host never waits.
+struct MixedCholOperator : Operator {
+    Factor *plan;
+    DevA A;
+    double shift, anorm;
+    RefineState *rf;
+    MixedCholOperator(Factor *p, const DevA &a, double sh, double an, RefineState *r)
+        : plan(p), A(a), shift(sh), anorm(an), rf(r) {}
+    void apply(const double *x, double *y, cudaStream_t st) override {
+        nops++;
+        plan->solve(x, y, st);
+        cudaMemsetAsync(rf->flag, 0, sizeof(int), st);
+        for (int it = 0; it <= rf->max_steps; it++) {
+            launch_refine_residual(A.n, A.rp, A.ci, A.va, shift, x, y, rf->r, rf->tol, anorm,
+                                   rf->flag, rf->count, rf->rs, st);
+            if (it == rf->max_steps) break;
+            plan->solve(rf->r, rf->d, st, rf->flag);
+            launch_axpy_unless(A.n, y, rf->d, rf->flag, st);
+        }
     }
     const int *error_word() const override { return plan->error_word(); }
 };
@@ -543,7 +602,14 @@ struct speigs_plan_s {
     bool factored = false;
     int32_t *d_rp = nullptr, *d_ci = nullptr;
     double *d_va = nullptr;
-    spx::MultifrontalPlan mf;
+    spx::Factor mf;
+    spx::RefineState refine;          // mixed precision only
+    int64_t refine_reported = 0;      // corrections already reported
+    int64_t last_refine = 0;          // corrections of the last solve
+    int64_t last_ops = 0;             // operator applications of the last solve
+    const double *ext_warm = nullptr; // start subspace (host, n x ext_warm_cols)
+    int64_t ext_warm_cols = 0;
+    int64_t last_warm = 0;            // start-subspace columns used by the last solve
     double t_analyze = 0;
     std::vector<void *> owned;
     double *pinned = nullptr;        // host scalars read back during a solve
@@ -572,7 +638,7 @@ static int plan_alloc(speigs_plan_s *p, void **ptr, size_t bytes) {
 
 // Build the plan from an already expanded full CSR (takes ownership of A).
 int plan_from_csr(HostCSR &A, speigs_which which, const speigs_opts &o, double anorm,
-                  speigs_plan_s **out) {
+                  const speigs_ext_opts *ext, speigs_plan_s **out) {
     g_err[0] = 0;
     int ndev = 0;
     cudaError_t e0 = cudaGetDeviceCount(&ndev);
@@ -588,6 +654,9 @@ int plan_from_csr(HostCSR &A, speigs_which which, const speigs_opts &o, double a
     p->which = which;
     p->opts = o;
     p->anorm = anorm;
+    p->mf.mixed = (which == SPEIGS_SM && ext && ext->precision == SPEIGS_B200_MIXED);
+    if (ext && ext->refine_max > 0) p->refine.max_steps = ext->refine_max;
+    if (ext && ext->refine_tol > 0) p->refine.tol = ext->refine_tol;
     if (p->stream.err != cudaSuccess) { int rc = cuda_fail(p->stream.err, "stream"); speigs_plan_destroy(p); return rc; }
     cudaStream_t st = p->stream.s;
     const int n = p->A.n;
@@ -614,6 +683,21 @@ int plan_from_csr(HostCSR &A, speigs_which which, const speigs_opts &o, double a
         spx_symbolic_free(&S);
         p->t_analyze = wall() - ta;
         if (rc) { speigs_plan_destroy(p); return rc; }
+        if (p->mf.mixed) {
+            RefineState &rf = p->refine;
+            const int nblk = (n + 127) / 128;
+            rc = rc ? rc : plan_alloc(p, (void **)&rf.r, sizeof(double) * n);
+            rc = rc ? rc : plan_alloc(p, (void **)&rf.d, sizeof(double) * n);
+            rc = rc ? rc : plan_alloc(p, (void **)&rf.flag, sizeof(int) * 2);
+            rc = rc ? rc : plan_alloc(p, (void **)&rf.count, sizeof(int) * 2);
+            rc = rc ? rc : plan_alloc(p, (void **)&rf.rs.part, sizeof(double) * 3 * (size_t)nblk);
+            rc = rc ? rc : plan_alloc(p, (void **)&rf.rs.counter, sizeof(unsigned) * 2);
+            if (rc) { speigs_plan_destroy(p); return rc; }
+            rf.rs.max_blocks = nblk;
+            rf.rs.max_cols = 3;
+            cudaMemsetAsync(rf.count, 0, sizeof(int) * 2, st);
+            cudaMemsetAsync(rf.rs.counter, 0, sizeof(unsigned) * 2, st);
+        }
     }
     *out = p;
     return 0;
@@ -629,7 +713,8 @@ static int plan_factor(speigs_plan_s *p, EngineStats *stats) {
     // A pivot that is rounding noise on the scale of ||A||_1 is treated as
     // not positive, so an exactly singular PSD matrix takes the shift route
     // deterministically instead of by the sign of its last rounding error.
-    const double pivtol = 128.0 * 2.220446049250313e-16 * p->anorm;
+    const double pivtol = 128.0 * (p->mf.mixed ? 1.1920928955078125e-07 : 2.220446049250313e-16) *
+                          p->anorm;
     int fr = p->mf.factorize(p->d_va, 0.0, pivtol, st);
     int attempts = 1;
     if (fr == 1) {
@@ -676,6 +761,7 @@ static int plan_solve(speigs_plan_s *p, int64_t k, double *lambda, double *V, do
     DevA dA{n, p->d_rp, p->d_ci, p->d_va};
     SpmvOperator spmv_op(dA);
     CholOperator chol_op(&p->mf);
+    MixedCholOperator mixed_op(&p->mf, dA, 0.0, p->anorm, &p->refine);
     Operator *op = &spmv_op;
     if (p->which == SPEIGS_LM) {
         info->path = SPEIGS_PATH_DIRECT;
@@ -684,7 +770,8 @@ static int plan_solve(speigs_plan_s *p, int64_t k, double *lambda, double *V, do
         int rc = plan_factor(p, stats);
         info->t_factor = wall() - tf;
         if (rc) return rc;
-        op = &chol_op;
+        mixed_op.shift = p->shift;
+        op = p->mf.mixed ? (Operator *)&mixed_op : (Operator *)&chol_op;
         info->shift = p->shift;
         info->path = SPEIGS_PATH_SHIFTINV;
     }
@@ -710,6 +797,17 @@ static int plan_solve(speigs_plan_s *p, int64_t k, double *lambda, double *V, do
         const double ti = wall();
         rc = lanczos_device(*op, dA, n, k, p->opts, p->anorm, lam_h.data(), res_h.data(), &X,
                             &ldx, &nout, info, stats, ar, p->pinned, st);
+        p->last_ops = op->nops;
+        if (rc == 0 && p->mf.mixed) {
+            int cnt = 0;
+            cudaMemcpyAsync(&cnt, p->refine.count, sizeof(int), cudaMemcpyDeviceToHost, st);
+            note_d2h(sizeof(int));
+            cudaStreamSynchronize(st);
+            p->last_refine = cnt - p->refine_reported;
+            p->refine_reported = cnt;
+        } else {
+            p->last_refine = 0;
+        }
         if (rc == 0) {
             // sort by |lambda|: ascending for 'sm', descending for 'lm'
             // (reference :994-1012); entries past nout keep the caller's memory
@@ -741,13 +839,25 @@ static int plan_solve(speigs_plan_s *p, int64_t k, double *lambda, double *V, do
     return rc;
 }
 
+static void fill_ext_info(const speigs_plan_s *p, speigs_ext_info *e) {
+    if (!e) return;
+    memset(e, 0, sizeof *e);
+    e->precision = p->mf.mixed ? SPEIGS_B200_MIXED : SPEIGS_B200_FP64;
+    e->refine_steps = p->last_refine;
+    e->factor_solves = p->which == SPEIGS_SM ? p->last_ops + p->last_refine : 0;
+    e->warm_cols = p->last_warm;
+}
+
 int device_krylov(HostCSR &A, int64_t k, speigs_which which, const speigs_opts &o,
                   double anorm, double *lambda, double *V, double *resid, speigs_info *info,
-                  EngineStats *stats) {
+                  EngineStats *stats, const speigs_ext_opts *ext, speigs_ext_info *einfo) {
     speigs_plan_s *p = nullptr;
-    int rc = plan_from_csr(A, which, o, anorm, &p);
+    int rc = plan_from_csr(A, which, o, anorm, ext, &p);
     if (rc) return rc;
+    p->ext_warm = ext ? ext->warm : nullptr;
+    p->ext_warm_cols = ext ? ext->warm_cols : 0;
     rc = plan_solve(p, k, lambda, V, resid, info, false, stats);
+    fill_ext_info(p, einfo);
     speigs_plan_destroy(p);
     return rc;
 }
@@ -884,6 +994,24 @@ extern "C" {
 int speigs_plan_create(speigs_int n, const speigs_int *Ap, const speigs_int *Ai,
                        const double *Ax, speigs_which which, const speigs_opts *opts,
                        speigs_plan *plan) {
+    return speigs_plan_create_ex(n, Ap, Ai, Ax, which, opts, nullptr, plan);
+}
+
+void speigs_default_ext_opts(speigs_ext_opts *e) {
+    if (!e) return;
+    memset(e, 0, sizeof *e);
+    e->precision = SPEIGS_B200_FP64;
+}
+
+int speigs_plan_ext_info(speigs_plan p, speigs_ext_info *e) {
+    if (!p || !e) return SPEIGS_ERR_ARG;
+    spx::fill_ext_info(p, e);
+    return SPEIGS_OK;
+}
+
+int speigs_plan_create_ex(speigs_int n, const speigs_int *Ap, const speigs_int *Ai,
+                          const double *Ax, speigs_which which, const speigs_opts *opts,
+                          const speigs_ext_opts *ext, speigs_plan *plan) {
     if (!plan) return SPEIGS_ERR_ARG;
     *plan = nullptr;
     speigs_opts defo;
@@ -897,10 +1025,12 @@ int speigs_plan_create(speigs_int n, const speigs_int *Ap, const speigs_int *Ai,
     int rc = spx::build_full_csr(n, Ap, Ai, Ax, &A);
     if (rc) return rc;
     speigs_plan_s *p = nullptr;
-    rc = spx::plan_from_csr(A, which, *opts, anorm, &p);
+    rc = spx::plan_from_csr(A, which, *opts, anorm, ext, &p);
     if (rc) return rc;
     p->Ap_copy.assign(Ap, Ap + n + 1);
     p->Ai_copy.assign(Ai, Ai + Ap[n]);
+    p->ext_warm = ext ? ext->warm : nullptr;
+    p->ext_warm_cols = ext ? ext->warm_cols : 0;
     *plan = p;
     return SPEIGS_OK;
 }
@@ -945,7 +1075,13 @@ int speigs_plan_apply_device(speigs_plan p, const double *x, double *y) {
             int rc = spx::plan_factor(p, nullptr);
             if (rc) return rc;
         }
-        p->mf.solve(x, y, st);
+        if (p->mf.mixed) {
+            spx::DevA dA{p->A.n, p->d_rp, p->d_ci, p->d_va};
+            spx::MixedCholOperator op(&p->mf, dA, p->shift, p->anorm, &p->refine);
+            op.apply(x, y, st);
+        } else {
+            p->mf.solve(x, y, st);
+        }
     }
     int herr = 0;
     if (p->which == SPEIGS_SM && p->mf.error_word())

@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include "../../include/speigs.h"
+#include "../../include/speigs_b200.h"
 #include "host/symbolic.h"
 
 namespace spx {
@@ -37,9 +38,12 @@ struct EngineStats {
 // buffers; entries are written for the converged-or-final Ritz pairs, in the
 // Lanczos order (the caller sorts).  Returns 0 or SPEIGS_ERR_*.
 // A is consumed (its host arrays are freed by the call).
+// ext (may be NULL) selects the operator precision; einfo (may be NULL)
+// receives the extension diagnostics.
 int device_krylov(HostCSR &A, int64_t k, speigs_which which, const speigs_opts &o,
                   double anorm, double *lambda, double *V, double *resid, speigs_info *info,
-                  EngineStats *stats);
+                  EngineStats *stats, const speigs_ext_opts *ext = nullptr,
+                  speigs_ext_info *einfo = nullptr);
 
 // Host set-up helpers shared by the C API entry points (driver.cpp).
 int    host_check_symmetry(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *Ax);

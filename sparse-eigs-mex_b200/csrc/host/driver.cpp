@@ -8,6 +8,7 @@
 // Host work here is setup only (pattern checks, union-find, ordering); every
 // numerical step of every route runs on the GPU.
 #include "../engine.h"
+#include "../../../include/speigs_b200.h"
 
 #include <math.h>
 #include <stdlib.h>
@@ -115,11 +116,17 @@ double norm1_upper(int64_t n, const int64_t *Ap, const int64_t *Ai, const double
 
 struct Cand { double key; int64_t idx; };
 
+int speigs_impl(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *Ax, int64_t k,
+                speigs_which which, const speigs_opts *opts, const speigs_ext_opts *ext,
+                double *lambda, double *V, double *resid, speigs_info *info,
+                speigs_ext_info *einfo);
+
 // Solve every component separately and merge by |lambda| (reference
 // blocks_path, src/speigs_core.c:532-632).
 int blocks_path(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *Ax, int64_t k,
-                speigs_which which, const speigs_opts *opts, const std::vector<int64_t> &comp,
-                int64_t ncomp, double *lambda, double *V, double *resid, speigs_info *info) {
+                speigs_which which, const speigs_opts *opts, const speigs_ext_opts *ext,
+                const std::vector<int64_t> &comp, int64_t ncomp, double *lambda, double *V,
+                double *resid, speigs_info *info, speigs_ext_info *einfo) {
     std::vector<int64_t> sz(ncomp, 0), off(ncomp + 1, 0), gidx(n), loc(n), fill(ncomp, 0);
     for (int64_t i = 0; i < n; i++) sz[comp[i]]++;
     for (int64_t c = 0; c < ncomp; c++) off[c + 1] = off[c] + sz[c];
@@ -149,9 +156,15 @@ int blocks_path(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *A
         std::vector<double> lv(kc), rv(kc);
         if (V) cvec[ci].assign((size_t)nc * kc, 0.0);
         speigs_info si;
-        int r2 = speigs(nc, sAp.data(), sAi.data(), sAx.data(), kc, which, opts, lv.data(),
-                        V ? cvec[ci].data() : nullptr, rv.data(), &si);
+        speigs_ext_info se;
+        int r2 = speigs_impl(nc, sAp.data(), sAi.data(), sAx.data(), kc, which, opts, ext,
+                             lv.data(), V ? cvec[ci].data() : nullptr, rv.data(), &si, &se);
         if (r2) return r2;
+        if (einfo) {
+            einfo->refine_steps += se.refine_steps;
+            einfo->factor_solves += se.factor_solves;
+            if (se.precision) einfo->precision = se.precision;
+        }
         info->nops += si.nops;
         if (si.flag) info->flag = 1;
         for (int64_t t = 0; t < kc; t++) {
@@ -220,6 +233,27 @@ const char *speigs_errmsg(int c) {
 int speigs(speigs_int n, const speigs_int *Ap, const speigs_int *Ai, const double *Ax,
            speigs_int k, speigs_which which, const speigs_opts *opts, double *lambda, double *V,
            double *resid, speigs_info *info) {
+    return speigs_impl(n, Ap, Ai, Ax, k, which, opts, nullptr, lambda, V, resid, info, nullptr);
+}
+
+int speigs_ex(speigs_int n, const speigs_int *Ap, const speigs_int *Ai, const double *Ax,
+              speigs_int k, speigs_which which, const speigs_opts *opts,
+              const speigs_ext_opts *ext, double *lambda, double *V, double *resid,
+              speigs_info *info, speigs_ext_info *einfo) {
+    return speigs_impl(n, Ap, Ai, Ax, k, which, opts, ext, lambda, V, resid, info, einfo);
+}
+
+}  // extern "C"
+
+namespace {
+
+int speigs_impl(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *Ax, int64_t k,
+                speigs_which which, const speigs_opts *opts, const speigs_ext_opts *ext,
+                double *lambda, double *V, double *resid, speigs_info *info,
+                speigs_ext_info *einfo) {
+    speigs_ext_info le;
+    if (!einfo) einfo = &le;
+    memset(einfo, 0, sizeof *einfo);
     speigs_opts defo;
     if (!opts) { speigs_default_opts(&defo); opts = &defo; }
     speigs_info li;
@@ -250,7 +284,8 @@ int speigs(speigs_int n, const speigs_int *Ap, const speigs_int *Ai, const doubl
         std::vector<int64_t> comp;
         const int64_t ncomp = find_components(n, Ap, Ai, Ax, comp);
         if (ncomp > 1) {
-            int rc = blocks_path(n, Ap, Ai, Ax, k, which, opts, comp, ncomp, lambda, V, resid, info);
+            int rc = blocks_path(n, Ap, Ai, Ax, k, which, opts, ext, comp, ncomp, lambda, V, resid,
+                                 info, einfo);
             info->t_iter = wall() - t0;
             return rc;
         }
@@ -262,7 +297,8 @@ int speigs(speigs_int n, const speigs_int *Ap, const speigs_int *Ai, const doubl
     int rc = spx::build_full_csr(n, Ap, Ai, Ax, &A);
     if (rc) return rc;
     // factor + Lanczos on the device; results come back sorted by |lambda|
-    return spx::device_krylov(A, k, which, *opts, anorm, lambda, V, resid, info, nullptr);
+    return spx::device_krylov(A, k, which, *opts, anorm, lambda, V, resid, info, nullptr, ext,
+                              einfo);
 }
 
-}  // extern "C"
+}  // namespace

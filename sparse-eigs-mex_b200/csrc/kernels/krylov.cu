@@ -399,6 +399,84 @@ void launch_rayleigh_resid(int n, int nvec, const double *X, int64_t ldx, const 
     }
 }
 
+// ------------------------------------------------------- refinement ------
+// One block per 128 rows (the SpMV layout above); per-block partial sums of
+// ||r||^2, ||y||^2 and ||b||^2 are reduced by the last block to arrive, in a
+// fixed order, which then takes the convergence decision.
+__global__ void __launch_bounds__(kSpmvRows)
+refine_residual_kernel(int n, const int32_t *__restrict__ rp, const int32_t *__restrict__ ci,
+                       const double *__restrict__ va, double shift, const double *__restrict__ b,
+                       const double *__restrict__ y, double *__restrict__ r, double tol,
+                       double anorm, int *flag, int *count, double *part, unsigned *counter) {
+    __shared__ double red[32];
+    __shared__ double fin[3 * kSpmvRows];
+    __shared__ bool am_last;
+    if (*(volatile const int *)flag) return;
+    const int row = blockIdx.x * kSpmvRows + threadIdx.x;
+    double r2 = 0.0, y2 = 0.0, b2 = 0.0;
+    if (row < n) {
+        double s = 0.0;
+        for (int q = rp[row]; q < rp[row + 1]; q++) s += va[q] * __ldg(y + ci[q]);
+        const double yi = y[row], bi = b[row];
+        const double ri = bi - s - shift * yi;
+        r[row] = ri;
+        r2 = ri * ri;
+        y2 = yi * yi;
+        b2 = bi * bi;
+    }
+    r2 = block_sum(r2, red);
+    y2 = block_sum(y2, red);
+    b2 = block_sum(b2, red);
+    if (threadIdx.x == 0) {
+        part[(size_t)blockIdx.x * 3 + 0] = r2;
+        part[(size_t)blockIdx.x * 3 + 1] = y2;
+        part[(size_t)blockIdx.x * 3 + 2] = b2;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) am_last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (!am_last) return;
+    __threadfence();
+    // fixed-order reduction: thread t sums blocks t, t+128, ... per column
+    for (int c = 0; c < 3; c++) {
+        double acc = 0.0;
+        for (int bk = threadIdx.x; bk < (int)gridDim.x; bk += blockDim.x)
+            acc += ((volatile double *)part)[(size_t)bk * 3 + c];
+        fin[c * kSpmvRows + threadIdx.x] = acc;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t[3] = {0.0, 0.0, 0.0};
+        for (int c = 0; c < 3; c++)
+            for (int i = 0; i < (int)blockDim.x; i++) t[c] += fin[c * kSpmvRows + i];
+        if (sqrt(t[0]) <= tol * (anorm * sqrt(t[1]) + sqrt(t[2]))) *flag = 1;
+        else *count += 1;
+        *counter = 0u;
+    }
+}
+
+void launch_refine_residual(int n, const int32_t *rowptr, const int32_t *col, const double *val,
+                            double shift, const double *b, const double *y, double *r,
+                            double tol, double anorm, int *flag, int *count,
+                            const ReduceScratch &rs, cudaStream_t st) {
+    const int nb = (n + kSpmvRows - 1) / kSpmvRows;
+    refine_residual_kernel<<<nb, kSpmvRows, 0, st>>>(n, rowptr, col, val, shift, b, y, r, tol,
+                                                     anorm, flag, count, rs.part, rs.counter);
+    note_launch();
+}
+
+__global__ void axpy_unless_kernel(int n, double *y, const double *d, const int *flag) {
+    if (*(volatile const int *)flag) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        y[i] += d[i];
+}
+void launch_axpy_unless(int n, double *y, const double *d, const int *flag, cudaStream_t st) {
+    const int nb = std::max(1, std::min(4096, (n + 255) / 256));
+    axpy_unless_kernel<<<nb, 256, 0, st>>>(n, y, d, flag);
+    note_launch();
+}
+
 // ------------------------------------------------------------ RNG ------
 // xorshift64* (reference src/speigs_core.c:49-54).  The state update is
 // linear over GF(2), so the state after s steps is M^s applied to the seed;

@@ -79,6 +79,18 @@ void launch_set_diag(int ldh, int nd, const double *d, double *H, cudaStream_t s
 void launch_set_beta(double *H, int ldh, int r, int c, const double *nrm2, int zero,
                      cudaStream_t st);
 
+// Iterative refinement of a solve with a lower-precision factor:
+//   r = b - (A + shift I) y, and flag <- 1 once
+//   ||r|| <= tol * (anorm ||y|| + ||b||)   (a backward-error test);
+// while the flag is 0 every evaluation adds one to *count (a correction
+// follows).  Does nothing when *flag is already set.
+void launch_refine_residual(int n, const int32_t *rowptr, const int32_t *col, const double *val,
+                            double shift, const double *b, const double *y, double *r,
+                            double tol, double anorm, int *flag, int *count,
+                            const ReduceScratch &rs, cudaStream_t st);
+// y += d unless *flag
+void launch_axpy_unless(int n, double *y, const double *d, const int *flag, cudaStream_t st);
+
 // generic helpers
 void launch_copy(int64_t n, const double *src, double *dst, cudaStream_t st);
 void launch_fill(int64_t n, double v, double *dst, cudaStream_t st);

@@ -25,9 +25,22 @@ namespace cg = cooperative_groups;
 #include <cstring>
 #include <new>
 
+#include <type_traits>
+
 #include "../../../include/speigs.h"
 
+// Storage type of the fronts and panels; this file is compiled once for
+// double (plain FP64 operator) and once for float (mixed precision).
+#ifndef SPX_REAL
+#define SPX_REAL double
+#endif
+
 namespace spx {
+
+using Real = SPX_REAL;
+// G panels: leading dimension and offsets in multiples of 16 bytes, the
+// granularity of the bulk copies that stage them in the solve
+constexpr int kLdgA = (int)(16 / sizeof(Real));
 
 // memory pool of the device (engine.cu): allocations are cached across calls
 cudaMemPool_t device_pool(int dev);
@@ -49,7 +62,7 @@ struct Sym {
 struct Front {
     int64_t fptr, gptr;
     int r, c, nkb, nt, first;
-    int ldg;          // leading dimension of the G panel: r rounded up to even
+    int ldg;          // leading dimension of the G panel: r rounded up to 16 bytes
 };
 
 // Front geometry with tiles of TS rows/columns: pivot tiles first, then the
@@ -64,7 +77,7 @@ SPX_DEV Front front_of(const Sym &y, int s) {
     f.nt = f.nkb + (f.r - f.c + TS - 1) / TS;
     f.fptr = y.frontptr[s];
     f.gptr = y.gptr[s];
-    f.ldg = (f.r + 1) & ~1;
+    f.ldg = (f.r + kLdgA - 1) & ~(kLdgA - 1);
     return f;
 }
 
@@ -76,7 +89,7 @@ SPX_DEV void tile_range(const Front &f, int I, int &a, int &b) {
 
 // ------------------------------------------------------------ assemble --
 __global__ void __launch_bounds__(kFThreads)
-mf_assemble(const int4 *__restrict__ tasks, Sym y, double *__restrict__ F,
+mf_assemble(const int4 *__restrict__ tasks, Sym y, Real *__restrict__ F,
             const int32_t *__restrict__ acolptr, const int32_t *__restrict__ atpos,
             const int32_t *__restrict__ asrc, const double *__restrict__ val,
             const double *__restrict__ params, const int *status) {
@@ -103,7 +116,7 @@ mf_assemble(const int4 *__restrict__ tasks, Sym y, double *__restrict__ F,
         const int hi = ib - ia, wj = jb - ja;
         (void)nb;
         if (hi > 0 && wj > 0) {
-            const double *U = F + y.frontptr[ch];
+            const Real *U = F + y.frontptr[ch];
             for (int t = threadIdx.x; t < hi * wj; t += blockDim.x) {
                 const int i = ia + t % hi, j = ja + t / hi;
                 if (i >= j)
@@ -124,10 +137,10 @@ mf_assemble(const int4 *__restrict__ tasks, Sym y, double *__restrict__ F,
         }
     }
     __syncthreads();
-    double *Fs = F + f.fptr;
+    Real *Fs = F + f.fptr;
     for (int t = threadIdx.x; t < T * T; t += blockDim.x) {
         const int i = t & (T - 1), j = t >> 5;
-        if (i < h && j < w) Fs[(int64_t)(ra + i) + (int64_t)(ca + j) * f.r] = S[i][j];
+        if (i < h && j < w) Fs[(int64_t)(ra + i) + (int64_t)(ca + j) * f.r] = (Real)S[i][j];
     }
 }
 
@@ -190,8 +203,8 @@ SPX_DEV void warp_tri_inverse(double (*M)[T + 1], const double *dinv, int c) {
 constexpr int kTinyWarps = 4;
 
 __global__ void __launch_bounds__(32 * kTinyWarps)
-mf_tiny_front(const int4 *__restrict__ tasks, int ntasks, Sym y, double *__restrict__ F,
-              double *__restrict__ G, const int32_t *__restrict__ acolptr,
+mf_tiny_front(const int4 *__restrict__ tasks, int ntasks, Sym y, Real *__restrict__ F,
+              Real *__restrict__ G, const int32_t *__restrict__ acolptr,
               const int32_t *__restrict__ atpos, const int32_t *__restrict__ asrc,
               const double *__restrict__ val, const double *__restrict__ params, int *status) {
     __shared__ double Ms[kTinyWarps][T][T + 1];
@@ -213,7 +226,7 @@ mf_tiny_front(const int4 *__restrict__ tasks, int ntasks, Sym y, double *__restr
         const int cch = y.sfirst[ch + 1] - y.sfirst[ch];
         const int nb = rch - cch;
         const int32_t *rm = y.relmap + y.rowptr[ch] + cch;
-        const double *U = F + y.frontptr[ch];
+        const Real *U = F + y.frontptr[ch];
         for (int e = lane; e < nb * nb; e += 32) {
             const int a2 = e % nb, b2 = e / nb;
             if (a2 >= b2) M[rm[a2]][rm[b2]] += U[(int64_t)(cch + a2) + (int64_t)(cch + b2) * rch];
@@ -228,22 +241,22 @@ mf_tiny_front(const int4 *__restrict__ tasks, int ntasks, Sym y, double *__restr
     __syncwarp();
     warp_cholesky(M, cols[wid], dinvs[wid], r, c, params[1], status, f.first);
     // update matrix (rows and columns c..r-1) for the parent's assembly
-    double *Fs = F + f.fptr;
+    Real *Fs = F + f.fptr;
     if (lane >= c && lane < r)
-        for (int k = c; k <= lane; k++) Fs[(int64_t)lane + (int64_t)k * r] = M[lane][k];
+        for (int k = c; k <= lane; k++) Fs[(int64_t)lane + (int64_t)k * r] = (Real)M[lane][k];
     const double *dinv = dinvs[wid];
     warp_tri_inverse(M, dinv, c);
-    double *Gs = G + f.gptr;
+    Real *Gs = G + f.gptr;
     if (lane < c) {
-        Gs[(int64_t)lane + (int64_t)lane * f.ldg] = dinv[lane];
-        for (int i = lane + 1; i < c; i++) Gs[(int64_t)i + (int64_t)lane * f.ldg] = M[lane][i];
+        Gs[(int64_t)lane + (int64_t)lane * f.ldg] = (Real)dinv[lane];
+        for (int i = lane + 1; i < c; i++) Gs[(int64_t)i + (int64_t)lane * f.ldg] = (Real)M[lane][i];
     }
     // W = L21 X: lane i >= c owns row i
     if (lane >= c && lane < r) {
         for (int j = 0; j < c; j++) {
             double acc = M[lane][j] * dinv[j];
             for (int t2 = j + 1; t2 < c; t2++) acc += M[lane][t2] * M[j][t2];
-            Gs[(int64_t)lane + (int64_t)j * f.ldg] = acc;
+            Gs[(int64_t)lane + (int64_t)j * f.ldg] = (Real)acc;
         }
     }
 }
@@ -281,35 +294,44 @@ SPX_DEV void cp_wait() {
     asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
     __syncthreads();
 }
+// one element of a tile: an asynchronous copy for FP64 storage, a load and
+// widening conversion for FP32 storage (zero when !valid)
+SPX_DEV void elem_copy(double *dst, const double *src, bool valid) { cp_async8(dst, src, valid); }
+SPX_DEV void elem_copy(double *dst, const float *src, bool valid) {
+    *dst = valid ? (double)*src : 0.0;
+}
 
 // s(i, j) = M(ra + i, ca + j) for i < h, j < w; zero elsewhere in the tile
-SPX_DEV void ftile_load(double *s, const double *M, int64_t ld, int ra, int h, int ca, int w) {
+template <class MT>
+SPX_DEV void ftile_load(double *s, const MT *M, int64_t ld, int ra, int h, int ca, int w) {
 #pragma unroll 8
     for (int q = 0; q < FT * FT / kGThreads; q++) {
         const int t = threadIdx.x + q * kGThreads;
         const int i = t & (FT - 1), j = t >> 6;
         const bool v = (i < h && j < w);
-        cp_async8(s + j * FLD + i, v ? M + (int64_t)(ra + i) + (int64_t)(ca + j) * ld : M, v);
+        elem_copy(s + j * FLD + i, v ? M + (int64_t)(ra + i) + (int64_t)(ca + j) * ld : M, v);
     }
 }
 // s(i, j) = M(ca + j, ra + i): the transpose of the stored block
-SPX_DEV void ftile_load_t(double *s, const double *M, int64_t ld, int ra, int h, int ca, int w) {
+template <class MT>
+SPX_DEV void ftile_load_t(double *s, const MT *M, int64_t ld, int ra, int h, int ca, int w) {
 #pragma unroll 8
     for (int q = 0; q < FT * FT / kGThreads; q++) {
         const int t = threadIdx.x + q * kGThreads;
         const int j = t & (FT - 1), i = t >> 6;
         const bool v = (i < h && j < w);
-        cp_async8(s + j * FLD + i, v ? M + (int64_t)(ca + j) + (int64_t)(ra + i) * ld : M, v);
+        elem_copy(s + j * FLD + i, v ? M + (int64_t)(ca + j) + (int64_t)(ra + i) * ld : M, v);
     }
 }
 // lower triangle of the w x w block at (a, a); zero elsewhere
-SPX_DEV void ftile_load_lower(double *s, const double *M, int64_t ld, int a, int w) {
+template <class MT>
+SPX_DEV void ftile_load_lower(double *s, const MT *M, int64_t ld, int a, int w) {
 #pragma unroll 8
     for (int q = 0; q < FT * FT / kGThreads; q++) {
         const int t = threadIdx.x + q * kGThreads;
         const int i = t & (FT - 1), j = t >> 6;
         const bool v = (i < w && j <= i);
-        cp_async8(s + j * FLD + i, v ? M + (int64_t)(a + i) + (int64_t)(a + j) * ld : M, v);
+        elem_copy(s + j * FLD + i, v ? M + (int64_t)(a + i) + (int64_t)(a + j) * ld : M, v);
     }
 }
 
@@ -350,8 +372,8 @@ SPX_DEV void warp_mma(Acc &acc, const double *As, const double *Bs, int kw, int 
 
 // M(ra + m, ca + n) = alpha * acc(m, n) (+ M when add), for m < h, n < w.
 // TRANS stores acc(m, n) at M(ca + n, ra + m) instead.
-template <bool TRANS>
-SPX_DEV void acc_store(const Acc &acc, double *M, int64_t ld, int ra, int h, int ca, int w,
+template <bool TRANS, class MT>
+SPX_DEV void acc_store(const Acc &acc, MT *M, int64_t ld, int ra, int h, int ca, int w,
                        double alpha, bool add) {
     const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
     const int wid = threadIdx.x >> 5, m0 = (wid & 1) * 32, n0 = (wid >> 1) * 32;
@@ -363,9 +385,9 @@ SPX_DEV void acc_store(const Acc &acc, double *M, int64_t ld, int ra, int h, int
             for (int e = 0; e < 2; e++) {
                 const int m = m0 + 8 * i + g, n = n0 + 8 * j + 2 * t + e;
                 if (m < h && n < w) {
-                    double *p = TRANS ? M + (int64_t)(ca + n) + (int64_t)(ra + m) * ld
-                                      : M + (int64_t)(ra + m) + (int64_t)(ca + n) * ld;
-                    *p = add ? *p + alpha * acc[i][j][e] : alpha * acc[i][j][e];
+                    MT *p = TRANS ? M + (int64_t)(ca + n) + (int64_t)(ra + m) * ld
+                                  : M + (int64_t)(ra + m) + (int64_t)(ca + n) * ld;
+                    *p = (MT)(add ? (double)*p + alpha * acc[i][j][e] : alpha * acc[i][j][e]);
                 }
             }
 }
@@ -497,8 +519,8 @@ SPX_DEV void chol_inv_rec(double *D, double *L, double *X, double *tmp, int w, d
 // tiles of a large front proceed in parallel; a small front's tiles share
 // one block.  task = (s, I0, nI, kb).
 __global__ void __launch_bounds__(kGThreads)
-mf_panel64(const int4 *__restrict__ tasks, Sym y, double *__restrict__ F,
-           double *__restrict__ G, const double *__restrict__ params, int *status) {
+mf_panel64(const int4 *__restrict__ tasks, Sym y, Real *__restrict__ F,
+           Real *__restrict__ G, const double *__restrict__ params, int *status) {
     extern __shared__ double fsm[];
     double *Ds = fsm, *Ls = fsm + kFTileDoubles, *Xs = fsm + 2 * kFTileDoubles;
     double *Ts = fsm + 3 * kFTileDoubles;
@@ -509,7 +531,7 @@ mf_panel64(const int4 *__restrict__ tasks, Sym y, double *__restrict__ F,
     int ka, kz;
     tile_range<FT>(f, kb, ka, kz);
     const int w = kz - ka;
-    double *Fs = F + f.fptr;
+    Real *Fs = F + f.fptr;
     ftile_load_lower(Ds, Fs, f.r, ka, w);
     cp_wait();
     chol_inv_rec<64>(Ds, Ls, Xs, Ts, w, params[1], status, f.first + ka, I0 == kb);
@@ -518,10 +540,11 @@ mf_panel64(const int4 *__restrict__ tasks, Sym y, double *__restrict__ F,
             // only inv(L_kk) is kept: nothing later reads a diagonal tile of
             // L, and the diagonal tile of F must stay as it is while the
             // other blocks of this step are still reading it
-            double *Gs = G + f.gptr;
+            Real *Gs = G + f.gptr;
             for (int t = threadIdx.x; t < FT * FT; t += blockDim.x) {
                 const int i = t & (FT - 1), j = t >> 6;
-                if (i < w && j <= i) Gs[(int64_t)(ka + i) + (int64_t)(ka + j) * f.ldg] = Xs[j * FLD + i];
+                if (i < w && j <= i)
+                    Gs[(int64_t)(ka + i) + (int64_t)(ka + j) * f.ldg] = (Real)Xs[j * FLD + i];
             }
             continue;
         }
@@ -538,11 +561,103 @@ mf_panel64(const int4 *__restrict__ tasks, Sym y, double *__restrict__ F,
     }
 }
 
+// ---- FP32 trailing update on the TF32 tensor cores (mixed precision) --
+// mma.sync m16n8k8 tf32 with FP32 accumulation; every operand is split into
+// a TF32 head and a TF32 tail (x = hi + lo) and the product is taken as
+// hi*hi + hi*lo + lo*hi, which keeps FP32 accuracy.  Tiles are FP32 in
+// shared memory with a leading dimension of 72 floats (conflict-free
+// fragment reads).
+constexpr int FLDF = 72;
+
+SPX_DEV void cp_async4(float *dst, const float *src, bool valid) {
+    const unsigned saddr = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(saddr), "l"(src),
+                 "r"(valid ? 4 : 0) : "memory");
+}
+SPX_DEV void ftile_load_f32(float *s, const float *M, int64_t ld, int ra, int h, int ca, int w) {
+#pragma unroll 8
+    for (int q = 0; q < FT * FT / kGThreads; q++) {
+        const int t = threadIdx.x + q * kGThreads;
+        const int i = t & (FT - 1), j = t >> 6;
+        const bool v = (i < h && j < w);
+        cp_async4(s + j * FLDF + i, v ? M + (int64_t)(ra + i) + (int64_t)(ca + j) * ld : M, v);
+    }
+}
+SPX_DEV uint32_t tf32_of(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+SPX_DEV void split_tf32(float x, uint32_t &hi, uint32_t &lo) {
+    hi = tf32_of(x);
+    lo = tf32_of(x - __uint_as_float(hi));
+}
+SPX_DEV void mma_tf32(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+        "{%8,%9}, {%0,%1,%2,%3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// F_IJ -= L_Ik L_Jk^T on FP32 tiles: warp tile 32 x 32 = 2 x 4 fragments
+SPX_DEV void update_tile_f32(float *Fs, int ld, int ra, int h, int ca, int w, int ka, int kw,
+                             float *As, float *Bs) {
+    ftile_load_f32(As, Fs, ld, ra, h, ka, kw);
+    ftile_load_f32(Bs, Fs, ld, ca, w, ka, kw);
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+    __syncthreads();
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    const int wid = threadIdx.x >> 5, m0 = (wid & 1) * 32, n0 = (wid >> 1) * 32;
+    if (m0 >= h || n0 >= w) return;
+    float acc[2][4][4];
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) acc[i][j][e] = 0.f;
+    const int kw8 = (kw + 7) & ~7;
+    for (int k = 0; k < kw8; k += 8) {
+        uint32_t ah[2][4], al[2][4], bh[4][2], bl[4][2];
+#pragma unroll
+        for (int i = 0; i < 2; i++) {
+            const int r = m0 + 16 * i + g;
+            split_tf32(As[(k + t) * FLDF + r], ah[i][0], al[i][0]);
+            split_tf32(As[(k + t) * FLDF + r + 8], ah[i][1], al[i][1]);
+            split_tf32(As[(k + t + 4) * FLDF + r], ah[i][2], al[i][2]);
+            split_tf32(As[(k + t + 4) * FLDF + r + 8], ah[i][3], al[i][3]);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int n = n0 + 8 * j + g;
+            split_tf32(Bs[(k + t) * FLDF + n], bh[j][0], bl[j][0]);
+            split_tf32(Bs[(k + t + 4) * FLDF + n], bh[j][1], bl[j][1]);
+        }
+#pragma unroll
+        for (int i = 0; i < 2; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                mma_tf32(acc[i][j], al[i], bh[j]);
+                mma_tf32(acc[i][j], ah[i], bl[j]);
+                mma_tf32(acc[i][j], ah[i], bh[j]);
+            }
+    }
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                const int m = m0 + 16 * i + g + 8 * (e >> 1), n = n0 + 8 * j + 2 * t + (e & 1);
+                if (m < h && n < w) Fs[(int64_t)(ra + m) + (int64_t)(ca + n) * ld] -= acc[i][j][e];
+            }
+}
+
 // F_IJ -= L_Ik L_Jk^T    task = (s, I, J, kb)
 __global__ void __launch_bounds__(kGThreads)
-mf_update64(const int4 *__restrict__ tasks, Sym y, double *__restrict__ F, const int *status) {
+mf_update64(const int4 *__restrict__ tasks, Sym y, Real *__restrict__ F, const int *status) {
     extern __shared__ double fsm[];
-    double *As = fsm, *Bs = fsm + kFTileDoubles;
     if (*(volatile const int *)status) return;
     const int4 tk = tasks[blockIdx.x];
     const int s = tk.x, I = tk.y, J = tk.z, kb = tk.w;
@@ -552,14 +667,20 @@ mf_update64(const int4 *__restrict__ tasks, Sym y, double *__restrict__ F, const
     tile_range<FT>(f, J, ca, cb);
     tile_range<FT>(f, kb, ka, kz);
     const int h = rb - ra, w = cb - ca, kw = kz - ka;
-    double *Fs = F + f.fptr;
-    ftile_load(As, Fs, f.r, ra, h, ka, kw);
-    ftile_load(Bs, Fs, f.r, ca, w, ka, kw);
-    cp_wait();
-    Acc acc;
-    acc_zero(acc);
-    warp_mma<true>(acc, As, Bs, (kw + 3) & ~3, h, w);
-    acc_store<false>(acc, Fs, f.r, ra, h, ca, w, -1.0, true);
+    Real *Fs = F + f.fptr;
+    if constexpr (std::is_same<Real, float>::value) {
+        float *As = reinterpret_cast<float *>(fsm), *Bs = As + FT * FLDF;
+        update_tile_f32(reinterpret_cast<float *>(Fs), f.r, ra, h, ca, w, ka, kw, As, Bs);
+    } else {
+        double *As = fsm, *Bs = fsm + kFTileDoubles;
+        ftile_load(As, Fs, f.r, ra, h, ka, kw);
+        ftile_load(Bs, Fs, f.r, ca, w, ka, kw);
+        cp_wait();
+        Acc acc;
+        acc_zero(acc);
+        warp_mma<true>(acc, As, Bs, (kw + 3) & ~3, h, w);
+        acc_store<false>(acc, Fs, f.r, ra, h, ca, w, -1.0, true);
+    }
 }
 
 // inv(L11) by recursive doubling over tile blocks.  After step l every
@@ -569,8 +690,8 @@ mf_update64(const int4 *__restrict__ tasks, Sym y, double *__restrict__ F, const
 //   X_CA = -X_C T         (mf_inv_x64)
 // task = (s, i, j, l): output tile (i, j), i in C, j in A.
 __global__ void __launch_bounds__(kGThreads)
-mf_inv_t64(const int4 *__restrict__ tasks, Sym y, double *__restrict__ F,
-           const double *__restrict__ G, const int *status) {
+mf_inv_t64(const int4 *__restrict__ tasks, Sym y, Real *__restrict__ F,
+           const Real *__restrict__ G, const int *status) {
     extern __shared__ double fsm[];
     double *As = fsm, *Bs = fsm + kFTileDoubles;
     if (*(volatile const int *)status) return;
@@ -582,8 +703,8 @@ mf_inv_t64(const int4 *__restrict__ tasks, Sym y, double *__restrict__ F,
     tile_range<FT>(f, i, ra, rb);
     tile_range<FT>(f, j, ca, cb);
     const int h = rb - ra, w = cb - ca;
-    double *Fs = F + f.fptr;
-    const double *Gs = G + f.gptr;
+    Real *Fs = F + f.fptr;
+    const Real *Gs = G + f.gptr;
     Acc acc;
     acc_zero(acc);
     for (int k = j; k < C0; k++) {
@@ -601,8 +722,8 @@ mf_inv_t64(const int4 *__restrict__ tasks, Sym y, double *__restrict__ F,
 }
 
 __global__ void __launch_bounds__(kGThreads)
-mf_inv_x64(const int4 *__restrict__ tasks, Sym y, const double *__restrict__ F,
-           double *__restrict__ G, const int *status) {
+mf_inv_x64(const int4 *__restrict__ tasks, Sym y, const Real *__restrict__ F,
+           Real *__restrict__ G, const int *status) {
     extern __shared__ double fsm[];
     double *As = fsm, *Bs = fsm + kFTileDoubles;
     if (*(volatile const int *)status) return;
@@ -614,8 +735,8 @@ mf_inv_x64(const int4 *__restrict__ tasks, Sym y, const double *__restrict__ F,
     tile_range<FT>(f, i, ra, rb);
     tile_range<FT>(f, j, ca, cb);
     const int h = rb - ra, w = cb - ca;
-    const double *Fs = F + f.fptr;
-    double *Gs = G + f.gptr;
+    const Real *Fs = F + f.fptr;
+    Real *Gs = G + f.gptr;
     Acc acc;
     acc_zero(acc);
     for (int k = C0; k <= i; k++) {
@@ -633,8 +754,8 @@ mf_inv_x64(const int4 *__restrict__ tasks, Sym y, const double *__restrict__ F,
 
 // W_IJ = sum_{K=J}^{nkb-1} L_IK X_KJ   (I a tile of the rows below the pivots)
 __global__ void __launch_bounds__(kGThreads)
-mf_wmul64(const int4 *__restrict__ tasks, Sym y, const double *__restrict__ F,
-          double *__restrict__ G, const int *status) {
+mf_wmul64(const int4 *__restrict__ tasks, Sym y, const Real *__restrict__ F,
+          Real *__restrict__ G, const int *status) {
     extern __shared__ double fsm[];
     double *As = fsm, *Bs = fsm + kFTileDoubles;
     if (*(volatile const int *)status) return;
@@ -645,8 +766,8 @@ mf_wmul64(const int4 *__restrict__ tasks, Sym y, const double *__restrict__ F,
     tile_range<FT>(f, I, ra, rb);
     tile_range<FT>(f, J, ca, cb);
     const int h = rb - ra, w = cb - ca;
-    const double *Fs = F + f.fptr;
-    double *Gs = G + f.gptr;
+    const Real *Fs = F + f.fptr;
+    Real *Gs = G + f.gptr;
     Acc acc;
     acc_zero(acc);
     for (int k = J; k < f.nkb; k++) {
@@ -721,7 +842,7 @@ struct SolveArgs {
     const STask *tasks;
     int ntasks, ns;
     const int32_t *bundle, *perm, *rows, *cptr, *cidx;
-    const double *G;
+    const Real *G;
     double *u, *yf, *x;
     const int32_t *fc_base, *fc_n, *bc_base, *bc_n;
     double *fpart, *bpart;
@@ -730,6 +851,7 @@ struct SolveArgs {
                         // backward arrivals [ns] | root forward arrivals [ns] | [ns] | err
     const double *b;
     double *out;
+    const int *skip;    // when set and nonzero: nothing to do
 };
 
 // relaxed-free publish: a release atomic orders every write that precedes it
@@ -790,7 +912,7 @@ SPX_DEV bool last_arrival(int *cnt, int n, int *flag) {
 // shared memory of one solve block.  gbuf holds one panel strip, staged by
 // bulk asynchronous copies (one per panel column) that complete on `bar`.
 struct SolveShared {
-    double gbuf[kStrip * kST];        // forward: 128 cols x 64 rows; backward: 64 x 128
+    Real gbuf[kStrip * kST];          // forward: 128 cols x 64 rows; backward: 64 x 128
     double part[4][kST];
     double vec[kStrip];               // f segment (forward) or v segment (backward)
     double colsum[kST];
@@ -878,14 +1000,14 @@ SPX_DEV void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;"
 // Stage columns [j0, j0+ncols) x rows [i0, i0+nrows) of a panel (leading
 // dimension ldg, column-major) into buf (column stride `stride` doubles):
 // one bulk copy per column, issued by the lanes of warp 0.  nrows is even.
-SPX_DEV void stage_panel(double *buf, int stride, const double *panel, int ldg, int i0, int nrows,
+SPX_DEV void stage_panel(Real *buf, int stride, const Real *panel, int ldg, int i0, int nrows,
                          int j0, int ncols, unsigned long long *bar) {
     if (threadIdx.x >= 32) return;
-    if (threadIdx.x == 0) mbar_expect(bar, (uint32_t)(ncols * nrows * 8));
+    if (threadIdx.x == 0) mbar_expect(bar, (uint32_t)(ncols * nrows * sizeof(Real)));
     __syncwarp();
     for (int jj = threadIdx.x; jj < ncols; jj += 32)
         bulk_load(buf + (size_t)jj * stride, panel + (int64_t)i0 + (int64_t)(j0 + jj) * ldg,
-                  (uint32_t)(nrows * 8), bar);
+                  (uint32_t)(nrows * sizeof(Real)), bar);
 }
 
 // ---- forward, one tiny leaf supernode (r <= 24, c <= 6) per thread.  A
@@ -895,7 +1017,7 @@ SPX_DEV void fwd_thread(const SolveArgs &a, int s) {
     int *const fcd = a.sync + 1, *const fchk = fcd + 3 * a.ns;
     const SNode m = a.meta[s];
     const int first = m.a.x, c = m.a.y, r = m.a.z, ldg = m.a.w, parent = m.b.x;
-    const double *Gs = a.G + m.p.x;
+    const Real *Gs = a.G + m.p.x;
     double f[kTinyC];
 #pragma unroll
     for (int j = 0; j < kTinyC; j++) f[j] = (j < c) ? a.b[a.perm[first + j]] : 0.0;
@@ -920,7 +1042,7 @@ SPX_DEV void bwd_thread(const SolveArgs &a, int s) {
     const SNode m = a.meta[s];
     const int first = m.a.x, c = m.a.y, r = m.a.z, ldg = m.a.w, parent = m.b.x;
     const int32_t *rows = a.rows + m.p.y;
-    const double *Gs = a.G + m.p.x;
+    const Real *Gs = a.G + m.p.x;
     int ri[kTinyR];
 #pragma unroll
     for (int i = 0; i < kTinyR; i++) ri[i] = (i >= c && i < r) ? rows[i] : 0;
@@ -953,7 +1075,7 @@ SPX_DEV void fwd_warp(const SolveArgs &a, int s, WarpShared &w) {
     const int first = m.a.x, c = m.a.y, r = m.a.z, ldg = m.a.w;
     const int parent = m.b.x, nchild = m.nchild, expect = m.b.y;
     const int64_t g0 = m.p.y;
-    const double *Gs = a.G + m.p.x;
+    const Real *Gs = a.G + m.p.x;
     const int lane = threadIdx.x & 31;
     const int nq = (r + 31) >> 5;
     double bv = 0.0;
@@ -1018,7 +1140,8 @@ SPX_DEV void fwd_tile(const SolveArgs &a, int s, int I, int S, int chunk, SolveS
     const int64_t g0 = m.p.y;
     const int i0 = I * kST, j0 = S * kStrip;
     const int jn = min(kStrip, c - j0);
-    const int hcopy = min(kST, ldg - i0);          // even: ldg is even, i0 is a multiple of 64
+    // a multiple of 16 bytes: ldg is, and i0 is a multiple of 64
+    const int hcopy = min(kST, ldg - i0);
     stage_panel(sh.gbuf, kST, a.G + m.p.x, ldg, i0, hcopy, j0, jn, bar);
     const int t = threadIdx.x;
     double bv = 0.0;
@@ -1086,7 +1209,7 @@ SPX_DEV void bwd_warp(const SolveArgs &a, int s) {
     const SNode m = a.meta[s];
     const int first = m.a.x, c = m.a.y, r = m.a.z, ldg = m.a.w, parent = m.b.x;
     const int32_t *rows = a.rows + m.p.y;
-    const double *Gs = a.G + m.p.x;
+    const Real *Gs = a.G + m.p.x;
     const int lane = threadIdx.x & 31;
     const int nq = (r + 31) >> 5;
     int rv[kWarpMaxR / 32];
@@ -1245,6 +1368,7 @@ __global__ void __launch_bounds__(kSThreads, 2) mf_solve_sf(SolveArgs a) {
     __shared__ __align__(8) unsigned long long s_bar;
     SolveShared &sh = *reinterpret_cast<SolveShared *>(smem_raw);
     WarpShared *ws = reinterpret_cast<WarpShared *>(smem_raw);
+    if (a.skip && *(volatile const int *)a.skip) return;
     const int wid = threadIdx.x >> 5;
     uint32_t phase = 0;
     if (threadIdx.x == 0) mbar_init(&s_bar);
@@ -1325,9 +1449,9 @@ static int dupload(Tp **p, const Tp *h, size_t cnt, cudaStream_t st) {
 
 }  // namespace
 
-MultifrontalPlan::~MultifrontalPlan() { release(0); }
+template <> MultifrontalPlanT<Real>::~MultifrontalPlanT() { release(0); }
 
-void MultifrontalPlan::release(cudaStream_t st) {
+template <> void MultifrontalPlanT<Real>::release(cudaStream_t st) {
     if (fgraph_) { cudaGraphExecDestroy(fgraph_); fgraph_ = nullptr; }
     fgraph_val_ = nullptr;
     if (d_params_) { cudaFreeAsync(d_params_, st); d_params_ = nullptr; }
@@ -1349,18 +1473,20 @@ void MultifrontalPlan::release(cudaStream_t st) {
     d_stask_ = nullptr;
     d_fpart_ = d_bpart_ = nullptr;
     d_cnt_ = d_sync_ = nullptr;
-    d_front_ = d_G_ = d_u_ = d_yf_ = d_x_ = nullptr;
+    d_front_ = nullptr;
+    d_G_ = nullptr;
+    d_u_ = d_yf_ = d_x_ = nullptr;
     d_status_ = nullptr;
 }
 
-int64_t MultifrontalPlan::solve_bytes() const {
+template <> int64_t MultifrontalPlanT<Real>::solve_bytes() const {
     // G read once forward and once backward (lower triangle of the pivot
     // block plus the rows below), the row lists read twice, and the
     // right-hand side, the intermediate and the result vectors.
-    return 2 * (8 * g_total_ + 4 * nrows_total_) + 24 * (int64_t)n_;
+    return 2 * ((int64_t)sizeof(Real) * g_total_ + 4 * nrows_total_) + 24 * (int64_t)n_;
 }
 
-int MultifrontalPlan::init(const spx_symbolic &S, const int64_t *rowptr, const int32_t *col,
+template <> int MultifrontalPlanT<Real>::init(const spx_symbolic &S, const int64_t *rowptr, const int32_t *col,
                            cudaStream_t st) {
     n_ = S.n;
     ns_ = S.nsuper;
@@ -1375,7 +1501,7 @@ int MultifrontalPlan::init(const spx_symbolic &S, const int64_t *rowptr, const i
         int64_t gtri = 0;
         for (int32_t s = 0; s < ns; s++) {
             int64_t r = S.rowptr[s + 1] - S.rowptr[s], c = S.sfirst[s + 1] - S.sfirst[s];
-            gptr[s + 1] = gptr[s] + ((r + 1) & ~(int64_t)1) * c;
+            gptr[s + 1] = gptr[s] + ((r + kLdgA - 1) & ~(int64_t)(kLdgA - 1)) * c;
             uptr[s + 1] = uptr[s] + (r - c);
             gtri += c * (c + 1) / 2 + (r - c) * c;
         }
@@ -1525,7 +1651,7 @@ int MultifrontalPlan::init(const spx_symbolic &S, const int64_t *rowptr, const i
             const int r = (int)(S.rowptr[s2 + 1] - S.rowptr[s2]);
             const int c = S.sfirst[s2 + 1] - S.sfirst[s2];
             SNodeH &m = meta[s2];
-            m.first = S.sfirst[s2]; m.c = c; m.r = r; m.ldg = (r + 1) & ~1;
+            m.first = S.sfirst[s2]; m.c = c; m.r = r; m.ldg = (r + kLdgA - 1) & ~(kLdgA - 1);
             m.parent = S.sparent[s2];
             m.nchild = S.child_ptr[s2 + 1] - S.child_ptr[s2];
             m.nrc = (r + kST - 1) / kST;
@@ -1708,7 +1834,7 @@ int MultifrontalPlan::init(const spx_symbolic &S, const int64_t *rowptr, const i
         rc = rc ? rc : dmalloc(&d_G_, (size_t)gptr[ns], st);
         // the solve reads whole tiles: the strictly upper part of every
         // inv(L11) block and the padding row stay zero for the plan's life
-        if (!rc) cudaMemsetAsync(d_G_, 0, sizeof(double) * (size_t)gptr[ns], st);
+        if (!rc) cudaMemsetAsync(d_G_, 0, sizeof(Real) * (size_t)gptr[ns], st);
         rc = rc ? rc : dmalloc(&d_u_, (size_t)u_total_, st);
         rc = rc ? rc : dmalloc(&d_yf_, (size_t)n, st);
         rc = rc ? rc : dmalloc(&d_x_, (size_t)n, st);
@@ -1739,7 +1865,7 @@ int MultifrontalPlan::init(const spx_symbolic &S, const int64_t *rowptr, const i
     return 0;
 }
 
-void MultifrontalPlan::launch_factor(const double *d_val, cudaStream_t st) {
+template <> void MultifrontalPlanT<Real>::launch_factor(const double *d_val, cudaStream_t st) {
     Sym y{d_sfirst_, d_rows_, d_relmap_, d_child_ptr_, d_child_list_, d_rowptr_, d_frontptr_,
           d_gptr_, d_cbnd_, d_cbnd_ptr_};
     for (const MfLaunch &L : launches_) {
@@ -1778,7 +1904,7 @@ void MultifrontalPlan::launch_factor(const double *d_val, cudaStream_t st) {
 // The launch sequence is fixed by the symbolic analysis, so it is captured
 // once into a CUDA graph and replayed; the shift and the pivot tolerance are
 // read from device memory by the kernels.
-int MultifrontalPlan::factorize(const double *d_val, double shift, double pivtol,
+template <> int MultifrontalPlanT<Real>::factorize(const double *d_val, double shift, double pivtol,
                                 cudaStream_t st) {
     if (!d_front_) {
         if (dmalloc(&d_front_, (size_t)front_total_, st)) return SPEIGS_ERR_MEM;
@@ -1815,7 +1941,8 @@ int MultifrontalPlan::factorize(const double *d_val, double shift, double pivtol
     return h_status ? 1 : 0;
 }
 
-void MultifrontalPlan::solve(const double *b, double *x, cudaStream_t st) {
+template <> void MultifrontalPlanT<Real>::solve(const double *b, double *x, cudaStream_t st,
+                                                const int *skip) {
     SolveArgs a;
     a.meta = (const SNode *)d_meta_;
     a.tasks = (const STask *)d_stask_;
@@ -1841,6 +1968,7 @@ void MultifrontalPlan::solve(const double *b, double *x, cudaStream_t st) {
     a.sync = d_sync_;
     a.b = b;
     a.out = x;
+    a.skip = skip;
     // queue, dependency counters and flags start at zero; the error word at
     // the end keeps its value so a failed solve stays visible until read
     cudaMemsetAsync(d_sync_, 0, sizeof(int) * (sync_ints_ - 1), st);
@@ -1848,6 +1976,6 @@ void MultifrontalPlan::solve(const double *b, double *x, cudaStream_t st) {
     note_launch();
 }
 
-int *MultifrontalPlan::error_word() const { return d_sync_ ? d_sync_ + (sync_ints_ - 1) : nullptr; }
+template <> int *MultifrontalPlanT<Real>::error_word() const { return d_sync_ ? d_sync_ + (sync_ints_ - 1) : nullptr; }
 
 }  // namespace spx

@@ -34,12 +34,17 @@ struct MfLaunch {
     int64_t count;   // tasks
 };
 
-class MultifrontalPlan {
+// Real is the storage type of the fronts and of the panels G: double for
+// the plain FP64 operator, float for the mixed-precision one (FP32 factor,
+// trailing updates on the TF32 tensor cores with an FP32-accurate 3-term
+// split; the caller refines each solve in FP64).  Vectors are FP64 always.
+template <class Real>
+class MultifrontalPlanT {
 public:
-    MultifrontalPlan() = default;
-    ~MultifrontalPlan();
-    MultifrontalPlan(const MultifrontalPlan &) = delete;
-    MultifrontalPlan &operator=(const MultifrontalPlan &) = delete;
+    MultifrontalPlanT() = default;
+    ~MultifrontalPlanT();
+    MultifrontalPlanT(const MultifrontalPlanT &) = delete;
+    MultifrontalPlanT &operator=(const MultifrontalPlanT &) = delete;
 
     // Upload the symbolic structure and build the task lists.  rowptr/col
     // are the host copy of the full symmetric CSR (original numbering) whose
@@ -53,8 +58,10 @@ public:
     // was not positive (A + shift*I not PD), or a negative error code.
     int factorize(const double *d_val, double shift, double pivtol, cudaStream_t st);
 
-    // x = (A + shift I)^{-1} b  (b, x device vectors in the original order)
-    void solve(const double *b, double *x, cudaStream_t st);
+    // x = (A + shift I)^{-1} b  (b, x device vectors in the original order).
+    // When `skip` is given and *skip is nonzero on the device, the launch
+    // does nothing (refinement steps that are no longer needed).
+    void solve(const double *b, double *x, cudaStream_t st, const int *skip = nullptr);
 
     void release(cudaStream_t st);
 
@@ -96,8 +103,8 @@ private:
     int solve_grid_ = 0;
     size_t solve_smem_ = 0;
     // numeric
-    double *d_front_ = nullptr;
-    double *d_G_ = nullptr;
+    Real *d_front_ = nullptr;
+    Real *d_G_ = nullptr;
     double *d_u_ = nullptr, *d_yf_ = nullptr, *d_x_ = nullptr;
     int *d_status_ = nullptr;
     double *d_params_ = nullptr;     // shift, pivot tolerance (read by the graph)
@@ -105,5 +112,26 @@ private:
     const double *fgraph_val_ = nullptr;
     int max_rows_ = 0;
 };
+
+using MultifrontalPlan = MultifrontalPlanT<double>;
+using MultifrontalPlan32 = MultifrontalPlanT<float>;
+
+// The members are defined in multifrontal.cu, which is compiled once per
+// storage type; each translation unit specialises them for its type.
+#define SPX_MF_DECLARE(R)                                                                    \
+    template <> MultifrontalPlanT<R>::~MultifrontalPlanT();                                \
+    template <> int MultifrontalPlanT<R>::init(const spx_symbolic &, const int64_t *,      \
+                                               const int32_t *, cudaStream_t);             \
+    template <> int MultifrontalPlanT<R>::factorize(const double *, double, double,        \
+                                                    cudaStream_t);                         \
+    template <> void MultifrontalPlanT<R>::solve(const double *, double *, cudaStream_t,   \
+                                                 const int *);                            \
+    template <> void MultifrontalPlanT<R>::release(cudaStream_t);                          \
+    template <> int *MultifrontalPlanT<R>::error_word() const;                             \
+    template <> int64_t MultifrontalPlanT<R>::solve_bytes() const;                         \
+    template <> void MultifrontalPlanT<R>::launch_factor(const double *, cudaStream_t);
+SPX_MF_DECLARE(double)
+SPX_MF_DECLARE(float)
+#undef SPX_MF_DECLARE
 
 }  // namespace spx

@@ -40,6 +40,23 @@ class Info(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class ExtOpts(ctypes.Structure):
+    """speigs_ext_opts (include/speigs_b200.h): operator precision, start subspace."""
+    _fields_ = [("precision", c_int), ("refine_max", c_int), ("refine_tol", c_double),
+                ("warm", c_void_p), ("warm_cols", c_int64)]
+
+
+class ExtInfo(ctypes.Structure):
+    """speigs_ext_info (include/speigs_b200.h)."""
+    _fields_ = [("precision", c_int), ("refine_steps", c_int64), ("factor_solves", c_int64),
+                ("warm_cols", c_int64)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+FP64, MIXED = 0, 1
+
 _I64P = POINTER(c_int64)
 _DP = POINTER(c_double)
 
@@ -63,6 +80,12 @@ _EXT_SIGNATURES = {
     "speigs_plan_costs": (c_int, [c_void_p, _DP, _DP, _DP]),
     "speigs_plan_destroy": (None, [c_void_p]),
     "speigs_b200_rand_vec": (c_int, [c_int64, c_uint64, _DP]),
+    "speigs_default_ext_opts": (None, [POINTER(ExtOpts)]),
+    "speigs_ex": (c_int, [c_int64, _I64P, _I64P, _DP, c_int64, c_int, POINTER(Opts),
+                          POINTER(ExtOpts), _DP, _DP, _DP, POINTER(Info), POINTER(ExtInfo)]),
+    "speigs_plan_create_ex": (c_int, [c_int64, _I64P, _I64P, _DP, c_int, POINTER(Opts),
+                                      POINTER(ExtOpts), POINTER(c_void_p)]),
+    "speigs_plan_ext_info": (c_int, [c_void_p, POINTER(ExtInfo)]),
     "speigs_b200_syev_small": (c_int, [c_int, _DP, _DP, _DP, POINTER(c_int)]),
     "speigs_b200_syev_small_noalloc": (c_int, [c_int, c_void_p, c_void_p, c_void_p, c_void_p,
                                                c_void_p, c_void_p]),
@@ -101,6 +124,19 @@ def default_opts(lib=None, **kw) -> Opts:
     return o
 
 
+def ext_opts(lib=None, warm=None, **kw) -> ExtOpts:
+    """Extension options; warm: optional (n, p) start subspace kept alive by the caller."""
+    lib = lib or load()
+    e = ExtOpts()
+    lib.speigs_default_ext_opts(ctypes.byref(e))
+    for k, v in kw.items():
+        setattr(e, k, v)
+    if warm is not None:
+        e.warm = warm.ctypes.data
+        e.warm_cols = warm.shape[1]
+    return e
+
+
 def _csc_arrays(A):
     """(n, Ap, Ai, Ax) int64/float64 contiguous from a scipy sparse matrix or a tuple."""
     if isinstance(A, tuple):
@@ -134,6 +170,30 @@ def speigs(A, k, which=SM, opts: Opts | None = None, vectors=True, lib=None):
     return rc, lam, (V.T.copy() if vectors else None), res, info.as_dict()
 
 
+def speigs_ex(A, k, which=SM, opts: Opts | None = None, ext: ExtOpts | None = None,
+              vectors=True, lib=None, warm=None):
+    """speigs_ex() through the C ABI: (rc, lam, V, resid, info, ext_info).
+
+    warm: optional (n, p) float64 start subspace (overrides ext.warm)."""
+    lib = lib or load()
+    n, Ap, Ai, Ax = _csc_arrays(A)
+    lam = np.zeros(k)
+    res = np.zeros(k)
+    V = np.zeros((k, n)) if vectors else None
+    info, einfo = Info(), ExtInfo()
+    o = opts if opts is not None else default_opts(lib)
+    e = ext if ext is not None else ext_opts(lib)
+    W = None
+    if warm is not None:
+        W = np.asfortranarray(warm, dtype=np.float64)
+        e.warm = W.ctypes.data
+        e.warm_cols = W.shape[1]
+    rc = lib.speigs_ex(n, _p(Ap, c_int64), _p(Ai, c_int64), _p(Ax), k, which, ctypes.byref(o),
+                       ctypes.byref(e), _p(lam), _p(V) if vectors else None, _p(res),
+                       ctypes.byref(info), ctypes.byref(einfo))
+    return rc, lam, (V.T.copy() if vectors else None), res, info.as_dict(), einfo.as_dict()
+
+
 def speigs_z(A_re, A_im, k, which=SM, opts: Opts | None = None, lib=None):
     """Complex Hermitian through the C ABI: A_re/A_im share one CSC pattern."""
     lib = lib or load()
@@ -161,14 +221,18 @@ def last_error(lib=None) -> str:
 class Plan:
     """speigs_plan: a matrix kept on the GPU across solves (speigs_b200.h)."""
 
-    def __init__(self, A, which=SM, opts: Opts | None = None, lib=None):
+    def __init__(self, A, which=SM, opts: Opts | None = None, lib=None,
+                 ext: ExtOpts | None = None):
         self.lib = lib or load()
         self.n, self._Ap, self._Ai, Ax = _csc_arrays(A)
         self.which = which
         h = c_void_p()
         o = opts if opts is not None else default_opts(self.lib)
-        rc = self.lib.speigs_plan_create(self.n, _p(self._Ap, c_int64), _p(self._Ai, c_int64),
-                                         _p(Ax), which, ctypes.byref(o), ctypes.byref(h))
+        self._ext = ext
+        rc = self.lib.speigs_plan_create_ex(self.n, _p(self._Ap, c_int64), _p(self._Ai, c_int64),
+                                            _p(Ax), which, ctypes.byref(o),
+                                            ctypes.byref(ext) if ext is not None else None,
+                                            ctypes.byref(h))
         if rc != 0:
             raise RuntimeError(f"speigs_plan_create: {errmsg(rc, self.lib)} ({last_error(self.lib)})")
         self.h = h
@@ -182,6 +246,11 @@ class Plan:
         rc = self.lib.speigs_plan_solve_device(self.h, k, lam_ptr, V_ptr, resid_ptr,
                                                ctypes.byref(info))
         return rc, info.as_dict()
+
+    def ext_info(self):
+        e = ExtInfo()
+        self.lib.speigs_plan_ext_info(self.h, ctypes.byref(e))
+        return e.as_dict()
 
     def apply_device(self, x_ptr, y_ptr):
         return self.lib.speigs_plan_apply_device(self.h, x_ptr, y_ptr)
