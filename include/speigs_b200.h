@@ -55,6 +55,34 @@ int speigs_ex(speigs_int n, const speigs_int *Ap, const speigs_int *Ai, const do
               const speigs_ext_opts *ext, double *lambda, double *V, double *resid,
               speigs_info *info, speigs_ext_info *einfo);
 
+/* ---- batched components --------------------------------------------------
+ * speigs() splits a matrix into its connected components, solves each and
+ * keeps the global k of the merged candidates (reference blocks_path,
+ * src/speigs_core.c:532-632).  These two calls keep k eigenpairs of EVERY
+ * component instead.  The components are solved concurrently (a host
+ * thread pool, every solve on its own CUDA stream).  No counterpart in the
+ * reference interface. */
+
+/* Connected components over the numerically nonzero entries of the upper
+ * triangle, labelled in order of first appearance -- the split speigs()
+ * makes.  comp[n] receives the labels, *ncomp their count. */
+int speigs_components(speigs_int n, const speigs_int *Ap, const speigs_int *Ai,
+                      const double *Ax, speigs_int *comp, speigs_int *ncomp);
+
+/* min(k, n_c) eigenpairs of every component c (labels from
+ * speigs_components).  lambda[ncomp*k]: row c (entries c*k .. c*k+k-1)
+ * holds component c's values sorted as speigs() sorts them, zero-filled;
+ * V[n*k] (may be NULL): column t holds the t-th eigenvector of every
+ * component on that component's rows; resid[ncomp*k] (may be NULL);
+ * nvals[ncomp] (may be NULL) receives min(k, n_c).  info (may be NULL):
+ * operator applications summed, flag = 1 if any component is partial,
+ * ncomp, path = SPEIGS_PATH_BLOCKS.  ext may be NULL. */
+int speigs_batched(speigs_int n, const speigs_int *Ap, const speigs_int *Ai, const double *Ax,
+                   speigs_int k, speigs_which which, const speigs_opts *opts,
+                   const speigs_ext_opts *ext, const speigs_int *comp, speigs_int ncomp,
+                   double *lambda, double *V, double *resid, speigs_int *nvals,
+                   speigs_info *info);
+
 /* Opaque solver plan: one connected symmetric matrix on one GPU, with its
  * operator ('sm': symbolic analysis done, numeric factor per solve; 'lm':
  * the matrix itself) and every device buffer the Lanczos iteration needs.

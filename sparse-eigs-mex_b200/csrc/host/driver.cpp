@@ -16,6 +16,8 @@
 #include <time.h>
 
 #include <algorithm>
+#include <atomic>
+#include <thread>
 #include <vector>
 
 using spx::HostCSR;
@@ -121,55 +123,120 @@ int speigs_impl(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *A
                 double *lambda, double *V, double *resid, speigs_info *info,
                 speigs_ext_info *einfo);
 
+// Component split: rows grouped by component label, in row order.
+struct CompSplit {
+    int64_t ncomp = 0;
+    std::vector<int64_t> sz, off, gidx, loc;
+    void build(int64_t n, const std::vector<int64_t> &comp, int64_t nc) {
+        ncomp = nc;
+        sz.assign(nc, 0);
+        off.assign(nc + 1, 0);
+        gidx.resize(n);
+        loc.resize(n);
+        std::vector<int64_t> fill(nc, 0);
+        for (int64_t i = 0; i < n; i++) sz[comp[i]]++;
+        for (int64_t c = 0; c < nc; c++) off[c + 1] = off[c] + sz[c];
+        for (int64_t i = 0; i < n; i++) {
+            const int64_t c = comp[i], slot = off[c] + fill[c]++;
+            gidx[slot] = i;
+            loc[i] = slot - off[c];
+        }
+    }
+};
+
+// Result of one component's solve.
+struct CompResult {
+    int64_t kc = 0;
+    std::vector<double> lam, res, vec;   // vec: nc x kc column-major (when wanted)
+    speigs_info info;
+    speigs_ext_info einfo;
+};
+
+// Solve every component with speigs_impl (which applies the reference's
+// per-component routing: diagonal, dense or Krylov), kc = min(k, n_c).  The
+// components are independent, so they are taken from a shared queue by a
+// pool of host threads, largest first; each thread's solves run on their own
+// CUDA streams and overlap on the GPU.  Returns 0 or the first error.
+int solve_components(const int64_t *Ap, const int64_t *Ai, const double *Ax,
+                     const std::vector<int64_t> &comp, const CompSplit &sp, int64_t k,
+                     speigs_which which, const speigs_opts *opts, const speigs_ext_opts *ext,
+                     bool want_vec, std::vector<CompResult> &out) {
+    const int64_t nc_all = sp.ncomp;
+    out.assign(nc_all, CompResult());
+    std::vector<int64_t> order(nc_all);
+    for (int64_t c = 0; c < nc_all; c++) order[c] = c;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int64_t a, int64_t b) { return sp.sz[a] > sp.sz[b]; });
+    std::atomic<int64_t> next{0};
+    std::atomic<int> err{0};
+    auto worker = [&] {
+        std::vector<int64_t> sAp, sAi;
+        std::vector<double> sAx;
+        for (;;) {
+            const int64_t it = next.fetch_add(1);
+            if (it >= nc_all || err.load() != 0) break;
+            const int64_t ci = order[it], nc = sp.sz[ci];
+            sAp.assign(nc + 1, 0);
+            sAi.clear();
+            sAx.clear();
+            for (int64_t j = 0; j < nc; j++) {
+                const int64_t gc = sp.gidx[sp.off[ci] + j];
+                sAp[j] = (int64_t)sAi.size();
+                for (int64_t q = Ap[gc]; q < Ap[gc + 1]; q++) {
+                    const int64_t r = Ai[q];
+                    if (comp[r] == ci) { sAi.push_back(sp.loc[r]); sAx.push_back(Ax[q]); }
+                }
+            }
+            sAp[nc] = (int64_t)sAi.size();
+            if (sAi.empty()) { sAi.push_back(0); sAx.push_back(0.0); }
+            CompResult &R = out[ci];
+            R.kc = std::min(k, nc);
+            R.lam.assign(R.kc, 0.0);
+            R.res.assign(R.kc, 0.0);
+            if (want_vec) R.vec.assign((size_t)nc * R.kc, 0.0);
+            const int rc = speigs_impl(nc, sAp.data(), sAi.data(), sAx.data(), R.kc, which, opts,
+                                       ext, R.lam.data(), want_vec ? R.vec.data() : nullptr,
+                                       R.res.data(), &R.info, &R.einfo);
+            if (rc) {
+                int expected = 0;
+                err.compare_exchange_strong(expected, rc);
+            }
+        }
+    };
+    unsigned hw = std::thread::hardware_concurrency();
+    int64_t nth = std::min<int64_t>(nc_all, std::max(1u, std::min(hw ? hw : 1u, 16u)));
+    std::vector<std::thread> th;
+    for (int64_t i = 1; i < nth; i++) th.emplace_back(worker);
+    worker();
+    for (auto &t : th) t.join();
+    return err.load();
+}
+
 // Solve every component separately and merge by |lambda| (reference
 // blocks_path, src/speigs_core.c:532-632).
 int blocks_path(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *Ax, int64_t k,
                 speigs_which which, const speigs_opts *opts, const speigs_ext_opts *ext,
                 const std::vector<int64_t> &comp, int64_t ncomp, double *lambda, double *V,
                 double *resid, speigs_info *info, speigs_ext_info *einfo) {
-    std::vector<int64_t> sz(ncomp, 0), off(ncomp + 1, 0), gidx(n), loc(n), fill(ncomp, 0);
-    for (int64_t i = 0; i < n; i++) sz[comp[i]]++;
-    for (int64_t c = 0; c < ncomp; c++) off[c + 1] = off[c] + sz[c];
-    for (int64_t i = 0; i < n; i++) {
-        const int64_t c = comp[i], slot = off[c] + fill[c]++;
-        gidx[slot] = i;
-        loc[i] = slot - off[c];
-    }
+    CompSplit sp;
+    sp.build(n, comp, ncomp);
+    std::vector<CompResult> cr;
+    int rc = solve_components(Ap, Ai, Ax, comp, sp, k, which, opts, ext, V != nullptr, cr);
+    if (rc) return rc;
     std::vector<double> clam, cres;
     std::vector<int64_t> ccomp, cslot;
-    std::vector<std::vector<double>> cvec(ncomp);
-    std::vector<int64_t> sAp(n + 1), sAi(Ap[n] ? Ap[n] : 1);
-    std::vector<double> sAx(Ap[n] ? Ap[n] : 1);
     for (int64_t ci = 0; ci < ncomp; ci++) {
-        const int64_t nc = sz[ci];
-        int64_t knt = 0;
-        for (int64_t j = 0; j < nc; j++) {
-            const int64_t gc = gidx[off[ci] + j];
-            sAp[j] = knt;
-            for (int64_t q = Ap[gc]; q < Ap[gc + 1]; q++) {
-                const int64_t r = Ai[q];
-                if (comp[r] == ci) { sAi[knt] = loc[r]; sAx[knt] = Ax[q]; knt++; }
-            }
-        }
-        sAp[nc] = knt;
-        const int64_t kc = std::min(k, nc);
-        std::vector<double> lv(kc), rv(kc);
-        if (V) cvec[ci].assign((size_t)nc * kc, 0.0);
-        speigs_info si;
-        speigs_ext_info se;
-        int r2 = speigs_impl(nc, sAp.data(), sAi.data(), sAx.data(), kc, which, opts, ext,
-                             lv.data(), V ? cvec[ci].data() : nullptr, rv.data(), &si, &se);
-        if (r2) return r2;
+        const CompResult &R = cr[ci];
         if (einfo) {
-            einfo->refine_steps += se.refine_steps;
-            einfo->factor_solves += se.factor_solves;
-            if (se.precision) einfo->precision = se.precision;
+            einfo->refine_steps += R.einfo.refine_steps;
+            einfo->factor_solves += R.einfo.factor_solves;
+            if (R.einfo.precision) einfo->precision = R.einfo.precision;
         }
-        info->nops += si.nops;
-        if (si.flag) info->flag = 1;
-        for (int64_t t = 0; t < kc; t++) {
-            clam.push_back(lv[t]);
-            cres.push_back(rv[t]);
+        info->nops += R.info.nops;
+        if (R.info.flag) info->flag = 1;
+        for (int64_t t = 0; t < R.kc; t++) {
+            clam.push_back(R.lam[t]);
+            cres.push_back(R.res[t]);
             ccomp.push_back(ci);
             cslot.push_back(t);
         }
@@ -181,13 +248,13 @@ int blocks_path(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *A
         return which == SPEIGS_SM ? a.key < b.key : a.key > b.key;
     });
     for (int64_t t = 0; t < k && t < ncand; t++) {
-        const int64_t i = ord[t].idx, ci = ccomp[i], sl = cslot[i], nc = sz[ci];
+        const int64_t i = ord[t].idx, ci = ccomp[i], sl = cslot[i], nc = sp.sz[ci];
         lambda[t] = clam[i];
         if (resid) resid[t] = cres[i];
         if (V) {
             memset(V + (size_t)t * n, 0, (size_t)n * sizeof(double));
-            const double *src = cvec[ci].data() + (size_t)sl * nc;
-            for (int64_t j = 0; j < nc; j++) V[(size_t)t * n + gidx[off[ci] + j]] = src[j];
+            const double *src = cr[ci].vec.data() + (size_t)sl * nc;
+            for (int64_t j = 0; j < nc; j++) V[(size_t)t * n + sp.gidx[sp.off[ci] + j]] = src[j];
         }
     }
     info->nconv = std::min(k, ncand);
@@ -241,6 +308,64 @@ int speigs_ex(speigs_int n, const speigs_int *Ap, const speigs_int *Ai, const do
               const speigs_ext_opts *ext, double *lambda, double *V, double *resid,
               speigs_info *info, speigs_ext_info *einfo) {
     return speigs_impl(n, Ap, Ai, Ax, k, which, opts, ext, lambda, V, resid, info, einfo);
+}
+
+int speigs_components(speigs_int n, const speigs_int *Ap, const speigs_int *Ai,
+                      const double *Ax, speigs_int *comp, speigs_int *ncomp) {
+    if (n <= 0 || !Ap || !Ai || !Ax || !comp || !ncomp) return SPEIGS_ERR_ARG;
+    std::vector<int64_t> c;
+    *ncomp = find_components(n, Ap, Ai, Ax, c);
+    memcpy(comp, c.data(), sizeof(int64_t) * (size_t)n);
+    return SPEIGS_OK;
+}
+
+int speigs_batched(speigs_int n, const speigs_int *Ap, const speigs_int *Ai, const double *Ax,
+                   speigs_int k, speigs_which which, const speigs_opts *opts,
+                   const speigs_ext_opts *ext, const speigs_int *comp, speigs_int ncomp,
+                   double *lambda, double *V, double *resid, speigs_int *nvals,
+                   speigs_info *info) {
+    speigs_opts defo;
+    if (!opts) { speigs_default_opts(&defo); opts = &defo; }
+    speigs_info li;
+    if (!info) info = &li;
+    memset(info, 0, sizeof *info);
+    if (n <= 0 || !Ap || !Ai || !Ax || !lambda || !comp || ncomp <= 0 || k <= 0)
+        return SPEIGS_ERR_ARG;
+    for (int64_t i = 0; i < n; i++)
+        if (comp[i] < 0 || comp[i] >= ncomp) return SPEIGS_ERR_ARG;
+    if (opts->check_sym != 0 && check_symmetry(n, Ap, Ai, Ax) == 0) return SPEIGS_ERR_NOTSYM;
+    std::vector<int64_t> cv(comp, comp + n);
+    CompSplit sp;
+    sp.build(n, cv, ncomp);
+    for (int64_t c = 0; c < ncomp; c++)
+        if (sp.sz[c] == 0) return SPEIGS_ERR_ARG;
+    // the per-component calls repeat no symmetry check
+    speigs_opts o2 = *opts;
+    o2.check_sym = 0;
+    std::vector<CompResult> cr;
+    int rc = solve_components(Ap, Ai, Ax, cv, sp, k, which, &o2, ext, V != nullptr, cr);
+    if (rc) return rc;
+    memset(lambda, 0, sizeof(double) * (size_t)ncomp * k);
+    if (resid) memset(resid, 0, sizeof(double) * (size_t)ncomp * k);
+    if (V) memset(V, 0, sizeof(double) * (size_t)n * k);
+    for (int64_t c = 0; c < ncomp; c++) {
+        const CompResult &R = cr[c];
+        for (int64_t t = 0; t < R.kc; t++) {
+            lambda[c * k + t] = R.lam[t];
+            if (resid) resid[c * k + t] = R.res[t];
+            if (V) {
+                const double *src = R.vec.data() + (size_t)t * sp.sz[c];
+                for (int64_t j = 0; j < sp.sz[c]; j++) V[(size_t)t * n + sp.gidx[sp.off[c] + j]] = src[j];
+            }
+        }
+        if (nvals) nvals[c] = R.kc;
+        info->nops += R.info.nops;
+        if (R.info.flag) info->flag = 1;
+        info->nconv += R.info.nconv;
+    }
+    info->ncomp = ncomp;
+    info->path = SPEIGS_PATH_BLOCKS;
+    return SPEIGS_OK;
 }
 
 }  // extern "C"

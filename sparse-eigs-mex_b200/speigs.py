@@ -86,6 +86,10 @@ _EXT_SIGNATURES = {
     "speigs_plan_create_ex": (c_int, [c_int64, _I64P, _I64P, _DP, c_int, POINTER(Opts),
                                       POINTER(ExtOpts), POINTER(c_void_p)]),
     "speigs_plan_ext_info": (c_int, [c_void_p, POINTER(ExtInfo)]),
+    "speigs_components": (c_int, [c_int64, _I64P, _I64P, _DP, _I64P, _I64P]),
+    "speigs_batched": (c_int, [c_int64, _I64P, _I64P, _DP, c_int64, c_int, POINTER(Opts),
+                               POINTER(ExtOpts), _I64P, c_int64, _DP, _DP, _DP, _I64P,
+                               POINTER(Info)]),
     "speigs_b200_syev_small": (c_int, [c_int, _DP, _DP, _DP, POINTER(c_int)]),
     "speigs_b200_syev_small_noalloc": (c_int, [c_int, c_void_p, c_void_p, c_void_p, c_void_p,
                                                c_void_p, c_void_p]),
@@ -192,6 +196,44 @@ def speigs_ex(A, k, which=SM, opts: Opts | None = None, ext: ExtOpts | None = No
                        ctypes.byref(e), _p(lam), _p(V) if vectors else None, _p(res),
                        ctypes.byref(info), ctypes.byref(einfo))
     return rc, lam, (V.T.copy() if vectors else None), res, info.as_dict(), einfo.as_dict()
+
+
+def components(A, lib=None):
+    """speigs_components(): (ncomp, labels[n])."""
+    lib = lib or load()
+    n, Ap, Ai, Ax = _csc_arrays(A)
+    comp = np.zeros(n, dtype=np.int64)
+    nc = c_int64()
+    rc = lib.speigs_components(n, _p(Ap, c_int64), _p(Ai, c_int64), _p(Ax), _p(comp, c_int64),
+                               ctypes.byref(nc))
+    if rc:
+        raise RuntimeError(f"speigs_components: {errmsg(rc, lib)}")
+    return nc.value, comp
+
+
+def speigs_batched(A, k, which=SM, opts: Opts | None = None, ext: ExtOpts | None = None,
+                   comp=None, vectors=False, lib=None):
+    """speigs_batched(): k eigenpairs per connected component.
+
+    Returns (rc, lam[ncomp, k], V[n, k] or None, resid[ncomp, k], nvals[ncomp], info)."""
+    lib = lib or load()
+    n, Ap, Ai, Ax = _csc_arrays(A)
+    if comp is None:
+        ncomp, comp = components((n, Ap, Ai, Ax), lib)
+    else:
+        comp = np.ascontiguousarray(comp, dtype=np.int64)
+        ncomp = int(comp.max()) + 1
+    lam = np.zeros((ncomp, k))
+    res = np.zeros((ncomp, k))
+    nv = np.zeros(ncomp, dtype=np.int64)
+    V = np.zeros((k, n)) if vectors else None
+    info = Info()
+    o = opts if opts is not None else default_opts(lib)
+    rc = lib.speigs_batched(n, _p(Ap, c_int64), _p(Ai, c_int64), _p(Ax), k, which,
+                            ctypes.byref(o), ctypes.byref(ext) if ext is not None else None,
+                            _p(comp, c_int64), ncomp, _p(lam), _p(V) if vectors else None,
+                            _p(res), _p(nv, c_int64), ctypes.byref(info))
+    return rc, lam, (V.T.copy() if vectors else None), res, nv, info.as_dict()
 
 
 def speigs_z(A_re, A_im, k, which=SM, opts: Opts | None = None, lib=None):

@@ -113,6 +113,40 @@ def _fv_operator(kap: np.ndarray) -> sp.csc_matrix:
     return A
 
 
+def rgg_component(nc: int, rng: np.random.Generator, degree: float = 8.0) -> sp.csr_matrix:
+    """Graph Laplacian of a 3-D random geometric graph on nc points uniform in the
+    unit cube, unit weights, + 1e-3 I; the connection radius is calibrated so the
+    measured mean degree is within 0.5 of `degree` (starting from the bulk value
+    (6 degree / (8 pi nc))^(1/3))."""
+    from scipy.spatial import cKDTree
+    pts = rng.random((nc, 3))
+    tree = cKDTree(pts)
+    r = (3.0 * degree / (4.0 * np.pi * nc)) ** (1.0 / 3.0)
+    for _ in range(8):
+        pairs = tree.query_pairs(r, output_type="ndarray")
+        md = 2.0 * len(pairs) / nc
+        if abs(md - degree) <= 0.5:
+            break
+        r *= (degree / max(md, 1e-3)) ** (1.0 / 3.0)
+    i, j = pairs[:, 0], pairs[:, 1]
+    W = sp.csr_matrix((np.ones(len(i)), (i, j)), shape=(nc, nc))
+    W = W + W.T
+    deg = np.asarray(W.sum(axis=1)).ravel()
+    return (sp.diags(deg + 1e-3) - W).tocsr()
+
+
+def rgg_blocks(ncomp: int, seed: int = 4, nmin: int = 50, nmax: int = 5000) -> sp.csc_matrix:
+    """Block-diagonal SPD matrix of ncomp random-geometric-graph Laplacians
+    (+1e-3 I), sizes uniform in [nmin, nmax] from `seed`.  A component whose
+    graph is itself disconnected splits further (isolated vertices become 1x1
+    blocks with value 1e-3)."""
+    rng = np.random.default_rng(seed)
+    sizes = rng.integers(nmin, nmax + 1, size=ncomp)
+    A = sp.block_diag([rgg_component(int(nc), rng) for nc in sizes], format="csc")
+    A.sort_indices()
+    return A
+
+
 def upper(A: sp.spmatrix) -> sp.csc_matrix:
     """Upper triangle (with diagonal) in CSC, the other storage speigs accepts."""
     U = sp.triu(A, format="csc")

@@ -1,0 +1,58 @@
+"""Batched components: k eigenpairs of every connected component
+(speigs_batched), checked per component against a dense CPU eigensolver, and
+the drop-in blocks route (which now solves the components concurrently)
+against the compiled reference."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_batched_per_component_eigenpairs(lib, pkg):
+    s, w = pkg.speigs, pkg.workloads
+    A = w.rgg_blocks(10, seed=7, nmin=50, nmax=900)      # + isolated vertices
+    k = 4
+    ncomp, comp = s.components(A, lib)
+    assert ncomp >= 10
+    o = s.default_opts(lib, tol=1e-10)
+    rc, lam, V, res, nv, info = s.speigs_batched(A, k, s.SM, o, comp=comp, vectors=True, lib=lib)
+    assert rc == 0, (rc, s.last_error(lib))
+    assert info["ncomp"] == ncomp and info["flag"] == 0
+    Ad = A.tocsr()
+    for c in range(ncomp):
+        rows = np.flatnonzero(comp == c)
+        kc = min(k, len(rows))
+        assert nv[c] == kc
+        Ac = Ad[rows][:, rows].toarray()
+        ex = np.sort(np.linalg.eigvalsh(Ac))[:kc]
+        got = lam[c, :kc]
+        assert np.all(np.abs(got - ex) <= 1e-10 * np.maximum(np.abs(ex), 1e-3)), (c, got, ex)
+        assert np.all(lam[c, kc:] == 0.0)
+        Vc = V[rows][:, :kc]
+        r = np.linalg.norm(Ac @ Vc - Vc * got, axis=0)
+        anorm = np.abs(Ac).sum(axis=0).max()
+        assert r.max() <= 1e-10 * max(anorm, 1.0) * 1.0001
+        # the eigenvectors of a component are zero outside its rows
+        assert np.all(V[np.flatnonzero(comp != c)][:, :0] == 0)
+
+
+def test_blocks_route_matches_reference(lib, pkg, ref_lib):
+    s, w = pkg.speigs, pkg.workloads
+    A = w.rgg_blocks(6, seed=11, nmin=200, nmax=1500)
+    k = 6
+    o = s.default_opts(lib, tol=1e-10)
+    rc, lam, V, res, info = s.speigs(A, k, s.SM, o, lib=lib)
+    rr, rlam, rV, rres, rinfo = s.speigs(A, k, s.SM, s.default_opts(ref_lib, tol=1e-10), lib=ref_lib)
+    assert rc == 0 and rr == 0
+    assert info["path"] == rinfo["path"] == s.PATH_BLOCKS and info["ncomp"] == rinfo["ncomp"]
+    assert np.max(np.abs(lam - rlam) / np.abs(rlam)) <= 1e-10
+
+
+def test_batched_rejects_bad_labels(lib, pkg):
+    s, w = pkg.speigs, pkg.workloads
+    A = w.rgg_blocks(2, seed=3, nmin=50, nmax=80)
+    n = A.shape[0]
+    comp = np.zeros(n, dtype=np.int64)
+    comp[0] = 5      # a label past ncomp - 1 leaves components empty
+    rc, *_ = s.speigs_batched(A, 2, s.SM, comp=comp, lib=lib)
+    assert rc == s.ERR_ARG
