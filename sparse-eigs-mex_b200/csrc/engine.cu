@@ -309,7 +309,9 @@ inline void orth_block(const LanczosBufs &b, const double *B, int m, double *w, 
 static int lanczos_device(Operator &op, const DevA &A, int n, int64_t k, const speigs_opts &o,
                           double anorm, double *lambda, double *resid, const double **Xdev,
                           int64_t *ldx, int *nout, speigs_info *info, EngineStats *stats,
-                          Arena &ar, double *pinned, cudaStream_t st) {
+                          Arena &ar, double *pinned, cudaStream_t st,
+                          const double *warm = nullptr, int64_t warm_cols = 0,
+                          int64_t *warm_used = nullptr) {
     int64_t ncv = o.ncv ? o.ncv : std::max<int64_t>(2 * k + 1, 20);
     if (ncv > n) ncv = n;
     if (ncv <= k) ncv = std::min<int64_t>(n, k + 1);
@@ -336,7 +338,7 @@ static int lanczos_device(Operator &op, const DevA &A, int n, int64_t k, const s
     b.AX = ar.alloc<double>((size_t)b.ldv * b.kk);
     b.lam = ar.alloc<double>(b.kk);
     b.r2 = ar.alloc<double>(b.kk);
-    b.xn2 = ar.alloc<double>(std::max<int64_t>(b.kk, 1));
+    b.xn2 = ar.alloc<double>(std::max<int64_t>(ncv + 1, b.kk));
     b.h1 = ar.alloc<double>(ncv + 1);
     b.h2 = ar.alloc<double>(ncv + 1);
     b.nrm2 = ar.alloc<double>(4);
@@ -382,15 +384,61 @@ static int lanczos_device(Operator &op, const DevA &A, int n, int64_t k, const s
         seed = rng_advance(seed, (uint64_t)n);
     };
 
-    // start vector (reference :187-191)
-    rand_vec(b.w);
-    launch_ts_norm(n, b.w, b.nrm2, b.rs, st);
-    double nr0 = 0;
-    if (int e = read_nrm(&nr0)) return e;
-    if (nr0 == 0.0) return SPEIGS_ERR_INTERNAL;
-    normalise(n, b.w, b.nrm2, b.V, st);
-
     int64_t j = 0, restarts = 0, nconv = 0;
+    if (warm_used) *warm_used = 0;
+    const int64_t pmax = std::min<int64_t>(warm_cols, ncv - 2);
+    if (warm && pmax >= 1) {
+        // Start subspace Y (device, n x warm_cols, leading dimension n): the
+        // start vector becomes the normalised sum of an orthonormal basis of
+        // Y plus a 1e-8 share of the reference's random start (so no
+        // eigenvector is missing from it), and the reference's algorithm runs
+        // unchanged from there.  Seeding the recurrence with a vector keeps
+        // the thick-restart invariant (a rank-one residual), which a set of
+        // retained vectors taken from Y would break.  Dependent columns of Y
+        // are dropped.
+        int q = 0;
+        double *acc = b.Vn + (size_t)ncv * b.ldv;   // running sum of the basis
+        launch_fill(n, 0.0, acc, st);
+        for (int i = 0; i < (int)pmax; i++) {
+            double *dst = b.Vn + (size_t)q * b.ldv;
+            launch_copy(n, warm + (size_t)i * n, dst, st);
+            launch_ts_norm(n, dst, b.nrm2, b.rs, st);
+            double n0 = 0;
+            if (int e = read_nrm(&n0)) return e;
+            if (!(n0 > 0.0)) continue;
+            orth_block(b, b.Vn, q, dst, nullptr, st);
+            double n1 = 0;
+            if (int e = read_nrm(&n1)) return e;
+            if (!(n1 > 1e-8 * n0)) continue;
+            normalise(n, dst, b.nrm2, dst, st);
+            launch_axpby(n, 1.0, dst, 1.0, acc, st);
+            q++;
+        }
+        if (q >= 1) {
+            rand_vec(b.w);
+            launch_ts_norm(n, b.w, b.nrm2, b.rs, st);
+            double nr = 0;
+            if (int e = read_nrm(&nr)) return e;
+            launch_axpby(n, 1.0 / std::sqrt((double)q), acc, 1e-8 / nr, b.w, st);
+            launch_ts_norm(n, b.w, b.nrm2, b.rs, st);
+            if (int e = read_nrm(&nr)) return e;
+            normalise(n, b.w, b.nrm2, b.V, st);
+            j = -1;   // start vector in place
+            if (warm_used) *warm_used = q;
+        }
+    }
+    if (j == -1) {
+        j = 0;
+    } else {
+        // start vector (reference :187-191)
+        rand_vec(b.w);
+        launch_ts_norm(n, b.w, b.nrm2, b.rs, st);
+        double nr0 = 0;
+        if (int e = read_nrm(&nr0)) return e;
+        if (nr0 == 0.0) return SPEIGS_ERR_INTERNAL;
+        normalise(n, b.w, b.nrm2, b.V, st);
+    }
+
     int rc = SPEIGS_OK;
     int last_nwant = 0;   // Ritz vectors of the last Rayleigh-Ritz stay in X
     for (;;) {
@@ -795,8 +843,20 @@ static int plan_solve(speigs_plan_s *p, int64_t k, double *lambda, double *V, do
         int64_t ldx = 0;
         int nout = 0;
         const double ti = wall();
+        // start subspace (host, n x ext_warm_cols) to the device
+        const double *dwarm = nullptr;
+        const int64_t wcols = p->ext_warm ? std::min<int64_t>(p->ext_warm_cols, 64) : 0;
+        if (wcols > 0) {
+            double *dw = ar.alloc<double>((size_t)n * wcols);
+            if (ar.failed) return SPEIGS_ERR_MEM;
+            copy_async(dw, p->ext_warm, sizeof(double) * (size_t)n * wcols,
+                       on_device ? cudaMemcpyDefault : cudaMemcpyHostToDevice, st);
+            dwarm = dw;
+        }
+        int64_t wused = 0;
         rc = lanczos_device(*op, dA, n, k, p->opts, p->anorm, lam_h.data(), res_h.data(), &X,
-                            &ldx, &nout, info, stats, ar, p->pinned, st);
+                            &ldx, &nout, info, stats, ar, p->pinned, st, dwarm, wcols, &wused);
+        p->last_warm = wused;
         p->last_ops = op->nops;
         if (rc == 0 && p->mf.mixed) {
             int cnt = 0;

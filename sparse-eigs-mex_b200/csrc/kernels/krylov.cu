@@ -725,6 +725,18 @@ void launch_syev_small_workspace(int m, const double *H, int ldh, double *theta,
     note_launch();
 }
 
+__global__ void axpby_kernel(int64_t n, double a, const double *x, double b, double *y) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        y[i] = a * x[i] + b * y[i];
+}
+void launch_axpby(int64_t n, double a, const double *x, double b, double *y, cudaStream_t st) {
+    if (n <= 0) return;
+    const int nb = (int)std::max<int64_t>(1, std::min<int64_t>(4096, (n + 255) / 256));
+    axpby_kernel<<<nb, 256, 0, st>>>(n, a, x, b, y);
+    note_launch();
+}
+
 // ------------------------------------------------------------- helpers --
 __global__ void set_diag_kernel(int ldh, int nd, const double *d, double *H) {
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ldh * ldh; t += gridDim.x * blockDim.x) {

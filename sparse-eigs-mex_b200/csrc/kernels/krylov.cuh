@@ -91,6 +91,9 @@ void launch_refine_residual(int n, const int32_t *rowptr, const int32_t *col, co
 // y += d unless *flag
 void launch_axpy_unless(int n, double *y, const double *d, const int *flag, cudaStream_t st);
 
+// y = a x + b y
+void launch_axpby(int64_t n, double a, const double *x, double b, double *y, cudaStream_t st);
+
 // generic helpers
 void launch_copy(int64_t n, const double *src, double *dst, cudaStream_t st);
 void launch_fill(int64_t n, double v, double *dst, cudaStream_t st);

@@ -77,6 +77,87 @@ def varcoef3d(N: int, seed: int = 3, sigma: float = 1.0) -> sp.csc_matrix:
     return _fv_operator(kap)
 
 
+def grf_conductivity(N: int, seed: int, corr_len: float = 0.1, variance: float = 1.0) -> np.ndarray:
+    """kappa = exp(g) on an N^3 cell grid, g a stationary Gaussian random field with
+    squared-exponential covariance variance * exp(-|x-y|^2 / (2 corr_len^2)) on the
+    unit cube, by spectral synthesis: white noise filtered by the square root of
+    the field's power spectrum on a periodic 2N grid (cropped), then scaled to
+    the requested variance.  Index order [z, y, x] like varcoef3d."""
+    rng = np.random.default_rng(seed)
+    M = 2 * N
+    h = 1.0 / N
+    k = 2.0 * np.pi * np.fft.fftfreq(M, d=h)
+    kx, ky, kz = np.meshgrid(k, k, k, indexing="ij")
+    spec = np.exp(-0.5 * corr_len ** 2 * (kx ** 2 + ky ** 2 + kz ** 2))
+    noise = rng.standard_normal((M, M, M))
+    g = np.fft.ifftn(np.fft.fftn(noise) * np.sqrt(spec)).real[:N, :N, :N]
+    g = (g - g.mean()) / g.std() * np.sqrt(variance)
+    return np.exp(g)
+
+
+def grf3d(N: int, seed: int) -> sp.csc_matrix:
+    """Finite-volume diffusion operator with kappa = exp(GRF) (grf_conductivity)."""
+    return _fv_operator(grf_conductivity(N, seed))
+
+
+class FVPattern:
+    """The fixed sparsity pattern of the N^3 finite-volume operator and the map
+    from face transmissibilities to its CSC values, so a family of operators
+    (same grid, new conductivities) is assembled without rebuilding the pattern."""
+
+    def __init__(self, N: int):
+        self.N = N
+        base = _fv_operator(np.ones((N, N, N)))
+        self.A = base
+        n = N ** 3
+        idx = np.arange(n).reshape(N, N, N)
+        # locate every matrix entry in CSC order: (row, col) -> position
+        A = base.tocsc()
+        cols = np.repeat(np.arange(n), np.diff(A.indptr))
+        rows = A.indices
+        key = rows.astype(np.int64) * n + cols
+        order = np.argsort(key)
+        sk = key[order]
+
+        def pos(r, c):
+            return order[np.searchsorted(sk, r.astype(np.int64) * n + c)]
+        self.faces = []
+        for ax in range(3):
+            a = [slice(None)] * 3
+            b = [slice(None)] * 3
+            a[ax] = slice(0, N - 1)
+            b[ax] = slice(1, N)
+            ia, ib = idx[tuple(a)].ravel(), idx[tuple(b)].ravel()
+            self.faces.append((tuple(a), tuple(b), ia, ib, pos(ia, ib), pos(ib, ia)))
+        self.diag_pos = pos(idx.ravel(), idx.ravel())
+
+    def values(self, kap: np.ndarray) -> np.ndarray:
+        """CSC values of the operator for cell conductivities kap[z, y, x]."""
+        N = self.N
+        x = np.zeros(self.A.nnz)
+        diag = np.zeros((N, N, N))
+        for ax, (a, b, ia, ib, pab, pba) in enumerate(self.faces):
+            ka, kb = kap[a], kap[b]
+            t = 2.0 * ka * kb / (ka + kb)
+            diag[a] += t
+            diag[b] += t
+            x[pab] = -t.ravel()
+            x[pba] = -t.ravel()
+            lo = [slice(None)] * 3
+            hi = [slice(None)] * 3
+            lo[ax] = 0
+            hi[ax] = N - 1
+            diag[tuple(lo)] += 2.0 * kap[tuple(lo)]
+            diag[tuple(hi)] += 2.0 * kap[tuple(hi)]
+        x[self.diag_pos] = diag.ravel()
+        return x
+
+    def matrix(self, kap: np.ndarray) -> sp.csc_matrix:
+        A = self.A.copy()
+        A.data = self.values(kap)
+        return A
+
+
 def _fv_operator(kap: np.ndarray) -> sp.csc_matrix:
     N = kap.shape[0]
     n = N ** 3
@@ -111,6 +192,23 @@ def _fv_operator(kap: np.ndarray) -> sp.csc_matrix:
     A.sum_duplicates()
     A.sort_indices()
     return A
+
+
+def laplace_modes(N: int, p: int) -> np.ndarray:
+    """The p lowest eigenvectors of the Dirichlet 7-point Laplacian on the N^3
+    grid (products of sines, closed form), n x p, unit 2-norm columns, ordered
+    by eigenvalue (ties in a fixed order).  Index order x fastest."""
+    m = int(np.ceil(p ** (1.0 / 3.0))) + 2
+    e1 = 2.0 - 2.0 * np.cos(np.arange(1, m + 1) * np.pi / (N + 1))
+    trip = [(e1[a] + e1[b] + e1[c], a, b, c) for a in range(m) for b in range(m) for c in range(m)]
+    trip.sort()
+    g = np.arange(1, N + 1) * np.pi / (N + 1)
+    Y = np.empty((N ** 3, p))
+    for t, (_, a, b, c) in enumerate(trip[:p]):
+        sx, sy, sz = np.sin((a + 1) * g), np.sin((b + 1) * g), np.sin((c + 1) * g)
+        f = (sz[:, None, None] * sy[None, :, None] * sx[None, None, :]).ravel()
+        Y[:, t] = f / np.linalg.norm(f)
+    return Y
 
 
 def rgg_component(nc: int, rng: np.random.Generator, degree: float = 8.0) -> sp.csr_matrix:
