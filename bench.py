@@ -59,6 +59,14 @@ def workloads(w, s):
         "varcoef64": dict(desc="3-D variable-coefficient FV diffusion 64^3 (n=262,144), log-normal "
                                "conductivity (sigma=1, seed 3), k=20 'sm', tol 1e-10",
                           build=lambda: w.varcoef3d(64, seed=3), k=20, which=s.SM, exact=None),
+        "grf48": dict(desc="3-D FV diffusion 48^3 (n=110,592), conductivity exp(GRF) (SE "
+                           "covariance, length 0.1, variance 1), held-out seed 3200, k=16 'sm', "
+                           "tol 1e-10",
+                      build=lambda: w.grf3d(48, 3200), k=16, which=s.SM, exact=None),
+        "rgg": dict(desc="block-diagonal SPD: 256 random-geometric-graph Laplacians (+1e-3 I), "
+                         "sizes U[50, 5000] (seed 4), mean degree 8, k=4 'sm' per component, "
+                         "tol 1e-10",
+                    build=lambda: w.rgg_blocks(256, seed=4), k=4, which=s.SM, exact=None),
     }
 
 
@@ -172,6 +180,159 @@ def run_reference(args, pkg, wl, rank):
     return 0
 
 
+def _dev_time(torch, fn, steps, warmup, stream):
+    for _ in range(warmup):
+        fn()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    ms = []
+    for _ in range(steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    return statistics.mean(ms), out
+
+
+def run_forms_grf(args, pkg, wl):
+    """The four forms on one held-out GRF operator, same B200: plain FP64 with
+    the reference's random start, FP64 with the learned start, mixed precision
+    with the random start, mixed with the learned start (the target form).
+    Device time per solve (factor + Lanczos, matrix resident), and end to end
+    through speigs_ex including the network's proposal."""
+    import torch
+    s, w, L = pkg.speigs, pkg.workloads, pkg.learned
+    lib = s.load()
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    A = wl["build"]()
+    n, k = A.shape[0], wl["k"]
+    opts = s.default_opts(lib, tol=TOL)
+    kap = w.grf_conductivity(48, 3200)
+    have_net = os.path.exists(L.CHECKPOINT)
+    net = L.WarmStartNet.load(L.CHECKPOINT, lib=lib) if have_net else None
+    t0 = time.perf_counter()
+    Y = L.propose(net, 48, kap) if net is not None else None
+    t_prop = time.perf_counter() - t0
+    Yf = np.asfortranarray(Y) if Y is not None else None
+    forms = {}
+    for name, prec, warm in (("fp64", s.FP64, None), ("fp64+learned", s.FP64, Yf),
+                             ("mixed", s.MIXED, None), ("mixed+learned", s.MIXED, Yf)):
+        if "learned" in name and warm is None:
+            continue
+        ext = s.ext_opts(lib, precision=prec, warm=warm)
+        plan = s.Plan(A, s.SM, opts, lib=lib, ext=ext)
+        pstream = torch.cuda.ExternalStream(plan.stream(), device=dev)
+        lam = torch.zeros(k, dtype=torch.float64, device=dev)
+        V = torch.zeros((k, n), dtype=torch.float64, device=dev)
+        res = torch.zeros(k, dtype=torch.float64, device=dev)
+        box = {}
+
+        def solve():
+            rc, info = plan.solve_device(k, lam.data_ptr(), V.data_ptr(), res.data_ptr())
+            if rc != 0:
+                raise RuntimeError(f"{name}: rc={rc} {s.last_error(lib)}")
+            box["info"] = info
+            return info
+        ms, info = _dev_time(torch, solve, args.steps, args.warmup, pstream)
+        ei = plan.ext_info()
+        lam_h = lam.cpu().numpy()
+        Vh = V.cpu().numpy().T
+        r = np.linalg.norm(A @ Vh - Vh * lam_h, axis=0)
+        plan.close()
+        e2e = []
+        for _ in range(max(2, min(args.steps, 3))):
+            t1 = time.perf_counter()
+            if "learned" in name:
+                Yp = L.propose(net, 48, kap)
+                ext2 = s.ext_opts(lib, precision=prec)
+                rc, *_ = s.speigs_ex(A, k, s.SM, opts, ext2, vectors=True, lib=lib, warm=Yp)
+            else:
+                rc, *_ = s.speigs_ex(A, k, s.SM, opts, ext, vectors=True, lib=lib)
+            e2e.append(time.perf_counter() - t1)
+        forms[name] = {"value_s": ms * 1e-3, "e2e_s": statistics.mean(e2e), "nops": int(info["nops"]),
+                       "restarts": int(info["restarts"]), "refine_steps": int(ei["refine_steps"]),
+                       "warm_cols": int(ei["warm_cols"]), "lam": lam_h.tolist(),
+                       "max_resid_over_anorm": float(r.max() / info["anorm"]),
+                       "t_factor": info["t_factor"], "t_iter": info["t_iter"]}
+    base = np.array(forms["fp64"]["lam"])
+    for f in forms.values():
+        f["eig_rel_err_vs_fp64"] = (np.abs(np.array(f.pop("lam")) - base) / np.abs(base)).tolist()
+    target = "mixed+learned" if "mixed+learned" in forms else "mixed"
+    line = {
+        "metric": METRIC, "value": forms[target]["value_s"], "unit": "s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": forms[target]["value_s"] * 1e3,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": wl["desc"], "n": int(n), "nnz": int(A.nnz), "k": k, "tol": TOL,
+                   "form": target, "checkpoint": os.path.relpath(L.CHECKPOINT, ROOT) if have_net else None,
+                   "l2": "256 MiB buffer written between timed steps"},
+        "forms": forms, "proposal_s": t_prop,
+        "ratio_target_over_fp64_value": forms[target]["value_s"] / forms["fp64"]["value_s"],
+        "e2e": {"value": forms[target]["e2e_s"], "unit": "s"},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def run_batched(args, pkg, wl):
+    """k eigenpairs of every component through speigs_batched (components
+    solved concurrently), end to end from host CSC arrays; the reference's CPU
+    solver timed per component on a bounded sample of the same components."""
+    s, w = pkg.speigs, pkg.workloads
+    lib = s.load()
+    A = wl["build"]()
+    n, k = A.shape[0], wl["k"]
+    opts = s.default_opts(lib, tol=TOL)
+    ncomp, comp = s.components(A, lib)
+    for _ in range(args.warmup):
+        rc, *_ = s.speigs_batched(A, k, s.SM, opts, comp=comp, lib=lib)
+    ts = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        rc, lam, V, res, nv, info = s.speigs_batched(A, k, s.SM, opts, comp=comp, lib=lib)
+        ts.append(time.perf_counter() - t0)
+        if rc != 0:
+            raise RuntimeError(f"batched rc={rc} {s.last_error(lib)}")
+    cpu = None
+    if os.path.exists(REF_LIB) and not args.no_cpu_baseline:
+        ref = s.load(REF_LIB)
+        o = s.default_opts(ref, tol=TOL)
+        Ad = A.tocsr()
+        sizes = np.bincount(comp)
+        big = np.flatnonzero(sizes > 1)[:12]
+        t_ref, n_ref = 0.0, 0
+        for c in big:
+            rows = np.flatnonzero(comp == c)
+            Ac = Ad[rows][:, rows].tocsc()
+            t0 = time.perf_counter()
+            rr, *_ = s.speigs(Ac, min(k, len(rows)), s.SM, o, vectors=True, lib=ref)
+            t_ref += time.perf_counter() - t0
+            n_ref += len(rows)
+        # scale by nodes: the reference solves components one after another
+        cpu = {"value": t_ref * (n / n_ref), "unit": "s", "cores": os.cpu_count(), "kind": "reference",
+               "sample": f"{len(big)} components ({n_ref} nodes) solved by the reference's "
+                         "src/speigs_core.c one by one, time scaled to all {n} nodes".replace("{n}", str(n))}
+    line = {
+        "metric": METRIC, "value": statistics.mean(ts), "unit": "s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.mean(ts) * 1e3,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": wl["desc"], "n": int(n), "nnz": int(A.nnz), "ncomp": int(ncomp),
+                   "k": k, "tol": TOL, "form": "batched (speigs_batched)",
+                   "value_scope": "end to end: host CSC in, per-component results out"},
+        "check": {"flag": int(info["flag"]), "nops": int(info["nops"])},
+        "cpu_baseline": cpu,
+        "e2e": {"value": statistics.mean(ts), "unit": "s"},
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -197,6 +358,10 @@ def main():
 
     if args.impl == "reference":
         return run_reference(args, pkg, wl, rank)
+    if args.workload == "grf48":
+        return run_forms_grf(args, pkg, wl)
+    if args.workload == "rgg":
+        return run_batched(args, pkg, wl)
 
     import torch
     import torch.distributed as dist

@@ -83,6 +83,35 @@ int speigs_batched(speigs_int n, const speigs_int *Ap, const speigs_int *Ai, con
                    double *lambda, double *V, double *resid, speigs_int *nvals,
                    speigs_info *info);
 
+/* ---- learned warm start: the message-passing network -----------------------
+ * h0 = tanh(W0 x + b0); h_l = tanh(W_l [h_{l-1}, A h_{l-1}] + b_l), l = 1..L;
+ * Y = W_o h_L + b_o.  x: nfeat features per node (FP32), A: a sparse
+ * normalised adjacency given as CSR (int32 row pointers and columns, FP32
+ * weights), Y: nout channels per node (FP32), all row-major (node-major) and
+ * in DEVICE memory.  Weights and activations are BF16 with FP32
+ * accumulation; the optimiser (Adam) keeps FP32 weights.  Training
+ * minimises 1 - trace(U^T P_Y U) / k, the share of the k target vectors U
+ * (orthonormal columns, node-major n x k) outside span(Y).  hidden must be
+ * 64; nfeat, nout <= 64; layers <= 8.  Calls on one network must not overlap.
+ * No counterpart in the reference interface. */
+typedef struct speigs_mpnn_s *speigs_mpnn;
+int  speigs_b200_mpnn_create(int nfeat, int hidden, int layers, int nout, uint64_t seed,
+                             speigs_mpnn *net);
+void speigs_b200_mpnn_destroy(speigs_mpnn net);
+/* FP32 weights to (set = 0) or from (set = 1) host memory; host == NULL
+ * reports the count in *count. */
+int  speigs_b200_mpnn_params(speigs_mpnn net, float *host, int64_t *count, int set);
+/* Gradient of the last training step (FP32, host). */
+int  speigs_b200_mpnn_grads(speigs_mpnn net, float *host);
+int  speigs_b200_mpnn_forward(speigs_mpnn net, int64_t n, const int32_t *rowptr,
+                              const int32_t *col, const float *w, const float *X, float *Y,
+                              void *stream);
+/* Forward, loss, backward and (lr > 0) one Adam step; *loss receives the
+ * loss before the step. */
+int  speigs_b200_mpnn_train_step(speigs_mpnn net, int64_t n, const int32_t *rowptr,
+                                 const int32_t *col, const float *w, const float *X,
+                                 const float *U, int k, float lr, double *loss, void *stream);
+
 /* Opaque solver plan: one connected symmetric matrix on one GPU, with its
  * operator ('sm': symbolic analysis done, numeric factor per solve; 'lm':
  * the matrix itself) and every device buffer the Lanczos iteration needs.

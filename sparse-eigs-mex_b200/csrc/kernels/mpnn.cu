@@ -1,0 +1,521 @@
+// Message-passing network that proposes a start subspace for the Lanczos
+// iteration of a finite-volume diffusion operator (the learned warm start).
+//
+//   h0   = tanh(W0 x + b0)                          x: F node features
+//   h_l  = tanh(W_l [h_{l-1}, A h_{l-1}] + b_l)     l = 1..L, A the normalised
+//                                                   adjacency of the operator
+//   Y    = W_o h_L + b_o                            P outputs per node
+//
+// Activations are stored in BF16, weights are used in BF16 and kept in FP32
+// for the optimiser; every product accumulates in FP32.  Training minimises
+// the subspace loss 1 - trace(U^T P_Y U) / k, P_Y the orthogonal projector
+// onto span(Y) and U the k eigenvectors the solver computed for the same
+// operator; its gradient is dL/dY = -(2/k) (U - Y C) C^T with
+// C = (Y^T Y)^{-1} Y^T U.  Adam updates the FP32 weights.
+#include "../common.cuh"
+#include "../counters.h"
+#include "../../../include/speigs_b200.h"
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+namespace spx {
+const char *set_last_error_text(const char *msg);
+cudaMemPool_t device_pool(int dev);
+}
+
+namespace {
+
+using bf16 = __nv_bfloat16;
+constexpr int kRows = 64;       // nodes per block in the dense layers
+constexpr int kThreads = 256;
+
+SPX_DEV float to_f(bf16 v) { return __bfloat162float(v); }
+SPX_DEV float to_f(float v) { return v; }
+template <class T> SPX_DEV T from_f(float v);
+template <> SPX_DEV bf16 from_f<bf16>(float v) { return __float2bfloat16(v); }
+template <> SPX_DEV float from_f<float>(float v) { return v; }
+
+// ---- message passing: out = A in (one warp per node, 2 features a lane)
+template <class TI, class TO>
+__global__ void spmm_kernel(int n, int hid, const int32_t *__restrict__ rp,
+                            const int32_t *__restrict__ ci, const float *__restrict__ w,
+                            const TI *__restrict__ in, TO *__restrict__ out, int accumulate) {
+    const int lane = threadIdx.x & 31;
+    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (row >= n) return;
+    for (int f0 = 0; f0 < hid; f0 += 64) {
+        float a0 = 0.f, a1 = 0.f;
+        const int f = f0 + 2 * lane;
+        for (int q = rp[row]; q < rp[row + 1]; q++) {
+            const float wq = w[q];
+            const TI *src = in + (size_t)ci[q] * hid;
+            if (f < hid) a0 += wq * to_f(src[f]);
+            if (f + 1 < hid) a1 += wq * to_f(src[f + 1]);
+        }
+        TO *dst = out + (size_t)row * hid;
+        if (f < hid) dst[f] = from_f<TO>(accumulate ? to_f(dst[f]) + a0 : a0);
+        if (f + 1 < hid) dst[f + 1] = from_f<TO>(accumulate ? to_f(dst[f + 1]) + a1 : a1);
+    }
+}
+
+// ---- dense layer forward: out[i, o] = act(b[o] + sum_k W[o, k] x[i, k]),
+// x = [X1[i, 0:K1], X2[i, 0:K2]] (X2 may be absent).  act: 0 identity, 1 tanh.
+template <class T1, class TO>
+__global__ void __launch_bounds__(kThreads)
+dense_fwd_kernel(int n, int K1, const T1 *__restrict__ X1, int K2, const bf16 *__restrict__ X2,
+                 int N, const bf16 *__restrict__ W, const float *__restrict__ b, int act,
+                 TO *__restrict__ out) {
+    extern __shared__ float sm[];
+    const int K = K1 + K2;
+    float *Xs = sm;                       // kRows x (K + 1)
+    float *Ws = Xs + kRows * (K + 1);     // N x (K + 1)
+    const int r0 = blockIdx.x * kRows;
+    for (int t = threadIdx.x; t < kRows * K; t += blockDim.x) {
+        const int r = t / K, k = t % K, i = r0 + r;
+        float v = 0.f;
+        if (i < n) v = (k < K1) ? to_f(X1[(size_t)i * K1 + k]) : to_f(X2[(size_t)i * K2 + (k - K1)]);
+        Xs[r * (K + 1) + k] = v;
+    }
+    for (int t = threadIdx.x; t < N * K; t += blockDim.x) Ws[(t / K) * (K + 1) + t % K] = to_f(W[t]);
+    __syncthreads();
+    for (int t = threadIdx.x; t < kRows * N; t += blockDim.x) {
+        const int r = t / N, o = t % N, i = r0 + r;
+        if (i >= n) continue;
+        float acc = b[o];
+        const float *xr = Xs + r * (K + 1), *wr = Ws + o * (K + 1);
+        for (int k = 0; k < K; k++) acc += xr[k] * wr[k];
+        out[(size_t)i * N + o] = from_f<TO>(act ? tanhf(acc) : acc);
+    }
+}
+
+// ---- dense layer backward.  dZ = dOut * act'(out); dX1/dX2 (FP32; added
+// when `accumulate`) = dZ W; dW += dZ^T x; db += column sums of dZ.
+template <class T1, class TOut>
+__global__ void __launch_bounds__(kThreads)
+dense_bwd_kernel(int n, int K1, const T1 *__restrict__ X1, int K2, const bf16 *__restrict__ X2,
+                 int N, const bf16 *__restrict__ W, int act, const TOut *__restrict__ out,
+                 const float *__restrict__ dout, float *dX1, float *dX2, int accumulate,
+                 float *__restrict__ dW, float *__restrict__ db) {
+    extern __shared__ float sm[];
+    const int K = K1 + K2;
+    float *Xs = sm;                        // kRows x (K + 1)
+    float *Ws = Xs + kRows * (K + 1);      // N x (K + 1)
+    float *Zs = Ws + N * (K + 1);          // kRows x (N + 1)
+    const int r0 = blockIdx.x * kRows;
+    for (int t = threadIdx.x; t < kRows * K; t += blockDim.x) {
+        const int r = t / K, k = t % K, i = r0 + r;
+        float v = 0.f;
+        if (i < n) v = (k < K1) ? to_f(X1[(size_t)i * K1 + k]) : to_f(X2[(size_t)i * K2 + (k - K1)]);
+        Xs[r * (K + 1) + k] = v;
+    }
+    for (int t = threadIdx.x; t < N * K; t += blockDim.x) Ws[(t / K) * (K + 1) + t % K] = to_f(W[t]);
+    for (int t = threadIdx.x; t < kRows * N; t += blockDim.x) {
+        const int r = t / N, o = t % N, i = r0 + r;
+        float z = 0.f;
+        if (i < n) {
+            z = dout[(size_t)i * N + o];
+            if (act) {
+                const float y = to_f(out[(size_t)i * N + o]);
+                z *= 1.f - y * y;
+            }
+        }
+        Zs[r * (N + 1) + o] = z;
+    }
+    __syncthreads();
+    // dX = dZ W
+    if (dX1 || dX2)
+        for (int t = threadIdx.x; t < kRows * K; t += blockDim.x) {
+            const int r = t / K, k = t % K, i = r0 + r;
+            if (i >= n) continue;
+            float acc = 0.f;
+            for (int o = 0; o < N; o++) acc += Zs[r * (N + 1) + o] * Ws[o * (K + 1) + k];
+            float *dst = (k < K1) ? (dX1 ? dX1 + (size_t)i * K1 + k : nullptr)
+                                  : (dX2 ? dX2 + (size_t)i * K2 + (k - K1) : nullptr);
+            if (dst) *dst = accumulate ? *dst + acc : acc;
+        }
+    // dW += dZ^T x, db += sum dZ
+    for (int t = threadIdx.x; t < N * (K + 1); t += blockDim.x) {
+        const int o = t / (K + 1), k = t % (K + 1);
+        float acc = 0.f;
+        if (k < K)
+            for (int r = 0; r < kRows; r++) acc += Zs[r * (N + 1) + o] * Xs[r * (K + 1) + k];
+        else
+            for (int r = 0; r < kRows; r++) acc += Zs[r * (N + 1) + o];
+        if (acc != 0.f) {
+            if (k < K) atomicAdd(dW + (size_t)o * K + k, acc);
+            else atomicAdd(db + o, acc);
+        }
+    }
+}
+
+// ---- loss: G = Y^T Y (P x P), B = Y^T U (P x k), FP64 sums
+__global__ void __launch_bounds__(kThreads)
+gram_kernel(int n, int P, const float *__restrict__ Y, int k, const float *__restrict__ U,
+            double *G, double *B) {
+    extern __shared__ float sm[];
+    const int R = 128;
+    float *Ys = sm, *Us = sm + R * P;
+    const int r0 = blockIdx.x * R;
+    for (int t = threadIdx.x; t < R * P; t += blockDim.x) {
+        const int i = r0 + t / P;
+        Ys[t] = (i < n) ? Y[(size_t)i * P + t % P] : 0.f;
+    }
+    for (int t = threadIdx.x; t < R * k; t += blockDim.x) {
+        const int i = r0 + t / k;
+        Us[t] = (i < n) ? U[(size_t)i * k + t % k] : 0.f;
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < P * (P + k); t += blockDim.x) {
+        const int a = t / (P + k), c = t % (P + k);
+        double acc = 0.0;
+        if (c < P) {
+            if (c < a) continue;                      // symmetric: upper part
+            for (int r = 0; r < R; r++) acc += (double)Ys[r * P + a] * Ys[r * P + c];
+            atomicAdd(G + a * P + c, acc);
+        } else {
+            const int bcol = c - P;
+            for (int r = 0; r < R; r++) acc += (double)Ys[r * P + a] * Us[r * k + bcol];
+            atomicAdd(B + a * k + bcol, acc);
+        }
+    }
+}
+
+// C = (G + eps tr(G)/P I)^{-1} B by Cholesky in one block (P <= 64);
+// loss = 1 - trace(B^T C) / k.  G holds its upper triangle.
+__global__ void small_solve_kernel(int P, int k, const double *G, const double *B, float *C,
+                                   double *loss) {
+    __shared__ double L[64 * 64];
+    if (threadIdx.x == 0) {
+        double tr = 0.0;
+        for (int a = 0; a < P; a++) tr += G[a * P + a];
+        const double eps = 1e-8 * tr / P + 1e-300;
+        for (int a = 0; a < P; a++)
+            for (int c = 0; c < P; c++) L[a * 64 + c] = (a <= c ? G[a * P + c] : G[c * P + a]) + (a == c ? eps : 0.0);
+        for (int j = 0; j < P; j++) {
+            double d = L[j * 64 + j];
+            for (int t = 0; t < j; t++) d -= L[j * 64 + t] * L[j * 64 + t];
+            d = sqrt(d > 0.0 ? d : 1e-300);
+            L[j * 64 + j] = d;
+            for (int i = j + 1; i < P; i++) {
+                double s = L[i * 64 + j];
+                for (int t = 0; t < j; t++) s -= L[i * 64 + t] * L[j * 64 + t];
+                L[i * 64 + j] = s / d;
+            }
+        }
+        double tr2 = 0.0;
+        for (int b = 0; b < k; b++) {
+            double z[64], x[64];
+            for (int i = 0; i < P; i++) {
+                double s = B[i * k + b];
+                for (int t = 0; t < i; t++) s -= L[i * 64 + t] * z[t];
+                z[i] = s / L[i * 64 + i];
+            }
+            for (int i = P - 1; i >= 0; i--) {
+                double s = z[i];
+                for (int t = i + 1; t < P; t++) s -= L[t * 64 + i] * x[t];
+                x[i] = s / L[i * 64 + i];
+            }
+            for (int i = 0; i < P; i++) {
+                tr2 += B[i * k + b] * x[i];
+                C[i * k + b] = (float)x[i];
+            }
+        }
+        *loss = 1.0 - tr2 / k;
+    }
+}
+
+// dY[i, a] = -(2/k) sum_b (U[i, b] - sum_c Y[i, c] C[c, b]) C[a, b]
+__global__ void dy_kernel(int n, int P, int k, const float *__restrict__ Y,
+                          const float *__restrict__ U, const float *__restrict__ C, float *dY) {
+    extern __shared__ float Cs[];
+    for (int t = threadIdx.x; t < P * k; t += blockDim.x) Cs[t] = C[t];
+    __syncthreads();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float e[64];
+    for (int b = 0; b < k; b++) {
+        float s = U[(size_t)i * k + b];
+        for (int c = 0; c < P; c++) s -= Y[(size_t)i * P + c] * Cs[c * k + b];
+        e[b] = s;
+    }
+    const float sc = -2.f / k;
+    for (int a = 0; a < P; a++) {
+        float s = 0.f;
+        for (int b = 0; b < k; b++) s += e[b] * Cs[a * k + b];
+        dY[(size_t)i * P + a] = sc * s;
+    }
+}
+
+// Adam on the FP32 weights, refreshing their BF16 copies
+__global__ void adam_kernel(int64_t cnt, float *p, const float *g, float *m, float *v, float lr,
+                            float b1, float b2, float c1, float c2, float eps, bf16 *pb) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < cnt;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.f - b1) * gi;
+        const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        const float pi = p[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+        p[i] = pi;
+        pb[i] = __float2bfloat16(pi);
+    }
+}
+
+__global__ void to_bf16_kernel(int64_t cnt, const float *src, bf16 *dst) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < cnt;
+         i += (int64_t)gridDim.x * blockDim.x)
+        dst[i] = __float2bfloat16(src[i]);
+}
+
+template <class T>
+T *dalloc(size_t cnt) {
+    void *p = nullptr;
+    if (cudaMalloc(&p, (cnt ? cnt : 1) * sizeof(T)) != cudaSuccess) { cudaGetLastError(); return nullptr; }
+    return (T *)p;
+}
+
+}  // namespace
+
+struct speigs_mpnn_s {
+    int F = 0, H = 64, L = 4, P = 0;
+    int64_t nparam = 0;
+    std::vector<int64_t> woff, boff;   // per layer (0 = input, 1..L, L+1 = output)
+    float *p = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;
+    bf16 *pb = nullptr;
+    int64_t step = 0;
+    int64_t ncap = 0;
+    bf16 *Hs = nullptr, *Ms = nullptr;   // (L+1) x n x H, L x n x H
+    float *Y = nullptr, *dY = nullptr, *dH = nullptr, *dH2 = nullptr, *dM = nullptr;
+    double *G = nullptr, *B = nullptr, *loss = nullptr;
+    float *C = nullptr;
+    int kcap = 0;
+    ~speigs_mpnn_s() {
+        void *ptrs[] = {p, g, m, v, pb, Hs, Ms, Y, dY, dH, dH2, dM, G, B, loss, C};
+        for (void *q : ptrs)
+            if (q) cudaFree(q);
+    }
+    int layer_in(int l) const { return l == 0 ? F : (l <= L ? 2 * H : H); }
+    int layer_out(int l) const { return l <= L ? H : P; }
+    int reserve(int64_t n, int k) {
+        if (n <= ncap && k <= kcap) return 0;
+        void *ptrs[] = {Hs, Ms, Y, dY, dH, dH2, dM, G, B, loss, C};
+        for (void *q : ptrs)
+            if (q) cudaFree(q);
+        ncap = std::max(n, ncap);
+        kcap = std::max(k, kcap);
+        Hs = dalloc<bf16>((size_t)(L + 1) * ncap * H);
+        Ms = dalloc<bf16>((size_t)L * ncap * H);
+        Y = dalloc<float>((size_t)ncap * P);
+        dY = dalloc<float>((size_t)ncap * P);
+        dH = dalloc<float>((size_t)ncap * H);
+        dH2 = dalloc<float>((size_t)ncap * H);
+        dM = dalloc<float>((size_t)ncap * H);
+        G = dalloc<double>((size_t)P * P);
+        B = dalloc<double>((size_t)P * std::max(kcap, 1));
+        loss = dalloc<double>(1);
+        C = dalloc<float>((size_t)P * std::max(kcap, 1));
+        if (!Hs || !Ms || !Y || !dY || !dH || !dH2 || !dM || !G || !B || !loss || !C)
+            return SPEIGS_ERR_MEM;
+        return 0;
+    }
+};
+
+namespace {
+
+size_t dense_smem(int K, int N, bool bwd) {
+    size_t f = (size_t)kRows * (K + 1) + (size_t)N * (K + 1) + (bwd ? (size_t)kRows * (N + 1) : 0);
+    return f * sizeof(float);
+}
+
+void set_smem_limits() {
+    const int big = 200 * 1024;
+    cudaFuncSetAttribute(gram_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    cudaFuncSetAttribute(dense_fwd_kernel<float, bf16>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    cudaFuncSetAttribute(dense_fwd_kernel<bf16, bf16>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    cudaFuncSetAttribute(dense_fwd_kernel<bf16, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    cudaFuncSetAttribute(dense_bwd_kernel<float, bf16>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    cudaFuncSetAttribute(dense_bwd_kernel<bf16, bf16>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    cudaFuncSetAttribute(dense_bwd_kernel<bf16, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+}
+
+// forward pass keeping the activations; Y (FP32) in net->Y
+void forward(speigs_mpnn_s *net, int n, const int32_t *rp, const int32_t *ci, const float *w,
+             const float *X, cudaStream_t st) {
+    const int H = net->H, L = net->L;
+    const int nb = (n + kRows - 1) / kRows;
+    const int sb = (n + 7) / 8;
+    bf16 *Hl = net->Hs;
+    dense_fwd_kernel<float, bf16><<<nb, kThreads, dense_smem(net->F, H, false), st>>>(
+        n, net->F, X, 0, nullptr, H, net->pb + net->woff[0], net->p + net->boff[0], 1, Hl);
+    spx::note_launch();
+    for (int l = 1; l <= L; l++) {
+        bf16 *Hp = net->Hs + (size_t)(l - 1) * n * H, *Hn = net->Hs + (size_t)l * n * H;
+        bf16 *Ml = net->Ms + (size_t)(l - 1) * n * H;
+        spmm_kernel<bf16, bf16><<<sb, 256, 0, st>>>(n, H, rp, ci, w, Hp, Ml, 0);
+        dense_fwd_kernel<bf16, bf16><<<nb, kThreads, dense_smem(2 * H, H, false), st>>>(
+            n, H, Hp, H, Ml, H, net->pb + net->woff[l], net->p + net->boff[l], 1, Hn);
+        spx::note_launch(2);
+    }
+    dense_fwd_kernel<bf16, float><<<nb, kThreads, dense_smem(H, net->P, false), st>>>(
+        n, H, net->Hs + (size_t)L * n * H, 0, nullptr, net->P, net->pb + net->woff[L + 1],
+        net->p + net->boff[L + 1], 0, net->Y);
+    spx::note_launch();
+}
+
+}  // namespace
+
+extern "C" {
+
+int speigs_b200_mpnn_create(int nfeat, int hidden, int layers, int nout, uint64_t seed,
+                            speigs_mpnn *out) {
+    if (!out || nfeat < 1 || nfeat > 64 || hidden != 64 || layers < 0 || layers > 8 || nout < 1 ||
+        nout > 64)
+        return SPEIGS_ERR_ARG;
+    *out = nullptr;
+    speigs_mpnn_s *net = new (std::nothrow) speigs_mpnn_s;
+    if (!net) return SPEIGS_ERR_MEM;
+    net->F = nfeat;
+    net->H = hidden;
+    net->L = layers;
+    net->P = nout;
+    int64_t off = 0;
+    for (int l = 0; l <= layers + 1; l++) {
+        net->woff.push_back(off);
+        off += (int64_t)net->layer_out(l) * net->layer_in(l);
+        net->boff.push_back(off);
+        off += net->layer_out(l);
+    }
+    net->nparam = off;
+    // Xavier-uniform weights from a seeded xorshift64* stream, zero biases
+    std::vector<float> hp(off, 0.f);
+    uint64_t s = seed ? seed : 88172645463325252ULL;
+    auto uni = [&]() {
+        s ^= s >> 12; s ^= s << 25; s ^= s >> 27;
+        return (double)((s * 0x2545F4914F6CDD1DULL) >> 11) / 9007199254740992.0;
+    };
+    for (int l = 0; l <= layers + 1; l++) {
+        const int fi = net->layer_in(l), fo = net->layer_out(l);
+        const double a = std::sqrt(6.0 / (fi + fo)) * (l == layers + 1 ? 0.1 : 1.0);
+        for (int64_t t = 0; t < (int64_t)fi * fo; t++) hp[net->woff[l] + t] = (float)((2.0 * uni() - 1.0) * a);
+    }
+    net->p = dalloc<float>(off);
+    net->g = dalloc<float>(off);
+    net->m = dalloc<float>(off);
+    net->v = dalloc<float>(off);
+    net->pb = dalloc<bf16>(off);
+    if (!net->p || !net->g || !net->m || !net->v || !net->pb) { delete net; return SPEIGS_ERR_MEM; }
+    cudaMemcpy(net->p, hp.data(), sizeof(float) * off, cudaMemcpyHostToDevice);
+    cudaMemset(net->m, 0, sizeof(float) * off);
+    cudaMemset(net->v, 0, sizeof(float) * off);
+    cudaMemset(net->g, 0, sizeof(float) * off);
+    to_bf16_kernel<<<64, 256>>>(off, net->p, net->pb);
+    spx::note_launch();
+    set_smem_limits();
+    if (cudaDeviceSynchronize() != cudaSuccess) { cudaGetLastError(); delete net; return SPEIGS_ERR_INTERNAL; }
+    *out = net;
+    return SPEIGS_OK;
+}
+
+void speigs_b200_mpnn_destroy(speigs_mpnn net) { delete net; }
+
+int speigs_b200_mpnn_params(speigs_mpnn net, float *host, int64_t *count, int set) {
+    if (!net || !count) return SPEIGS_ERR_ARG;
+    if (!host) { *count = net->nparam; return SPEIGS_OK; }
+    if (*count < net->nparam) return SPEIGS_ERR_ARG;
+    if (set) {
+        cudaMemcpy(net->p, host, sizeof(float) * net->nparam, cudaMemcpyHostToDevice);
+        to_bf16_kernel<<<64, 256>>>(net->nparam, net->p, net->pb);
+        spx::note_launch();
+    } else {
+        cudaMemcpy(host, net->p, sizeof(float) * net->nparam, cudaMemcpyDeviceToHost);
+    }
+    *count = net->nparam;
+    return cudaDeviceSynchronize() == cudaSuccess ? SPEIGS_OK : SPEIGS_ERR_INTERNAL;
+}
+
+int speigs_b200_mpnn_grads(speigs_mpnn net, float *host) {
+    if (!net || !host) return SPEIGS_ERR_ARG;
+    cudaMemcpy(host, net->g, sizeof(float) * net->nparam, cudaMemcpyDeviceToHost);
+    return cudaDeviceSynchronize() == cudaSuccess ? SPEIGS_OK : SPEIGS_ERR_INTERNAL;
+}
+
+int speigs_b200_mpnn_forward(speigs_mpnn net, int64_t n, const int32_t *rowptr, const int32_t *col,
+                             const float *w, const float *X, float *Y, void *stream) {
+    if (!net || n <= 0 || n > INT32_MAX || !rowptr || !col || !w || !X || !Y) return SPEIGS_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (net->reserve(n, 1)) return SPEIGS_ERR_MEM;
+    forward(net, (int)n, rowptr, col, w, X, st);
+    cudaMemcpyAsync(Y, net->Y, sizeof(float) * (size_t)n * net->P, cudaMemcpyDeviceToDevice, st);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) { spx::set_last_error_text(cudaGetErrorString(e)); return SPEIGS_ERR_INTERNAL; }
+    return SPEIGS_OK;
+}
+
+int speigs_b200_mpnn_train_step(speigs_mpnn net, int64_t n, const int32_t *rowptr,
+                                const int32_t *col, const float *w, const float *X,
+                                const float *U, int k, float lr, double *loss, void *stream) {
+    if (!net || n <= 0 || n > INT32_MAX || !rowptr || !col || !w || !X || !U || k < 1 || k > 64)
+        return SPEIGS_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (net->reserve(n, k)) return SPEIGS_ERR_MEM;
+    const int H = net->H, L = net->L, P = net->P, nn = (int)n;
+    const int nb = (nn + kRows - 1) / kRows, sb = (nn + 7) / 8;
+    forward(net, nn, rowptr, col, w, X, st);
+    // loss and dL/dY
+    cudaMemsetAsync(net->G, 0, sizeof(double) * P * P, st);
+    cudaMemsetAsync(net->B, 0, sizeof(double) * P * k, st);
+    gram_kernel<<<(nn + 127) / 128, kThreads, sizeof(float) * 128 * (P + k), st>>>(nn, P, net->Y, k, U,
+                                                                               net->G, net->B);
+    small_solve_kernel<<<1, 32, 0, st>>>(P, k, net->G, net->B, net->C, net->loss);
+    dy_kernel<<<(nn + 127) / 128, 128, sizeof(float) * P * k, st>>>(nn, P, k, net->Y, U, net->C, net->dY);
+    spx::note_launch(3);
+    // backward
+    cudaMemsetAsync(net->g, 0, sizeof(float) * net->nparam, st);
+    bf16 *HL = net->Hs + (size_t)L * nn * H;
+    dense_bwd_kernel<bf16, float><<<nb, kThreads, dense_smem(H, P, true), st>>>(
+        nn, H, HL, 0, nullptr, P, net->pb + net->woff[L + 1], 0, net->Y, net->dY, net->dH, nullptr,
+        0, net->g + net->woff[L + 1], net->g + net->boff[L + 1]);
+    spx::note_launch();
+    for (int l = L; l >= 1; l--) {
+        bf16 *Hp = net->Hs + (size_t)(l - 1) * nn * H, *Hn = net->Hs + (size_t)l * nn * H;
+        bf16 *Ml = net->Ms + (size_t)(l - 1) * nn * H;
+        // dH currently holds dL/dh_l; produce dL/dh_{l-1} (direct part) and dL/dm_l
+        float *dHn = net->dH;
+        dense_bwd_kernel<bf16, bf16><<<nb, kThreads, dense_smem(2 * H, H, true), st>>>(
+            nn, H, Hp, H, Ml, H, net->pb + net->woff[l], 1, Hn, dHn, net->dH2, net->dM, 0,
+            net->g + net->woff[l], net->g + net->boff[l]);
+        // dL/dh_{l-1} = direct part + A^T dL/dm_l (A symmetric)
+        spmm_kernel<float, float><<<sb, 256, 0, st>>>(nn, H, rowptr, col, w, net->dM, net->dH2, 1);
+        std::swap(net->dH, net->dH2);
+        spx::note_launch(2);
+    }
+    dense_bwd_kernel<float, bf16><<<nb, kThreads, dense_smem(net->F, H, true), st>>>(
+        nn, net->F, X, 0, nullptr, H, net->pb + net->woff[0], 1, net->Hs, net->dH, nullptr,
+        nullptr, 0, net->g + net->woff[0], net->g + net->boff[0]);
+    spx::note_launch();
+    if (lr > 0.f) {
+        net->step++;
+        const float b1 = 0.9f, b2 = 0.999f;
+        const float c1 = 1.f - powf(b1, (float)net->step), c2 = 1.f - powf(b2, (float)net->step);
+        adam_kernel<<<256, 256, 0, st>>>(net->nparam, net->p, net->g, net->m, net->v, lr, b1, b2, c1,
+                                         c2, 1e-8f, net->pb);
+        spx::note_launch();
+    }
+    double hl = 0.0;
+    cudaMemcpyAsync(&hl, net->loss, sizeof(double), cudaMemcpyDeviceToHost, st);
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) { spx::set_last_error_text(cudaGetErrorString(e)); return SPEIGS_ERR_INTERNAL; }
+    if (loss) *loss = hl;
+    return SPEIGS_OK;
+}
+
+}  // extern "C"

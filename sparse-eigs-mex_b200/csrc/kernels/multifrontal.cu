@@ -296,9 +296,10 @@ SPX_DEV void cp_wait() {
 }
 // one element of a tile: an asynchronous copy for FP64 storage, a load and
 // widening conversion for FP32 storage (zero when !valid)
-SPX_DEV void elem_copy(double *dst, const double *src, bool valid) { cp_async8(dst, src, valid); }
-SPX_DEV void elem_copy(double *dst, const float *src, bool valid) {
-    *dst = valid ? (double)*src : 0.0;
+template <class MT>
+SPX_DEV void elem_copy(double *dst, const MT *src, bool valid) {
+    if constexpr (std::is_same<MT, double>::value) cp_async8(dst, src, valid);
+    else *dst = valid ? (double)*src : 0.0;
 }
 
 // s(i, j) = M(ra + i, ca + j) for i < h, j < w; zero elsewhere in the tile

@@ -1,0 +1,184 @@
+"""Learned warm start for the 'sm' Lanczos on finite-volume diffusion operators.
+
+A small message-passing network (csrc/kernels/mpnn.cu, reached through the C
+ABI of include/speigs_b200.h) reads the operator's graph -- the normalised
+face transmissibilities of the N^3 grid -- and per-node features (the log
+conductivity and the lowest closed-form Laplace modes) and proposes P vectors
+whose span should hold the k wanted eigenvectors.  speigs_ex() turns the
+proposal into the Lanczos start vector (speigs_ext_opts.warm); the random
+start stays the fallback, and the true-residual test of the Lanczos decides
+convergence either way, so the proposal changes the cost, never the answer.
+
+The network is trained on eigenvectors this solver computes for a family of
+operators (GRF conductivities, workloads.grf_conductivity): see
+train_warmstart.py beside this file.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, c_double, c_float, c_int, c_int64, c_uint64, c_void_p
+
+import numpy as np
+
+from . import speigs as _s
+from . import workloads as _w
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CHECKPOINT = os.path.join(HERE, "data", "warmstart_grf48.npz")
+NMODES = 7          # Laplace modes among the node features
+HIDDEN = 64
+
+
+def _bind(lib):
+    sig = {
+        "speigs_b200_mpnn_create": (c_int, [c_int, c_int, c_int, c_int, c_uint64,
+                                            POINTER(c_void_p)]),
+        "speigs_b200_mpnn_destroy": (None, [c_void_p]),
+        "speigs_b200_mpnn_params": (c_int, [c_void_p, c_void_p, POINTER(c_int64), c_int]),
+        "speigs_b200_mpnn_grads": (c_int, [c_void_p, c_void_p]),
+        "speigs_b200_mpnn_forward": (c_int, [c_void_p, c_int64, c_void_p, c_void_p, c_void_p,
+                                             c_void_p, c_void_p, c_void_p]),
+        "speigs_b200_mpnn_train_step": (c_int, [c_void_p, c_int64, c_void_p, c_void_p, c_void_p,
+                                                c_void_p, c_void_p, c_int, c_float,
+                                                POINTER(c_double), c_void_p]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype, fn.argtypes = res, args
+    return lib
+
+
+def grid_graph(N: int, kap: np.ndarray):
+    """Normalised adjacency of the N^3 finite-volume operator: w_ij = t_ij /
+    sqrt(s_i s_j), t the face transmissibilities, s_i = sum_j t_ij.  Returns
+    (rowptr int32, col int32, w float32), rows in the operator's order."""
+    n = N ** 3
+    idx = np.arange(n).reshape(N, N, N)
+    rows, cols, vals = [], [], []
+    for ax in range(3):
+        a = [slice(None)] * 3
+        b = [slice(None)] * 3
+        a[ax] = slice(0, N - 1)
+        b[ax] = slice(1, N)
+        ka, kb = kap[tuple(a)], kap[tuple(b)]
+        t = (2.0 * ka * kb / (ka + kb)).ravel()
+        ia, ib = idx[tuple(a)].ravel(), idx[tuple(b)].ravel()
+        rows += [ia, ib]
+        cols += [ib, ia]
+        vals += [t, t]
+    r = np.concatenate(rows)
+    c = np.concatenate(cols)
+    v = np.concatenate(vals)
+    s = np.bincount(r, weights=v, minlength=n)
+    v = v / np.sqrt(s[r] * s[c])
+    order = np.lexsort((c, r))
+    r, c, v = r[order], c[order], v[order]
+    rowptr = np.zeros(n + 1, dtype=np.int32)
+    np.cumsum(np.bincount(r, minlength=n), out=rowptr[1:])
+    return rowptr, c.astype(np.int32), v.astype(np.float32)
+
+
+_MODES: dict = {}
+
+
+def features(N: int, kap: np.ndarray) -> np.ndarray:
+    """n x (1 + NMODES) float32: standardised log conductivity and the lowest
+    Laplace modes scaled to unit RMS."""
+    if N not in _MODES:
+        _MODES[N] = (_w.laplace_modes(N, NMODES) * np.sqrt(N ** 3)).astype(np.float32)
+    g = np.log(kap).ravel()
+    g = (g - g.mean()) / (g.std() + 1e-12)
+    return np.concatenate([g[:, None].astype(np.float32), _MODES[N]], axis=1)
+
+
+class WarmStartNet:
+    """The device network (C ABI) with numpy-side save/load."""
+
+    def __init__(self, nout: int = 24, layers: int = 4, nfeat: int = 1 + NMODES, seed: int = 7,
+                 lib=None):
+        self.lib = _bind(lib or _s.load())
+        self.nout, self.layers, self.nfeat = nout, layers, nfeat
+        h = c_void_p()
+        rc = self.lib.speigs_b200_mpnn_create(nfeat, HIDDEN, layers, nout, seed, ctypes.byref(h))
+        if rc != 0:
+            raise RuntimeError(f"mpnn_create: {_s.errmsg(rc, self.lib)} ({_s.last_error(self.lib)})")
+        self.h = h
+        cnt = c_int64()
+        self.lib.speigs_b200_mpnn_params(self.h, None, ctypes.byref(cnt), 0)
+        self.nparam = cnt.value
+
+    def get_params(self) -> np.ndarray:
+        p = np.zeros(self.nparam, dtype=np.float32)
+        cnt = c_int64(self.nparam)
+        self.lib.speigs_b200_mpnn_params(self.h, p.ctypes.data, ctypes.byref(cnt), 0)
+        return p
+
+    def set_params(self, p: np.ndarray):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        assert p.size == self.nparam
+        cnt = c_int64(self.nparam)
+        rc = self.lib.speigs_b200_mpnn_params(self.h, p.ctypes.data, ctypes.byref(cnt), 1)
+        if rc != 0:
+            raise RuntimeError("mpnn_params")
+
+    def grads(self) -> np.ndarray:
+        g = np.zeros(self.nparam, dtype=np.float32)
+        self.lib.speigs_b200_mpnn_grads(self.h, g.ctypes.data)
+        return g
+
+    def forward_device(self, n, rowptr, col, w, X, Y, stream=0):
+        """All arguments are device pointers (ints)."""
+        return self.lib.speigs_b200_mpnn_forward(self.h, n, rowptr, col, w, X, Y, stream)
+
+    def train_step_device(self, n, rowptr, col, w, X, U, k, lr, stream=0):
+        loss = c_double()
+        rc = self.lib.speigs_b200_mpnn_train_step(self.h, n, rowptr, col, w, X, U, k, lr,
+                                                  ctypes.byref(loss), stream)
+        if rc != 0:
+            raise RuntimeError(f"mpnn_train_step rc={rc}: {_s.last_error(self.lib)}")
+        return loss.value
+
+    def save(self, path: str, **meta):
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        np.savez(path, params=self.get_params(), nout=self.nout, layers=self.layers,
+                 nfeat=self.nfeat, **meta)
+
+    @classmethod
+    def load(cls, path: str = CHECKPOINT, lib=None):
+        z = np.load(path)
+        net = cls(int(z["nout"]), int(z["layers"]), int(z["nfeat"]), lib=lib)
+        net.set_params(z["params"])
+        return net
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.speigs_b200_mpnn_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def propose(net: WarmStartNet, N: int, kap: np.ndarray) -> np.ndarray:
+    """The network's proposal for one operator: n x nout float64 (host)."""
+    import torch
+    rowptr, col, w = grid_graph(N, kap)
+    X = features(N, kap)
+    dev = torch.device("cuda")
+    t_rp = torch.from_numpy(rowptr).to(dev)
+    t_ci = torch.from_numpy(col).to(dev)
+    t_w = torch.from_numpy(w).to(dev)
+    t_X = torch.from_numpy(X).to(dev)
+    n = N ** 3
+    t_Y = torch.empty((n, net.nout), dtype=torch.float32, device=dev)
+    torch.cuda.synchronize()
+    rc = net.forward_device(n, t_rp.data_ptr(), t_ci.data_ptr(), t_w.data_ptr(), t_X.data_ptr(),
+                            t_Y.data_ptr(), 0)
+    if rc != 0:
+        raise RuntimeError(f"mpnn_forward rc={rc}")
+    torch.cuda.synchronize()
+    return t_Y.double().cpu().numpy()

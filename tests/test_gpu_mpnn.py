@@ -1,0 +1,66 @@
+"""Device kernels of the warm-start network (BF16 weights and activations,
+FP32 accumulation) against the FP64 oracle: forward output and the
+gradient of the subspace loss.  Tolerances reflect BF16 storage."""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+pytestmark = pytest.mark.gpu
+
+
+def _device_case(pkg, N=6, seed=0, P=6, k=4, L=4):
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(seed)
+    kap = np.exp(rng.standard_normal((N, N, N)))
+    rowptr, col, w = pkg.learned.grid_graph(N, kap)
+    X = pkg.learned.features(N, kap)
+    n = N ** 3
+    U, _ = np.linalg.qr(rng.standard_normal((n, k)))
+    net = pkg.learned.WarmStartNet(nout=P, layers=L, seed=11)
+    dev = torch.device("cuda")
+    t = {name: torch.from_numpy(np.ascontiguousarray(a)).to(dev) for name, a in
+         [("rp", rowptr), ("ci", col), ("w", w), ("X", X), ("U", U.astype(np.float32))]}
+    A = sp.csr_matrix((w.astype(np.float64), col, rowptr), shape=(n, n))
+    return torch, net, t, A, X.astype(np.float64), U, n, (X.shape[1], 64, L, P), k
+
+
+def test_forward_matches_oracle(pkg, oracle):
+    import mpnn_oracle as mo
+    torch, net, t, A, X, U, n, dims, k = _device_case(pkg)
+    Y = torch.empty((n, dims[3]), dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    rc = net.forward_device(n, t["rp"].data_ptr(), t["ci"].data_ptr(), t["w"].data_ptr(),
+                            t["X"].data_ptr(), Y.data_ptr(), 0)
+    assert rc == 0
+    torch.cuda.synchronize()
+    Yd = Y.double().cpu().numpy()
+    Yo, _ = mo.forward(net.get_params().astype(np.float64), A, X, *dims)
+    err = np.linalg.norm(Yd - Yo) / np.linalg.norm(Yo)
+    assert err < 2e-2, err
+
+
+def test_gradient_matches_oracle(pkg, oracle):
+    import mpnn_oracle as mo
+    torch, net, t, A, X, U, n, dims, k = _device_case(pkg)
+    torch.cuda.synchronize()
+    loss_d = net.train_step_device(n, t["rp"].data_ptr(), t["ci"].data_ptr(), t["w"].data_ptr(),
+                                   t["X"].data_ptr(), t["U"].data_ptr(), k, 0.0, 0)
+    gd = net.grads().astype(np.float64)
+    params = net.get_params().astype(np.float64)
+    Yo, cache = mo.forward(params, A, X, *dims)
+    loss_o, dY = mo.loss_and_dY(Yo, U)
+    go = mo.backward(params, A, cache, dY, *dims)
+    assert abs(loss_d - loss_o) < 2e-2 * max(abs(loss_o), 1e-3)
+    cos = gd @ go / (np.linalg.norm(gd) * np.linalg.norm(go))
+    assert cos > 0.995, cos
+    assert np.linalg.norm(gd - go) / np.linalg.norm(go) < 0.1
+
+
+def test_training_reduces_loss(pkg):
+    torch, net, t, A, X, U, n, dims, k = _device_case(pkg, N=8, seed=2)
+    args = (n, t["rp"].data_ptr(), t["ci"].data_ptr(), t["w"].data_ptr(), t["X"].data_ptr(),
+            t["U"].data_ptr(), k)
+    first = net.train_step_device(*args, 3e-3, 0)
+    for _ in range(60):
+        last = net.train_step_device(*args, 3e-3, 0)
+    assert last < 0.8 * first, (first, last)
