@@ -43,6 +43,10 @@ typedef struct {
     speigs_int   refine_steps;   /* FP64 refinement corrections made (mixed)        */
     speigs_int   factor_solves;  /* solves with the factor: applications + corrections */
     speigs_int   warm_cols;      /* start-subspace columns used (0: random start)   */
+    /* host wall time (s) of the Krylov route outside speigs_info's t_analyze /
+     * t_factor / t_iter: input checks and the CSR build, plan set-up (device
+     * buffers, uploads), copy-out and release */
+    double       t_checks, t_setup, t_release;
 } speigs_ext_info;
 
 /* Fill *e with the defaults (FP64, no start subspace). */

@@ -912,13 +912,20 @@ int device_krylov(HostCSR &A, int64_t k, speigs_which which, const speigs_opts &
                   double anorm, double *lambda, double *V, double *resid, speigs_info *info,
                   EngineStats *stats, const speigs_ext_opts *ext, speigs_ext_info *einfo) {
     speigs_plan_s *p = nullptr;
+    const double t0 = wall();
     int rc = plan_from_csr(A, which, o, anorm, ext, &p);
     if (rc) return rc;
+    const double t_setup = wall() - t0 - p->t_analyze;
     p->ext_warm = ext ? ext->warm : nullptr;
     p->ext_warm_cols = ext ? ext->warm_cols : 0;
     rc = plan_solve(p, k, lambda, V, resid, info, false, stats);
     fill_ext_info(p, einfo);
+    const double t1 = wall();
     speigs_plan_destroy(p);
+    if (einfo) {
+        einfo->t_setup = t_setup;
+        einfo->t_release = wall() - t1;
+    }
     return rc;
 }
 

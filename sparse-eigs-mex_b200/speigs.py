@@ -49,7 +49,8 @@ class ExtOpts(ctypes.Structure):
 class ExtInfo(ctypes.Structure):
     """speigs_ext_info (include/speigs_b200.h)."""
     _fields_ = [("precision", c_int), ("refine_steps", c_int64), ("factor_solves", c_int64),
-                ("warm_cols", c_int64)]
+                ("warm_cols", c_int64), ("t_checks", c_double), ("t_setup", c_double),
+                ("t_release", c_double)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
