@@ -393,6 +393,25 @@ SPX_DEV void acc_store(const Acc &acc, MT *M, int64_t ld, int ra, int h, int ca,
             }
 }
 
+// M(ra + m, ca + n) = Cs(m, n) - acc(m, n) for m < h, n < w (Cs: the staged
+// output tile, column-major FLD)
+template <class MT>
+SPX_DEV void acc_sub_store(const Acc &acc, const double *Cs, MT *M, int64_t ld, int ra, int h,
+                           int ca, int w) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    const int wid = threadIdx.x >> 5, m0 = (wid & 1) * 32, n0 = (wid >> 1) * 32;
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                const int m = m0 + 8 * i + g, n = n0 + 8 * j + 2 * t + e;
+                if (m < h && n < w)
+                    M[(int64_t)(ra + m) + (int64_t)(ca + n) * ld] = (MT)(Cs[n * FLD + m] - acc[i][j][e]);
+            }
+}
+
 // ---- recursive Cholesky + inverse of a diagonal tile (w <= 64) --------
 // chol_inv_rec<N>: L (lower) and X = inv(L) of the leading w x w part of the
 // N x N lower matrix D (all column-major, leading dimension FLD), by the 128
@@ -405,7 +424,10 @@ SPX_DEV void acc_store(const Acc &acc, MT *M, int64_t ld, int ra, int h, int ca,
 // need no edge tests.  D is destroyed; `tmp` is a scratch tile (64 x FLD).
 
 // 8 x 8 base case by warp 0, lanes 0..7 holding rows in registers
-SPX_DEV void chol_inv8(double *D, double *L, double *X, int w, double pivtol, int *status,
+// (not inlined: one copy of the code serves every call site, which keeps the
+// recursion's instruction footprint small)
+__device__ __noinline__ void chol_inv8(double *D, double *L, double *X, int w, double pivtol,
+                                       int *status,
                        int colbase, bool record) {
     if (threadIdx.x >= 32) return;
     const unsigned full = 0xffffffffu;
@@ -459,7 +481,8 @@ SPX_DEV void chol_inv8(double *D, double *L, double *X, int w, double pivtol, in
 // mode 0: C = A B^T (A, B both stored row-index-first, i.e. B(j, k))
 // mode 1: C = A B   (B(k, j))
 template <int H, int MODE>
-SPX_DEV void small_mm(const double *A, const double *B, double *C, double alpha, bool accumulate) {
+__device__ __noinline__ void small_mm(const double *A, const double *B, double *C, double alpha,
+                                      bool accumulate) {
     constexpr int NOUT = H * H;
     for (int o = threadIdx.x; o < NOUT; o += blockDim.x) {
         const int i = o % H, j = o / H;
@@ -673,14 +696,17 @@ mf_update64(const int4 *__restrict__ tasks, Sym y, Real *__restrict__ F, const i
         float *As = reinterpret_cast<float *>(fsm), *Bs = As + FT * FLDF;
         update_tile_f32(reinterpret_cast<float *>(Fs), f.r, ra, h, ca, w, ka, kw, As, Bs);
     } else {
-        double *As = fsm, *Bs = fsm + kFTileDoubles;
+        // the output tile is staged with the operands, so the subtraction
+        // does not wait on global loads after the products
+        double *As = fsm, *Bs = fsm + kFTileDoubles, *Cs = fsm + 2 * kFTileDoubles;
         ftile_load(As, Fs, f.r, ra, h, ka, kw);
         ftile_load(Bs, Fs, f.r, ca, w, ka, kw);
+        ftile_load(Cs, Fs, f.r, ra, h, ca, w);
         cp_wait();
         Acc acc;
         acc_zero(acc);
         warp_mma<true>(acc, As, Bs, (kw + 3) & ~3, h, w);
-        acc_store<false>(acc, Fs, f.r, ra, h, ca, w, -1.0, true);
+        acc_sub_store(acc, Cs, Fs, f.r, ra, h, ca, w);
     }
 }
 
@@ -1846,7 +1872,8 @@ template <> int MultifrontalPlanT<Real>::init(const spx_symbolic &S, const int64
         // persistent grid for the task-queue solve
         // factor tile kernels stage two or three 64 x 64 tiles
         cudaFuncSetAttribute(mf_panel64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelSmem);
-        cudaFuncSetAttribute(mf_update64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPairSmem);
+        cudaFuncSetAttribute(mf_update64, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(3 * sizeof(double) * kFTileDoubles));
         cudaFuncSetAttribute(mf_inv_t64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPairSmem);
         cudaFuncSetAttribute(mf_inv_x64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPairSmem);
         cudaFuncSetAttribute(mf_wmul64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPairSmem);
@@ -1887,7 +1914,8 @@ template <> void MultifrontalPlanT<Real>::launch_factor(const double *d_val, cud
                                                                d_status_);
                 break;
             case MF_UPDATE:
-                mf_update64<<<nb, kGThreads, kPairSmem, st>>>(tk, y, d_front_, d_status_);
+                mf_update64<<<nb, kGThreads, 3 * sizeof(double) * kFTileDoubles, st>>>(
+                    tk, y, d_front_, d_status_);
                 break;
             case MF_INV_T:
                 mf_inv_t64<<<nb, kGThreads, kPairSmem, st>>>(tk, y, d_front_, d_G_, d_status_);
