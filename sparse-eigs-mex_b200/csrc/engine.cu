@@ -660,8 +660,6 @@ struct speigs_plan_s {
     int64_t last_warm = 0;            // start-subspace columns used by the last solve
     double t_analyze = 0;
     std::vector<void *> owned;
-    double *pinned = nullptr;        // host scalars read back during a solve
-    size_t pinned_n = 0;
 };
 
 namespace spx {
@@ -678,7 +676,11 @@ static int plan_upload_values(speigs_plan_s *p) {
 }
 
 static int plan_alloc(speigs_plan_s *p, void **ptr, size_t bytes) {
-    cudaError_t e = cudaMallocAsync(ptr, bytes ? bytes : 1, p->stream.s);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaMemPool_t pool = device_pool(dev);
+    cudaError_t e = pool ? cudaMallocFromPoolAsync(ptr, bytes ? bytes : 1, pool, p->stream.s)
+                         : cudaMallocAsync(ptr, bytes ? bytes : 1, p->stream.s);
     if (e != cudaSuccess) { cudaGetLastError(); return SPEIGS_ERR_MEM; }
     p->owned.push_back(*ptr);
     return 0;
@@ -795,6 +797,26 @@ static int plan_factor(speigs_plan_s *p, EngineStats *stats) {
 
 struct Cand2 { double key; int idx; };
 
+// Page-locked host scalars that a solve reads back, one buffer per host
+// thread, grown on demand and kept for the thread's life: cudaMallocHost and
+// cudaFreeHost are slow and synchronise the device, so they are not paid per
+// call (which matters when several threads solve components at once).
+static double *pinned_scalars(size_t need) {
+    thread_local double *buf = nullptr;
+    thread_local size_t cap = 0;
+    if (cap >= need) return buf;
+    size_t want = std::max<size_t>(need, 256);
+    double *nb = nullptr;
+    if (cudaMallocHost(&nb, sizeof(double) * want) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    if (buf) cudaFreeHost(buf);
+    buf = nb;
+    cap = want;
+    return buf;
+}
+
 // Factor (if 'sm') and iterate; results sorted by |lambda| into host or
 // device buffers.
 static int plan_solve(speigs_plan_s *p, int64_t k, double *lambda, double *V, double *resid,
@@ -826,17 +848,8 @@ static int plan_solve(speigs_plan_s *p, int64_t k, double *lambda, double *V, do
     std::vector<double> lam_h(k, 0.0), res_h(k, 0.0);
     int rc = 0;
     const size_t need = 2 * (size_t)k + 8;
-    if (p->pinned_n < need) {
-        if (p->pinned) cudaFreeHost(p->pinned);
-        p->pinned = nullptr;
-        p->pinned_n = 0;
-        if (cudaMallocHost(&p->pinned, sizeof(double) * need) != cudaSuccess) {
-            cudaGetLastError();
-            p->pinned = nullptr;
-            return SPEIGS_ERR_MEM;
-        }
-        p->pinned_n = need;
-    }
+    double *pinbuf = pinned_scalars(need);
+    if (!pinbuf) return SPEIGS_ERR_MEM;
     {
         Arena ar(st);
         const double *X = nullptr;
@@ -855,7 +868,7 @@ static int plan_solve(speigs_plan_s *p, int64_t k, double *lambda, double *V, do
         }
         int64_t wused = 0;
         rc = lanczos_device(*op, dA, n, k, p->opts, p->anorm, lam_h.data(), res_h.data(), &X,
-                            &ldx, &nout, info, stats, ar, p->pinned, st, dwarm, wcols, &wused);
+                            &ldx, &nout, info, stats, ar, pinbuf, st, dwarm, wcols, &wused);
         p->last_warm = wused;
         p->last_ops = op->nops;
         if (rc == 0 && p->mf.mixed) {
@@ -1186,8 +1199,6 @@ void speigs_plan_destroy(speigs_plan p) {
     for (void *q : p->owned) cudaFreeAsync(q, st);
     p->owned.clear();
     cudaStreamSynchronize(st);
-    if (p->pinned) cudaFreeHost(p->pinned);
-    p->pinned = nullptr;
     spx::free_csr(&p->A);
     delete p;
 }
