@@ -195,7 +195,7 @@ def _dev_time(torch, fn, steps, warmup, stream):
         e1.record(stream)
         e1.synchronize()
         ms.append(e0.elapsed_time(e1))
-    return statistics.mean(ms), out
+    return statistics.mean(ms), out, ms
 
 
 def run_forms_grf(args, pkg, wl):
@@ -238,7 +238,7 @@ def run_forms_grf(args, pkg, wl):
                 raise RuntimeError(f"{name}: rc={rc} {s.last_error(lib)}")
             box["info"] = info
             return info
-        ms, info = _dev_time(torch, solve, args.steps, args.warmup, pstream)
+        ms, info, ms_steps = _dev_time(torch, solve, args.steps, args.warmup, pstream)
         ei = plan.ext_info()
         lam_h = lam.cpu().numpy()
         Vh = np.ascontiguousarray(V.cpu().numpy().T)
@@ -255,7 +255,8 @@ def run_forms_grf(args, pkg, wl):
             else:
                 rc, *_ = s.speigs_ex(A, k, s.SM, opts, ext, vectors=True, lib=lib)
             e2e.append(time.perf_counter() - t1)
-        forms[name] = {"value_s": ms * 1e-3, "e2e_s": statistics.mean(e2e), "nops": int(info["nops"]),
+        forms[name] = {"value_s": ms * 1e-3, "step_ms": [round(x, 3) for x in ms_steps],
+                       "e2e_s": statistics.mean(e2e), "nops": int(info["nops"]),
                        "restarts": int(info["restarts"]), "refine_steps": int(ei["refine_steps"]),
                        "warm_cols": int(ei["warm_cols"]), "lam": lam_h.tolist(),
                        "max_resid_over_anorm": float(r.max() / info["anorm"]),
@@ -411,7 +412,7 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
         l0 = s.counters(lib)[0]
-        step_ms = []
+        step_ms, step_phase = [], []
         for _ in range(steps):
             flush.zero_()
             torch.cuda.synchronize()
@@ -422,6 +423,7 @@ def main():
             e1.record(pstream)
             e1.synchronize()
             step_ms.append(e0.elapsed_time(e1))
+            step_phase.append([round(info["t_factor"], 4), round(info["t_iter"], 4)])
         torch.cuda.synchronize()
         launches = (s.counters(lib)[0] - l0) // max(steps, 1)
         if world > 1:
@@ -464,8 +466,9 @@ def main():
             rc, l2, V2, r2, inf2, ei2 = s.speigs_ex(A, k, wl["which"], opts, ext, vectors=True,
                                                     lib=lib)
             e2e_t.append(time.perf_counter() - t0)
-            e2e_lib.append(inf2["t_analyze"] + inf2["t_factor"] + inf2["t_iter"] +
-                           ei2["t_checks"] + ei2["t_setup"] + ei2["t_release"])
+            e2e_lib.append([round(v, 4) for v in (inf2["t_analyze"], ei2["t_checks"],
+                                                  ei2["t_setup"], inf2["t_factor"],
+                                                  inf2["t_iter"], ei2["t_release"])])
             if rc != 0:
                 raise RuntimeError(f"speigs rc={rc}")
         c1 = s.counters(lib)
@@ -473,10 +476,13 @@ def main():
                "h2d_bytes_per_step": (c1[1] - c0[1]) // steps,
                "d2h_bytes_per_step": (c1[2] - c0[2]) // steps,
                "steps_s": [round(x, 4) for x in e2e_t],
-               "steps_timed_inside_library_s": [round(x, 4) for x in e2e_lib],
+               "steps_inside_library_s": {
+                   "fields": ["analyze", "checks", "setup", "factor", "iterate", "release"],
+                   "steps": e2e_lib},
                "phase_s": dict({kk: inf2[kk] for kk in ("t_analyze", "t_factor", "t_iter")},
                             **{kk: ei2[kk] for kk in ("t_checks", "t_setup", "t_release")})}
-        return dict(ms=ms, step_ms=step_ms, info=info, einfo=einfo, lam=lam_h, V=Vh,
+        return dict(ms=ms, step_ms=step_ms, step_phase=step_phase, info=info, einfo=einfo,
+                    lam=lam_h, V=Vh,
                     launches=launches, clocks=clocks, costs=costs,
                     op_s=statistics.mean(op_ms) * 1e-3, e2e=e2e)
 
@@ -531,6 +537,8 @@ def main():
         fp64_lam = om["lam"] if other == "fp64" else lam_h
         mixed_lam = lam_h if other == "fp64" else om["lam"]
         compare = {"precision": other, "value": om["ms"] * 1e-3, "unit": "s",
+                   "step_ms": [round(x, 3) for x in om["step_ms"]],
+                   "step_factor_iterate_s": om["step_phase"],
                    "e2e": om["e2e"]["value"], "nops": int(om["info"]["nops"]),
                    "refine_steps": int(om["einfo"]["refine_steps"]),
                    "mixed_over_fp64_value": (om["ms"] / ms) if other == "mixed" else (ms / om["ms"]),
@@ -561,6 +569,7 @@ def main():
             "check": check, "roofline": roofline, "cpu_baseline": cpu, "e2e": main_m["e2e"],
             "gpu_launches": int(main_m["launches"]), "clocks": main_m["clocks"],
             "step_ms": [round(x, 3) for x in main_m["step_ms"]],
+            "step_factor_iterate_s": main_m["step_phase"],
             "phase_s": {kk: info[kk] for kk in ("t_factor", "t_iter", "t_op", "t_ortho",
                                                 "t_resid", "t_ritz")},
             "compare": compare,

@@ -273,7 +273,7 @@ struct LanczosBufs {
            *thsave = nullptr, *w = nullptr, *X = nullptr, *AX = nullptr, *lam = nullptr,
            *r2 = nullptr, *xn2 = nullptr, *h1 = nullptr, *h2 = nullptr, *nrm2 = nullptr,
            *jwork = nullptr;
-    int *ord = nullptr, *jstat = nullptr;
+    int *ord = nullptr, *jstat = nullptr, *dflag = nullptr;
     ReduceScratch rs;
 };
 
@@ -344,6 +344,7 @@ static int lanczos_device(Operator &op, const DevA &A, int n, int64_t k, const s
     b.nrm2 = ar.alloc<double>(4);
     b.ord = ar.alloc<int>(ncv);
     b.jstat = ar.alloc<int>(2);
+    b.dflag = ar.alloc<int>(1);
     const int me = (int)((ncv + 1) & ~1);
     b.jwork = ((int)ncv > syev_small_smem_limit()) ? ar.alloc<double>((size_t)2 * me * me) : nullptr;
     const int nblk = (n + 511) / 512 + 1;
@@ -356,9 +357,14 @@ static int lanczos_device(Operator &op, const DevA &A, int n, int64_t k, const s
     cudaMemsetAsync(b.rs.counter, 0, sizeof(unsigned), st);
     cudaMemsetAsync(b.H, 0, sizeof(double) * ncv * ncv, st);
 
-    // pinned scalars read back by the host (the caller's buffer holds >= 2k+8)
+    // pinned scalars read back by the host (the caller's buffer holds >= 2k+16):
+    // Ritz values and residuals, a norm and the operator's error word, the
+    // betas and error words of two pipelined steps, the restart flag
     double *hs = pinned;
     double *h_lam = hs, *h_r2 = hs + b.kk, *h_nrm = hs + 2 * b.kk;
+    double *h_beta = h_nrm + 4;
+    int *h_sterr = reinterpret_cast<int *>(h_nrm + 6);
+    int *h_rflag = reinterpret_cast<int *>(h_nrm + 7);
 
     PhaseTimer tm(st);
     double ms_op = 0, ms_ortho = 0, ms_resid = 0, ms_ritz = 0;
@@ -439,33 +445,84 @@ static int lanczos_device(Operator &op, const DevA &A, int n, int64_t k, const s
         normalise(n, b.w, b.nrm2, b.V, st);
     }
 
+    // Step jj of the recurrence: operator application, orthogonalisation,
+    // and the read-back of beta_jj, complete when evb[jj & 1] is.  The host
+    // tests beta_j for breakdown one step late: step j+1 is queued, on the
+    // assumption that beta_j passes, before the host waits for beta_j, so
+    // the device never idles while the host decides.  A breakdown (rare)
+    // drains the stream, runs the reference's recovery and queues step j+1
+    // again; everything the speculative step wrote is written again.
+    struct StepEvents {
+        cudaEvent_t e[2] = {nullptr, nullptr};
+        ~StepEvents() { for (auto x : e) if (x) cudaEventDestroy(x); }
+    } evb;
+    for (auto &x : evb.e)
+        if (cudaEventCreateWithFlags(&x, cudaEventDisableTiming) != cudaSuccess)
+            return cuda_fail(cudaGetLastError(), "event");
+    auto issue_step = [&](int64_t jj) {
+        double *vj = b.V + (size_t)jj * b.ldv;
+        int t0 = tm.begin();
+        op.apply(vj, b.w, st);
+        tm.end(t0, &ms_op);
+        int t1 = tm.begin();
+        orth_block(b, b.V, (int)(jj + 1), b.w, b.H + (size_t)jj * ldh, st);
+        tm.end(t1, &ms_ortho);
+        copy_async(h_beta + (jj & 1), b.nrm2, sizeof(double), cudaMemcpyDeviceToHost, st);
+        if (op_err) copy_async(h_sterr + (jj & 1), op_err, sizeof(int), cudaMemcpyDeviceToHost, st);
+        cudaEventRecord(evb.e[jj & 1], st);
+    };
+    auto wait_beta = [&](int64_t jj, double *beta) -> int {
+        cudaError_t e = cudaEventSynchronize(evb.e[jj & 1]);
+        if (e != cudaSuccess) return cuda_fail(e, "lanczos sync");
+        if (op_err && h_sterr[jj & 1]) {
+            set_last_error_text("operator application failed: a solve dependency wait ran out");
+            return SPEIGS_ERR_INTERNAL;
+        }
+        *beta = sqrt(h_beta[jj & 1]);
+        return 0;
+    };
+    auto drain = [&]() -> int {
+        cudaError_t e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return cuda_fail(e, "lanczos sync");
+        tm.resolve();
+        return 0;
+    };
+
     int rc = SPEIGS_OK;
     int last_nwant = 0;   // Ritz vectors of the last Rayleigh-Ritz stay in X
     for (;;) {
         // ---- extend the basis from j to ncv (reference :197-229)
+        if (j < ncv) issue_step(j);
         for (; j < ncv; j++) {
-            double *vj = b.V + (size_t)j * b.ldv;
-            int t0 = tm.begin();
-            op.apply(vj, b.w, st);
-            tm.end(t0, &ms_op);
-            int t1 = tm.begin();
-            double *hcol = b.H + (size_t)j * ldh;
-            orth_block(b, b.V, (int)(j + 1), b.w, hcol, st);
-            tm.end(t1, &ms_ortho);
+            normalise(n, b.w, b.nrm2, b.V + (size_t)(j + 1) * b.ldv, st);
+            if (j + 1 < ncv) {
+                launch_set_beta(b.H, ldh, (int)(j + 1), (int)j, b.nrm2, 0, st);
+                issue_step(j + 1);
+            }
             double beta = 0;
-            if (int e = read_nrm(&beta)) return e;
-            int zero_rec = 0;
+            if (int e = wait_beta(j, &beta)) return e;
+            if (beta > bthr) continue;
+            // breakdown at step j (reference :205-216); the speculative step
+            // j+1 does not count as an operator application
+            if (int e = drain()) return e;
+            if (j + 1 < ncv) op.nops--;
+            for (int att = 0; att < 3 && beta <= bthr; att++) {
+                rand_vec(b.w);
+                orth_block(b, b.V, (int)(j + 1), b.w, nullptr, st);
+                if (int e = read_nrm(&beta)) return e;
+            }
             if (beta <= bthr) {
-                zero_rec = 1;
-                for (int att = 0; att < 3 && beta <= bthr; att++) {
-                    rand_vec(b.w);
-                    orth_block(b, b.V, (int)(j + 1), b.w, nullptr, st);
-                    if (int e = read_nrm(&beta)) return e;
-                }
-                if (beta <= bthr) { ncv = j + 1; break; }
+                // column j+1 holds the speculative normalisation, which is
+                // not part of the basis
+                launch_fill(n, 0.0, b.V + (size_t)(j + 1) * b.ldv, st);
+                ncv = j + 1;
+                break;
             }
             normalise(n, b.w, b.nrm2, b.V + (size_t)(j + 1) * b.ldv, st);
-            if (j + 1 < ncv) launch_set_beta(b.H, ldh, (int)(j + 1), (int)j, b.nrm2, zero_rec, st);
+            if (j + 1 < ncv) {
+                launch_set_beta(b.H, ldh, (int)(j + 1), (int)j, b.nrm2, 1, st);
+                issue_step(j + 1);
+            }
         }
 
         // ---- projected eigenproblem (reference :231-240)
@@ -506,26 +563,59 @@ static int lanczos_device(Operator &op, const DevA &A, int n, int64_t k, const s
         // ---- thick restart: keep the top-l Ritz vectors (reference :270-303)
         int64_t l = std::min<int64_t>(k + 5, ncv - 1);
         if (l < 1) l = 1;
+        // The retained vectors are queued without host reads; a vector that
+        // orthogonalisation leaves with norm < 1e-10 raises dflag, and then
+        // the loop is redone with the reference's per-vector test, which
+        // skips such vectors.
         int nret = 0;
-        int tk = tm.begin();
-        for (int t = 0; t < m && nret < l; t++) {
-            double *dst = b.Vn + (size_t)nret * b.ldv;
-            launch_ritz_vectors(b.V, b.ldv, n, m, b.S, m, b.ord, t, 1, dst, b.ldv, b.xn2, b.rs, st);
-            orth_block(b, b.Vn, nret, dst, nullptr, st);
-            double nr = 0;
-            if (int e = read_nrm(&nr)) return e;
-            if (nr < 1e-10) continue;
-            normalise(n, dst, b.nrm2, dst, st);
-            thsave_kernel<<<1, 1, 0, st>>>(b.theta, b.ord, t, b.thsave, nret);
-            note_launch();
-            nret++;
-        }
-        tm.end(tk, &ms_ritz);
-        // the (m+1)-th Lanczos vector continues the recurrence
-        launch_copy(n, b.V + (size_t)m * b.ldv, b.w, st);
-        orth_block(b, b.Vn, nret, b.w, nullptr, st);
         double nr = 0;
-        if (int e = read_nrm(&nr)) return e;
+        auto continuation = [&]() -> int {
+            // the (m+1)-th Lanczos vector continues the recurrence
+            launch_copy(n, b.V + (size_t)m * b.ldv, b.w, st);
+            orth_block(b, b.Vn, nret, b.w, nullptr, st);
+            return read_nrm(&nr);
+        };
+        bool per_vector = l > m;
+        if (!per_vector) {
+            int tk = tm.begin();
+            cudaMemsetAsync(b.dflag, 0, sizeof(int), st);
+            // all l Ritz vectors in one pass over V (each column is summed
+            // in the same order as when it is formed alone)
+            launch_ritz_vectors(b.V, b.ldv, n, m, b.S, m, b.ord, 0, (int)l, b.Vn, b.ldv, b.xn2,
+                                b.rs, st);
+            for (int t = 0; t < (int)l; t++) {
+                double *dst = b.Vn + (size_t)t * b.ldv;
+                orth_block(b, b.Vn, t, dst, nullptr, st);
+                launch_flag_if_below(b.nrm2, 1e-20, b.dflag, st);
+                normalise(n, dst, b.nrm2, dst, st);
+                thsave_kernel<<<1, 1, 0, st>>>(b.theta, b.ord, t, b.thsave, t);
+                note_launch();
+            }
+            copy_async(h_rflag, b.dflag, sizeof(int), cudaMemcpyDeviceToHost, st);
+            tm.end(tk, &ms_ritz);
+            nret = (int)l;
+            if (int e = continuation()) return e;
+            per_vector = *h_rflag != 0;
+        }
+        if (per_vector) {
+            nret = 0;
+            int tk = tm.begin();
+            for (int t = 0; t < m && nret < l; t++) {
+                double *dst = b.Vn + (size_t)nret * b.ldv;
+                launch_ritz_vectors(b.V, b.ldv, n, m, b.S, m, b.ord, t, 1, dst, b.ldv, b.xn2, b.rs,
+                                    st);
+                orth_block(b, b.Vn, nret, dst, nullptr, st);
+                double nv = 0;
+                if (int e = read_nrm(&nv)) return e;
+                if (nv < 1e-10) continue;
+                normalise(n, dst, b.nrm2, dst, st);
+                thsave_kernel<<<1, 1, 0, st>>>(b.theta, b.ord, t, b.thsave, nret);
+                note_launch();
+                nret++;
+            }
+            tm.end(tk, &ms_ritz);
+            if (int e = continuation()) return e;
+        }
         if (nr < 1e-10) {
             rand_vec(b.w);
             orth_block(b, b.Vn, nret, b.w, nullptr, st);
@@ -847,7 +937,7 @@ static int plan_solve(speigs_plan_s *p, int64_t k, double *lambda, double *V, do
     }
     std::vector<double> lam_h(k, 0.0), res_h(k, 0.0);
     int rc = 0;
-    const size_t need = 2 * (size_t)k + 8;
+    const size_t need = 2 * (size_t)k + 16;
     double *pinbuf = pinned_scalars(need);
     if (!pinbuf) return SPEIGS_ERR_MEM;
     {

@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <atomic>
 #include <thread>
+#include <utility>
 #include <vector>
 
 using spx::HostCSR;
@@ -117,6 +118,18 @@ double norm1_upper(int64_t n, const int64_t *Ap, const int64_t *Ai, const double
 }
 
 struct Cand { double key; int64_t idx; };
+
+// stored entries from which the pattern checks run on side threads
+constexpr int64_t kSideThreadsMin = 1 << 17;
+
+// a side thread that is joined on every way out of its scope
+struct SideThread {
+    std::thread t;
+    template <class F>
+    void start(F &&f) { t = std::thread(std::forward<F>(f)); }
+    void join() { if (t.joinable()) t.join(); }
+    ~SideThread() { join(); }
+};
 
 int speigs_impl(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *Ax, int64_t k,
                 speigs_which which, const speigs_opts *opts, const speigs_ext_opts *ext,
@@ -390,8 +403,24 @@ int speigs_impl(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *A
     if (n <= 0 || !Ap || !Ai || !Ax || !lambda) return SPEIGS_ERR_ARG;
     if (k <= 0 || k > n) return SPEIGS_ERR_ARG;
     const double tc = wall();
-    if (opts->check_sym != 0 && check_symmetry(n, Ap, Ai, Ax) == 0) return SPEIGS_ERR_NOTSYM;
+    // The symmetry check and the component labels run on their own threads
+    // beside the 1-norm and the CSR expansion (large matrices only); the
+    // route is taken in the reference's order once each result is in, and
+    // nothing is written to the outputs before the symmetry verdict.
+    const bool side = Ap[n] >= kSideThreadsMin;
+    int sym = 1;
+    SideThread sym_th;
+    if (opts->check_sym != 0) {
+        if (side) sym_th.start([&] { sym = check_symmetry(n, Ap, Ai, Ax); });
+        else sym = check_symmetry(n, Ap, Ai, Ax);
+    }
+    auto sym_failed = [&] {
+        sym_th.join();
+        return sym == 0;
+    };
+    if (!side && sym_failed()) return SPEIGS_ERR_NOTSYM;
     if (n == 1) {
+        if (sym_failed()) return SPEIGS_ERR_NOTSYM;
         // a 1 x 1 matrix is its own eigenvalue: no numerical work to do
         double a = 0.0;
         for (int64_t p = Ap[0]; p < Ap[1]; p++) if (Ai[p] == 0) a = Ax[p];
@@ -406,6 +435,7 @@ int speigs_impl(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *A
     const double t0 = wall();
     const int dmax = opts->dense_max < 0 ? 800 : opts->dense_max;
     if (opts->detect && is_diagonal(n, Ap, Ai)) {
+        if (sym_failed()) return SPEIGS_ERR_NOTSYM;
         std::vector<double> d(n, 0.0);
         for (int64_t c = 0; c < n; c++)
             for (int64_t p = Ap[c]; p < Ap[c + 1]; p++) if (Ai[p] == c) d[c] = Ax[p];
@@ -414,28 +444,35 @@ int speigs_impl(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *A
     if (dmax > 0 && (n <= dmax || 4 * k > n)) {
         HostCSR A;
         int rc = spx::build_full_csr(n, Ap, Ai, Ax, &A);
+        if (sym_failed()) { spx::free_csr(&A); return SPEIGS_ERR_NOTSYM; }
         if (rc) return rc;
         rc = spx::device_dense_path(A, k, which, lambda, V, resid, info);
         spx::free_csr(&A);
         info->t_iter = wall() - t0;
         return rc;
     }
+    std::vector<int64_t> comp;
+    int64_t ncomp = 1;
+    SideThread comp_th;
     if (opts->detect) {
-        std::vector<int64_t> comp;
-        const int64_t ncomp = find_components(n, Ap, Ai, Ax, comp);
-        if (ncomp > 1) {
-            int rc = blocks_path(n, Ap, Ai, Ax, k, which, opts, ext, comp, ncomp, lambda, V, resid,
-                                 info, einfo);
-            info->t_iter = wall() - t0;
-            return rc;
-        }
+        if (side) comp_th.start([&] { ncomp = find_components(n, Ap, Ai, Ax, comp); });
+        else ncomp = find_components(n, Ap, Ai, Ax, comp);
     }
     double anorm = norm1_upper(n, Ap, Ai, Ax);
     if (anorm <= 0) anorm = 1.0;
-    info->anorm = anorm;
     HostCSR A;
     int rc = spx::build_full_csr(n, Ap, Ai, Ax, &A);
+    comp_th.join();
+    if (sym_failed()) { spx::free_csr(&A); return SPEIGS_ERR_NOTSYM; }
+    if (ncomp > 1) {
+        spx::free_csr(&A);
+        rc = blocks_path(n, Ap, Ai, Ax, k, which, opts, ext, comp, ncomp, lambda, V, resid, info,
+                         einfo);
+        info->t_iter = wall() - t0;
+        return rc;
+    }
     if (rc) return rc;
+    info->anorm = anorm;
     const double t_checks = wall() - tc;
     // factor + Lanczos on the device; results come back sorted by |lambda|
     rc = spx::device_krylov(A, k, which, *opts, anorm, lambda, V, resid, info, nullptr, ext,

@@ -6,6 +6,7 @@
 // the ordering choice at :859-863).  The numeric work it prepares runs on the
 // device.
 #include "symbolic.h"
+#include "parallel.h"
 
 #include <algorithm>
 #include <atomic>
@@ -114,8 +115,10 @@ struct NDState {
     }
 
     // Order the vertices `verts` (all carrying region id `id`) into
-    // perm[lo .. lo+|verts|).
-    void order_region(std::vector<int32_t> verts, int32_t id, int32_t lo) {
+    // perm[lo .. lo+|verts|).  `hint` (or -1) is a vertex of the region that
+    // was peripheral in the parent's level structure: the start of the
+    // parent's BFS for the near half, its deepest vertex for the far half.
+    void order_region(std::vector<int32_t> verts, int32_t id, int32_t lo, int32_t hint = -1) {
         const int32_t m = (int32_t)verts.size();
         if (m == 0) return;
         if (m <= 64) {
@@ -123,11 +126,16 @@ struct NDState {
             return;
         }
         std::vector<int32_t> queue(m);
-        // pseudo-peripheral start: lowest degree vertex, then repeated BFS
-        int32_t src = verts[0], bestdeg = degree_in(verts[0], id);
-        for (int32_t v : verts) {
-            int32_t d = degree_in(v, id);
-            if (d < bestdeg) { bestdeg = d; src = v; }
+        // pseudo-peripheral start: the hint, else the lowest degree vertex;
+        // then repeated BFS from the deepest level
+        int32_t src = hint;
+        if (src < 0 || part[src] != id) {
+            src = verts[0];
+            int32_t bestdeg = degree_in(verts[0], id);
+            for (int32_t v : verts) {
+                int32_t d = degree_in(v, id);
+                if (d < bestdeg) { bestdeg = d; src = v; }
+            }
         }
         int32_t depth = 0, cnt = bfs(id, src, &depth, queue);
         if (cnt < m) {
@@ -166,13 +174,14 @@ struct NDState {
             clear_levels(queue, cnt);
             int32_t d2 = 0;
             bfs(id, cand, &d2, queue);
-            if (d2 <= depth) {
-                // no improvement: redo the BFS from src to keep its levels
+            if (d2 < depth) {
+                // shallower: redo the BFS from src to keep its levels
                 clear_levels(queue, cnt);
                 bfs(id, src, &depth, queue);
                 break;
             }
             src = cand;
+            if (d2 == depth) break;  // as deep: keep the candidate's levels
             depth = d2;
         }
         if (depth < 2) {
@@ -207,6 +216,9 @@ struct NDState {
             if (best < 0) best = depth / 2;
         }
         const int32_t ida = next_id++, idb = next_id++, ids = next_id++;
+        // peripheral vertices of the two halves: the BFS start (level 0) and
+        // the last vertex reached (level `depth`)
+        const int32_t hint_a = src, hint_b = queue[cnt - 1];
         std::vector<int32_t> A, B, Sp;
         for (int32_t i = 0; i < cnt; i++) {
             int32_t v = queue[i], l = level[v];
@@ -245,14 +257,17 @@ struct NDState {
         queue.clear();
         queue.shrink_to_fit();
         if (na > kParallelMin && nb > kParallelMin && spare_threads.fetch_sub(1) > 0) {
-            std::thread t([this, &A, ida, lo] { order_region(std::move(A), ida, lo); });
-            order_region(std::move(B), idb, lo + na);
+            // the helper returns its slot as soon as its half is done
+            std::thread t([this, &A, ida, lo, hint_a] {
+                order_region(std::move(A), ida, lo, hint_a);
+                spare_threads.fetch_add(1);
+            });
+            order_region(std::move(B), idb, lo + na, hint_b);
             t.join();
-            spare_threads.fetch_add(1);
         } else {
             if (na > kParallelMin && nb > kParallelMin) spare_threads.fetch_add(1);
-            order_region(std::move(A), ida, lo);
-            order_region(std::move(B), idb, lo + na);
+            order_region(std::move(A), ida, lo, hint_a);
+            order_region(std::move(B), idb, lo + na, hint_b);
         }
     }
     static constexpr int32_t kParallelMin = 4096;
@@ -310,6 +325,9 @@ extern "C" void spx_symbolic_free(spx_symbolic *S) {
     memset(S, 0, sizeof *S);
 }
 
+// items per host thread below which a pass stays on one thread
+constexpr int64_t kGrain = 16384;
+
 template <class T>
 static T *xalloc(size_t cnt) {
     T *p = (T *)malloc((cnt ? cnt : 1) * sizeof(T));
@@ -332,19 +350,24 @@ extern "C" int spx_analyze(int32_t n, const int64_t *rowptr, const int32_t *col,
 
         // ---- 2. permuted adjacency (new numbering), without the diagonal
         std::vector<int64_t> prp(n + 1, 0);
-        for (int32_t j = 0; j < n; j++) {
-            int32_t o = perm0[j];
-            int64_t c = 0;
-            for (int64_t p = rowptr[o]; p < rowptr[o + 1]; p++) c += (col[p] != o);
-            prp[j + 1] = prp[j] + c;
-        }
+        spx::parallel_ranges(n, kGrain, [&](int64_t lo, int64_t hi) {
+            for (int64_t j = lo; j < hi; j++) {
+                const int32_t o = perm0[j];
+                int64_t c = 0;
+                for (int64_t p = rowptr[o]; p < rowptr[o + 1]; p++) c += (col[p] != o);
+                prp[j + 1] = c;
+            }
+        });
+        for (int32_t j = 0; j < n; j++) prp[j + 1] += prp[j];
         std::vector<int32_t> pci(prp[n]);
-        for (int32_t j = 0; j < n; j++) {
-            int32_t o = perm0[j];
-            int64_t q = prp[j];
-            for (int64_t p = rowptr[o]; p < rowptr[o + 1]; p++)
-                if (col[p] != o) pci[q++] = ip0[col[p]];
-        }
+        spx::parallel_ranges(n, kGrain, [&](int64_t lo, int64_t hi) {
+            for (int64_t j = lo; j < hi; j++) {
+                const int32_t o = perm0[j];
+                int64_t q = prp[j];
+                for (int64_t p = rowptr[o]; p < rowptr[o + 1]; p++)
+                    if (col[p] != o) pci[q++] = ip0[col[p]];
+            }
+        });
 
         // ---- 3. elimination tree (Liu, with path compression)
         std::vector<int32_t> parent(n, -1), anc(n, -1);
@@ -403,10 +426,13 @@ extern "C" int spx_analyze(int32_t n, const int64_t *rowptr, const int32_t *col,
             std::vector<int64_t> rp2(n + 1, 0);
             for (int32_t k = 0; k < n; k++) rp2[k + 1] = rp2[k] + (prp[post[k] + 1] - prp[post[k]]);
             std::vector<int32_t> ci2(rp2[n]);
-            for (int32_t k = 0; k < n; k++) {
-                int64_t q = rp2[k];
-                for (int64_t p = prp[post[k]]; p < prp[post[k] + 1]; p++) ci2[q++] = ipost[pci[p]];
-            }
+            spx::parallel_ranges(n, kGrain, [&](int64_t lo, int64_t hi) {
+                for (int64_t k = lo; k < hi; k++) {
+                    int64_t q = rp2[k];
+                    for (int64_t p = prp[post[k]]; p < prp[post[k] + 1]; p++)
+                        ci2[q++] = ipost[pci[p]];
+                }
+            });
             prp.swap(rp2);
             pci.swap(ci2);
         }
@@ -607,31 +633,35 @@ extern "C" int spx_analyze(int32_t n, const int64_t *rowptr, const int32_t *col,
         }
         std::vector<int64_t> rptr(ns + 1, 0);
         for (int32_t s = 0; s < ns; s++) rptr[s + 1] = rptr[s] + (int64_t)rs[s].size();
-        std::vector<int32_t> rows(rptr[ns]);
-        for (int32_t s = 0; s < ns; s++) {
-            std::copy(rs[s].begin(), rs[s].end(), rows.begin() + rptr[s]);
-            std::vector<int32_t>().swap(rs[s]);
-        }
         const int64_t nrows_total = rptr[ns];
         S->rowptr = xalloc<int64_t>(ns + 1);
         memcpy(S->rowptr, rptr.data(), (ns + 1) * sizeof(int64_t));
         S->rows = xalloc<int32_t>(nrows_total);
-        memcpy(S->rows, rows.data(), nrows_total * sizeof(int32_t));
+        spx::parallel_ranges(ns, kGrain, [&](int64_t lo, int64_t hi) {
+            for (int64_t s = lo; s < hi; s++) {
+                std::copy(rs[s].begin(), rs[s].end(), S->rows + rptr[s]);
+                std::vector<int32_t>().swap(rs[s]);
+            }
+        });
+        const int32_t *rows = S->rows;
 
         // ---- 9. relative maps into the parent's row list
+        // (every child has one parent, so the parents' writes are disjoint)
         S->relmap = xalloc<int32_t>(nrows_total);
-        std::vector<int32_t> pos(n, -1);
-        for (int64_t t = 0; t < nrows_total; t++) S->relmap[t] = -1;
-        for (int32_t p = 0; p < ns; p++) {
-            if (cptr[p] == cptr[p + 1]) continue;
-            for (int64_t t = rptr[p]; t < rptr[p + 1]; t++) pos[rows[t]] = (int32_t)(t - rptr[p]);
-            for (int32_t q = cptr[p]; q < cptr[p + 1]; q++) {
-                int32_t c = clist[q];
-                int32_t cc0 = S->sfirst[c + 1] - S->sfirst[c];
-                for (int64_t t = rptr[c] + cc0; t < rptr[c + 1]; t++) S->relmap[t] = pos[rows[t]];
+        std::fill(S->relmap, S->relmap + nrows_total, -1);
+        spx::parallel_ranges(ns, kGrain, [&](int64_t lo, int64_t hi) {
+            std::vector<int32_t> pos(n, -1);
+            for (int64_t p = lo; p < hi; p++) {
+                if (cptr[p] == cptr[p + 1]) continue;
+                for (int64_t t = rptr[p]; t < rptr[p + 1]; t++) pos[rows[t]] = (int32_t)(t - rptr[p]);
+                for (int32_t q = cptr[p]; q < cptr[p + 1]; q++) {
+                    int32_t c = clist[q];
+                    int32_t cc0 = S->sfirst[c + 1] - S->sfirst[c];
+                    for (int64_t t = rptr[c] + cc0; t < rptr[c + 1]; t++) S->relmap[t] = pos[rows[t]];
+                }
+                for (int64_t t = rptr[p]; t < rptr[p + 1]; t++) pos[rows[t]] = -1;
             }
-            for (int64_t t = rptr[p]; t < rptr[p + 1]; t++) pos[rows[t]] = -1;
-        }
+        });
 
         // ---- 10. levels, fronts, statistics
         std::vector<int32_t> lev(ns, 0);

@@ -112,9 +112,17 @@ __device__ void last_block_reduce(double *part, unsigned *counter, int ncols, do
     for (int t = threadIdx.x; t < ncols * segs; t += blockDim.x) {
         int c = t % ncols, s = t / ncols;
         int b0 = s * per, b1 = min(nb, b0 + per);
-        double acc = 0.0;
-        for (int b = b0; b < b1; b++) acc += ((volatile double *)part)[(size_t)b * ncols + c];
-        sh[s * ncols + c] = acc;
+        // four independent sums keep four L2 loads in flight per thread
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+        int b = b0;
+        for (; b + 3 < b1; b += 4) {
+            a0 += __ldcg(part + (size_t)b * ncols + c);
+            a1 += __ldcg(part + (size_t)(b + 1) * ncols + c);
+            a2 += __ldcg(part + (size_t)(b + 2) * ncols + c);
+            a3 += __ldcg(part + (size_t)(b + 3) * ncols + c);
+        }
+        for (; b < b1; b++) a0 += __ldcg(part + (size_t)b * ncols + c);
+        sh[s * ncols + c] = (a0 + a1) + (a2 + a3);
     }
     __syncthreads();
     for (int c = threadIdx.x; c < ncols; c += blockDim.x) {
@@ -127,87 +135,97 @@ __device__ void last_block_reduce(double *part, unsigned *counter, int ncols, do
     if (threadIdx.x == 0) *counter = 0u;
 }
 
+// One launch covers every row: a block takes 512-row segments
+// blockIdx.x, blockIdx.x + gridDim.x, ... (the grid is capped at a few
+// blocks per SM), reduces each segment's column sums eight at a time and
+// keeps the block's running sums in shared memory; the last block to
+// finish combines the blocks' sums.
 template <int MODE>
 __global__ void __launch_bounds__(kTsThreads) ts_kernel(TsParams p) {
     extern __shared__ double sh[];
-    double *hs = sh;                       // m coefficients
-    double *red = sh + ((p.m + 1) & ~1);   // block reduce scratch (>= 32)
-    double *fin = red + 32;                // last-block scratch
     const int n = p.n, m = p.m;
+    const int ncols = (MODE == TS_DOT || MODE == TS_UPDATE_DOT) ? m : 1;
+    double *hs = sh;                                  // m coefficients
+    double *bacc = hs + ((m + 1) & ~1);               // the block's column sums
+    double *red = bacc + ((ncols + 1) & ~1);          // block reduce scratch (64)
+    double *fin = red + 64;                           // last-block scratch
     if (MODE == TS_UPDATE_DOT || MODE == TS_UPDATE_NORM)
         for (int c = threadIdx.x; c < m; c += blockDim.x) hs[c] = p.hin[c];
+    for (int c = threadIdx.x; c < ncols; c += blockDim.x) bacc[c] = 0.0;
     __syncthreads();
-    const int base = blockIdx.x * (kTsThreads * kTsRows) + threadIdx.x;
-    double wv[kTsRows];
-#pragma unroll
-    for (int r = 0; r < kTsRows; r++) {
-        int i = base + r * kTsThreads;
-        wv[r] = (i < n) ? p.w[i] : 0.0;
-    }
-    if (MODE == TS_UPDATE_DOT || MODE == TS_UPDATE_NORM) {
-        double s[kTsRows];
-#pragma unroll
-        for (int r = 0; r < kTsRows; r++) s[r] = 0.0;
-        for (int c = 0; c < m; c++) {
-            const double hc = hs[c];
-            const double *vc = p.V + (size_t)c * p.ldv;
-#pragma unroll
-            for (int r = 0; r < kTsRows; r++) {
-                int i = base + r * kTsThreads;
-                if (i < n) s[r] += vc[i] * hc;
-            }
-        }
+    constexpr int kSeg = kTsThreads * kTsRows;
+    for (int64_t seg = blockIdx.x; seg * kSeg < n; seg += gridDim.x) {
+        const int64_t base = seg * kSeg + threadIdx.x;
+        double wv[kTsRows];
 #pragma unroll
         for (int r = 0; r < kTsRows; r++) {
-            int i = base + r * kTsThreads;
-            if (i < n) { wv[r] -= s[r]; p.w[i] = wv[r]; }
+            const int64_t i = base + r * kTsThreads;
+            wv[r] = (i < n) ? p.w[i] : 0.0;
         }
-    }
-    int ncols;
-    if (MODE == TS_DOT || MODE == TS_UPDATE_DOT) {
-        ncols = m;
-        for (int c0 = 0; c0 < m; c0 += kTsChunk) {
-            double acc[kTsChunk];
+        if (MODE == TS_UPDATE_DOT || MODE == TS_UPDATE_NORM) {
+            double s[kTsRows];
 #pragma unroll
-            for (int q = 0; q < kTsChunk; q++) acc[q] = 0.0;
+            for (int r = 0; r < kTsRows; r++) s[r] = 0.0;
+            for (int c = 0; c < m; c++) {
+                const double hc = hs[c];
+                const double *vc = p.V + (size_t)c * p.ldv;
 #pragma unroll
-            for (int q = 0; q < kTsChunk; q++) {
-                if (c0 + q < m) {
-                    const double *vc = p.V + (size_t)(c0 + q) * p.ldv;
+                for (int r = 0; r < kTsRows; r++) {
+                    const int64_t i = base + r * kTsThreads;
+                    if (i < n) s[r] += vc[i] * hc;
+                }
+            }
 #pragma unroll
-                    for (int r = 0; r < kTsRows; r++) {
-                        int i = base + r * kTsThreads;
-                        if (i < n) acc[q] += vc[i] * wv[r];
+            for (int r = 0; r < kTsRows; r++) {
+                const int64_t i = base + r * kTsThreads;
+                if (i < n) { wv[r] -= s[r]; p.w[i] = wv[r]; }
+            }
+        }
+        if (MODE == TS_DOT || MODE == TS_UPDATE_DOT) {
+            for (int c0 = 0; c0 < m; c0 += kTsChunk) {
+                double acc[kTsChunk];
+#pragma unroll
+                for (int q = 0; q < kTsChunk; q++) acc[q] = 0.0;
+#pragma unroll
+                for (int q = 0; q < kTsChunk; q++) {
+                    if (c0 + q < m) {
+                        const double *vc = p.V + (size_t)(c0 + q) * p.ldv;
+#pragma unroll
+                        for (int r = 0; r < kTsRows; r++) {
+                            const int64_t i = base + r * kTsThreads;
+                            if (i < n) acc[q] += vc[i] * wv[r];
+                        }
                     }
                 }
+                const double t = block_sum8(acc, red);
+                if (threadIdx.x < kTsChunk && c0 + (int)threadIdx.x < m) bacc[c0 + threadIdx.x] += t;
             }
+        } else {
+            double acc = 0.0;
 #pragma unroll
-            for (int q = 0; q < kTsChunk; q++) {
-                if (c0 + q < m) {
-                    double t = block_sum(acc[q], red);
-                    if (threadIdx.x == 0) p.part[(size_t)blockIdx.x * m + c0 + q] = t;
-                }
-            }
+            for (int r = 0; r < kTsRows; r++) acc += wv[r] * wv[r];
+            const double t = block_sum(acc, red);
+            if (threadIdx.x == 0) bacc[0] += t;
         }
-    } else {
-        ncols = 1;
-        double acc = 0.0;
-#pragma unroll
-        for (int r = 0; r < kTsRows; r++) acc += wv[r] * wv[r];
-        double t = block_sum(acc, red);
-        if (threadIdx.x == 0) p.part[blockIdx.x] = t;
     }
+    __syncthreads();
+    for (int c = threadIdx.x; c < ncols; c += blockDim.x)
+        p.part[(size_t)blockIdx.x * ncols + c] = bacc[c];
     last_block_reduce(p.part, p.counter, ncols, p.out, p.hcol, p.hmode, fin);
 }
 
 static size_t ts_smem(int ncols_h, int ncols_red) {
     int segs = std::max(1, kTsThreads / std::max(ncols_red, 1));
-    return sizeof(double) * ((size_t)((ncols_h + 1) & ~1) + 32 + (size_t)ncols_red * segs);
+    return sizeof(double) * ((size_t)((ncols_h + 1) & ~1) + (size_t)((ncols_red + 1) & ~1) + 64 +
+                             (size_t)ncols_red * segs);
 }
+
+// blocks of a tall-skinny launch: one per 512-row segment, at most four per SM
+constexpr int kTsMaxBlocks = 4 * 148;
 
 template <int MODE>
 static void ts_launch(const TsParams &p, int ncols_red, cudaStream_t st) {
-    int nb = ts_blocks(p.n);
+    int nb = std::min(ts_blocks(p.n), kTsMaxBlocks);
     size_t smem = ts_smem(p.m, ncols_red);
     ts_kernel<MODE><<<nb, kTsThreads, smem, st>>>(p);
     note_launch();
@@ -326,12 +344,19 @@ void launch_ritz_vectors(const double *V, int64_t ldv, int n, int m, const doubl
                          const int *idx, int idx_off, int nvec, double *X, int64_t ldx,
                          double *nrm2, const ReduceScratch &rs, cudaStream_t st) {
     if (nvec <= 0) return;
-    RitzParams p{V, ldv, n, m, S, lds, idx, idx_off, nvec, X, ldx, nrm2, rs.part, rs.counter};
-    int nb = ts_blocks(n);
-    int segs = std::max(1, kTsThreads / nvec);
-    size_t smem = sizeof(double) * ((((size_t)m * nvec + 1) & ~1) + 32 + (size_t)nvec * segs);
-    ritz_kernel<<<nb, kTsThreads, smem, st>>>(p);
-    note_launch();
+    // vectors per launch: the m x nv block of S fits the default 48 KB of
+    // dynamic shared memory beside the reduction scratch
+    const int cap = std::max(1, (6144 - 32 - 2 * kTsThreads) / std::max(1, m));
+    for (int v0 = 0; v0 < nvec; v0 += cap) {
+        const int nv = std::min(cap, nvec - v0);
+        RitzParams p{V, ldv, n, m, S, lds, idx, idx_off + v0, nv, X + (size_t)v0 * ldx, ldx,
+                     nrm2 + v0, rs.part, rs.counter};
+        int nb = ts_blocks(n);
+        int segs = std::max(1, kTsThreads / nv);
+        size_t smem = sizeof(double) * ((((size_t)m * nv + 1) & ~1) + 32 + (size_t)nv * segs);
+        ritz_kernel<<<nb, kTsThreads, smem, st>>>(p);
+        note_launch();
+    }
 }
 
 __global__ void scale_cols_kernel(int n, int nvec, double *X, int64_t ldx, const double *nrm2) {
@@ -747,6 +772,14 @@ __global__ void set_diag_kernel(int ldh, int nd, const double *d, double *H) {
 void launch_set_diag(int ldh, int nd, const double *d, double *H, cudaStream_t st) {
     int nb = std::max(1, std::min(256, (ldh * ldh + 255) / 256));
     set_diag_kernel<<<nb, 256, 0, st>>>(ldh, nd, d, H);
+    note_launch();
+}
+
+__global__ void flag_if_below_kernel(const double *nrm2, double thr, int *flag) {
+    if (!(nrm2[0] >= thr)) *flag = 1;
+}
+void launch_flag_if_below(const double *nrm2, double thr, int *flag, cudaStream_t st) {
+    flag_if_below_kernel<<<1, 1, 0, st>>>(nrm2, thr, flag);
     note_launch();
 }
 

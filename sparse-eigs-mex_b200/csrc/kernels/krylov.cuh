@@ -76,6 +76,8 @@ void launch_syev_small_workspace(int m, const double *H, int ldh, double *theta,
 // H (ldh x ldh) = diag(d[0..nd)) with zeros elsewhere in the leading m x m part
 void launch_set_diag(int ldh, int nd, const double *d, double *H, cudaStream_t st);
 // H[r + c*ldh] = H[c + r*ldh] = sqrt(nrm2[0]) or 0 if zero_flag
+// *flag = 1 when nrm2[0] < thr (device-side test of a squared norm)
+void launch_flag_if_below(const double *nrm2, double thr, int *flag, cudaStream_t st);
 void launch_set_beta(double *H, int ldh, int r, int c, const double *nrm2, int zero,
                      cudaStream_t st);
 

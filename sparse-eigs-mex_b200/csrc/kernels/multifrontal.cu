@@ -17,6 +17,7 @@
 #include "multifrontal.cuh"
 #include "../common.cuh"
 #include "../counters.h"
+#include "../host/parallel.h"
 
 #include <cooperative_groups.h>
 namespace cg = cooperative_groups;
@@ -1534,32 +1535,98 @@ template <> int MultifrontalPlanT<Real>::init(const spx_symbolic &S, const int64
         }
         g_total_ = gtri;
         u_total_ = uptr[ns];
-        // assembly entries: for new column j, the entries of A's column
-        // perm[j] with new row index >= j, as (row position in the front,
-        // index into the CSR values), sorted by row position
+        // The assembly entries, the solve gather lists and the child tile
+        // bounds are independent of the task lists: they are built on side
+        // threads while this thread builds the factor and solve task lists.
         std::vector<int32_t> acolptr(n + 1, 0);
         std::vector<int32_t> atpos, asrc;
-        atpos.reserve((size_t)rowptr[n] / 2 + n);
-        asrc.reserve((size_t)rowptr[n] / 2 + n);
-        std::vector<int32_t> pos(n, -1);
-        std::vector<std::pair<int32_t, int32_t>> tmp;
-        for (int32_t s = 0; s < ns; s++) {
-            const int64_t r0 = S.rowptr[s], r1 = S.rowptr[s + 1];
-            for (int64_t t = r0; t < r1; t++) pos[S.rows[t]] = (int32_t)(t - r0);
-            for (int32_t j = S.sfirst[s]; j < S.sfirst[s + 1]; j++) {
-                const int32_t o = S.perm[j];
-                tmp.clear();
-                for (int64_t p = rowptr[o]; p < rowptr[o + 1]; p++) {
-                    const int32_t i = S.iperm[col[p]];
-                    if (i < j) continue;
-                    tmp.emplace_back(pos[i], (int32_t)p);
+        std::vector<int32_t> cptr(nrows_total_ + 1, 0), cidx;
+        std::vector<int64_t> cbnd_ptr(ns + 1, 0);
+        std::vector<int32_t> cbnd;
+        TaskGroup side(rowptr[n] >= (1 << 17));
+        side.run([&] {
+            // assembly entries: for new column j, the entries of A's column
+            // perm[j] with new row index >= j, as (row position in the front,
+            // index into the CSR values), sorted by row position
+            // (counted per column first, so that ranges of supernodes fill
+            // their own columns' slices in parallel)
+            parallel_ranges(n, 16384, [&](int64_t lo, int64_t hi) {
+                for (int64_t j = lo; j < hi; j++) {
+                    const int32_t o = S.perm[j];
+                    int32_t c = 0;
+                    for (int64_t p = rowptr[o]; p < rowptr[o + 1]; p++) c += S.iperm[col[p]] >= j;
+                    acolptr[j + 1] = c;
                 }
-                std::sort(tmp.begin(), tmp.end());
-                for (auto &e : tmp) { atpos.push_back(e.first); asrc.push_back(e.second); }
-                acolptr[j + 1] = (int32_t)atpos.size();
+            });
+            for (int32_t j = 0; j < n; j++) acolptr[j + 1] += acolptr[j];
+            atpos.resize(acolptr[n]);
+            asrc.resize(acolptr[n]);
+            parallel_ranges(ns, 2048, [&](int64_t lo, int64_t hi) {
+                std::vector<int32_t> pos(n, -1);
+                std::vector<std::pair<int32_t, int32_t>> tmp;
+                for (int64_t s = lo; s < hi; s++) {
+                    const int64_t r0 = S.rowptr[s], r1 = S.rowptr[s + 1];
+                    for (int64_t t = r0; t < r1; t++) pos[S.rows[t]] = (int32_t)(t - r0);
+                    for (int32_t j = S.sfirst[s]; j < S.sfirst[s + 1]; j++) {
+                        const int32_t o = S.perm[j];
+                        tmp.clear();
+                        for (int64_t p = rowptr[o]; p < rowptr[o + 1]; p++) {
+                            const int32_t i = S.iperm[col[p]];
+                            if (i < j) continue;
+                            tmp.emplace_back(pos[i], (int32_t)p);
+                        }
+                        std::sort(tmp.begin(), tmp.end());
+                        int32_t d = acolptr[j];
+                        for (auto &e : tmp) { atpos[d] = e.first; asrc[d] = e.second; d++; }
+                    }
+                    for (int64_t t = r0; t < r1; t++) pos[S.rows[t]] = -1;
+                }
+            });
+        });
+        side.run([&] {
+            // gather lists: for every front row (global row-list index g) the
+            // update-vector entries of the children that land on it, children in
+            // their fixed order
+            for (int32_t par = 0; par < ns; par++)
+                for (int32_t q = S.child_ptr[par]; q < S.child_ptr[par + 1]; q++) {
+                    const int ch = S.child_list[q];
+                    const int cc = S.sfirst[ch + 1] - S.sfirst[ch];
+                    for (int64_t t = S.rowptr[ch] + cc; t < S.rowptr[ch + 1]; t++)
+                        cptr[S.rowptr[par] + S.relmap[t] + 1]++;
+                }
+            for (int64_t g = 0; g < nrows_total_; g++) cptr[g + 1] += cptr[g];
+            cidx.assign(cptr[nrows_total_], 0);
+            {
+                std::vector<int32_t> fill(cptr.begin(), cptr.end() - 1);
+                for (int32_t par = 0; par < ns; par++)
+                    for (int32_t q = S.child_ptr[par]; q < S.child_ptr[par + 1]; q++) {
+                        const int ch = S.child_list[q];
+                        const int cc = S.sfirst[ch + 1] - S.sfirst[ch];
+                        for (int64_t t = S.rowptr[ch] + cc; t < S.rowptr[ch + 1]; t++)
+                            cidx[fill[S.rowptr[par] + S.relmap[t]]++] =
+                                (int32_t)(uptr[ch] + (t - S.rowptr[ch] - cc));
+                    }
             }
-            for (int64_t t = r0; t < r1; t++) pos[S.rows[t]] = -1;
-        }
+        });
+        side.run([&] {
+            // child tile bounds for the assembly (32-row tiles of the parent)
+            for (int32_t ch = 0; ch < ns; ch++) {
+                const int p = S.sparent[ch];
+                cbnd_ptr[ch] = (int64_t)cbnd.size();
+                if (p < 0) continue;
+                const int rp = (int)(S.rowptr[p + 1] - S.rowptr[p]);
+                const int cp = S.sfirst[p + 1] - S.sfirst[p];
+                const int nkb = (cp + T - 1) / T, ntp = nkb + (rp - cp + T - 1) / T;
+                const int cch = S.sfirst[ch + 1] - S.sfirst[ch];
+                const int32_t *rm = S.relmap + S.rowptr[ch] + cch;
+                const int nb = (int)(S.rowptr[ch + 1] - S.rowptr[ch]) - cch;
+                for (int I = 0; I <= ntp; I++) {
+                    const int start = (I == ntp) ? rp : (I < nkb ? I * T : cp + (I - nkb) * T);
+                    cbnd.push_back((int32_t)(std::lower_bound(rm, rm + nb, start) - rm));
+                }
+            }
+            cbnd_ptr[ns] = (int64_t)cbnd.size();
+        });
         // tile task lists, level by level
         std::vector<int4> tasks;
         launches_.clear();
@@ -1774,49 +1841,7 @@ template <> int MultifrontalPlanT<Real>::init(const spx_symbolic &S, const int64
             }
         }
         ntasks_ = (int)tasks_s.size();
-        // gather lists: for every front row (global row-list index g) the
-        // update-vector entries of the children that land on it, children in
-        // their fixed order
-        std::vector<int32_t> cptr(nrows_total_ + 1, 0), cidx;
-        for (int32_t par = 0; par < ns; par++)
-            for (int32_t q = S.child_ptr[par]; q < S.child_ptr[par + 1]; q++) {
-                const int ch = S.child_list[q];
-                const int cc = S.sfirst[ch + 1] - S.sfirst[ch];
-                for (int64_t t = S.rowptr[ch] + cc; t < S.rowptr[ch + 1]; t++)
-                    cptr[S.rowptr[par] + S.relmap[t] + 1]++;
-            }
-        for (int64_t g = 0; g < nrows_total_; g++) cptr[g + 1] += cptr[g];
-        cidx.assign(cptr[nrows_total_], 0);
-        {
-            std::vector<int32_t> fill(cptr.begin(), cptr.end() - 1);
-            for (int32_t par = 0; par < ns; par++)
-                for (int32_t q = S.child_ptr[par]; q < S.child_ptr[par + 1]; q++) {
-                    const int ch = S.child_list[q];
-                    const int cc = S.sfirst[ch + 1] - S.sfirst[ch];
-                    for (int64_t t = S.rowptr[ch] + cc; t < S.rowptr[ch + 1]; t++)
-                        cidx[fill[S.rowptr[par] + S.relmap[t]]++] =
-                            (int32_t)(uptr[ch] + (t - S.rowptr[ch] - cc));
-                }
-        }
-        // child tile bounds for the assembly (32-row tiles of the parent)
-        std::vector<int64_t> cbnd_ptr(ns + 1, 0);
-        std::vector<int32_t> cbnd;
-        for (int32_t ch = 0; ch < ns; ch++) {
-            const int p = S.sparent[ch];
-            cbnd_ptr[ch] = (int64_t)cbnd.size();
-            if (p < 0) continue;
-            const int rp = (int)(S.rowptr[p + 1] - S.rowptr[p]);
-            const int cp = S.sfirst[p + 1] - S.sfirst[p];
-            const int nkb = (cp + T - 1) / T, ntp = nkb + (rp - cp + T - 1) / T;
-            const int cch = S.sfirst[ch + 1] - S.sfirst[ch];
-            const int32_t *rm = S.relmap + S.rowptr[ch] + cch;
-            const int nb = (int)(S.rowptr[ch + 1] - S.rowptr[ch]) - cch;
-            for (int I = 0; I <= ntp; I++) {
-                const int start = (I == ntp) ? rp : (I < nkb ? I * T : cp + (I - nkb) * T);
-                cbnd.push_back((int32_t)(std::lower_bound(rm, rm + nb, start) - rm));
-            }
-        }
-        cbnd_ptr[ns] = (int64_t)cbnd.size();
+        side.wait();
         int rc = 0;
         rc = rc ? rc : dupload(&d_cbnd_, cbnd.data(), cbnd.size(), st);
         rc = rc ? rc : dupload(&d_cbnd_ptr_, cbnd_ptr.data(), cbnd_ptr.size(), st);
