@@ -8,6 +8,7 @@
 // only reads back the scalars the reference branches on (a step's beta, the
 // number of converged pairs, a restart vector's norm).
 #include "engine.h"
+#include "host/parallel.h"
 #include "../../include/speigs_b200.h"
 #include "kernels/krylov.cuh"
 #include "kernels/multifrontal.cuh"
@@ -707,6 +708,37 @@ int build_full_csr(int64_t n, const int64_t *Ap, const int64_t *Ai, const double
     }
     out->n = (int32_t)n;
     out->rowptr = cnt;
+    out->col = ci;
+    out->val = cx;
+    return SPEIGS_OK;
+}
+
+int build_full_csr_sorted(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *Ax,
+                          HostCSR *out) {
+    if (n <= 0 || n > INT32_MAX) return SPEIGS_ERR_ARG;
+    const int64_t nnz = Ap[n];
+    if (nnz > INT32_MAX) return SPEIGS_ERR_MEM;
+    int64_t *rp = (int64_t *)malloc((size_t)(n + 1) * sizeof(int64_t));
+    int32_t *ci = (int32_t *)malloc((size_t)(nnz ? nnz : 1) * sizeof(int32_t));
+    double *cx = (double *)malloc((size_t)(nnz ? nnz : 1) * sizeof(double));
+    if (!rp || !ci || !cx) { free(rp); free(ci); free(cx); return SPEIGS_ERR_MEM; }
+    memcpy(rp, Ap, (size_t)(n + 1) * sizeof(int64_t));
+    parallel_ranges(n, 8192, [&](int64_t lo, int64_t hi) {
+        for (int64_t i = lo; i < hi; i++)
+            for (int64_t q = Ap[i]; q < Ap[i + 1]; q++) {
+                const int64_t r = Ai[q];
+                ci[q] = (int32_t)r;
+                if (r <= i) {
+                    cx[q] = Ax[q];                       // (r, i) is in the upper triangle
+                } else {
+                    // the upper-triangle mirror (i, r) sits in column r
+                    const int64_t *f = std::lower_bound(Ai + Ap[r], Ai + Ap[r + 1], i);
+                    cx[q] = Ax[f - Ai];
+                }
+            }
+    });
+    out->n = (int32_t)n;
+    out->rowptr = rp;
     out->col = ci;
     out->val = cx;
     return SPEIGS_OK;

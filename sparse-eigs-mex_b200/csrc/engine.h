@@ -22,6 +22,12 @@ struct HostCSR {
 };
 int  build_full_csr(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *Ax,
                     HostCSR *out);
+// The same CSR for an input whose pattern is symmetric with both triangles
+// stored and strictly increasing row indices in every column (as the
+// parallel symmetry check establishes): row i is column i, with the values
+// of the upper triangle; built by parallel passes.
+int  build_full_csr_sorted(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *Ax,
+                           HostCSR *out);
 void free_csr(HostCSR *A);
 
 // Extended results not in speigs_info (device-side phase times in ms).

@@ -9,6 +9,7 @@
 // numerical step of every route runs on the GPU.
 #include "../engine.h"
 #include "../../../include/speigs_b200.h"
+#include "parallel.h"
 
 #include <math.h>
 #include <stdlib.h>
@@ -17,6 +18,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <memory>
 #include <thread>
 #include <utility>
 #include <vector>
@@ -95,6 +97,97 @@ int64_t find_components(int64_t n, const int64_t *Ap, const int64_t *Ai, const d
     int64_t nc = 0;
     for (int64_t i = 0; i < n; i++) {
         int64_t r = uf_find(p, i);
+        if (lab[r] < 0) lab[r] = nc++;
+        comp[i] = lab[r];
+    }
+    return nc;
+}
+
+// check_symmetry for large inputs: the same verdict, from parallel passes.
+// When every column's row indices are strictly increasing, "the transpose
+// equals A entry for entry" is "every (r, c) has its mirror (c, r), with a
+// value within 1e-12 relative", which each column tests on its own by binary
+// search; otherwise the transposition above decides.  *full_sorted is set
+// when the verdict is 1 with both triangles stored and sorted columns.
+int check_symmetry_par(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *Ax,
+                       bool *full_sorted) {
+    *full_sorted = false;
+    std::atomic<int> up{0}, lo{0}, unsorted{0};
+    spx::parallel_ranges(n, 8192, [&](int64_t c0, int64_t c1) {
+        bool u = false, l = false, uns = false;
+        for (int64_t c = c0; c < c1; c++)
+            for (int64_t q = Ap[c]; q < Ap[c + 1]; q++) {
+                if (Ai[q] < c) u = true;
+                else if (Ai[q] > c) l = true;
+                if (q > Ap[c] && Ai[q] <= Ai[q - 1]) uns = true;
+            }
+        if (u) up = 1;
+        if (l) lo = 1;
+        if (uns) unsorted = 1;
+    });
+    if (!lo && up) return 2;
+    if (!up && lo) return 3;
+    if (!up && !lo) return 1;
+    if (unsorted) return check_symmetry(n, Ap, Ai, Ax);
+    std::atomic<int> bad{0};
+    spx::parallel_ranges(n, 8192, [&](int64_t c0, int64_t c1) {
+        for (int64_t c = c0; c < c1 && !bad.load(std::memory_order_relaxed); c++)
+            for (int64_t q = Ap[c]; q < Ap[c + 1]; q++) {
+                const int64_t r = Ai[q];
+                if (r == c) continue;
+                if (r < 0 || r >= n) { bad = 1; break; }
+                const int64_t *b = Ai + Ap[r], *e = Ai + Ap[r + 1];
+                const int64_t *f = std::lower_bound(b, e, c);
+                if (f == e || *f != c) { bad = 1; break; }
+                const double a = Ax[q], t = Ax[f - Ai];
+                const double m = std::max(fabs(a), fabs(t));
+                if (fabs(a - t) > 1e-12 * (m > 0 ? m : 1.0)) { bad = 1; break; }
+            }
+    });
+    if (bad) return 0;
+    *full_sorted = true;
+    return 1;
+}
+
+// find_components for large inputs: the same labels (components over the
+// numerically nonzero entries, numbered in order of first appearance), with
+// the unions done in parallel on a lock-free union-find (a root is linked
+// under a smaller root by compare-and-swap, so links never form a cycle).
+int64_t find_components_par(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *Ax,
+                            std::vector<int64_t> &comp) {
+    std::unique_ptr<std::atomic<int64_t>[]> p(new std::atomic<int64_t>[n]);
+    spx::parallel_ranges(n, 65536, [&](int64_t a, int64_t b) {
+        for (int64_t i = a; i < b; i++) p[i].store(i, std::memory_order_relaxed);
+    });
+    auto find = [&](int64_t x) {
+        for (;;) {
+            int64_t px = p[x].load(std::memory_order_relaxed);
+            if (px == x) return x;
+            int64_t gx = p[px].load(std::memory_order_relaxed);
+            if (gx != px) p[x].compare_exchange_weak(px, gx, std::memory_order_relaxed);
+            x = gx;
+        }
+    };
+    spx::parallel_ranges(n, 8192, [&](int64_t c0, int64_t c1) {
+        for (int64_t c = c0; c < c1; c++)
+            for (int64_t q = Ap[c]; q < Ap[c + 1]; q++) {
+                if (Ax[q] == 0.0) continue;
+                int64_t a = Ai[q], b = c;
+                for (;;) {
+                    a = find(a);
+                    b = find(b);
+                    if (a == b) break;
+                    if (a < b) std::swap(a, b);
+                    int64_t expect = a;
+                    if (p[a].compare_exchange_strong(expect, b, std::memory_order_relaxed)) break;
+                }
+            }
+    });
+    std::vector<int64_t> lab(n, -1);
+    comp.assign(n, 0);
+    int64_t nc = 0;
+    for (int64_t i = 0; i < n; i++) {
+        const int64_t r = find(i);
         if (lab[r] < 0) lab[r] = nc++;
         comp[i] = lab[r];
     }
@@ -327,7 +420,8 @@ int speigs_components(speigs_int n, const speigs_int *Ap, const speigs_int *Ai,
                       const double *Ax, speigs_int *comp, speigs_int *ncomp) {
     if (n <= 0 || !Ap || !Ai || !Ax || !comp || !ncomp) return SPEIGS_ERR_ARG;
     std::vector<int64_t> c;
-    *ncomp = find_components(n, Ap, Ai, Ax, c);
+    *ncomp = Ap[n] >= kSideThreadsMin ? find_components_par(n, Ap, Ai, Ax, c)
+                                      : find_components(n, Ap, Ai, Ax, c);
     memcpy(comp, c.data(), sizeof(int64_t) * (size_t)n);
     return SPEIGS_OK;
 }
@@ -403,24 +497,17 @@ int speigs_impl(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *A
     if (n <= 0 || !Ap || !Ai || !Ax || !lambda) return SPEIGS_ERR_ARG;
     if (k <= 0 || k > n) return SPEIGS_ERR_ARG;
     const double tc = wall();
-    // The symmetry check and the component labels run on their own threads
-    // beside the 1-norm and the CSR expansion (large matrices only); the
-    // route is taken in the reference's order once each result is in, and
-    // nothing is written to the outputs before the symmetry verdict.
-    const bool side = Ap[n] >= kSideThreadsMin;
-    int sym = 1;
-    SideThread sym_th;
+    // Large inputs: the symmetry check and the component labels run as
+    // parallel passes, and the labels, the 1-norm and the CSR expansion side
+    // by side; the route is taken in the reference's order.
+    const bool par = Ap[n] >= kSideThreadsMin;
+    bool full_sorted = false;
     if (opts->check_sym != 0) {
-        if (side) sym_th.start([&] { sym = check_symmetry(n, Ap, Ai, Ax); });
-        else sym = check_symmetry(n, Ap, Ai, Ax);
+        const int sym = par ? check_symmetry_par(n, Ap, Ai, Ax, &full_sorted)
+                            : check_symmetry(n, Ap, Ai, Ax);
+        if (sym == 0) return SPEIGS_ERR_NOTSYM;
     }
-    auto sym_failed = [&] {
-        sym_th.join();
-        return sym == 0;
-    };
-    if (!side && sym_failed()) return SPEIGS_ERR_NOTSYM;
     if (n == 1) {
-        if (sym_failed()) return SPEIGS_ERR_NOTSYM;
         // a 1 x 1 matrix is its own eigenvalue: no numerical work to do
         double a = 0.0;
         for (int64_t p = Ap[0]; p < Ap[1]; p++) if (Ai[p] == 0) a = Ax[p];
@@ -435,7 +522,6 @@ int speigs_impl(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *A
     const double t0 = wall();
     const int dmax = opts->dense_max < 0 ? 800 : opts->dense_max;
     if (opts->detect && is_diagonal(n, Ap, Ai)) {
-        if (sym_failed()) return SPEIGS_ERR_NOTSYM;
         std::vector<double> d(n, 0.0);
         for (int64_t c = 0; c < n; c++)
             for (int64_t p = Ap[c]; p < Ap[c + 1]; p++) if (Ai[p] == c) d[c] = Ax[p];
@@ -444,7 +530,6 @@ int speigs_impl(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *A
     if (dmax > 0 && (n <= dmax || 4 * k > n)) {
         HostCSR A;
         int rc = spx::build_full_csr(n, Ap, Ai, Ax, &A);
-        if (sym_failed()) { spx::free_csr(&A); return SPEIGS_ERR_NOTSYM; }
         if (rc) return rc;
         rc = spx::device_dense_path(A, k, which, lambda, V, resid, info);
         spx::free_csr(&A);
@@ -455,15 +540,19 @@ int speigs_impl(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *A
     int64_t ncomp = 1;
     SideThread comp_th;
     if (opts->detect) {
-        if (side) comp_th.start([&] { ncomp = find_components(n, Ap, Ai, Ax, comp); });
+        if (par) comp_th.start([&] { ncomp = find_components_par(n, Ap, Ai, Ax, comp); });
         else ncomp = find_components(n, Ap, Ai, Ax, comp);
     }
-    double anorm = norm1_upper(n, Ap, Ai, Ax);
-    if (anorm <= 0) anorm = 1.0;
+    double anorm = 0.0;
+    SideThread norm_th;
+    if (par) norm_th.start([&] { anorm = norm1_upper(n, Ap, Ai, Ax); });
+    else anorm = norm1_upper(n, Ap, Ai, Ax);
     HostCSR A;
-    int rc = spx::build_full_csr(n, Ap, Ai, Ax, &A);
+    int rc = full_sorted ? spx::build_full_csr_sorted(n, Ap, Ai, Ax, &A)
+                         : spx::build_full_csr(n, Ap, Ai, Ax, &A);
     comp_th.join();
-    if (sym_failed()) { spx::free_csr(&A); return SPEIGS_ERR_NOTSYM; }
+    norm_th.join();
+    if (anorm <= 0) anorm = 1.0;
     if (ncomp > 1) {
         spx::free_csr(&A);
         rc = blocks_path(n, Ap, Ai, Ax, k, which, opts, ext, comp, ncomp, lambda, V, resid, info,

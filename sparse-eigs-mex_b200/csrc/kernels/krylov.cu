@@ -610,8 +610,17 @@ jacobi_kernel(int m, const double *__restrict__ H, int ldh, double *theta, doubl
         A[t] = a;
         V[t] = (i == j) ? 1.0 : 0.0;
     }
-    for (int t = threadIdx.x; t < me; t += blockDim.x) pos[t] = t;
     __syncthreads();
+    // round-robin pairing: index 0 stays, the others shift by one per round,
+    // so in round r position t >= 1 holds 1 + ((t - 1 - r) mod (me - 1))
+    auto slot = [&](int t, int r) {
+        return t == 0 ? 0 : 1 + ((t - 1 - r) % (me - 1) + (me - 1)) % (me - 1);
+    };
+    auto pair_of = [&](int pi, int r, int &p, int &q) {
+        p = slot(pi, r);
+        q = slot(me - 1 - pi, r);
+        if (p > q) { int t = p; p = q; q = t; }
+    };
     int sweep = 0;
     const int max_sweeps = 60;
     for (; sweep < max_sweeps; sweep++) {
@@ -620,8 +629,8 @@ jacobi_kernel(int m, const double *__restrict__ H, int ldh, double *theta, doubl
         for (int round = 0; round < me - 1; round++) {
             // 1. rotation parameters for every disjoint pair
             for (int pi = threadIdx.x; pi < half; pi += blockDim.x) {
-                int p = pos[pi], q = pos[me - 1 - pi];
-                if (p > q) { int t = p; p = q; q = t; }
+                int p, q;
+                pair_of(pi, round, p, q);
                 double c = 1.0, s = 0.0;
                 if (q < m) {
                     const double apq = A[p + (size_t)q * me];
@@ -640,46 +649,35 @@ jacobi_kernel(int m, const double *__restrict__ H, int ldh, double *theta, doubl
                 cs[pi] = c; sn[pi] = s;
             }
             __syncthreads();
-            // 2. A <- A J and V <- V J (column pairs)
+            // 2. A <- J^T A J as 2 x 2 blocks (row pair P, column pair Q; the
+            // blocks are disjoint, and each is rotated by columns first, then
+            // by rows), and V <- V J
+            for (int t = threadIdx.x; t < half * half; t += blockDim.x) {
+                const int P = t % half, Q = t / half;
+                const double c1 = cs[P], s1 = sn[P], c2 = cs[Q], s2 = sn[Q];
+                if (s1 == 0.0 && s2 == 0.0) continue;
+                int p1, q1, p2, q2;
+                pair_of(P, round, p1, q1);
+                pair_of(Q, round, p2, q2);
+                double *a11 = A + p1 + (size_t)p2 * me, *a12 = A + p1 + (size_t)q2 * me;
+                double *a21 = A + q1 + (size_t)p2 * me, *a22 = A + q1 + (size_t)q2 * me;
+                const double b11 = c2 * *a11 - s2 * *a12, b12 = s2 * *a11 + c2 * *a12;
+                const double b21 = c2 * *a21 - s2 * *a22, b22 = s2 * *a21 + c2 * *a22;
+                *a11 = c1 * b11 - s1 * b21;
+                *a21 = s1 * b11 + c1 * b21;
+                *a12 = c1 * b12 - s1 * b22;
+                *a22 = s1 * b12 + c1 * b22;
+                if (P == Q && s1 != 0.0) { *a12 = 0.0; *a21 = 0.0; }   // exactly decoupled
+            }
             for (int t = threadIdx.x; t < half * me; t += blockDim.x) {
-                int pi = t / me, k = t % me;
-                double c = cs[pi], s = sn[pi];
+                const int Q = t / me, k = t % me;
+                const double c = cs[Q], s = sn[Q];
                 if (s == 0.0) continue;
-                int p = pos[pi], q = pos[me - 1 - pi];
-                if (p > q) { int u = p; p = q; q = u; }
-                double akp = A[k + (size_t)p * me], akq = A[k + (size_t)q * me];
-                A[k + (size_t)p * me] = c * akp - s * akq;
-                A[k + (size_t)q * me] = s * akp + c * akq;
-                double vkp = V[k + (size_t)p * me], vkq = V[k + (size_t)q * me];
+                int p, q;
+                pair_of(Q, round, p, q);
+                const double vkp = V[k + (size_t)p * me], vkq = V[k + (size_t)q * me];
                 V[k + (size_t)p * me] = c * vkp - s * vkq;
                 V[k + (size_t)q * me] = s * vkp + c * vkq;
-            }
-            __syncthreads();
-            // 3. A <- J^T A (row pairs)
-            for (int t = threadIdx.x; t < half * me; t += blockDim.x) {
-                int pi = t / me, k = t % me;
-                double c = cs[pi], s = sn[pi];
-                if (s == 0.0) continue;
-                int p = pos[pi], q = pos[me - 1 - pi];
-                if (p > q) { int u = p; p = q; q = u; }
-                double apk = A[p + (size_t)k * me], aqk = A[q + (size_t)k * me];
-                A[p + (size_t)k * me] = c * apk - s * aqk;
-                A[q + (size_t)k * me] = s * apk + c * aqk;
-            }
-            __syncthreads();
-            // the rotated pair is exactly decoupled
-            for (int pi = threadIdx.x; pi < half; pi += blockDim.x) {
-                if (sn[pi] == 0.0) continue;
-                int p = pos[pi], q = pos[me - 1 - pi];
-                A[p + (size_t)q * me] = 0.0;
-                A[q + (size_t)p * me] = 0.0;
-            }
-            __syncthreads();
-            // 4. next pairing: rotate positions 1..me-1
-            if (threadIdx.x == 0) {
-                int last = pos[me - 1];
-                for (int t = me - 1; t > 1; t--) pos[t] = pos[t - 1];
-                pos[1] = last;
             }
             __syncthreads();
         }

@@ -275,7 +275,7 @@ constexpr int FLD = 68;
 constexpr int kGThreads = 128;
 constexpr int kFTileDoubles = FT * FLD;
 constexpr int kPanelGroup = 4;   // panel tiles of a small front share one block
-constexpr size_t kPanelSmem = 4 * sizeof(double) * kFTileDoubles;
+constexpr size_t kPanelSmem = 5 * sizeof(double) * kFTileDoubles;
 constexpr size_t kPairSmem = 2 * sizeof(double) * kFTileDoubles;
 
 SPX_DEV void dmma(double &d0, double &d1, double a, double b) {
@@ -293,6 +293,12 @@ SPX_DEV void cp_async8(double *dst, const double *src, bool valid) {
 }
 SPX_DEV void cp_wait() {
     asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+    __syncthreads();
+}
+SPX_DEV void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// wait until at most one committed group (the most recent) is still in flight
+SPX_DEV void cp_wait_all_but_last() {
+    asm volatile("cp.async.wait_group 1;" ::: "memory");
     __syncthreads();
 }
 // one element of a tile: an asynchronous copy for FP64 storage, a load and
@@ -548,7 +554,7 @@ mf_panel64(const int4 *__restrict__ tasks, Sym y, Real *__restrict__ F,
            Real *__restrict__ G, const double *__restrict__ params, int *status) {
     extern __shared__ double fsm[];
     double *Ds = fsm, *Ls = fsm + kFTileDoubles, *Xs = fsm + 2 * kFTileDoubles;
-    double *Ts = fsm + 3 * kFTileDoubles;
+    double *Ts = fsm + 3 * kFTileDoubles, *Ps = fsm + 4 * kFTileDoubles;
     if (*(volatile int *)status) return;
     const int4 tk = tasks[blockIdx.x];
     const int s = tk.x, I0 = tk.y, nI = tk.z, kb = tk.w;
@@ -557,32 +563,51 @@ mf_panel64(const int4 *__restrict__ tasks, Sym y, Real *__restrict__ F,
     tile_range<FT>(f, kb, ka, kz);
     const int w = kz - ka;
     Real *Fs = F + f.fptr;
+    // the row tiles below the diagonal, in order; each one is loaded while
+    // the block works on the one before it (the first during the Cholesky)
+    auto next_tile = [&](int I) {
+        for (int J = I + 1; J < I0 + nI; J++)
+            if (J != kb) return J;
+        return -1;
+    };
+    auto load_tile = [&](double *buf, int I) {
+        int ra, rb;
+        tile_range<FT>(f, I, ra, rb);
+        ftile_load(buf, Fs, f.r, ra, rb - ra, ka, w);
+    };
     ftile_load_lower(Ds, Fs, f.r, ka, w);
-    cp_wait();
+    cp_commit();
+    int In = next_tile(I0 - 1);
+    if (In >= 0) load_tile(Ps, In);
+    cp_commit();
+    cp_wait_all_but_last();          // the diagonal tile is in
     chol_inv_rec<64>(Ds, Ls, Xs, Ts, w, params[1], status, f.first + ka, I0 == kb);
-    for (int I = I0; I < I0 + nI; I++) {
-        if (I == kb) {
-            // only inv(L_kk) is kept: nothing later reads a diagonal tile of
-            // L, and the diagonal tile of F must stay as it is while the
-            // other blocks of this step are still reading it
-            Real *Gs = G + f.gptr;
-            for (int t = threadIdx.x; t < FT * FT; t += blockDim.x) {
-                const int i = t & (FT - 1), j = t >> 6;
-                if (i < w && j <= i)
-                    Gs[(int64_t)(ka + i) + (int64_t)(ka + j) * f.ldg] = (Real)Xs[j * FLD + i];
-            }
-            continue;
+    if (I0 <= kb && kb < I0 + nI) {
+        // only inv(L_kk) is kept: nothing later reads a diagonal tile of
+        // L, and the diagonal tile of F must stay as it is while the other
+        // blocks of this step are still reading it
+        Real *Gs = G + f.gptr;
+        for (int t = threadIdx.x; t < FT * FT; t += blockDim.x) {
+            const int i = t & (FT - 1), j = t >> 6;
+            if (i < w && j <= i)
+                Gs[(int64_t)(ka + i) + (int64_t)(ka + j) * f.ldg] = (Real)Xs[j * FLD + i];
         }
+    }
+    double *cur = Ps, *spare = Ds;   // Ds is free once the Cholesky is done
+    for (int I = In; I >= 0; I = In) {
+        In = next_tile(I);
+        if (In >= 0) load_tile(spare, In);
+        cp_commit();
+        cp_wait_all_but_last();      // tile I is in
         int ra, rb;
         tile_range<FT>(f, I, ra, rb);
         const int h = rb - ra;
-        ftile_load(Ds, Fs, f.r, ra, h, ka, w);
-        cp_wait();
         Acc acc;
         acc_zero(acc);
-        warp_mma<true>(acc, Ds, Xs, (w + 3) & ~3, h, w);
+        warp_mma<true>(acc, cur, Xs, (w + 3) & ~3, h, w);
         acc_store<false>(acc, Fs, f.r, ra, h, ka, w, 1.0, false);
         __syncthreads();
+        double *t = cur; cur = spare; spare = t;
     }
 }
 
