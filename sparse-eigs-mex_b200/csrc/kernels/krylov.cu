@@ -612,14 +612,13 @@ jacobi_kernel(int m, const double *__restrict__ H, int ldh, double *theta, doubl
     }
     __syncthreads();
     // round-robin pairing: index 0 stays, the others shift by one per round,
-    // so in round r position t >= 1 holds 1 + ((t - 1 - r) mod (me - 1))
+    // so in round r position t >= 1 holds 1 + ((t - 1 - r) mod (me - 1));
+    // phase 1 of a round stores pair pi as (pos[pi], pos[half + pi]), p < q
     auto slot = [&](int t, int r) {
-        return t == 0 ? 0 : 1 + ((t - 1 - r) % (me - 1) + (me - 1)) % (me - 1);
-    };
-    auto pair_of = [&](int pi, int r, int &p, int &q) {
-        p = slot(pi, r);
-        q = slot(me - 1 - pi, r);
-        if (p > q) { int t = p; p = q; q = t; }
+        if (t == 0) return 0;
+        int x = t - 1 - r;             // in (-(me - 1), me - 1)
+        if (x < 0) x += me - 1;
+        return 1 + x;
     };
     int sweep = 0;
     const int max_sweeps = 60;
@@ -629,8 +628,10 @@ jacobi_kernel(int m, const double *__restrict__ H, int ldh, double *theta, doubl
         for (int round = 0; round < me - 1; round++) {
             // 1. rotation parameters for every disjoint pair
             for (int pi = threadIdx.x; pi < half; pi += blockDim.x) {
-                int p, q;
-                pair_of(pi, round, p, q);
+                int p = slot(pi, round), q = slot(me - 1 - pi, round);
+                if (p > q) { int t = p; p = q; q = t; }
+                pos[pi] = p;
+                pos[half + pi] = q;
                 double c = 1.0, s = 0.0;
                 if (q < m) {
                     const double apq = A[p + (size_t)q * me];
@@ -656,9 +657,7 @@ jacobi_kernel(int m, const double *__restrict__ H, int ldh, double *theta, doubl
                 const int P = t % half, Q = t / half;
                 const double c1 = cs[P], s1 = sn[P], c2 = cs[Q], s2 = sn[Q];
                 if (s1 == 0.0 && s2 == 0.0) continue;
-                int p1, q1, p2, q2;
-                pair_of(P, round, p1, q1);
-                pair_of(Q, round, p2, q2);
+                const int p1 = pos[P], q1 = pos[half + P], p2 = pos[Q], q2 = pos[half + Q];
                 double *a11 = A + p1 + (size_t)p2 * me, *a12 = A + p1 + (size_t)q2 * me;
                 double *a21 = A + q1 + (size_t)p2 * me, *a22 = A + q1 + (size_t)q2 * me;
                 const double b11 = c2 * *a11 - s2 * *a12, b12 = s2 * *a11 + c2 * *a12;
@@ -673,8 +672,7 @@ jacobi_kernel(int m, const double *__restrict__ H, int ldh, double *theta, doubl
                 const int Q = t / me, k = t % me;
                 const double c = cs[Q], s = sn[Q];
                 if (s == 0.0) continue;
-                int p, q;
-                pair_of(Q, round, p, q);
+                const int p = pos[Q], q = pos[half + Q];
                 const double vkp = V[k + (size_t)p * me], vkq = V[k + (size_t)q * me];
                 V[k + (size_t)p * me] = c * vkp - s * vkq;
                 V[k + (size_t)q * me] = s * vkp + c * vkq;
