@@ -275,7 +275,8 @@ constexpr int FLD = 68;
 constexpr int kGThreads = 128;
 constexpr int kFTileDoubles = FT * FLD;
 constexpr int kPanelGroup = 4;   // panel tiles of a small front share one block
-constexpr size_t kPanelSmem = 5 * sizeof(double) * kFTileDoubles;
+constexpr size_t kPanelSmem = 4 * sizeof(double) * kFTileDoubles;   // mf_diag64
+constexpr size_t kRowsSmem = 3 * sizeof(double) * kFTileDoubles;    // mf_rows64
 constexpr size_t kPairSmem = 2 * sizeof(double) * kFTileDoubles;
 
 SPX_DEV void dmma(double &d0, double &d1, double a, double b) {
@@ -543,18 +544,45 @@ SPX_DEV void chol_inv_rec(double *D, double *L, double *X, double *tmp, int w, d
     }
 }
 
-// Panel step kb of a front: Cholesky and inverse of the (updated) diagonal
-// tile kb, then the block's own tiles I0 .. I0+nI-1 of column block kb: the
-// diagonal (inv(L_kk) into G) or a tile below it, L_Ik = F_Ik inv(L_kk)^T.
-// The diagonal factorization is redone by every block of the step, so the
-// tiles of a large front proceed in parallel; a small front's tiles share
-// one block.  task = (s, I0, nI, kb).
+// Panel step kb of a front, in two kernels that run on separate streams of
+// the factor graph.  mf_diag64 (one block per front, task = (s, kb, 0, 0)):
+// Cholesky and inverse of the updated diagonal tile kb; inv(L_kk) goes to G
+// (only inv(L_kk) is kept: nothing later reads a diagonal tile of L).  It
+// needs only the update of that one tile by step kb-1, so it runs beside the
+// rest of that step's trailing update.
 __global__ void __launch_bounds__(kGThreads)
-mf_panel64(const int4 *__restrict__ tasks, Sym y, Real *__restrict__ F,
-           Real *__restrict__ G, const double *__restrict__ params, int *status) {
+mf_diag64(const int4 *__restrict__ tasks, Sym y, Real *__restrict__ F, Real *__restrict__ G,
+          const double *__restrict__ params, int *status) {
     extern __shared__ double fsm[];
     double *Ds = fsm, *Ls = fsm + kFTileDoubles, *Xs = fsm + 2 * kFTileDoubles;
-    double *Ts = fsm + 3 * kFTileDoubles, *Ps = fsm + 4 * kFTileDoubles;
+    double *Ts = fsm + 3 * kFTileDoubles;
+    if (*(volatile int *)status) return;
+    const int4 tk = tasks[blockIdx.x];
+    const int s = tk.x, kb = tk.y;
+    const Front f = front_of<FT>(y, s);
+    int ka, kz;
+    tile_range<FT>(f, kb, ka, kz);
+    const int w = kz - ka;
+    ftile_load_lower(Ds, F + f.fptr, f.r, ka, w);
+    cp_wait();
+    chol_inv_rec<64>(Ds, Ls, Xs, Ts, w, params[1], status, f.first + ka, true);
+    Real *Gs = G + f.gptr;
+    for (int t = threadIdx.x; t < FT * FT; t += blockDim.x) {
+        const int i = t & (FT - 1), j = t >> 6;
+        if (i < w && j <= i)
+            Gs[(int64_t)(ka + i) + (int64_t)(ka + j) * f.ldg] = (Real)Xs[j * FLD + i];
+    }
+}
+
+// mf_rows64 (task = (s, I0, nI, kb)): the tiles I0 .. I0+nI-1 below the
+// diagonal of column block kb, L_Ik = F_Ik inv(L_kk)^T, with inv(L_kk) read
+// back from G.  A large front's tiles get a block each, a small front's
+// share one; each tile is loaded while the block works on the one before.
+__global__ void __launch_bounds__(kGThreads)
+mf_rows64(const int4 *__restrict__ tasks, Sym y, Real *__restrict__ F,
+          const Real *__restrict__ G, int *status) {
+    extern __shared__ double fsm[];
+    double *Xs = fsm, *Ps = fsm + kFTileDoubles, *Ds = fsm + 2 * kFTileDoubles;
     if (*(volatile int *)status) return;
     const int4 tk = tasks[blockIdx.x];
     const int s = tk.x, I0 = tk.y, nI = tk.z, kb = tk.w;
@@ -563,42 +591,19 @@ mf_panel64(const int4 *__restrict__ tasks, Sym y, Real *__restrict__ F,
     tile_range<FT>(f, kb, ka, kz);
     const int w = kz - ka;
     Real *Fs = F + f.fptr;
-    // the row tiles below the diagonal, in order; each one is loaded while
-    // the block works on the one before it (the first during the Cholesky)
-    auto next_tile = [&](int I) {
-        for (int J = I + 1; J < I0 + nI; J++)
-            if (J != kb) return J;
-        return -1;
-    };
     auto load_tile = [&](double *buf, int I) {
         int ra, rb;
         tile_range<FT>(f, I, ra, rb);
         ftile_load(buf, Fs, f.r, ra, rb - ra, ka, w);
     };
-    ftile_load_lower(Ds, Fs, f.r, ka, w);
+    ftile_load_lower(Xs, G + f.gptr, f.ldg, ka, w);
+    load_tile(Ps, I0);
     cp_commit();
-    int In = next_tile(I0 - 1);
-    if (In >= 0) load_tile(Ps, In);
-    cp_commit();
-    cp_wait_all_but_last();          // the diagonal tile is in
-    chol_inv_rec<64>(Ds, Ls, Xs, Ts, w, params[1], status, f.first + ka, I0 == kb);
-    if (I0 <= kb && kb < I0 + nI) {
-        // only inv(L_kk) is kept: nothing later reads a diagonal tile of
-        // L, and the diagonal tile of F must stay as it is while the other
-        // blocks of this step are still reading it
-        Real *Gs = G + f.gptr;
-        for (int t = threadIdx.x; t < FT * FT; t += blockDim.x) {
-            const int i = t & (FT - 1), j = t >> 6;
-            if (i < w && j <= i)
-                Gs[(int64_t)(ka + i) + (int64_t)(ka + j) * f.ldg] = (Real)Xs[j * FLD + i];
-        }
-    }
-    double *cur = Ps, *spare = Ds;   // Ds is free once the Cholesky is done
-    for (int I = In; I >= 0; I = In) {
-        In = next_tile(I);
-        if (In >= 0) load_tile(spare, In);
+    double *cur = Ps, *spare = Ds;
+    for (int I = I0; I < I0 + nI; I++) {
+        if (I + 1 < I0 + nI) load_tile(spare, I + 1);
         cp_commit();
-        cp_wait_all_but_last();      // tile I is in
+        cp_wait_all_but_last();      // inv(L_kk) and tile I are in
         int ra, rb;
         tile_range<FT>(f, I, ra, rb);
         const int h = rb - ra;
@@ -1507,6 +1512,9 @@ template <> MultifrontalPlanT<Real>::~MultifrontalPlanT() { release(0); }
 template <> void MultifrontalPlanT<Real>::release(cudaStream_t st) {
     if (fgraph_) { cudaGraphExecDestroy(fgraph_); fgraph_ = nullptr; }
     fgraph_val_ = nullptr;
+    for (auto &e : fev_)
+        if (e) { cudaEventDestroy(e); e = nullptr; }
+    if (fside_) { cudaStreamDestroy(fside_); fside_ = nullptr; }
     if (d_params_) { cudaFreeAsync(d_params_, st); d_params_ = nullptr; }
     void *ptrs[] = {d_cbnd_, d_cbnd_ptr_, d_perm_, d_sfirst_, d_rows_, d_relmap_, d_child_ptr_, d_child_list_,
                     d_rowptr_, d_frontptr_, d_gptr_, d_uptr_, d_acolptr_, d_atpos_, d_asrc_,
@@ -1698,6 +1706,15 @@ template <> int MultifrontalPlanT<Real>::init(const spx_symbolic &S, const int64
                 geo(s, r, c, nkb, nt);
                 nkbmax = std::max(nkbmax, nkb);
             }
+            // step kb: the diagonal tile (mf_diag64), the tiles below it
+            // (mf_rows64), the update of column block kb+1 (the next
+            // diagonal tile depends only on it), then the rest of the
+            // trailing update, which runs beside the next diagonal step.
+            // These four launches are recorded even when empty: they carry
+            // the cross-stream ordering of the factor graph.
+            auto emit_always = [&](int kind, size_t before) {
+                launches_.push_back({kind, (int64_t)before, (int64_t)(tasks.size() - before)});
+            };
             for (int kb = 0; kb < nkbmax; kb++) {
                 size_t b0 = tasks.size();
                 for (int32_t q = q0; q < q1; q++) {
@@ -1705,24 +1722,43 @@ template <> int MultifrontalPlanT<Real>::init(const spx_symbolic &S, const int64
                     if (is_tiny(s)) continue;
                     int r, c, nkb, nt;
                     geo(s, r, c, nkb, nt);
-                    if (nkb <= kb) continue;
-                    // a front with few tiles left: one block; else one per tile
-                    if (nt - kb <= kPanelGroup) tasks.push_back(make_int4(s, kb, nt - kb, kb));
-                    else
-                        for (int I = kb; I < nt; I++) tasks.push_back(make_int4(s, I, 1, kb));
+                    if (nkb > kb) tasks.push_back(make_int4(s, kb, 0, 0));
                 }
-                emit(MF_PANEL, b0);
-                size_t b2 = tasks.size();
+                emit_always(MF_DIAG, b0);
+                b0 = tasks.size();
+                for (int32_t q = q0; q < q1; q++) {
+                    const int s = S.level_sup[q];
+                    if (is_tiny(s)) continue;
+                    int r, c, nkb, nt;
+                    geo(s, r, c, nkb, nt);
+                    if (nkb <= kb || nt - kb <= 1) continue;
+                    // a front with few tiles left: one block; else one per tile
+                    if (nt - kb - 1 <= kPanelGroup) tasks.push_back(make_int4(s, kb + 1, nt - kb - 1, kb));
+                    else
+                        for (int I = kb + 1; I < nt; I++) tasks.push_back(make_int4(s, I, 1, kb));
+                }
+                emit_always(MF_ROWS, b0);
+                b0 = tasks.size();
                 for (int32_t q = q0; q < q1; q++) {
                     const int s = S.level_sup[q];
                     if (is_tiny(s)) continue;
                     int r, c, nkb, nt;
                     geo(s, r, c, nkb, nt);
                     if (nkb <= kb) continue;
-                    for (int I = kb + 1; I < nt; I++)
-                        for (int J = kb + 1; J <= I; J++) tasks.push_back(make_int4(s, I, J, kb));
+                    for (int I = kb + 1; I < nt; I++) tasks.push_back(make_int4(s, I, kb + 1, kb));
                 }
-                emit(MF_UPDATE, b2);
+                emit_always(MF_UPD_NEXT, b0);
+                b0 = tasks.size();
+                for (int32_t q = q0; q < q1; q++) {
+                    const int s = S.level_sup[q];
+                    if (is_tiny(s)) continue;
+                    int r, c, nkb, nt;
+                    geo(s, r, c, nkb, nt);
+                    if (nkb <= kb) continue;
+                    for (int I = kb + 2; I < nt; I++)
+                        for (int J = kb + 2; J <= I; J++) tasks.push_back(make_int4(s, I, J, kb));
+                }
+                emit(MF_UPDATE, b0);
             }
             for (int l = 0; (1 << l) < nkbmax; l++) {
                 const int half = 1 << l;
@@ -1921,7 +1957,8 @@ template <> int MultifrontalPlanT<Real>::init(const spx_symbolic &S, const int64
         if (cudaStreamSynchronize(st) != cudaSuccess) return SPEIGS_ERR_INTERNAL;
         // persistent grid for the task-queue solve
         // factor tile kernels stage two or three 64 x 64 tiles
-        cudaFuncSetAttribute(mf_panel64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelSmem);
+        cudaFuncSetAttribute(mf_diag64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelSmem);
+        cudaFuncSetAttribute(mf_rows64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRowsSmem);
         cudaFuncSetAttribute(mf_update64, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(3 * sizeof(double) * kFTileDoubles));
         cudaFuncSetAttribute(mf_inv_t64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPairSmem);
@@ -1953,15 +1990,30 @@ template <> void MultifrontalPlanT<Real>::launch_factor(const double *d_val, cud
             case MF_ASSEMBLE:
                 mf_assemble<<<nb, kFThreads, 0, st>>>(tk, y, d_front_, d_acolptr_, d_atpos_,
                                                       d_asrc_, d_val, d_params_, d_status_);
+                cudaEventRecord(fev_[0], st);
                 break;
             case MF_TINY:
                 mf_tiny_front<<<(nb + kTinyWarps - 1) / kTinyWarps, 32 * kTinyWarps, 0, st>>>(
                     tk, (int)nb, y, d_front_, d_G_, d_acolptr_, d_atpos_, d_asrc_, d_val, d_params_,
                     d_status_);
                 break;
-            case MF_PANEL:
-                mf_panel64<<<nb, kGThreads, kPanelSmem, st>>>(tk, y, d_front_, d_G_, d_params_,
-                                                               d_status_);
+            case MF_DIAG:
+                // after the update of this diagonal tile (the last record of
+                // fev_[0] on st), beside the rest of the previous update
+                cudaStreamWaitEvent(fside_, fev_[0], 0);
+                if (nb) mf_diag64<<<nb, kGThreads, kPanelSmem, fside_>>>(tk, y, d_front_, d_G_,
+                                                                          d_params_, d_status_);
+                break;
+            case MF_ROWS:
+                if (nb) mf_rows64<<<nb, kGThreads, kRowsSmem, fside_>>>(tk, y, d_front_, d_G_,
+                                                                         d_status_);
+                cudaEventRecord(fev_[1], fside_);
+                break;
+            case MF_UPD_NEXT:
+                cudaStreamWaitEvent(st, fev_[1], 0);
+                if (nb) mf_update64<<<nb, kGThreads, 3 * sizeof(double) * kFTileDoubles, st>>>(
+                    tk, y, d_front_, d_status_);
+                cudaEventRecord(fev_[0], st);
                 break;
             case MF_UPDATE:
                 mf_update64<<<nb, kGThreads, 3 * sizeof(double) * kFTileDoubles, st>>>(
@@ -1995,6 +2047,19 @@ template <> int MultifrontalPlanT<Real>::factorize(const double *d_val, double s
     cudaMemcpyAsync(d_params_, hp, sizeof hp, cudaMemcpyHostToDevice, st);
     note_h2d(sizeof hp);
     cudaMemsetAsync(d_status_, 0, sizeof(int), st);
+    if (!fside_) {
+        // the factor graph's second branch (diagonal steps) and its joins;
+        // the branch has the highest priority, so its blocks are scheduled
+        // ahead of the waiting blocks of a large trailing update
+        int prio_lo = 0, prio_hi = 0;
+        cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+        if (cudaStreamCreateWithPriority(&fside_, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
+            cudaEventCreateWithFlags(&fev_[0], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&fev_[1], cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            return SPEIGS_ERR_INTERNAL;
+        }
+    }
     if (!fgraph_ || fgraph_val_ != d_val) {
         if (fgraph_) { cudaGraphExecDestroy(fgraph_); fgraph_ = nullptr; }
         cudaGraph_t g = nullptr;
@@ -2005,13 +2070,15 @@ template <> int MultifrontalPlanT<Real>::factorize(const double *d_val, double s
             cudaGetLastError();
             return SPEIGS_ERR_INTERNAL;
         }
-        cudaError_t e = cudaGraphInstantiate(&fgraph_, g, 0);
+        cudaError_t e = cudaGraphInstantiate(&fgraph_, g, cudaGraphInstantiateFlagUseNodePriority);
         cudaGraphDestroy(g);
         if (e != cudaSuccess) { cudaGetLastError(); fgraph_ = nullptr; return SPEIGS_ERR_INTERNAL; }
         fgraph_val_ = d_val;
     }
     if (cudaGraphLaunch(fgraph_, st) != cudaSuccess) { cudaGetLastError(); return SPEIGS_ERR_INTERNAL; }
-    note_launch((long long)launches_.size());
+    long long nk = 0;
+    for (const MfLaunch &L : launches_) nk += L.count > 0;
+    note_launch(nk);
     int h_status = 0;
     cudaMemcpyAsync(&h_status, d_status_, sizeof(int), cudaMemcpyDeviceToHost, st);
     note_d2h(sizeof(int));

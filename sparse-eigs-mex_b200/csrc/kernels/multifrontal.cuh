@@ -25,8 +25,8 @@ namespace spx {
 
 constexpr int kTile = 32;
 
-enum MfTaskKind { MF_ASSEMBLE = 0, MF_PANEL, MF_UPDATE, MF_INV_T, MF_INV_X, MF_WMUL,
-                  MF_TINY, MF_NKIND };
+enum MfTaskKind { MF_ASSEMBLE = 0, MF_DIAG, MF_ROWS, MF_UPD_NEXT, MF_UPDATE, MF_INV_T,
+                  MF_INV_X, MF_WMUL, MF_TINY, MF_NKIND };
 
 struct MfLaunch {
     int     kind;
@@ -109,6 +109,8 @@ private:
     int *d_status_ = nullptr;
     double *d_params_ = nullptr;     // shift, pivot tolerance (read by the graph)
     cudaGraphExec_t fgraph_ = nullptr;
+    cudaStream_t fside_ = nullptr;             // second branch of the factor graph
+    cudaEvent_t fev_[2] = {nullptr, nullptr};  // [0] column kb+1 updated, [1] step kb's panel done
     const double *fgraph_val_ = nullptr;
     int max_rows_ = 0;
 };
