@@ -539,6 +539,9 @@ uint64_t rng_advance(uint64_t seed, uint64_t steps) {
 
 constexpr int kRngChunk = 64;
 
+// memory pool of the device (engine.cu): allocations are cached across calls
+cudaMemPool_t device_pool(int dev);
+
 __global__ void rand_vec_kernel(int n, uint64_t seed, const uint64_t *__restrict__ jt,
                                 double *v) {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
@@ -565,8 +568,16 @@ void launch_rand_vec(int n, uint64_t seed, double *v, cudaStream_t st) {
     // the jump table travels with the launch as a small device copy that is
     // owned by this call (no global device state)
     const JumpTable &T = jump_table();
+    // (from the library's pool, which keeps its memory: CUDA's default pool
+    // returns freed memory to the driver at every synchronisation, and
+    // mapping it again on the next call can take milliseconds)
     uint64_t *dj = nullptr;
-    if (cudaMallocAsync(&dj, sizeof(T.col), st) != cudaSuccess) return;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaMemPool_t pool = device_pool(dev);
+    cudaError_t ea = pool ? cudaMallocFromPoolAsync((void **)&dj, sizeof(T.col), pool, st)
+                          : cudaMallocAsync((void **)&dj, sizeof(T.col), st);
+    if (ea != cudaSuccess) { cudaGetLastError(); return; }
     cudaMemcpyAsync(dj, T.col, sizeof(T.col), cudaMemcpyHostToDevice, st);
     note_h2d(sizeof(T.col));
     int threads = (n + kRngChunk - 1) / kRngChunk;
