@@ -1512,6 +1512,7 @@ template <> MultifrontalPlanT<Real>::~MultifrontalPlanT() { release(0); }
 template <> void MultifrontalPlanT<Real>::release(cudaStream_t st) {
     if (fgraph_) { cudaGraphExecDestroy(fgraph_); fgraph_ = nullptr; }
     fgraph_val_ = nullptr;
+    direct_val_ = nullptr;
     for (auto &e : fev_)
         if (e) { cudaEventDestroy(e); e = nullptr; }
     if (fside_) { cudaStreamDestroy(fside_); fside_ = nullptr; }
@@ -1663,6 +1664,7 @@ template <> int MultifrontalPlanT<Real>::init(const spx_symbolic &S, const int64
         // tile task lists, level by level
         std::vector<int4> tasks;
         launches_.clear();
+        use_side_ = false;
         auto emit = [&](int kind, size_t before) {
             if (tasks.size() > before)
                 launches_.push_back({kind, (int64_t)before, (int64_t)(tasks.size() - before)});
@@ -1715,6 +1717,7 @@ template <> int MultifrontalPlanT<Real>::init(const spx_symbolic &S, const int64
             auto emit_always = [&](int kind, size_t before) {
                 launches_.push_back({kind, (int64_t)before, (int64_t)(tasks.size() - before)});
             };
+            if (nkbmax >= 2) use_side_ = true;
             for (int kb = 0; kb < nkbmax; kb++) {
                 size_t b0 = tasks.size();
                 for (int32_t q = q0; q < q1; q++) {
@@ -1983,6 +1986,10 @@ template <> int MultifrontalPlanT<Real>::init(const spx_symbolic &S, const int64
 template <> void MultifrontalPlanT<Real>::launch_factor(const double *d_val, cudaStream_t st) {
     Sym y{d_sfirst_, d_rows_, d_relmap_, d_child_ptr_, d_child_list_, d_rowptr_, d_frontptr_,
           d_gptr_, d_cbnd_, d_cbnd_ptr_};
+    // with no front of two or more column blocks there is nothing to overlap:
+    // every launch goes on st, in order
+    const bool side = use_side_ && fside_;
+    cudaStream_t sd = side ? fside_ : st;
     for (const MfLaunch &L : launches_) {
         const int4 *tk = d_tasks_ + L.off;
         const unsigned nb = (unsigned)L.count;
@@ -1990,7 +1997,7 @@ template <> void MultifrontalPlanT<Real>::launch_factor(const double *d_val, cud
             case MF_ASSEMBLE:
                 mf_assemble<<<nb, kFThreads, 0, st>>>(tk, y, d_front_, d_acolptr_, d_atpos_,
                                                       d_asrc_, d_val, d_params_, d_status_);
-                cudaEventRecord(fev_[0], st);
+                if (side) cudaEventRecord(fev_[0], st);
                 break;
             case MF_TINY:
                 mf_tiny_front<<<(nb + kTinyWarps - 1) / kTinyWarps, 32 * kTinyWarps, 0, st>>>(
@@ -2000,20 +2007,20 @@ template <> void MultifrontalPlanT<Real>::launch_factor(const double *d_val, cud
             case MF_DIAG:
                 // after the update of this diagonal tile (the last record of
                 // fev_[0] on st), beside the rest of the previous update
-                cudaStreamWaitEvent(fside_, fev_[0], 0);
-                if (nb) mf_diag64<<<nb, kGThreads, kPanelSmem, fside_>>>(tk, y, d_front_, d_G_,
-                                                                          d_params_, d_status_);
+                if (side) cudaStreamWaitEvent(sd, fev_[0], 0);
+                if (nb) mf_diag64<<<nb, kGThreads, kPanelSmem, sd>>>(tk, y, d_front_, d_G_,
+                                                                      d_params_, d_status_);
                 break;
             case MF_ROWS:
-                if (nb) mf_rows64<<<nb, kGThreads, kRowsSmem, fside_>>>(tk, y, d_front_, d_G_,
-                                                                         d_status_);
-                cudaEventRecord(fev_[1], fside_);
+                if (nb) mf_rows64<<<nb, kGThreads, kRowsSmem, sd>>>(tk, y, d_front_, d_G_,
+                                                                     d_status_);
+                if (side) cudaEventRecord(fev_[1], sd);
                 break;
             case MF_UPD_NEXT:
-                cudaStreamWaitEvent(st, fev_[1], 0);
+                if (side) cudaStreamWaitEvent(st, fev_[1], 0);
                 if (nb) mf_update64<<<nb, kGThreads, 3 * sizeof(double) * kFTileDoubles, st>>>(
                     tk, y, d_front_, d_status_);
-                cudaEventRecord(fev_[0], st);
+                if (side) cudaEventRecord(fev_[0], st);
                 break;
             case MF_UPDATE:
                 mf_update64<<<nb, kGThreads, 3 * sizeof(double) * kFTileDoubles, st>>>(
@@ -2047,7 +2054,7 @@ template <> int MultifrontalPlanT<Real>::factorize(const double *d_val, double s
     cudaMemcpyAsync(d_params_, hp, sizeof hp, cudaMemcpyHostToDevice, st);
     note_h2d(sizeof hp);
     cudaMemsetAsync(d_status_, 0, sizeof(int), st);
-    if (!fside_) {
+    if (use_side_ && !fside_) {
         // the factor graph's second branch (diagonal steps) and its joins;
         // the branch has the highest priority, so its blocks are scheduled
         // ahead of the waiting blocks of a large trailing update
@@ -2060,8 +2067,17 @@ template <> int MultifrontalPlanT<Real>::factorize(const double *d_val, double s
             return SPEIGS_ERR_INTERNAL;
         }
     }
+    bool direct = false;
     if (!fgraph_ || fgraph_val_ != d_val) {
         if (fgraph_) { cudaGraphExecDestroy(fgraph_); fgraph_ = nullptr; }
+    }
+    if (!fgraph_ && direct_val_ != d_val) {
+        // the first factorization from these values is launched directly: a
+        // graph pays for its capture only when the plan factors again
+        launch_factor(d_val, st);
+        direct_val_ = d_val;
+        direct = true;
+    } else if (!fgraph_) {
         cudaGraph_t g = nullptr;
         if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
             return SPEIGS_ERR_INTERNAL;
@@ -2075,7 +2091,10 @@ template <> int MultifrontalPlanT<Real>::factorize(const double *d_val, double s
         if (e != cudaSuccess) { cudaGetLastError(); fgraph_ = nullptr; return SPEIGS_ERR_INTERNAL; }
         fgraph_val_ = d_val;
     }
-    if (cudaGraphLaunch(fgraph_, st) != cudaSuccess) { cudaGetLastError(); return SPEIGS_ERR_INTERNAL; }
+    if (!direct && cudaGraphLaunch(fgraph_, st) != cudaSuccess) {
+        cudaGetLastError();
+        return SPEIGS_ERR_INTERNAL;
+    }
     long long nk = 0;
     for (const MfLaunch &L : launches_) nk += L.count > 0;
     note_launch(nk);

@@ -109,9 +109,11 @@ private:
     int *d_status_ = nullptr;
     double *d_params_ = nullptr;     // shift, pivot tolerance (read by the graph)
     cudaGraphExec_t fgraph_ = nullptr;
+    bool use_side_ = false;                    // some front has >= 2 column blocks
     cudaStream_t fside_ = nullptr;             // second branch of the factor graph
     cudaEvent_t fev_[2] = {nullptr, nullptr};  // [0] column kb+1 updated, [1] step kb's panel done
     const double *fgraph_val_ = nullptr;
+    const double *direct_val_ = nullptr;       // values last factored by direct launches
     int max_rows_ = 0;
 };
 
