@@ -72,31 +72,33 @@ void leaf_mindeg(const Graph &g, const std::vector<int32_t> &verts,
 // already final.
 struct NDState {
     const Graph &g;
-    std::vector<int32_t> part;   // region id of every vertex
-    std::vector<int32_t> level;  // BFS level scratch
+    // region id and BFS level scratch of every vertex, side by side: a BFS
+    // step reads both for each neighbour
+    struct PartLevel { int32_t part, level; };
+    std::vector<PartLevel> pl;
     std::vector<int32_t> local;  // leaf-local index scratch
     std::atomic<int32_t> next_id{1};
     std::atomic<int> spare_threads{0};
     int32_t *perm;
     explicit NDState(const Graph &gg, int32_t *p)
-        : g(gg), part(gg.n, 0), level(gg.n, -1), local(gg.n, -1), perm(p) {}
+        : g(gg), pl(gg.n, PartLevel{0, -1}), local(gg.n, -1), perm(p) {}
 
-    // BFS inside region `id` from `src`; fills queue[0..cnt), level[]; returns
+    // BFS inside region `id` from `src`; fills queue[0..cnt), pl[].level; returns
     // the number reached and the eccentricity in *depth.  `queue` holds at
     // least as many entries as the region has vertices.
     int32_t bfs(int32_t id, int32_t src, int32_t *depth, std::vector<int32_t> &queue) {
         int32_t head = 0, tail = 0;
         queue[tail++] = src;
-        level[src] = 0;
+        pl[src].level = 0;
         int32_t d = 0;
         while (head < tail) {
             int32_t v = queue[head++];
-            int32_t lv = level[v];
+            int32_t lv = pl[v].level;
             if (lv > d) d = lv;
             for (int64_t p = g.rp[v]; p < g.rp[v + 1]; p++) {
                 int32_t u = g.ci[p];
-                if (part[u] == id && level[u] < 0) {
-                    level[u] = lv + 1;
+                if (pl[u].part == id && pl[u].level < 0) {
+                    pl[u].level = lv + 1;
                     queue[tail++] = u;
                 }
             }
@@ -105,12 +107,12 @@ struct NDState {
         return tail;
     }
     void clear_levels(const std::vector<int32_t> &queue, int32_t cnt) {
-        for (int32_t i = 0; i < cnt; i++) level[queue[i]] = -1;
+        for (int32_t i = 0; i < cnt; i++) pl[queue[i]].level = -1;
     }
     int32_t degree_in(int32_t v, int32_t id) const {
         int32_t d = 0;
         for (int64_t p = g.rp[v]; p < g.rp[v + 1]; p++)
-            if (part[g.ci[p]] == id) d++;
+            if (pl[g.ci[p]].part == id) d++;
         return d;
     }
 
@@ -129,7 +131,7 @@ struct NDState {
         // pseudo-peripheral start: the hint, else the lowest degree vertex;
         // then repeated BFS from the deepest level
         int32_t src = hint;
-        if (src < 0 || part[src] != id) {
+        if (src < 0 || pl[src].part != id) {
             src = verts[0];
             int32_t bestdeg = degree_in(verts[0], id);
             for (int32_t v : verts) {
@@ -145,14 +147,14 @@ struct NDState {
             pieces.emplace_back(queue.begin(), queue.begin() + cnt);
             clear_levels(queue, cnt);
             ids.push_back(next_id++);
-            for (int32_t v : pieces[0]) part[v] = ids[0];
+            for (int32_t v : pieces[0]) pl[v].part = ids[0];
             for (int32_t v : verts) {
-                if (part[v] != id) continue;
+                if (pl[v].part != id) continue;
                 int32_t d2 = 0, c2 = bfs(id, v, &d2, queue);
                 pieces.emplace_back(queue.begin(), queue.begin() + c2);
                 clear_levels(queue, c2);
                 ids.push_back(next_id++);
-                for (int32_t u : pieces.back()) part[u] = ids.back();
+                for (int32_t u : pieces.back()) pl[u].part = ids.back();
             }
             verts.clear();
             verts.shrink_to_fit();
@@ -167,7 +169,7 @@ struct NDState {
         for (int it = 0; it < 6; it++) {
             // candidate: min-degree vertex in the last level
             int32_t cand = -1, cd = 1 << 30;
-            for (int32_t i = cnt - 1; i >= 0 && level[queue[i]] == depth; i--) {
+            for (int32_t i = cnt - 1; i >= 0 && pl[queue[i]].level == depth; i--) {
                 int32_t d = degree_in(queue[i], id);
                 if (d < cd) { cd = d; cand = queue[i]; }
             }
@@ -196,7 +198,7 @@ struct NDState {
         }
         // level sizes
         std::vector<int32_t> lsz(depth + 1, 0);
-        for (int32_t i = 0; i < cnt; i++) lsz[level[queue[i]]]++;
+        for (int32_t i = 0; i < cnt; i++) lsz[pl[queue[i]].level]++;
         std::vector<int64_t> cum(depth + 2, 0);
         for (int32_t l = 0; l <= depth; l++) cum[l + 1] = cum[l] + lsz[l];
         // choose separator level: smallest level subject to balance
@@ -221,28 +223,28 @@ struct NDState {
         const int32_t hint_a = src, hint_b = queue[cnt - 1];
         std::vector<int32_t> A, B, Sp;
         for (int32_t i = 0; i < cnt; i++) {
-            int32_t v = queue[i], l = level[v];
-            if (l < best) { part[v] = ida; }
-            else if (l > best) { part[v] = idb; }
-            else { part[v] = ids; }
+            int32_t v = queue[i], l = pl[v].level;
+            if (l < best) { pl[v].part = ida; }
+            else if (l > best) { pl[v].part = idb; }
+            else { pl[v].part = ids; }
         }
         clear_levels(queue, cnt);
         // thin the separator: a separator vertex with no neighbour on one side
         // can join the other side.
         for (int32_t v : verts) {
-            if (part[v] != ids) continue;
+            if (pl[v].part != ids) continue;
             bool hasA = false, hasB = false;
             for (int64_t p = g.rp[v]; p < g.rp[v + 1]; p++) {
                 int32_t u = g.ci[p];
-                if (part[u] == ida) hasA = true;
-                else if (part[u] == idb) hasB = true;
+                if (pl[u].part == ida) hasA = true;
+                else if (pl[u].part == idb) hasB = true;
             }
-            if (!hasB) part[v] = ida;
-            else if (!hasA) part[v] = idb;
+            if (!hasB) pl[v].part = ida;
+            else if (!hasA) pl[v].part = idb;
         }
         for (int32_t v : verts) {
-            if (part[v] == ida) A.push_back(v);
-            else if (part[v] == idb) B.push_back(v);
+            if (pl[v].part == ida) A.push_back(v);
+            else if (pl[v].part == idb) B.push_back(v);
             else Sp.push_back(v);
         }
         const int32_t na = (int32_t)A.size(), nb = (int32_t)B.size();
@@ -562,8 +564,20 @@ extern "C" int spx_analyze(int32_t n, const int64_t *rowptr, const int32_t *col,
         // ascending.  Supernodes are in postorder, so a subtree is a
         // contiguous range ending at its root; disjoint subtrees are built
         // on separate threads (each with its own mark array), then the
-        // supernodes above them in order.
-        std::vector<std::vector<int32_t>> rs(ns);
+        // supernodes above them in order.  The lists are written in place
+        // into S->rows at offsets from the row counts the amalgamation
+        // predicts (a merged supernode's rows are its own columns and its
+        // parent's rows, so the prediction is exact); should a list ever
+        // come out at another length, every list is built again into
+        // separate vectors and the offsets follow the lists.
+        std::vector<int64_t> rptr(ns + 1, 0);
+        for (int32_t s = 0; s < nfs; s++)
+            if (!absorbed[s]) rptr[rank[fin_of_fs[s]] + 1] = mrows[s];
+        for (int32_t s = 0; s < ns; s++) rptr[s + 1] += rptr[s];
+        S->rows = xalloc<int32_t>(rptr[ns]);
+        std::vector<std::vector<int32_t>> rs;          // only when a prediction fails
+        bool flat = true;
+        std::atomic<int> mismatch{0};
         auto build_rows = [&](int32_t s, std::vector<int32_t> &mark, std::vector<int32_t> &tmp) {
             int32_t f = S->sfirst[s], l = S->sfirst[s + 1];
             tmp.clear();
@@ -576,17 +590,26 @@ extern "C" int spx_analyze(int32_t n, const int64_t *rowptr, const int32_t *col,
             for (int32_t q = cptr[s]; q < cptr[s + 1]; q++) {
                 int32_t c = clist[q];
                 int32_t cc0 = S->sfirst[c + 1] - S->sfirst[c];
-                const std::vector<int32_t> &rc = rs[c];
-                for (size_t p = (size_t)cc0; p < rc.size(); p++) {
+                const int32_t *rc = flat ? S->rows + rptr[c] : rs[c].data();
+                const size_t nrc = flat ? (size_t)(rptr[c + 1] - rptr[c]) : rs[c].size();
+                for (size_t p = (size_t)cc0; p < nrc; p++) {
                     int32_t i = rc[p];
                     if (i >= l && mark[i] != s) { mark[i] = s; tmp.push_back(i); }
                 }
             }
             std::sort(tmp.begin(), tmp.end());
-            std::vector<int32_t> &out = rs[s];
-            out.reserve((size_t)(l - f) + tmp.size());
-            for (int32_t j = f; j < l; j++) out.push_back(j);
-            out.insert(out.end(), tmp.begin(), tmp.end());
+            const size_t len = (size_t)(l - f) + tmp.size();
+            if (flat) {
+                if ((int64_t)len != rptr[s + 1] - rptr[s]) { mismatch = 1; return; }
+                int32_t *out = S->rows + rptr[s];
+                for (int32_t j = f; j < l; j++) *out++ = j;
+                std::copy(tmp.begin(), tmp.end(), out);
+            } else {
+                std::vector<int32_t> &out = rs[s];
+                out.reserve(len);
+                for (int32_t j = f; j < l; j++) out.push_back(j);
+                out.insert(out.end(), tmp.begin(), tmp.end());
+            }
         };
         {
             // subtree sizes and first descendants (postorder)
@@ -615,34 +638,40 @@ extern "C" int spx_analyze(int32_t n, const int64_t *rowptr, const int32_t *col,
             for (int32_t r : task_root)
                 for (int32_t s = fdesc[r]; s <= r; s++) in_task[s] = 1;
             const unsigned nth = (hw > 1 && ns > 2048) ? hw : 1u;
-            std::atomic<size_t> next{0};
-            auto worker = [&] {
+            auto build_all = [&] {
+                std::atomic<size_t> next{0};
+                auto worker = [&] {
+                    std::vector<int32_t> mark(n, -1), tmp;
+                    for (size_t t; (t = next.fetch_add(1)) < task_root.size();) {
+                        const int32_t r = task_root[t];
+                        for (int32_t s = fdesc[r]; s <= r; s++) build_rows(s, mark, tmp);
+                    }
+                };
+                std::vector<std::thread> th;
+                for (unsigned i = 1; i < nth; i++) th.emplace_back(worker);
+                worker();
+                for (auto &t : th) t.join();
                 std::vector<int32_t> mark(n, -1), tmp;
-                for (size_t t; (t = next.fetch_add(1)) < task_root.size();) {
-                    const int32_t r = task_root[t];
-                    for (int32_t s = fdesc[r]; s <= r; s++) build_rows(s, mark, tmp);
-                }
+                for (int32_t s = 0; s < ns && !(flat && mismatch); s++)
+                    if (!in_task[s]) build_rows(s, mark, tmp);
             };
-            std::vector<std::thread> th;
-            for (unsigned i = 1; i < nth; i++) th.emplace_back(worker);
-            worker();
-            for (auto &t : th) t.join();
-            std::vector<int32_t> mark(n, -1), tmp;
-            for (int32_t s = 0; s < ns; s++)
-                if (!in_task[s]) build_rows(s, mark, tmp);
+            build_all();
+            if (mismatch) {
+                flat = false;
+                rs.assign(ns, {});
+                build_all();
+                for (int32_t s = 0; s < ns; s++) rptr[s + 1] = rptr[s] + (int64_t)rs[s].size();
+                free(S->rows);
+                S->rows = nullptr;
+                S->rows = xalloc<int32_t>(rptr[ns]);
+                for (int32_t s = 0; s < ns; s++)
+                    std::copy(rs[s].begin(), rs[s].end(), S->rows + rptr[s]);
+                std::vector<std::vector<int32_t>>().swap(rs);
+            }
         }
-        std::vector<int64_t> rptr(ns + 1, 0);
-        for (int32_t s = 0; s < ns; s++) rptr[s + 1] = rptr[s] + (int64_t)rs[s].size();
         const int64_t nrows_total = rptr[ns];
         S->rowptr = xalloc<int64_t>(ns + 1);
         memcpy(S->rowptr, rptr.data(), (ns + 1) * sizeof(int64_t));
-        S->rows = xalloc<int32_t>(nrows_total);
-        spx::parallel_ranges(ns, kGrain, [&](int64_t lo, int64_t hi) {
-            for (int64_t s = lo; s < hi; s++) {
-                std::copy(rs[s].begin(), rs[s].end(), S->rows + rptr[s]);
-                std::vector<int32_t>().swap(rs[s]);
-            }
-        });
         const int32_t *rows = S->rows;
 
         // ---- 9. relative maps into the parent's row list
