@@ -9,6 +9,9 @@
 #include "parallel.h"
 
 #include <algorithm>
+#include <mutex>
+#include <functional>
+#include <map>
 #include <atomic>
 #include <cstdlib>
 #include <cstring>
@@ -79,6 +82,22 @@ struct NDState {
     std::vector<int32_t> local;  // leaf-local index scratch
     std::atomic<int32_t> next_id{1};
     std::atomic<int> spare_threads{0};
+    // Independent ranges of the ordering, for the elimination tree: a
+    // region [lo, lo + m) of at least kRecordMin vertices whose columns
+    // split into child ranges that reach only themselves and later columns
+    // (the halves of a separation, or the connected pieces of a region),
+    // followed by the columns of the separator (none for pieces).
+    struct Split {
+        int32_t lo, m;
+        std::vector<std::pair<int32_t, int32_t>> parts;   // (first, count)
+    };
+    std::mutex split_mu;
+    std::vector<Split> splits;
+    static constexpr int32_t kRecordMin = 8192;
+    void record(Split &&sp) {
+        std::lock_guard<std::mutex> lk(split_mu);
+        splits.push_back(std::move(sp));
+    }
     int32_t *perm;
     explicit NDState(const Graph &gg, int32_t *p)
         : g(gg), pl(gg.n, PartLevel{0, -1}), local(gg.n, -1), perm(p) {}
@@ -158,6 +177,15 @@ struct NDState {
             }
             verts.clear();
             verts.shrink_to_fit();
+            if (m >= kRecordMin) {
+                Split sp{lo, m, {}};
+                int32_t at2 = lo;
+                for (auto &pc : pieces) {
+                    sp.parts.push_back({at2, (int32_t)pc.size()});
+                    at2 += (int32_t)pc.size();
+                }
+                record(std::move(sp));
+            }
             int32_t at = lo;
             for (size_t i = 0; i < pieces.size(); i++) {
                 int32_t sz = (int32_t)pieces[i].size();
@@ -248,6 +276,7 @@ struct NDState {
             else Sp.push_back(v);
         }
         const int32_t na = (int32_t)A.size(), nb = (int32_t)B.size();
+        if (m >= kRecordMin) record(Split{lo, m, {{lo, na}, {lo + na, nb}}});
         // separator last, ordered by minimum degree when small
         if ((int32_t)Sp.size() <= 64) {
             leaf_mindeg(g, Sp, local, perm + lo + na + nb);
@@ -277,9 +306,11 @@ struct NDState {
 
 }  // namespace
 
-extern "C" int spx_order(int32_t n, const int64_t *rowptr, const int32_t *col,
-                         int ordering, int32_t *perm) {
-    (void)ordering;  // nested dissection for every size; leaves by minimum degree
+namespace {
+using Splits = std::vector<NDState::Split>;
+
+int order_nd(int32_t n, const int64_t *rowptr, const int32_t *col, int32_t *perm,
+             Splits *splits) {
     if (n <= 0 || !rowptr || !col || !perm) return -1;
     try {
         Graph g{n, rowptr, col};
@@ -289,10 +320,18 @@ extern "C" int spx_order(int32_t n, const int64_t *rowptr, const int32_t *col,
         std::vector<int32_t> all(n);
         for (int32_t i = 0; i < n; i++) all[i] = i;
         st.order_region(std::move(all), 0, 0);
+        if (splits) splits->swap(st.splits);
     } catch (const std::bad_alloc &) {
         return -2;
     }
     return 0;
+}
+}  // namespace
+
+extern "C" int spx_order(int32_t n, const int64_t *rowptr, const int32_t *col,
+                         int ordering, int32_t *perm) {
+    (void)ordering;  // nested dissection for every size; leaves by minimum degree
+    return order_nd(n, rowptr, col, perm, nullptr);
 }
 
 namespace {
@@ -345,7 +384,9 @@ extern "C" int spx_analyze(int32_t n, const int64_t *rowptr, const int32_t *col,
         S->n = n;
         // ---- 1. ordering
         std::vector<int32_t> perm0(n);
-        int rc = spx_order(n, rowptr, col, ordering, perm0.data());
+        Splits splits;
+        (void)ordering;  // nested dissection for every size; leaves by minimum degree
+        int rc = order_nd(n, rowptr, col, perm0.data(), &splits);
         if (rc) return rc;
         std::vector<int32_t> ip0(n);
         for (int32_t i = 0; i < n; i++) ip0[perm0[i]] = i;
@@ -372,17 +413,46 @@ extern "C" int spx_analyze(int32_t n, const int64_t *rowptr, const int32_t *col,
         });
 
         // ---- 3. elimination tree (Liu, with path compression)
+        // The columns of each part of a recorded split reach, below
+        // themselves, only their own part, and Liu's walks from them stay
+        // inside it; the parts are processed side by side and the
+        // separator's columns after them.  The tree is unique, so the result
+        // does not depend on the schedule.
         std::vector<int32_t> parent(n, -1), anc(n, -1);
-        for (int32_t k = 0; k < n; k++) {
-            for (int64_t p = prp[k]; p < prp[k + 1]; p++) {
-                int32_t i = pci[p];
-                while (i != -1 && i < k) {
-                    int32_t inext = anc[i];
-                    anc[i] = k;
-                    if (inext == -1) parent[i] = k;
-                    i = inext;
+        auto liu = [&](int32_t c0, int32_t c1) {
+            for (int32_t k = c0; k < c1; k++) {
+                for (int64_t p = prp[k]; p < prp[k + 1]; p++) {
+                    int32_t i = pci[p];
+                    while (i != -1 && i < k) {
+                        int32_t inext = anc[i];
+                        anc[i] = k;
+                        if (inext == -1) parent[i] = k;
+                        i = inext;
+                    }
                 }
             }
+        };
+        {
+            std::map<std::pair<int32_t, int32_t>, const NDState::Split *> split_of;
+            for (const auto &sp : splits) split_of[{sp.lo, sp.m}] = &sp;
+            std::function<void(int32_t, int32_t)> tree_range = [&](int32_t lo, int32_t m) {
+                auto it = split_of.find({lo, m});
+                if (it == split_of.end()) { liu(lo, lo + m); return; }
+                const NDState::Split &sp = *it->second;
+                {
+                    spx::TaskGroup g;
+                    for (size_t q = 1; q < sp.parts.size(); q++) {
+                        const auto pr = sp.parts[q];
+                        g.run([&tree_range, pr] { tree_range(pr.first, pr.second); });
+                    }
+                    if (!sp.parts.empty()) tree_range(sp.parts[0].first, sp.parts[0].second);
+                    g.wait();
+                }
+                int32_t end = lo;
+                for (const auto &pr : sp.parts) end = std::max(end, pr.first + pr.second);
+                liu(end, lo + m);
+            };
+            tree_range(0, n);
         }
 
         // ---- 4. postorder, children in increasing order
