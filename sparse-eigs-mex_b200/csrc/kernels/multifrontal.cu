@@ -1661,137 +1661,140 @@ template <> int MultifrontalPlanT<Real>::init(const spx_symbolic &S, const int64
             }
             cbnd_ptr[ns] = (int64_t)cbnd.size();
         });
-        // tile task lists, level by level
+        // tile task lists, level by level (on a side thread: nothing below
+        // reads them before the uploads)
         std::vector<int4> tasks;
-        launches_.clear();
-        use_side_ = false;
-        auto emit = [&](int kind, size_t before) {
-            if (tasks.size() > before)
-                launches_.push_back({kind, (int64_t)before, (int64_t)(tasks.size() - before)});
-        };
-        auto is_tiny = [&](int s) { return S.rowptr[s + 1] - S.rowptr[s] <= T; };
-        for (int l = 0; l < S.nlevels; l++) {
-            const int32_t q0 = S.level_ptr[l], q1 = S.level_ptr[l + 1];
-            int nkbmax = 0;
-            {
-                size_t bt = tasks.size();
-                for (int32_t q = q0; q < q1; q++)
-                    if (is_tiny(S.level_sup[q])) tasks.push_back(make_int4(S.level_sup[q], 0, 0, 0));
-                emit(MF_TINY, bt);
-            }
-            size_t b = tasks.size();
-            for (int32_t q = q0; q < q1; q++) {
-                const int s = S.level_sup[q];
-                if (is_tiny(s)) continue;
-                const int r = (int)(S.rowptr[s + 1] - S.rowptr[s]);
-                const int c = S.sfirst[s + 1] - S.sfirst[s];
-                const int nkb = (c + T - 1) / T, nt = nkb + (r - c + T - 1) / T;
-                nkbmax = std::max(nkbmax, nkb);
-                for (int I = 0; I < nt; I++)
-                    for (int J = 0; J <= I; J++) tasks.push_back(make_int4(s, I, J, 0));
-            }
-            emit(MF_ASSEMBLE, b);
-            // factor steps on 64-tiles: panel kb (diagonal Cholesky + the
-            // tiles below it), then the right-looking update of the trailing
-            // tiles, Schur complement included
-            auto geo = [&](int s, int &r, int &c, int &nkb, int &nt) {
-                r = (int)(S.rowptr[s + 1] - S.rowptr[s]);
-                c = S.sfirst[s + 1] - S.sfirst[s];
-                nkb = (c + FT - 1) / FT;
-                nt = nkb + (r - c + FT - 1) / FT;
+        side.run([&] {
+            launches_.clear();
+            use_side_ = false;
+            auto emit = [&](int kind, size_t before) {
+                if (tasks.size() > before)
+                    launches_.push_back({kind, (int64_t)before, (int64_t)(tasks.size() - before)});
             };
-            nkbmax = 0;
-            for (int32_t q = q0; q < q1; q++) {
-                const int s = S.level_sup[q];
-                if (is_tiny(s)) continue;
-                int r, c, nkb, nt;
-                geo(s, r, c, nkb, nt);
-                nkbmax = std::max(nkbmax, nkb);
-            }
-            // step kb: the diagonal tile (mf_diag64), the tiles below it
-            // (mf_rows64), the update of column block kb+1 (the next
-            // diagonal tile depends only on it), then the rest of the
-            // trailing update, which runs beside the next diagonal step.
-            // These four launches are recorded even when empty: they carry
-            // the cross-stream ordering of the factor graph.
-            auto emit_always = [&](int kind, size_t before) {
-                launches_.push_back({kind, (int64_t)before, (int64_t)(tasks.size() - before)});
-            };
-            if (nkbmax >= 2) use_side_ = true;
-            for (int kb = 0; kb < nkbmax; kb++) {
-                size_t b0 = tasks.size();
+            auto is_tiny = [&](int s) { return S.rowptr[s + 1] - S.rowptr[s] <= T; };
+            for (int l = 0; l < S.nlevels; l++) {
+                const int32_t q0 = S.level_ptr[l], q1 = S.level_ptr[l + 1];
+                int nkbmax = 0;
+                {
+                    size_t bt = tasks.size();
+                    for (int32_t q = q0; q < q1; q++)
+                        if (is_tiny(S.level_sup[q])) tasks.push_back(make_int4(S.level_sup[q], 0, 0, 0));
+                    emit(MF_TINY, bt);
+                }
+                size_t b = tasks.size();
+                for (int32_t q = q0; q < q1; q++) {
+                    const int s = S.level_sup[q];
+                    if (is_tiny(s)) continue;
+                    const int r = (int)(S.rowptr[s + 1] - S.rowptr[s]);
+                    const int c = S.sfirst[s + 1] - S.sfirst[s];
+                    const int nkb = (c + T - 1) / T, nt = nkb + (r - c + T - 1) / T;
+                    nkbmax = std::max(nkbmax, nkb);
+                    for (int I = 0; I < nt; I++)
+                        for (int J = 0; J <= I; J++) tasks.push_back(make_int4(s, I, J, 0));
+                }
+                emit(MF_ASSEMBLE, b);
+                // factor steps on 64-tiles: panel kb (diagonal Cholesky + the
+                // tiles below it), then the right-looking update of the trailing
+                // tiles, Schur complement included
+                auto geo = [&](int s, int &r, int &c, int &nkb, int &nt) {
+                    r = (int)(S.rowptr[s + 1] - S.rowptr[s]);
+                    c = S.sfirst[s + 1] - S.sfirst[s];
+                    nkb = (c + FT - 1) / FT;
+                    nt = nkb + (r - c + FT - 1) / FT;
+                };
+                nkbmax = 0;
                 for (int32_t q = q0; q < q1; q++) {
                     const int s = S.level_sup[q];
                     if (is_tiny(s)) continue;
                     int r, c, nkb, nt;
                     geo(s, r, c, nkb, nt);
-                    if (nkb > kb) tasks.push_back(make_int4(s, kb, 0, 0));
+                    nkbmax = std::max(nkbmax, nkb);
                 }
-                emit_always(MF_DIAG, b0);
-                b0 = tasks.size();
-                for (int32_t q = q0; q < q1; q++) {
-                    const int s = S.level_sup[q];
-                    if (is_tiny(s)) continue;
-                    int r, c, nkb, nt;
-                    geo(s, r, c, nkb, nt);
-                    if (nkb <= kb || nt - kb <= 1) continue;
-                    // a front with few tiles left: one block; else one per tile
-                    if (nt - kb - 1 <= kPanelGroup) tasks.push_back(make_int4(s, kb + 1, nt - kb - 1, kb));
-                    else
-                        for (int I = kb + 1; I < nt; I++) tasks.push_back(make_int4(s, I, 1, kb));
-                }
-                emit_always(MF_ROWS, b0);
-                b0 = tasks.size();
-                for (int32_t q = q0; q < q1; q++) {
-                    const int s = S.level_sup[q];
-                    if (is_tiny(s)) continue;
-                    int r, c, nkb, nt;
-                    geo(s, r, c, nkb, nt);
-                    if (nkb <= kb) continue;
-                    for (int I = kb + 1; I < nt; I++) tasks.push_back(make_int4(s, I, kb + 1, kb));
-                }
-                emit_always(MF_UPD_NEXT, b0);
-                b0 = tasks.size();
-                for (int32_t q = q0; q < q1; q++) {
-                    const int s = S.level_sup[q];
-                    if (is_tiny(s)) continue;
-                    int r, c, nkb, nt;
-                    geo(s, r, c, nkb, nt);
-                    if (nkb <= kb) continue;
-                    for (int I = kb + 2; I < nt; I++)
-                        for (int J = kb + 2; J <= I; J++) tasks.push_back(make_int4(s, I, J, kb));
-                }
-                emit(MF_UPDATE, b0);
-            }
-            for (int l = 0; (1 << l) < nkbmax; l++) {
-                const int half = 1 << l;
-                for (int phase = 0; phase < 2; phase++) {
+                // step kb: the diagonal tile (mf_diag64), the tiles below it
+                // (mf_rows64), the update of column block kb+1 (the next
+                // diagonal tile depends only on it), then the rest of the
+                // trailing update, which runs beside the next diagonal step.
+                // These four launches are recorded even when empty: they carry
+                // the cross-stream ordering of the factor graph.
+                auto emit_always = [&](int kind, size_t before) {
+                    launches_.push_back({kind, (int64_t)before, (int64_t)(tasks.size() - before)});
+                };
+                if (nkbmax >= 2) use_side_ = true;
+                for (int kb = 0; kb < nkbmax; kb++) {
                     size_t b0 = tasks.size();
                     for (int32_t q = q0; q < q1; q++) {
                         const int s = S.level_sup[q];
                         if (is_tiny(s)) continue;
                         int r, c, nkb, nt;
                         geo(s, r, c, nkb, nt);
-                        for (int A0 = 0; A0 + half < nkb; A0 += 2 * half) {
-                            const int C0 = A0 + half, C1 = std::min(A0 + 2 * half, nkb);
-                            for (int i = C0; i < C1; i++)
-                                for (int j = A0; j < C0; j++) tasks.push_back(make_int4(s, i, j, l));
-                        }
+                        if (nkb > kb) tasks.push_back(make_int4(s, kb, 0, 0));
                     }
-                    emit(phase == 0 ? MF_INV_T : MF_INV_X, b0);
+                    emit_always(MF_DIAG, b0);
+                    b0 = tasks.size();
+                    for (int32_t q = q0; q < q1; q++) {
+                        const int s = S.level_sup[q];
+                        if (is_tiny(s)) continue;
+                        int r, c, nkb, nt;
+                        geo(s, r, c, nkb, nt);
+                        if (nkb <= kb || nt - kb <= 1) continue;
+                        // a front with few tiles left: one block; else one per tile
+                        if (nt - kb - 1 <= kPanelGroup) tasks.push_back(make_int4(s, kb + 1, nt - kb - 1, kb));
+                        else
+                            for (int I = kb + 1; I < nt; I++) tasks.push_back(make_int4(s, I, 1, kb));
+                    }
+                    emit_always(MF_ROWS, b0);
+                    b0 = tasks.size();
+                    for (int32_t q = q0; q < q1; q++) {
+                        const int s = S.level_sup[q];
+                        if (is_tiny(s)) continue;
+                        int r, c, nkb, nt;
+                        geo(s, r, c, nkb, nt);
+                        if (nkb <= kb) continue;
+                        for (int I = kb + 1; I < nt; I++) tasks.push_back(make_int4(s, I, kb + 1, kb));
+                    }
+                    emit_always(MF_UPD_NEXT, b0);
+                    b0 = tasks.size();
+                    for (int32_t q = q0; q < q1; q++) {
+                        const int s = S.level_sup[q];
+                        if (is_tiny(s)) continue;
+                        int r, c, nkb, nt;
+                        geo(s, r, c, nkb, nt);
+                        if (nkb <= kb) continue;
+                        for (int I = kb + 2; I < nt; I++)
+                            for (int J = kb + 2; J <= I; J++) tasks.push_back(make_int4(s, I, J, kb));
+                    }
+                    emit(MF_UPDATE, b0);
                 }
+                for (int l = 0; (1 << l) < nkbmax; l++) {
+                    const int half = 1 << l;
+                    for (int phase = 0; phase < 2; phase++) {
+                        size_t b0 = tasks.size();
+                        for (int32_t q = q0; q < q1; q++) {
+                            const int s = S.level_sup[q];
+                            if (is_tiny(s)) continue;
+                            int r, c, nkb, nt;
+                            geo(s, r, c, nkb, nt);
+                            for (int A0 = 0; A0 + half < nkb; A0 += 2 * half) {
+                                const int C0 = A0 + half, C1 = std::min(A0 + 2 * half, nkb);
+                                for (int i = C0; i < C1; i++)
+                                    for (int j = A0; j < C0; j++) tasks.push_back(make_int4(s, i, j, l));
+                            }
+                        }
+                        emit(phase == 0 ? MF_INV_T : MF_INV_X, b0);
+                    }
+                }
+                size_t bw = tasks.size();
+                for (int32_t q = q0; q < q1; q++) {
+                    const int s = S.level_sup[q];
+                    if (is_tiny(s)) continue;
+                    int r, c, nkb, nt;
+                    geo(s, r, c, nkb, nt);
+                    for (int I = nkb; I < nt; I++)
+                        for (int J = 0; J < nkb; J++) tasks.push_back(make_int4(s, I, J, 0));
+                }
+                emit(MF_WMUL, bw);
             }
-            size_t bw = tasks.size();
-            for (int32_t q = q0; q < q1; q++) {
-                const int s = S.level_sup[q];
-                if (is_tiny(s)) continue;
-                int r, c, nkb, nt;
-                geo(s, r, c, nkb, nt);
-                for (int I = nkb; I < nt; I++)
-                    for (int J = 0; J < nkb; J++) tasks.push_back(make_int4(s, I, J, 0));
-            }
-            emit(MF_WMUL, bw);
-        }
+        });
         // solve: per-supernode metadata and the task queue.  Forward tasks
         // level by level from the leaves (tiles of large supernodes first,
         // then bundles of up to 8 small ones), then backward tasks level by
