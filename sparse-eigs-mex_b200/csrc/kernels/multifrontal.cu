@@ -7,9 +7,12 @@
 // the rows below the pivots), every tile product on the FP64 tensor cores:
 //   assemble  F = A(pivot columns) + shift*I + extend-add of the children's
 //             update matrices (pulled per tile, children in a fixed order)
-//   for kb:   panel: Cholesky + inverse of the diagonal tile kb (inv into
-//             G), the tiles below it as L_Ik = F_Ik inv(L_kk)^T;
-//             update of the trailing tiles, update matrix included
+//   for kb:   diag: Cholesky + inverse of the diagonal tile kb (inv into
+//             G); rows: the tiles below it as L_Ik = F_Ik inv(L_kk)^T;
+//             update of column block kb+1, then of the other trailing
+//             tiles, update matrix included.  diag and rows run on a
+//             high-priority second branch of the factor graph, so the
+//             diagonal step kb+1 overlaps the rest of update kb.
 //   invert    the off-diagonal tiles of inv(L11) by recursive doubling
 //   wmul      G's lower part = L21 * inv(L11)
 // A pivot that is not positive records the failing column in a device status
@@ -1693,9 +1696,9 @@ template <> int MultifrontalPlanT<Real>::init(const spx_symbolic &S, const int64
                         for (int J = 0; J <= I; J++) tasks.push_back(make_int4(s, I, J, 0));
                 }
                 emit(MF_ASSEMBLE, b);
-                // factor steps on 64-tiles: panel kb (diagonal Cholesky + the
-                // tiles below it), then the right-looking update of the trailing
-                // tiles, Schur complement included
+                // factor steps on 64-tiles: diagonal tile kb, the tiles below
+                // it, then the right-looking update of the trailing tiles,
+                // Schur complement included
                 auto geo = [&](int s, int &r, int &c, int &nkb, int &nt) {
                     r = (int)(S.rowptr[s + 1] - S.rowptr[s]);
                     c = S.sfirst[s + 1] - S.sfirst[s];
