@@ -482,17 +482,24 @@ extern "C" int spx_analyze(int32_t n, const int64_t *rowptr, const int32_t *col,
             }
         }
         // relabel: final perm = perm0[post[.]]
+        // (permutation scatters and gathers: every index is written once)
         std::vector<int32_t> ipost(n);
-        for (int32_t k = 0; k < n; k++) ipost[post[k]] = k;
         S->perm = xalloc<int32_t>(n);
         S->iperm = xalloc<int32_t>(n);
-        for (int32_t k = 0; k < n; k++) S->perm[k] = perm0[post[k]];
-        for (int32_t k = 0; k < n; k++) S->iperm[S->perm[k]] = k;
+        spx::parallel_ranges(n, kGrain, [&](int64_t lo, int64_t hi) {
+            for (int64_t k = lo; k < hi; k++) {
+                ipost[post[k]] = (int32_t)k;
+                S->perm[k] = perm0[post[k]];
+                S->iperm[perm0[post[k]]] = (int32_t)k;
+            }
+        });
         std::vector<int32_t> par(n);
-        for (int32_t k = 0; k < n; k++) {
-            int32_t p = parent[post[k]];
-            par[k] = (p == -1) ? -1 : ipost[p];
-        }
+        spx::parallel_ranges(n, kGrain, [&](int64_t lo, int64_t hi) {
+            for (int64_t k = lo; k < hi; k++) {
+                const int32_t p = parent[post[k]];
+                par[k] = (p == -1) ? -1 : ipost[p];
+            }
+        });
         // adjacency in final numbering
         {
             std::vector<int64_t> rp2(n + 1, 0);
