@@ -923,20 +923,28 @@ struct Cand2 { double key; int idx; };
 // thread, grown on demand and kept for the thread's life: cudaMallocHost and
 // cudaFreeHost are slow and synchronise the device, so they are not paid per
 // call (which matters when several threads solve components at once).
+// The calling thread's page-locked read-back buffer, released when the
+// thread exits (the batched path solves on short-lived worker threads).
+struct PinnedScalars {
+    double *buf = nullptr;
+    size_t cap = 0;
+    ~PinnedScalars() {
+        if (buf) cudaFreeHost(buf);   // an error at process exit is harmless
+    }
+};
 static double *pinned_scalars(size_t need) {
-    thread_local double *buf = nullptr;
-    thread_local size_t cap = 0;
-    if (cap >= need) return buf;
+    thread_local PinnedScalars ps;
+    if (ps.cap >= need) return ps.buf;
     size_t want = std::max<size_t>(need, 256);
     double *nb = nullptr;
     if (cudaMallocHost(&nb, sizeof(double) * want) != cudaSuccess) {
         cudaGetLastError();
         return nullptr;
     }
-    if (buf) cudaFreeHost(buf);
-    buf = nb;
-    cap = want;
-    return buf;
+    if (ps.buf) cudaFreeHost(ps.buf);
+    ps.buf = nb;
+    ps.cap = want;
+    return ps.buf;
 }
 
 // Factor (if 'sm') and iterate; results sorted by |lambda| into host or
