@@ -73,3 +73,26 @@ def test_nonsymmetric_rejected_before_gpu(lib, pkg):
     A = sp.diags([-4 * np.ones(n - 1), 5 * np.ones(n), -np.ones(n - 1)], [-1, 0, 1], format="csc")
     rc, *_ = pkg.speigs.speigs(A, 3, lib=lib)
     assert rc == pkg.speigs.ERR_NOTSYM
+
+
+def test_extension_argument_errors_need_no_gpu(lib, pkg):
+    """The extension entry points reject bad arguments before any device
+    work: component labels outside [0, ncomp) or a label with no rows, k <= 0,
+    and a non-symmetric matrix for the batched call."""
+    import numpy as np
+    import scipy.sparse as sp
+    s = pkg.speigs
+    A = sp.block_diag([pkg.workloads.lap3d(3), pkg.workloads.lap3d(3)], format="csc")
+    n = A.shape[0]
+    comp = np.repeat([0, 1], n // 2)
+    rc, *_ = s.speigs_batched(A, 0, comp=comp, lib=lib)
+    assert rc == s.ERR_ARG
+    # labels 1 and 2 only: ncomp is 3 and label 0 has no rows
+    rc, *_ = s.speigs_batched(A, 2, comp=np.where(comp == 0, 2, comp), lib=lib)
+    assert rc == s.ERR_ARG
+    B = A.tolil()
+    B[0, 1] = 7.0
+    rc, *_ = s.speigs_batched(B.tocsc(), 2, comp=comp, lib=lib)
+    assert rc == s.ERR_NOTSYM
+    rc, *_ = s.speigs_ex(A, 0, lib=lib)
+    assert rc == s.ERR_ARG
