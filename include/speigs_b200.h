@@ -191,7 +191,13 @@ int speigs_b200_syev_small(int m, const double *H, double *theta, double *S, int
  * The workspace is a 1 MiB array compiled into the library, held by every
  * GPU that loads it until the process exits and shared by all calls: calls
  * that overlap on the GPU race.  The first call on each device looks up the
- * array's device address; make that first call before any stream capture. */
+ * array's device address; make that first call before any stream capture.
+ * That address is kept per device ordinal for the life of the process, so it
+ * belongs to the context that was current at the first call: after
+ * cudaDeviceReset, or with a different driver context made current on that
+ * device, do not call this entry point again.  If a CUDA error from earlier
+ * work is pending on the calling thread, nothing is launched and the call
+ * returns SPEIGS_ERR_INTERNAL, naming that error. */
 int speigs_b200_syev_small_noalloc(int m, const double *H, double *theta, double *S, int *ord,
                                    int *status, void *stream);
 

@@ -44,6 +44,21 @@ const char *set_last_error_text(const char *msg) {
     return g_err;
 }
 
+int current_device() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return dev;
+}
+
+void use_device(int dev) {
+    int cur = -1;
+    if (cudaGetDevice(&cur) == cudaSuccess && cur == dev) return;
+    if (cudaSetDevice(dev) != cudaSuccess) cudaGetLastError();
+}
+
 static int cuda_fail(cudaError_t e, const char *where) {
     snprintf(g_err, sizeof g_err, "%s: %s", where, cudaGetErrorString(e));
     cudaGetLastError();

@@ -61,6 +61,13 @@ int device_diag_path(int64_t n, const double *diag, int64_t k, speigs_which whic
 int device_dense_path(const HostCSR &A, int64_t k, speigs_which which, double *lambda,
                       double *V, double *resid, speigs_info *info);
 
+// The calling thread's current CUDA device (0 when it cannot be read), and
+// making `dev` current on the calling thread.  Host worker threads start on
+// device 0, so a pool that solves on the caller's GPU adopts its device
+// first.
+int  current_device();
+void use_device(int dev);
+
 // Thread-local text of the last CUDA failure seen by the engine.
 const char *last_cuda_error();
 

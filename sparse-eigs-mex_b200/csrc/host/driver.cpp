@@ -33,128 +33,100 @@ double wall() {
     return t.tv_sec + 1e-9 * t.tv_nsec;
 }
 
-// 1: symmetric with both triangles, 2: upper only, 3: lower only, 0: not
-// symmetric (reference check_symmetry, src/speigs_core.c:363-401; transposed
-// entries must agree to 1e-12 relative).
-int check_symmetry(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *Ax) {
-    bool up = false, lo = false;
-    for (int64_t c = 0; c < n && !(up && lo); c++)
-        for (int64_t q = Ap[c]; q < Ap[c + 1]; q++) {
-            if (Ai[q] < c) up = true;
-            else if (Ai[q] > c) lo = true;
-        }
-    if (!lo && up) return 2;
-    if (!up && lo) return 3;
-    if (!up && !lo) return 1;
-    const int64_t nnz = Ap[n];
-    std::vector<int64_t> Tp(n + 1, 0), Ti(nnz ? nnz : 1), wk(n, 0);
-    std::vector<double> Tx(nnz ? nnz : 1);
-    for (int64_t q = 0; q < nnz; q++) wk[Ai[q]]++;
-    for (int64_t i = 0; i < n; i++) { Tp[i + 1] = Tp[i] + wk[i]; wk[i] = Tp[i]; }
-    for (int64_t c = 0; c < n; c++)
-        for (int64_t q = Ap[c]; q < Ap[c + 1]; q++) {
-            int64_t d = wk[Ai[q]]++;
-            Ti[d] = c;
-            Tx[d] = Ax[q];
-        }
-    for (int64_t i = 0; i <= n; i++) if (Tp[i] != Ap[i]) return 0;
-    for (int64_t q = 0; q < nnz; q++) {
-        if (Ti[q] != Ai[q]) return 0;
-        const double a = Ax[q], b = Tx[q];
-        const double m = std::max(fabs(a), fabs(b));
-        if (fabs(a - b) > 1e-12 * (m > 0 ? m : 1.0)) return 0;
-    }
-    return 1;
-}
-
-bool is_diagonal(int64_t n, const int64_t *Ap, const int64_t *Ai) {
-    for (int64_t c = 0; c < n; c++)
-        for (int64_t p = Ap[c]; p < Ap[c + 1]; p++)
-            if (Ai[p] != c) return false;
-    return true;
-}
-
-int64_t uf_find(std::vector<int64_t> &p, int64_t x) {
-    while (p[x] != x) { p[x] = p[p[x]]; x = p[x]; }
-    return x;
-}
-
-// Components over the numerically nonzero entries (reference
-// find_components, src/speigs_core.c:445-466): labels in order of first
-// appearance.
-int64_t find_components(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *Ax,
-                        std::vector<int64_t> &comp) {
-    std::vector<int64_t> p(n);
-    for (int64_t i = 0; i < n; i++) p[i] = i;
-    for (int64_t c = 0; c < n; c++)
-        for (int64_t q = Ap[c]; q < Ap[c + 1]; q++)
-            if (Ax[q] != 0.0) {
-                int64_t a = uf_find(p, Ai[q]), b = uf_find(p, c);
-                if (a != b) p[a] = b;
-            }
-    std::vector<int64_t> lab(n, -1);
-    comp.assign(n, 0);
-    int64_t nc = 0;
-    for (int64_t i = 0; i < n; i++) {
-        int64_t r = uf_find(p, i);
-        if (lab[r] < 0) lab[r] = nc++;
-        comp[i] = lab[r];
-    }
-    return nc;
-}
-
-// check_symmetry for large inputs: the same verdict, from parallel passes.
-// When every column's row indices are strictly increasing, "the transpose
-// equals A entry for entry" is "every (r, c) has its mirror (c, r), with a
-// value within 1e-12 relative", which each column tests on its own by binary
-// search; otherwise the transposition above decides.  *full_sorted is set
-// when the verdict is 1 with both triangles stored and sorted columns.
-int check_symmetry_par(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *Ax,
-                       bool *full_sorted) {
+// Symmetry verdict of the reference's input check (src/speigs_core.c:363-401):
+// 1 when both triangles are stored and A equals its transpose entry for
+// entry (values within 1e-12 relative), 2 when only the upper triangle is
+// stored, 3 when only the lower, 0 otherwise.
+//
+// The reference builds the transpose by a counting sort, whose columns come
+// out with nondecreasing row indices, and compares the two CSC arrays.  So,
+// with both triangles stored, a column whose row indices decrease anywhere
+// fails, and otherwise A equals its transpose exactly when every stored
+// (r, c) -- the t-th entry of the run of row index r in column c -- meets,
+// in column r, a run of row index c of the same length whose t-th value
+// agrees.  Each column tests its own entries by binary search into the
+// columns they mirror, so the columns are checked in parallel ranges.
+// *full_sorted is set when the verdict is 1 and every column's row indices
+// strictly increase (the layout build_full_csr_sorted expects).
+int symmetry_verdict(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *Ax,
+                     bool *full_sorted) {
     *full_sorted = false;
-    std::atomic<int> up{0}, lo{0}, unsorted{0};
+    std::atomic<int> up{0}, lo{0}, descending{0}, repeated{0}, outside{0};
     spx::parallel_ranges(n, 8192, [&](int64_t c0, int64_t c1) {
-        bool u = false, l = false, uns = false;
-        for (int64_t c = c0; c < c1; c++)
-            for (int64_t q = Ap[c]; q < Ap[c + 1]; q++) {
-                if (Ai[q] < c) u = true;
-                else if (Ai[q] > c) l = true;
-                if (q > Ap[c] && Ai[q] <= Ai[q - 1]) uns = true;
+        bool u = false, l = false, dsc = false, rep = false, out = false;
+        for (int64_t c = c0; c < c1; c++) {
+            const int64_t *b = Ai + Ap[c], *e = Ai + Ap[c + 1];
+            for (const int64_t *q = b; q < e; q++) {
+                u |= *q < c;
+                l |= *q > c;
+                out |= *q < 0 || *q >= n;
+                if (q > b) {
+                    dsc |= q[0] < q[-1];
+                    rep |= q[0] == q[-1];
+                }
             }
+        }
         if (u) up = 1;
         if (l) lo = 1;
-        if (uns) unsorted = 1;
+        if (dsc) descending = 1;
+        if (rep) repeated = 1;
+        if (out) outside = 1;
     });
     if (!lo && up) return 2;
     if (!up && lo) return 3;
     if (!up && !lo) return 1;
-    if (unsorted) return check_symmetry(n, Ap, Ai, Ax);
+    if (descending || outside) return 0;
     std::atomic<int> bad{0};
     spx::parallel_ranges(n, 8192, [&](int64_t c0, int64_t c1) {
-        for (int64_t c = c0; c < c1 && !bad.load(std::memory_order_relaxed); c++)
-            for (int64_t q = Ap[c]; q < Ap[c + 1]; q++) {
-                const int64_t r = Ai[q];
-                if (r == c) continue;
-                if (r < 0 || r >= n) { bad = 1; break; }
-                const int64_t *b = Ai + Ap[r], *e = Ai + Ap[r + 1];
-                const int64_t *f = std::lower_bound(b, e, c);
-                if (f == e || *f != c) { bad = 1; break; }
-                const double a = Ax[q], t = Ax[f - Ai];
-                const double m = std::max(fabs(a), fabs(t));
-                if (fabs(a - t) > 1e-12 * (m > 0 ? m : 1.0)) { bad = 1; break; }
+        for (int64_t c = c0; c < c1 && !bad.load(std::memory_order_relaxed); c++) {
+            const int64_t *cb = Ai + Ap[c], *ce = Ai + Ap[c + 1];
+            for (const int64_t *q = cb; q < ce; q++) {
+                const int64_t r = *q;
+                if (r == c) continue;   // a diagonal run mirrors itself
+                const int64_t *mb = Ai + Ap[r], *me = Ai + Ap[r + 1];
+                const int64_t *m0 = std::lower_bound(mb, me, c);
+                int64_t t = 0, len_here = 1, len_there = 0;
+                if (repeated) {
+                    // position within this column's run of r, and both run lengths
+                    const auto run = std::equal_range(cb, ce, r);
+                    t = q - run.first;
+                    len_here = run.second - run.first;
+                    len_there = std::upper_bound(m0, me, c) - m0;
+                } else {
+                    len_there = (m0 != me && *m0 == c) ? 1 : 0;
+                }
+                if (len_there != len_here) { bad = 1; break; }
+                const double a = Ax[q - Ai], m = Ax[(m0 - Ai) + t];
+                const double big = std::max(fabs(a), fabs(m));
+                if (fabs(a - m) > 1e-12 * (big > 0 ? big : 1.0)) { bad = 1; break; }
             }
+        }
     });
     if (bad) return 0;
-    *full_sorted = true;
+    *full_sorted = !repeated;
     return 1;
 }
 
-// find_components for large inputs: the same labels (components over the
-// numerically nonzero entries, numbered in order of first appearance), with
-// the unions done in parallel on a lock-free union-find (a root is linked
-// under a smaller root by compare-and-swap, so links never form a cycle).
-int64_t find_components_par(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *Ax,
-                            std::vector<int64_t> &comp) {
+// The reference's diagonal gate (src/speigs_core.c:801): no stored entry
+// off the diagonal, whatever its value.
+bool pattern_is_diagonal(int64_t n, const int64_t *Ap, const int64_t *Ai) {
+    std::atomic<int> off{0};
+    spx::parallel_ranges(n, 1 << 16, [&](int64_t c0, int64_t c1) {
+        for (int64_t c = c0; c < c1 && !off.load(std::memory_order_relaxed); c++)
+            if (std::any_of(Ai + Ap[c], Ai + Ap[c + 1], [c](int64_t r) { return r != c; }))
+                off = 1;
+    });
+    return !off;
+}
+
+// Connected components over the numerically nonzero stored entries, labelled
+// 0, 1, ... in the order in which each component's first row appears -- the
+// split the reference makes (find_components, src/speigs_core.c:445-466).
+// The unions run in parallel ranges of columns on a lock-free union-find: a
+// root is linked under a smaller root by compare-and-swap, so links never
+// form a cycle, and finds halve their paths as they go.
+int64_t find_components(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *Ax,
+                        std::vector<int64_t> &comp) {
     std::unique_ptr<std::atomic<int64_t>[]> p(new std::atomic<int64_t>[n]);
     spx::parallel_ranges(n, 65536, [&](int64_t a, int64_t b) {
         for (int64_t i = a; i < b; i++) p[i].store(i, std::memory_order_relaxed);
@@ -183,6 +155,8 @@ int64_t find_components_par(int64_t n, const int64_t *Ap, const int64_t *Ai, con
                 }
             }
     });
+    // roots are the smallest row of their component, so a component's label
+    // is fixed when its root is reached in row order
     std::vector<int64_t> lab(n, -1);
     comp.assign(n, 0);
     int64_t nc = 0;
@@ -273,48 +247,40 @@ int solve_components(const int64_t *Ap, const int64_t *Ai, const double *Ax,
     for (int64_t c = 0; c < nc_all; c++) order[c] = c;
     std::stable_sort(order.begin(), order.end(),
                      [&](int64_t a, int64_t b) { return sp.sz[a] > sp.sz[b]; });
-    std::atomic<int64_t> next{0};
     std::atomic<int> err{0};
-    auto worker = [&] {
-        std::vector<int64_t> sAp, sAi;
-        std::vector<double> sAx;
-        for (;;) {
-            const int64_t it = next.fetch_add(1);
-            if (it >= nc_all || err.load() != 0) break;
-            const int64_t ci = order[it], nc = sp.sz[ci];
-            sAp.assign(nc + 1, 0);
-            sAi.clear();
-            sAx.clear();
-            for (int64_t j = 0; j < nc; j++) {
-                const int64_t gc = sp.gidx[sp.off[ci] + j];
-                sAp[j] = (int64_t)sAi.size();
-                for (int64_t q = Ap[gc]; q < Ap[gc + 1]; q++) {
-                    const int64_t r = Ai[q];
-                    if (comp[r] == ci) { sAi.push_back(sp.loc[r]); sAx.push_back(Ax[q]); }
-                }
+    // the caller's device: worker threads start on device 0 and adopt it
+    const int dev = spx::current_device();
+    auto solve_one = [&](int64_t it) {
+        const int64_t ci = order[it], nc = sp.sz[ci];
+        std::vector<int64_t> tAp(nc + 1, 0), tAi;
+        std::vector<double> tAx;
+        for (int64_t j = 0; j < nc; j++) {
+            const int64_t gc = sp.gidx[sp.off[ci] + j];
+            tAp[j] = (int64_t)tAi.size();
+            for (int64_t q = Ap[gc]; q < Ap[gc + 1]; q++) {
+                const int64_t r = Ai[q];
+                if (comp[r] == ci) { tAi.push_back(sp.loc[r]); tAx.push_back(Ax[q]); }
             }
-            sAp[nc] = (int64_t)sAi.size();
-            if (sAi.empty()) { sAi.push_back(0); sAx.push_back(0.0); }
-            CompResult &R = out[ci];
-            R.kc = std::min(k, nc);
-            R.lam.assign(R.kc, 0.0);
-            R.res.assign(R.kc, 0.0);
-            if (want_vec) R.vec.assign((size_t)nc * R.kc, 0.0);
-            const int rc = speigs_impl(nc, sAp.data(), sAi.data(), sAx.data(), R.kc, which, opts,
-                                       ext, R.lam.data(), want_vec ? R.vec.data() : nullptr,
-                                       R.res.data(), &R.info, &R.einfo);
-            if (rc) {
-                int expected = 0;
-                err.compare_exchange_strong(expected, rc);
-            }
+        }
+        tAp[nc] = (int64_t)tAi.size();
+        if (tAi.empty()) { tAi.push_back(0); tAx.push_back(0.0); }
+        CompResult &R = out[ci];
+        R.kc = std::min(k, nc);
+        R.lam.assign(R.kc, 0.0);
+        R.res.assign(R.kc, 0.0);
+        if (want_vec) R.vec.assign((size_t)nc * R.kc, 0.0);
+        const int rc = speigs_impl(nc, tAp.data(), tAi.data(), tAx.data(), R.kc, which, opts,
+                                   ext, R.lam.data(), want_vec ? R.vec.data() : nullptr,
+                                   R.res.data(), &R.info, &R.einfo);
+        if (rc) {
+            int expected = 0;
+            err.compare_exchange_strong(expected, rc);
         }
     };
     unsigned hw = std::thread::hardware_concurrency();
-    int64_t nth = std::min<int64_t>(nc_all, std::max(1u, std::min(hw ? hw : 1u, 16u)));
-    std::vector<std::thread> th;
-    for (int64_t i = 1; i < nth; i++) th.emplace_back(worker);
-    worker();
-    for (auto &t : th) t.join();
+    const int nth = (int)std::min<int64_t>(nc_all, std::max(1u, std::min(hw ? hw : 1u, 16u)));
+    spx::run_pool(nc_all, nth, [dev] { spx::use_device(dev); }, solve_one,
+                  [&] { return err.load() != 0; });
     return err.load();
 }
 
@@ -373,7 +339,8 @@ int blocks_path(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *A
 
 namespace spx {
 int host_check_symmetry(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *Ax) {
-    return check_symmetry(n, Ap, Ai, Ax);
+    bool full_sorted = false;
+    return symmetry_verdict(n, Ap, Ai, Ax, &full_sorted);
 }
 double host_norm1_upper(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *Ax) {
     return norm1_upper(n, Ap, Ai, Ax);
@@ -420,8 +387,7 @@ int speigs_components(speigs_int n, const speigs_int *Ap, const speigs_int *Ai,
                       const double *Ax, speigs_int *comp, speigs_int *ncomp) {
     if (n <= 0 || !Ap || !Ai || !Ax || !comp || !ncomp) return SPEIGS_ERR_ARG;
     std::vector<int64_t> c;
-    *ncomp = Ap[n] >= kSideThreadsMin ? find_components_par(n, Ap, Ai, Ax, c)
-                                      : find_components(n, Ap, Ai, Ax, c);
+    *ncomp = find_components(n, Ap, Ai, Ax, c);
     memcpy(comp, c.data(), sizeof(int64_t) * (size_t)n);
     return SPEIGS_OK;
 }
@@ -440,7 +406,9 @@ int speigs_batched(speigs_int n, const speigs_int *Ap, const speigs_int *Ai, con
         return SPEIGS_ERR_ARG;
     for (int64_t i = 0; i < n; i++)
         if (comp[i] < 0 || comp[i] >= ncomp) return SPEIGS_ERR_ARG;
-    if (opts->check_sym != 0 && check_symmetry(n, Ap, Ai, Ax) == 0) return SPEIGS_ERR_NOTSYM;
+    bool full_sorted = false;
+    if (opts->check_sym != 0 && symmetry_verdict(n, Ap, Ai, Ax, &full_sorted) == 0)
+        return SPEIGS_ERR_NOTSYM;
     std::vector<int64_t> cv(comp, comp + n);
     CompSplit sp;
     sp.build(n, cv, ncomp);
@@ -503,8 +471,7 @@ int speigs_impl(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *A
     const bool par = Ap[n] >= kSideThreadsMin;
     bool full_sorted = false;
     if (opts->check_sym != 0) {
-        const int sym = par ? check_symmetry_par(n, Ap, Ai, Ax, &full_sorted)
-                            : check_symmetry(n, Ap, Ai, Ax);
+        const int sym = symmetry_verdict(n, Ap, Ai, Ax, &full_sorted);
         if (sym == 0) return SPEIGS_ERR_NOTSYM;
     }
     if (n == 1) {
@@ -521,7 +488,7 @@ int speigs_impl(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *A
 
     const double t0 = wall();
     const int dmax = opts->dense_max < 0 ? 800 : opts->dense_max;
-    if (opts->detect && is_diagonal(n, Ap, Ai)) {
+    if (opts->detect && pattern_is_diagonal(n, Ap, Ai)) {
         std::vector<double> d(n, 0.0);
         for (int64_t c = 0; c < n; c++)
             for (int64_t p = Ap[c]; p < Ap[c + 1]; p++) if (Ai[p] == c) d[c] = Ax[p];
@@ -540,7 +507,7 @@ int speigs_impl(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *A
     int64_t ncomp = 1;
     SideThread comp_th;
     if (opts->detect) {
-        if (par) comp_th.start([&] { ncomp = find_components_par(n, Ap, Ai, Ax, comp); });
+        if (par) comp_th.start([&] { ncomp = find_components(n, Ap, Ai, Ax, comp); });
         else ncomp = find_components(n, Ap, Ai, Ax, comp);
     }
     double anorm = 0.0;

@@ -6,6 +6,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <atomic>
 #include <exception>
 #include <mutex>
 #include <thread>
@@ -83,6 +84,28 @@ void parallel_ranges(int64_t n, int64_t grain, F &&f) {
     }
     f((int64_t)0, n / nt);
     g.wait();
+}
+
+// Items [0, count) taken in order from a shared counter by `nthreads`
+// threads, the calling thread among them.  Every thread runs enter() once
+// before its first item: a new std::thread starts on CUDA device 0, so a
+// pool whose items launch GPU work passes a callable that makes the
+// caller's device current.  A thread stops taking items once stop() is true.
+template <class Enter, class Work, class Stop>
+void run_pool(int64_t count, int nthreads, Enter &&enter, Work &&work, Stop &&stop) {
+    std::atomic<int64_t> next{0};
+    auto body = [&] {
+        enter();
+        for (;;) {
+            const int64_t it = next.fetch_add(1);
+            if (it >= count || stop()) break;
+            work(it);
+        }
+    };
+    std::vector<std::thread> th;
+    for (int i = 1; i < nthreads; i++) th.emplace_back(body);
+    body();
+    for (auto &t : th) t.join();
 }
 
 }  // namespace spx

@@ -85,9 +85,20 @@ extern "C" int speigs_b200_syev_small_noalloc(int m, const double *H, double *th
     // the status word sits after the two matrices unless the caller wants it
     int *st = status ? status : (int *)(work + kNoAllocWorkDoubles);
     cudaStream_t cs = (cudaStream_t)stream;
+    // An error left pending by earlier, unrelated CUDA work on this thread
+    // would be read back below as this launch's failure; report it as what
+    // it is, leave it pending for its owner, and launch nothing.
+    cudaError_t e = cudaPeekAtLastError();
+    if (e != cudaSuccess) {
+        char msg[192];
+        snprintf(msg, sizeof msg, "a CUDA error from earlier work is pending (%s); nothing was "
+                 "launched", cudaGetErrorString(e));
+        spx::set_last_error_text(msg);
+        return SPEIGS_ERR_INTERNAL;
+    }
     // the workspace is fully rewritten from H by the kernel: no clearing needed
     spx::launch_syev_small_workspace(m, H, m, theta, S, ord, work, st, cs);
-    cudaError_t e = cudaGetLastError();
+    e = cudaGetLastError();
     if (e != cudaSuccess) {
         spx::set_last_error_text(cudaGetErrorString(e));
         return SPEIGS_ERR_INTERNAL;

@@ -233,16 +233,46 @@ def rgg_component(nc: int, rng: np.random.Generator, degree: float = 8.0) -> sp.
     return (sp.diags(deg + 1e-3) - W).tocsr()
 
 
-def rgg_blocks(ncomp: int, seed: int = 4, nmin: int = 50, nmax: int = 5000) -> sp.csc_matrix:
+def rgg_blocks(ncomp: int, seed: int = 4, nmin: int = 50, nmax: int = 5000,
+               first: int | None = None) -> sp.csc_matrix:
     """Block-diagonal SPD matrix of ncomp random-geometric-graph Laplacians
     (+1e-3 I), sizes uniform in [nmin, nmax] from `seed`.  A component whose
     graph is itself disconnected splits further (isolated vertices become 1x1
-    blocks with value 1e-3)."""
+    blocks with value 1e-3).  first: keep only the first `first` blocks of
+    the ncomp-block family -- the same blocks, bit for bit, as in the full
+    matrix, since each block draws from the generator after the ones before it."""
     rng = np.random.default_rng(seed)
     sizes = rng.integers(nmin, nmax + 1, size=ncomp)
+    if first is not None:
+        sizes = sizes[:first]
     A = sp.block_diag([rgg_component(int(nc), rng) for nc in sizes], format="csc")
     A.sort_indices()
     return A
+
+
+def rgg_sample(nblocks: int = 120) -> sp.csc_matrix:
+    """The first `nblocks` blocks of the 4,096-block random-geometric-graph
+    workload (sizes U[50, 5000], seed 4): a sample of it small enough for a
+    per-component comparison with a CPU solver."""
+    return rgg_blocks(4096, seed=4, first=nblocks)
+
+
+def components_of(A: sp.spmatrix) -> tuple[int, np.ndarray]:
+    """Connected components over the nonzero entries, labelled in order of
+    first appearance by row (the labelling speigs_components returns)."""
+    from scipy.sparse.csgraph import connected_components
+    A = A.tocsr().copy()
+    A.eliminate_zeros()
+    nc, lab = connected_components(A, directed=False)
+    first = np.full(nc, -1, dtype=np.int64)
+    seen = 0
+    remap = np.empty(nc, dtype=np.int64)
+    for i, l in enumerate(lab):
+        if first[l] < 0:
+            first[l] = i
+            remap[l] = seen
+            seen += 1
+    return int(nc), remap[lab].astype(np.int64)
 
 
 def upper(A: sp.spmatrix) -> sp.csc_matrix:

@@ -113,14 +113,23 @@ def test_ref8_blocks(pkg, lib):
 
 
 def test_ref9_banded_1d(pkg, lib):
-    """1-D Laplacian n=20,000: the reference takes its banded LAPACK route;
-    the device library factors the band with the supernodal Cholesky."""
+    """1-D Laplacian n=20,000 (reference test_banded, test/test_speigs.c:276-297):
+    eigenvalues against the closed form."""
     n = 20000
     A = pkg.workloads.lap1d(n)
     rc, lam, V, res, info = call(pkg, lib, A, 4, vectors=False)
     assert rc == 0
     ex = 2.0 - 2.0 * np.cos(np.arange(1, 5) * np.pi / (n + 1))
     assert np.all(np.abs(lam - ex) <= 1e-9 * np.maximum(1e-6, np.abs(ex)))
+
+
+@pytest.mark.xfail(strict=True, reason="the banded route is not on the device yet")
+def test_ref9_banded_route(pkg, lib):
+    """The reference takes its banded route on the 1-D Laplacian
+    (test/test_speigs.c:289 asserts SPEIGS_PATH_BANDED)."""
+    A = pkg.workloads.lap1d(20000)
+    rc, lam, V, res, info = call(pkg, lib, A, 4, vectors=False)
+    assert rc == 0 and info["path"] == pkg.speigs.PATH_BANDED
 
 
 def test_ref10_isolated(pkg, lib):
@@ -225,7 +234,8 @@ def test_parity_varcoef_sm(pkg, lib, ref_lib):
     """Variable-coefficient FV operator 24^3, k=8 'sm' (no closed form)."""
     A = pkg.workloads.varcoef3d(24, seed=3)
     info, rinfo = _parity(pkg, lib, ref_lib, A, 8, 0)
-    assert abs(info["nops"] - rinfo["nops"]) <= info["nops"] // 4
+    # same start vector, same recurrence: the same number of applications
+    assert info["nops"] == rinfo["nops"] and info["restarts"] == rinfo["restarts"]
 
 
 def test_parity_varcoef_lm(pkg, lib, ref_lib):
