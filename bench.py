@@ -1,6 +1,13 @@
 #!/usr/bin/env python
 """Time to k eigenpairs at residual <= 1e-10 ||A||_1 on B200.
 
+Default workload: the metric's own configuration -- the held-out 48^3
+finite-volume operator with conductivity exp(GRF) (seed 3200), k=16 'sm' --
+timed in every form on the same B200: the plain FP64 drop-in, mixed
+precision, the learned block start, and both together (the line's `value`).
+Other workloads (--workload lap46, lap20, lap2d1000, varcoef64, rgg) time
+one form of the drop-in path.
+
 A step is one complete solve of the workload: numeric factorization ('sm')
 plus thick-restart Lanczos to convergence, with the k eigenpairs left in
 device memory.  `value` times steps with the matrix and its symbolic
@@ -198,87 +205,239 @@ def _dev_time(torch, fn, steps, warmup, stream):
     return statistics.mean(ms), out, ms
 
 
-def run_forms_grf(args, pkg, wl):
-    """The four forms on one held-out GRF operator, same B200: plain FP64 with
-    the reference's random start, FP64 with the learned start, mixed precision
-    with the random start, mixed with the learned start (the target form).
-    Device time per solve (factor + Lanczos, matrix resident), and end to end
-    through speigs_ex including the network's proposal."""
+def block_solve_bytes(op_bytes_single, n, b):
+    """Algorithmic bytes of one block solve of b columns: the panels and row
+    lists once forward and once backward (the single solve's figure), plus
+    three n-vectors per column (right-hand side in, intermediate, result)."""
+    return op_bytes_single + 24.0 * n * (b - 1)
+
+
+def run_metric(args, pkg, wl, ctx):
+    """The headline: time to k=16 eigenpairs of the held-out 48^3 GRF operator
+    at residual <= 1e-10 ||A||_1, mixed precision with the learned block start
+    (`value`) against the plain FP64 drop-in and the other forms, same B200.
+
+    Device timing (`value`, `forms[*].value_s`): one solve per step on a plan
+    whose matrix and symbolic analysis are resident -- numeric factor, the
+    network's proposal on the device (learned forms), the Lanczos to
+    convergence -- on the plan's stream with CUDA events, a 256 MiB buffer
+    written between steps to flush L2.  End to end (`e2e`): host CSC and host
+    conductivity in, host eigenpairs out: the proposal (graph and features
+    built on the host, uploaded, network forward, result downloaded) and
+    speigs_ex() with every copy inside."""
     import torch
     s, w, L = pkg.speigs, pkg.workloads, pkg.learned
-    lib = s.load()
-    torch.cuda.set_device(0)
-    dev = torch.device("cuda", 0)
+    lib = ctx["lib"]
+    dev = ctx["dev"]
+    N, seed = 48, 3200
     A = wl["build"]()
-    n, k = A.shape[0], wl["k"]
+    n, k, nnz = A.shape[0], wl["k"], A.nnz
+    kap = w.grf_conductivity(N, seed)
     opts = s.default_opts(lib, tol=TOL)
-    kap = w.grf_conductivity(48, 3200)
     have_net = os.path.exists(L.CHECKPOINT)
     net = L.WarmStartNet.load(L.CHECKPOINT, lib=lib) if have_net else None
-    t0 = time.perf_counter()
-    Y = L.propose(net, 48, kap) if net is not None else None
-    t_prop = time.perf_counter() - t0
-    Yf = np.asfortranarray(Y) if Y is not None else None
-    forms = {}
-    for name, prec, warm in (("fp64", s.FP64, None), ("fp64+learned", s.FP64, Yf),
-                             ("mixed", s.MIXED, None), ("mixed+learned", s.MIXED, Yf)):
-        if "learned" in name and warm is None:
-            continue
-        ext = s.ext_opts(lib, precision=prec, warm=warm)
+    P = net.nout if net is not None else 24
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    peak, peak_kind = measured_peaks()
+
+    # the proposal's inputs on the device (the learned forms read them there)
+    rowptr, col, wts = L.grid_graph(N, kap)
+    X = L.features(N, kap)
+    t_rp = torch.from_numpy(rowptr).to(dev)
+    t_ci = torch.from_numpy(col).to(dev)
+    t_w = torch.from_numpy(wts).to(dev)
+    t_X = torch.from_numpy(X).to(dev)
+    Y32 = torch.empty((n, P), dtype=torch.float32, device=dev)
+    Yw = torch.zeros((P, n), dtype=torch.float64, device=dev)      # column-major n x P
+
+    def propose_device(stream):
+        rc = net.forward_device(n, t_rp.data_ptr(), t_ci.data_ptr(), t_w.data_ptr(),
+                                t_X.data_ptr(), Y32.data_ptr(), stream.cuda_stream)
+        if rc != 0:
+            raise RuntimeError(f"mpnn forward rc={rc}")
+        with torch.cuda.stream(stream):
+            Yw.copy_(Y32.t())
+
+    forms_spec = [("fp64", s.FP64, False, -1), ("mixed", s.MIXED, False, -1)]
+    if net is not None:
+        forms_spec += [("fp64+learned", s.FP64, True, 0), ("mixed+learned", s.MIXED, True, 0)]
+    forms_spec += [("fp64+block(random)", s.FP64, False, P),
+                   ("mixed+block(random)", s.MIXED, False, P)]
+    target = "mixed+learned" if net is not None else "mixed"
+    forms, keep = {}, {}
+    for name, prec, learned, block in forms_spec:
+        ext = s.ext_opts(lib, precision=prec, block=block)
+        if learned:
+            ext.warm = Yw.data_ptr()
+            ext.warm_cols = P
         plan = s.Plan(A, s.SM, opts, lib=lib, ext=ext)
         pstream = torch.cuda.ExternalStream(plan.stream(), device=dev)
         lam = torch.zeros(k, dtype=torch.float64, device=dev)
         V = torch.zeros((k, n), dtype=torch.float64, device=dev)
         res = torch.zeros(k, dtype=torch.float64, device=dev)
-        box = {}
 
-        def solve():
+        def step():
+            if learned:
+                propose_device(pstream)
             rc, info = plan.solve_device(k, lam.data_ptr(), V.data_ptr(), res.data_ptr())
             if rc != 0:
                 raise RuntimeError(f"{name}: rc={rc} {s.last_error(lib)}")
-            box["info"] = info
             return info
-        ms, info, ms_steps = _dev_time(torch, solve, args.steps, args.warmup, pstream)
+        torch.cuda.synchronize()
+        for _ in range(args.warmup):
+            info = step()
+        is_target = name == target
+        steps = args.steps if is_target or name == "fp64" else max(2, min(args.steps, 3))
+        sampler = ClockSampler()
+        if is_target:
+            sampler.start()
+        ctx["barrier"]()
+        torch.cuda.synchronize()
+        l0 = s.counters(lib)[0]
+        step_ms, t_op, t_all = [], 0.0, []
+        for _ in range(steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(pstream)
+            info = step()
+            e1.record(pstream)
+            e1.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+            t_op += info["t_op"]
+            t_all.append({kk: round(info[kk], 5) for kk in ("t_factor", "t_op", "t_ortho",
+                                                               "t_resid", "t_ritz")})
+        torch.cuda.synchronize()
+        launches = (s.counters(lib)[0] - l0) // max(steps, 1)
+        ctx["barrier"]()
+        clocks = sampler.stop() if is_target else None
         ei = plan.ext_info()
+        costs = plan.costs()
         lam_h = lam.cpu().numpy()
         Vh = np.ascontiguousarray(V.cpu().numpy().T)
         r = np.linalg.norm(A @ Vh - Vh * lam_h[None, :], axis=0)
-        vnorm = float(np.linalg.norm(Vh))
         plan.close()
-        e2e = []
-        for _ in range(max(2, min(args.steps, 3))):
-            t1 = time.perf_counter()
-            if "learned" in name:
-                Yp = L.propose(net, 48, kap)
-                ext2 = s.ext_opts(lib, precision=prec)
-                rc, *_ = s.speigs_ex(A, k, s.SM, opts, ext2, vectors=True, lib=lib, warm=Yp)
-            else:
-                rc, *_ = s.speigs_ex(A, k, s.SM, opts, ext, vectors=True, lib=lib)
-            e2e.append(time.perf_counter() - t1)
-        forms[name] = {"value_s": ms * 1e-3, "step_ms": [round(x, 3) for x in ms_steps],
-                       "e2e_s": statistics.mean(e2e), "nops": int(info["nops"]),
-                       "restarts": int(info["restarts"]), "refine_steps": int(ei["refine_steps"]),
-                       "warm_cols": int(ei["warm_cols"]), "lam": lam_h.tolist(),
+        forms[name] = {"value_s": statistics.mean(step_ms) * 1e-3,
+                       "step_ms": [round(x, 3) for x in step_ms],
+                       "nops": int(info["nops"]), "restarts": int(info["restarts"]),
+                       "flag": int(info["flag"]), "block": int(ei["block"]),
+                       "block_solves": int(ei["block_solves"]),
+                       "refine_steps": int(ei["refine_steps"]), "warm_cols": int(ei["warm_cols"]),
                        "max_resid_over_anorm": float(r.max() / info["anorm"]),
-                       "vectors_fro_norm": vnorm,
-                       "t_factor": info["t_factor"], "t_iter": info["t_iter"]}
-    base = np.array(forms["fp64"]["lam"])
-    for f in forms.values():
-        f["eig_rel_err_vs_fp64"] = (np.abs(np.array(f.pop("lam")) - base) / np.abs(base)).tolist()
-    target = "mixed+learned" if "mixed+learned" in forms else "mixed"
-    line = {
-        "metric": METRIC, "value": forms[target]["value_s"], "unit": "s", "n_gpus": 1,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": forms[target]["value_s"] * 1e3,
-        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic",
-        "config": {"workload": wl["desc"], "n": int(n), "nnz": int(A.nnz), "k": k, "tol": TOL,
-                   "form": target, "checkpoint": os.path.relpath(L.CHECKPOINT, ROOT) if have_net else None,
-                   "l2": "256 MiB buffer written between timed steps"},
-        "forms": forms, "proposal_s": t_prop,
-        "ratio_target_over_fp64_value": forms[target]["value_s"] / forms["fp64"]["value_s"],
-        "e2e": {"value": forms[target]["e2e_s"], "unit": "s"},
-    }
-    print(json.dumps(line))
+                       "phases_s": t_all[-1]}
+        keep[name] = dict(lam=lam_h, info=info, ei=ei, costs=costs, launches=launches,
+                          clocks=clocks, t_op=t_op / steps, steps=steps)
+
+    # ---- end to end through the public API: host in, host out
+    def e2e_run(name):
+        prec = s.MIXED if name.startswith("mixed") else s.FP64
+        learned = "learned" in name
+        c0 = s.counters(lib)
+        t0 = time.perf_counter()
+        extra_h2d = extra_d2h = 0
+        if learned:
+            Yp = L.propose(net, N, kap)
+            extra_h2d = rowptr.nbytes + col.nbytes + wts.nbytes + X.nbytes
+            extra_d2h = Yp.nbytes // 2          # float32 on the device, widened on the host
+            ext = s.ext_opts(lib, precision=prec)
+            rc, *_ = s.speigs_ex(A, k, s.SM, opts, ext, vectors=True, lib=lib, warm=Yp)
+        else:
+            ext = s.ext_opts(lib, precision=prec, block=-1)
+            rc, *_ = s.speigs_ex(A, k, s.SM, opts, ext, vectors=True, lib=lib)
+        dt = time.perf_counter() - t0
+        c1 = s.counters(lib)
+        if rc != 0:
+            raise RuntimeError(f"e2e {name}: rc={rc} {s.last_error(lib)}")
+        return dt, c1[1] - c0[1] + extra_h2d, c1[2] - c0[2] + extra_d2h
+    e2e = {}
+    for name in (target, "fp64"):
+        for _ in range(max(1, min(args.warmup, 2))):
+            e2e_run(name)
+        ts, h2d, d2h = [], 0, 0
+        for _ in range(max(2, min(args.steps, 3))):
+            dt, h2d, d2h = e2e_run(name)
+            ts.append(dt)
+        e2e[name] = {"value": statistics.mean(ts), "unit": "s", "h2d_bytes_per_step": int(h2d),
+                     "d2h_bytes_per_step": int(d2h), "steps_s": [round(x, 4) for x in ts]}
+
+    # ---- roofline of the dominant kernel of the timed form: its operator
+    # application (block solve with the FP32 panels, and the FP64 block
+    # residuals and corrections of the refinement), bytes from the plan's
+    # figures, time = the device time of the applications inside the timed
+    # solves (CUDA events on the plan's stream)
+    kt = keep[target]
+    ei, info = kt["ei"], kt["info"]
+    bsz = max(1, int(ei["block"]))
+    apps = max(1, int(ei["block_solves"]) - int(ei["refine_steps"])) if bsz > 1 else max(1, int(info["nops"]))
+    corr = int(ei["refine_steps"])
+    if bsz > 1:
+        bs_bytes = block_solve_bytes(kt["costs"]["op_bytes"], n, bsz)
+        res_bytes = 12.0 * nnz + 4.0 * n + 24.0 * n * bsz
+        total = (apps + corr) * (bs_bytes + res_bytes) + corr * 24.0 * n * bsz
+    else:
+        total = info["nops"] * kt["costs"]["op_bytes"]
+    achieved = total / kt["t_op"] / 1e9 if kt["t_op"] > 0 else None
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get(f"grf48:{target}")
+        except Exception:
+            traffic = None
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                "kernel": "refined block application: mf_bsolve (FP32 panels, %d columns) + "
+                          "FP64 block residuals and corrections" % bsz if target.startswith("mixed")
+                          else "block shift-invert solve",
+                "bytes_per_solve": total,
+                "op_time_s": kt["t_op"], "block_applications": apps, "corrections": corr,
+                "peak_source": peak_kind}
+
+    # ---- the reference's CPU solver on the same operator (rank 0, N=1)
+    cpu, check = None, {}
+    base = keep["fp64"]["lam"]
+    tl = keep[target]["lam"]
+    check["eig_rel_err_vs_fp64"] = [float(x) for x in np.abs(tl - base) / np.abs(base)]
+    check["max_resid_over_anorm"] = forms[target]["max_resid_over_anorm"]
+    check["flag"] = forms[target]["flag"]
+    if ctx["rank"] == 0 and ctx["world"] == 1 and not args.no_cpu_baseline and os.path.exists(REF_LIB):
+        times, rlam, rinfo = cpu_reference_times(pkg, A, wl, steps=2, warmup=1, budget_s=30.0)
+        cpu = {"value": statistics.median(times), "unit": "s", "cores": os.cpu_count(),
+               "kind": "reference",
+               "sample": f"{len(times)} full solve(s) of the same operator by the reference's "
+                         "src/speigs_core.c (CHOLMOD stand-in + OpenBLAS, all host threads), "
+                         "median"}
+        rlam = np.sort(np.asarray(rlam))
+        check["eig_rel_err_vs_reference"] = [float(x) for x in np.abs(np.sort(tl) - rlam) /
+                                             np.abs(rlam)]
+        check["reference_nops"] = int(rinfo["nops"])
+    tv = forms[target]["value_s"]
+    t = torch.tensor([tv], dtype=torch.float64, device=dev)
+    ctx["max"](t)
+    tv = float(t.item())
+    if ctx["rank"] == 0:
+        line = {
+            "metric": METRIC, "value": tv, "unit": "s", "n_gpus": ctx["world"],
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": tv * 1e3,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 factor panels, f64 refinement / recurrence / Ritz" if target.startswith(
+                "mixed") else "f64",
+            "data": "synthetic",
+            "config": {"workload": wl["desc"], "n": int(n), "nnz": int(nnz), "k": k, "tol": TOL,
+                       "form": target + (" (block thick-restart Lanczos, first block = the "
+                                         "network's %d-column proposal)" % P if net else ""),
+                       "checkpoint": os.path.relpath(L.CHECKPOINT, ROOT) if have_net else None,
+                       "parallelism": f"replicas x{ctx['world']}",
+                       "l2": "256 MiB buffer written between timed steps",
+                       "value_scope": "numeric factor + proposal on the device + Lanczos, "
+                                      "matrix and analysis resident"},
+            "ratio_target_over_fp64": tv / forms["fp64"]["value_s"],
+            "forms": forms, "check": check, "roofline": roofline, "cpu_baseline": cpu,
+            "e2e": e2e[target], "e2e_fp64": e2e["fp64"],
+            "gpu_launches": int(keep[target]["launches"]), "clocks": keep[target]["clocks"],
+        }
+        print(json.dumps(line))
     return 0
 
 
@@ -342,7 +501,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="lap46")
+    ap.add_argument("--workload", default="grf48")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="operator of the timed line: plain FP64 factor, or FP32 factor on the "
@@ -361,8 +520,6 @@ def main():
 
     if args.impl == "reference":
         return run_reference(args, pkg, wl, rank)
-    if args.workload == "grf48":
-        return run_forms_grf(args, pkg, wl)
     if args.workload == "rgg":
         return run_batched(args, pkg, wl)
 
@@ -377,6 +534,20 @@ def main():
         torch.cuda.set_device(0)
     dev = torch.device("cuda", torch.cuda.current_device())
     lib = s.load()
+    if args.workload == "grf48":
+        def barrier():
+            if world > 1:
+                dist.barrier()
+
+        def tmax(t):
+            if world > 1:
+                dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ctx = {"lib": lib, "dev": dev, "rank": rank, "world": world, "barrier": barrier,
+               "max": tmax}
+        rc = run_metric(args, pkg, wl, ctx)
+        if world > 1:
+            dist.destroy_process_group()
+        return rc
 
     A = wl["build"]()
     n, k = A.shape[0], wl["k"]

@@ -36,13 +36,30 @@ typedef struct {
     const double *warm;        /* optional start subspace, n x warm_cols, column-major,
                                   host memory; NULL => the reference's random start   */
     speigs_int   warm_cols;
+    int          block;        /* 'sm' Krylov method (see below); 0 => automatic        */
 } speigs_ext_opts;
+
+/* speigs_ext_opts.block selects the Krylov method of the 'sm' route:
+ *   0   automatic: with a start subspace (warm), a block thick-restart
+ *       Lanczos whose first block is that subspace (width min(warm_cols,
+ *       32)); without one, the reference's single-vector Lanczos;
+ *   b   (1..32) the block method with blocks of b vectors; a start subspace
+ *       fills the first block, the reference's random stream the rest;
+ *  -1   the single-vector Lanczos always; a start subspace is then folded
+ *       into its start vector.
+ * The block method reads the factor once per block of b vectors (one
+ * persistent launch for all of them) and converges to the same eigenpairs
+ * under the same test: ||A x - lambda x|| <= tol max(||A||_1, 1) for the k
+ * wanted pairs.  Its operator-application count (speigs_info.nops) counts
+ * vectors; its restart count counts restart cycles. */
 
 typedef struct {
     int          precision;      /* precision actually used                         */
     speigs_int   refine_steps;   /* FP64 refinement corrections made (mixed)        */
     speigs_int   factor_solves;  /* solves with the factor: applications + corrections */
     speigs_int   warm_cols;      /* start-subspace columns used (0: random start)   */
+    int          block;          /* block size of the block method (0: single vector) */
+    speigs_int   block_solves;   /* block solves: applications + corrections        */
     /* host wall time (s) of the Krylov route outside speigs_info's t_analyze /
      * t_factor / t_iter: input checks and the CSR build, plan set-up (device
      * buffers, uploads), copy-out and release */
@@ -154,6 +171,15 @@ int speigs_plan_solve_device(speigs_plan plan, speigs_int k, double *lambda, dou
 /* y = Op x on the device (Op = A for 'lm', (A + shift I)^{-1} for 'sm' after
  * a solve or speigs_plan_factor); x, y are device vectors of length n. */
 int speigs_plan_apply_device(speigs_plan plan, const double *x, double *y);
+
+/* Y = Op X for nr <= 32 vectors at once (X, Y column-major n x nr device
+ * arrays, leading dimensions ldx, ldy >= n).  For 'sm' one persistent launch
+ * solves all nr columns, reading the factor once (mixed precision: each
+ * column refined in FP64 as in speigs_plan_apply_device); for 'lm' the
+ * columns are multiplied by A one after another.  No counterpart in the
+ * reference interface. */
+int speigs_plan_apply_block_device(speigs_plan plan, const double *X, int64_t ldx, double *Y,
+                                   int64_t ldy, int nr);
 
 /* Numeric factorization only ('sm'); *shift receives the delta used. */
 int speigs_plan_factor(speigs_plan plan, double *shift);

@@ -12,6 +12,8 @@
 #include "../../include/speigs_b200.h"
 #include "kernels/krylov.cuh"
 #include "kernels/multifrontal.cuh"
+#include "kernels/block_krylov.cuh"
+#include "kernels/dense_lu.cuh"
 #include "counters.h"
 
 #include <cuda_runtime.h>
@@ -217,6 +219,11 @@ struct Factor {
         if (mixed) f32.solve(b, x, st, skip);
         else f64.solve(b, x, st, skip);
     }
+    int solve_block(const double *B, int64_t ldb, double *X, int64_t ldx, int nr, cudaStream_t st,
+                    const int *skip = nullptr) {
+        return mixed ? f32.solve_block(B, ldb, X, ldx, nr, st, skip)
+                     : f64.solve_block(B, ldb, X, ldx, nr, st, skip);
+    }
     int *error_word() const { return mixed ? f32.error_word() : f64.error_word(); }
     double factor_flops() const { return mixed ? f32.factor_flops() : f64.factor_flops(); }
     int64_t solve_bytes() const { return mixed ? f32.solve_bytes() : f64.solve_bytes(); }
@@ -239,6 +246,18 @@ struct SpmvOperator : Operator {
     void apply(const double *x, double *y, cudaStream_t st) override {
         nops++;
         launch_spmv(A.n, A.rp, A.ci, A.va, x, y, st);
+    }
+};
+
+// The indefinite route: y = A^{-1} x with the dense inverse (reference
+// operator mode 2, src/speigs_core.c:111-115).
+struct DenseInvOperator : Operator {
+    int n;
+    const double *M;
+    DenseInvOperator(int n_, const double *m) : n(n_), M(m) {}
+    void apply(const double *x, double *y, cudaStream_t st) override {
+        nops++;
+        launch_dense_apply(n, M, x, y, st);
     }
 };
 
@@ -275,6 +294,72 @@ struct MixedCholOperator : Operator {
             plan->solve(rf->r, rf->d, st, rf->flag);
             launch_axpy_unless(A.n, y, rf->d, rf->flag, st);
         }
+    }
+    const int *error_word() const override { return plan->error_word(); }
+};
+
+// Operator on a block of b <= 32 vectors: W = Op V (column-major, leading
+// dimensions ldv, ldw).  The block Lanczos counts block applications and the
+// vectors they carry.
+struct BlockOperator {
+    virtual ~BlockOperator() = default;
+    virtual int apply(const double *V, int64_t ldv, double *W, int64_t ldw, int b,
+                      cudaStream_t st) = 0;
+    virtual const int *error_word() const { return nullptr; }
+    int64_t napps = 0, nvecs = 0;
+};
+
+struct BlockCholOperator : BlockOperator {
+    Factor *plan;
+    explicit BlockCholOperator(Factor *p) : plan(p) {}
+    int apply(const double *V, int64_t ldv, double *W, int64_t ldw, int b,
+              cudaStream_t st) override {
+        napps++;
+        nvecs += b;
+        return plan->solve_block(V, ldv, W, ldw, b, st);
+    }
+    const int *error_word() const override { return plan->error_word(); }
+};
+
+// Device state of the FP64 refinement of a mixed-precision block solve.
+struct BlockRefineState {
+    double *R = nullptr, *D = nullptr, *part = nullptr;
+    int64_t ld = 0;
+    int *flag = nullptr, *count = nullptr;
+    unsigned *counter = nullptr;
+    int max_steps = 10;
+    double tol = 1e-14;
+};
+
+// Mixed precision on a block: X = M^{-1} B with the FP32 factor, then
+// R = B - (A + shift I) X and X += M^{-1} R until every column passes the
+// backward-error test or max_steps corrections were made.  As for one
+// vector, the whole loop is queued; once the flag is set, the remaining
+// solves and updates return at once on the device.
+struct BlockMixedOperator : BlockOperator {
+    Factor *plan;
+    DevA A;
+    double shift, anorm;
+    BlockRefineState *rf;
+    BlockMixedOperator(Factor *p, const DevA &a, double sh, double an, BlockRefineState *r)
+        : plan(p), A(a), shift(sh), anorm(an), rf(r) {}
+    int apply(const double *V, int64_t ldv, double *W, int64_t ldw, int b,
+              cudaStream_t st) override {
+        napps++;
+        nvecs += b;
+        int rc = plan->solve_block(V, ldv, W, ldw, b, st);
+        if (rc) return rc;
+        cudaMemsetAsync(rf->flag, 0, sizeof(int), st);
+        for (int it = 0; it <= rf->max_steps; it++) {
+            launch_block_refine_residual(A.n, A.rp, A.ci, A.va, shift, V, ldv, W, ldw, rf->R,
+                                         rf->ld, b, rf->tol, anorm, rf->flag, rf->count,
+                                         rf->part, rf->counter, st);
+            if (it == rf->max_steps) break;
+            rc = plan->solve_block(rf->R, rf->ld, rf->D, rf->ld, b, st, rf->flag);
+            if (rc) return rc;
+            launch_block_axpy_unless(A.n, b, W, ldw, rf->D, rf->ld, rf->flag, st);
+        }
+        return 0;
     }
     const int *error_word() const override { return plan->error_word(); }
 };
@@ -667,6 +752,304 @@ static int lanczos_device(Operator &op, const DevA &A, int n, int64_t k, const s
     return SPEIGS_OK;
 }
 
+// ------------------------------------------------------- block Lanczos --
+// Block thick-restart Lanczos for the shift-invert operator: the Rayleigh-
+// Ritz projection of Op on a basis grown a block of b vectors at a time,
+// restarted from the l = k + 5 wanted Ritz vectors plus the current
+// residual block.  It starts from a block -- the caller's start subspace
+// (the learned proposal), completed with the reference's random stream --
+// so a proposal that already holds the wanted eigenvectors is used in full,
+// and every block application reads the factor once for b vectors.
+//
+// Layout: V is n x (mmax + b) column-major (ld padded to 32); after a block
+// at columns [jc, jc + b) is applied, H[0 : jc + b, jc : jc + b] = V^T Op V
+// (two Gram-Schmidt passes, both summed) and the orthonormalised residual
+// becomes the next block at [jc + b, jc + 2b).  H is read from its upper
+// triangle, so it is exactly the projection V^T Op V whatever the block
+// structure; dependent residual columns are replaced by vectors of the
+// random stream.  Convergence is decided as in the reference: true
+// residuals ||A x - lambda x|| <= tol max(||A||_1, 1) with lambda the
+// Rayleigh quotient of A, for the k Ritz vectors of largest |theta|.  The
+// residual of the block recurrence (cheap: a b x b Gram matrix) gates when
+// that test runs.
+namespace {
+
+struct BlockLanczosBufs {
+    int n = 0, b = 0, mmax = 0;
+    int64_t ldv = 0;
+    double *V = nullptr, *Vn = nullptr, *H = nullptr, *S = nullptr, *theta = nullptr,
+           *hb = nullptr, *G = nullptr, *Gres = nullptr, *Rinv = nullptr, *est2 = nullptr,
+           *X = nullptr, *AX = nullptr, *lam = nullptr, *r2 = nullptr, *xn2 = nullptr,
+           *jwork = nullptr;
+    int *ord = nullptr, *jstat = nullptr, *cstat = nullptr;
+    ReduceScratch rs;
+    BlockScratch bs;
+};
+
+}  // namespace
+
+static int block_lanczos_device(BlockOperator &op, const DevA &A, int n, int64_t k, int b,
+                                const speigs_opts &o, double anorm, double shift, double *lambda,
+                                double *resid, const double **Xdev, int64_t *ldx, int *nout,
+                                speigs_info *info, EngineStats *stats, Arena &ar, double *pinned,
+                                cudaStream_t st, const double *Y, int64_t p, int64_t *warm_used) {
+    const int64_t maxit = o.maxit ? o.maxit : 300;
+    const double tol = o.tol > 0 ? o.tol : 1e-14;
+    const double rtol = tol * std::max(anorm, 1.0);
+    const double bthr = 1e-13 * std::max(anorm, 1.0);
+    const int64_t ncv_ref = o.ncv ? o.ncv : std::max<int64_t>(2 * k + 1, 20);
+    const int kk = (int)k;
+    const int l0 = (int)std::min<int64_t>(k + 5, n);
+    int mmax = (int)std::max<int64_t>(ncv_ref, l0 + 3 * b);
+    mmax = std::min(mmax, kBlockMaxM);
+    mmax = std::min<int>(mmax, n - b);
+    if (mmax < l0 + b || mmax < kk) return SPEIGS_ERR_ARG;
+
+    BlockLanczosBufs B;
+    B.n = n;
+    B.b = b;
+    B.mmax = mmax;
+    B.ldv = ((int64_t)n + 31) & ~(int64_t)31;
+    const int ldh = mmax;
+    const int cols = mmax + b;
+    B.V = ar.alloc<double>((size_t)B.ldv * cols);
+    B.Vn = ar.alloc<double>((size_t)B.ldv * cols);
+    B.H = ar.alloc<double>((size_t)ldh * ldh);
+    B.S = ar.alloc<double>((size_t)ldh * ldh);
+    B.theta = ar.alloc<double>(ldh);
+    B.hb = ar.alloc<double>((size_t)ldh * b);
+    B.G = ar.alloc<double>((size_t)b * b);
+    B.Gres = ar.alloc<double>((size_t)b * b);
+    B.Rinv = ar.alloc<double>((size_t)b * b);
+    B.est2 = ar.alloc<double>(kk);
+    B.X = ar.alloc<double>((size_t)B.ldv * kk);
+    B.AX = ar.alloc<double>((size_t)B.ldv * kk);
+    B.lam = ar.alloc<double>(kk);
+    B.r2 = ar.alloc<double>(kk);
+    B.xn2 = ar.alloc<double>(std::max(cols, kk));
+    B.ord = ar.alloc<int>(ldh);
+    B.jstat = ar.alloc<int>(2);
+    B.cstat = ar.alloc<int>(2);
+    const int me = (mmax + 1) & ~1;
+    B.jwork = (mmax > syev_small_smem_limit()) ? ar.alloc<double>((size_t)2 * me * me) : nullptr;
+    const int nblk = (n + 511) / 512 + 1;
+    const int maxc = std::max(cols, kk) + 1;
+    B.rs.part = ar.alloc<double>((size_t)nblk * maxc);
+    B.rs.counter = ar.alloc<unsigned>(1);
+    B.rs.max_blocks = nblk;
+    B.rs.max_cols = maxc;
+    B.bs.max_parts = tsb_parts(n);
+    B.bs.part = ar.alloc<double>((size_t)B.bs.max_parts * kBlockMaxM * kBlockMaxB);
+    if (ar.failed) return SPEIGS_ERR_MEM;
+    cudaMemsetAsync(B.rs.counter, 0, sizeof(unsigned), st);
+    cudaMemsetAsync(B.H, 0, sizeof(double) * ldh * ldh, st);
+
+    // pinned read-back: lam[k], r2[k], est2[k], theta of the wanted[k],
+    // a status pair and the operator's error word
+    double *h_lam = pinned, *h_r2 = pinned + kk, *h_est = pinned + 2 * kk,
+           *h_th = pinned + 3 * kk;
+    int *h_stat = reinterpret_cast<int *>(pinned + 4 * kk);
+    int *h_jst = h_stat + 2;
+    int *h_operr = h_stat + 4;
+    const int *op_err = op.error_word();
+
+    PhaseTimer tm(st);
+    double ms_op = 0, ms_ortho = 0, ms_resid = 0, ms_ritz = 0;
+    auto sync = [&](const char *where) -> int {
+        if (op_err) copy_async(h_operr, op_err, sizeof(int), cudaMemcpyDeviceToHost, st);
+        cudaError_t e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return cuda_fail(e, where);
+        tm.resolve();
+        if (op_err && *h_operr) {
+            set_last_error_text("operator application failed: a solve dependency wait ran out");
+            return SPEIGS_ERR_INTERNAL;
+        }
+        return 0;
+    };
+
+    uint64_t seed = o.seed ? o.seed : 88172645463325252ULL;
+    auto rand_col = [&](double *dst) {
+        launch_rand_vec(n, seed, dst, st);
+        seed = rng_advance(seed, (uint64_t)n);
+    };
+    // W (b columns at Wp) <- (I - V V^T) W twice against V[:, 0:m]; with
+    // hcol, the two passes' coefficients are summed into H[0:m, hcol..]
+    auto cgs2 = [&](double *Wp, int m, double *hcol) {
+        if (m <= 0) return;
+        double *V = B.V;
+        if (hcol) {
+            launch_tsb_tn(V, B.ldv, n, m, Wp, B.ldv, b, hcol, ldh, 0, B.bs, st);
+            launch_tsb_nn_sub(V, B.ldv, n, m, hcol, ldh, Wp, B.ldv, b, st);
+        } else {
+            launch_tsb_tn(V, B.ldv, n, m, Wp, B.ldv, b, B.hb, ldh, 0, B.bs, st);
+            launch_tsb_nn_sub(V, B.ldv, n, m, B.hb, ldh, Wp, B.ldv, b, st);
+        }
+        launch_tsb_tn(V, B.ldv, n, m, Wp, B.ldv, b, B.hb, ldh, 0, B.bs, st);
+        launch_tsb_nn_sub(V, B.ldv, n, m, B.hb, ldh, Wp, B.ldv, b, st);
+        if (hcol) launch_block_axpy_unless(m, b, hcol, ldh, B.hb, ldh, nullptr, st);
+    };
+    // Orthonormalise the block at Wp against V[:, 0:m] (already projected
+    // out) and within itself by two Cholesky QR passes.  Columns found
+    // dependent are replaced by random vectors and the block is projected
+    // again (up to three times).  *replaced gets the columns replaced in the
+    // first test; returns 1 when the block stays dependent (no extension).
+    auto orthonormalise = [&](double *Wp, int m, unsigned *replaced, bool keep_gram) -> int {
+        unsigned first_mask = 0;
+        for (int att = 0;; att++) {
+            launch_tsb_tn(Wp, B.ldv, n, b, Wp, B.ldv, b, B.G, b, 0, B.bs, st);
+            if (keep_gram && att == 0)
+                cudaMemcpyAsync(B.Gres, B.G, sizeof(double) * b * b, cudaMemcpyDeviceToDevice, st);
+            launch_block_chol(b, B.G, b, B.Rinv, bthr, 1e-14, B.cstat, st);
+            copy_async(h_stat, B.cstat, 2 * sizeof(int), cudaMemcpyDeviceToHost, st);
+            if (int e = sync("block orthonormalisation")) return e;
+            const unsigned mask = (unsigned)h_stat[0];
+            if (att == 0) first_mask = mask;
+            if (!h_stat[1]) break;
+            if (att == 3) {
+                if (replaced) *replaced = first_mask;
+                return 1;
+            }
+            for (int c = 0; c < b; c++)
+                if ((mask >> c) & 1u) rand_col(Wp + (size_t)c * B.ldv);
+            cgs2(Wp, m, nullptr);
+        }
+        launch_tsb_right_mul(n, b, Wp, B.ldv, B.Rinv, st);
+        launch_tsb_tn(Wp, B.ldv, n, b, Wp, B.ldv, b, B.G, b, 0, B.bs, st);
+        launch_block_chol(b, B.G, b, B.Rinv, 0.0, 0.0, B.cstat, st);
+        launch_tsb_right_mul(n, b, Wp, B.ldv, B.Rinv, st);
+        if (replaced) *replaced = first_mask;
+        return 0;
+    };
+
+    // ---- start block: the proposal's columns, completed with random ones
+    if (warm_used) *warm_used = 0;
+    const int pp = (int)std::min<int64_t>(Y ? p : 0, b);
+    for (int c = 0; c < b; c++) {
+        double *dst = B.V + (size_t)c * B.ldv;
+        if (c < pp) launch_copy(n, Y + (size_t)c * n, dst, st);
+        else rand_col(dst);
+    }
+    {
+        unsigned rep = 0;
+        int e = orthonormalise(B.V, 0, &rep, false);
+        if (e < 0) return e;
+        if (e == 1) return SPEIGS_ERR_INTERNAL;
+        int used = 0;
+        for (int c = 0; c < pp; c++) used += ((rep >> c) & 1u) ? 0 : 1;
+        if (warm_used) *warm_used = used;
+    }
+
+    int jc = 0, mm = 0;
+    int64_t restarts = 0, nconv = 0;
+    int last_nwant = 0;
+    int rc = SPEIGS_OK;
+    bool have_result = false;
+    for (;;) {
+        // ---- apply Op to the block at [jc, jc + b); project; orthonormalise
+        double *Vb = B.V + (size_t)jc * B.ldv;
+        double *Wp = B.V + (size_t)(jc + b) * B.ldv;
+        int t0 = tm.begin();
+        if (int e = op.apply(Vb, B.ldv, Wp, B.ldv, b, st)) return e;
+        tm.end(t0, &ms_op);
+        mm = jc + b;
+        int t1 = tm.begin();
+        cgs2(Wp, mm, B.H + (size_t)jc * ldh);
+        unsigned rep = 0;
+        const int stuck = orthonormalise(Wp, mm, &rep, true);
+        if (stuck < 0) return stuck;
+        tm.end(t1, &ms_ortho);
+        const bool cycle_end = stuck == 1 || mm + b > mmax;
+
+        // ---- Rayleigh-Ritz on H[0:mm, 0:mm]; the recurrence's residual
+        // estimates gate the true-residual test
+        const int nwant = std::min(kk, mm);
+        int tr = tm.begin();
+        launch_syev_small(mm, B.H, ldh, B.theta, B.S, B.ord, B.jwork, B.jstat, st);
+        launch_block_ritz_est(nwant, b, B.S, mm, jc, B.ord, B.Gres, b, B.est2, st);
+        tm.end(tr, &ms_ritz);
+        {
+            // theta of the wanted pairs, in ord order
+            copy_async(h_est, B.est2, sizeof(double) * nwant, cudaMemcpyDeviceToHost, st);
+            copy_async(h_jst, B.jstat, sizeof(int), cudaMemcpyDeviceToHost, st);
+            std::vector<int> ordh(nwant);
+            std::vector<double> thh(mm);
+            copy_async(ordh.data(), B.ord, sizeof(int) * nwant, cudaMemcpyDeviceToHost, st);
+            copy_async(thh.data(), B.theta, sizeof(double) * mm, cudaMemcpyDeviceToHost, st);
+            if (int e = sync("block ritz")) return e;
+            if (h_jst[0] < 0) { rc = SPEIGS_ERR_LAPACK; break; }
+            for (int t = 0; t < nwant; t++) h_th[t] = thh[ordh[t]];
+        }
+        bool gate = nwant >= kk;
+        for (int t = 0; t < nwant && gate; t++) {
+            const double th = std::fabs(h_th[t]);
+            const double est = std::sqrt(std::max(h_est[t], 0.0)) * (anorm + std::fabs(shift)) /
+                               std::max(th, 1e-300);
+            if (!(est <= 10.0 * rtol)) gate = false;
+        }
+        if (gate || cycle_end) {
+            int t2 = tm.begin();
+            launch_ritz_vectors(B.V, B.ldv, n, mm, B.S, mm, B.ord, 0, nwant, B.X, B.ldv, B.xn2,
+                                B.rs, st);
+            launch_scale_cols(n, nwant, B.X, B.ldv, B.xn2, st);
+            for (int t = 0; t < nwant; t++)
+                launch_spmv(A.n, A.rp, A.ci, A.va, B.X + (size_t)t * B.ldv,
+                            B.AX + (size_t)t * B.ldv, st);
+            launch_rayleigh_resid(n, nwant, B.X, B.ldv, B.AX, B.ldv, B.lam, B.r2, B.rs, st);
+            tm.end(t2, &ms_resid);
+            copy_async(h_lam, B.lam, sizeof(double) * nwant, cudaMemcpyDeviceToHost, st);
+            copy_async(h_r2, B.r2, sizeof(double) * nwant, cudaMemcpyDeviceToHost, st);
+            if (int e = sync("block residuals")) return e;
+            nconv = 0;
+            for (int t = 0; t < nwant; t++) {
+                const double r = std::sqrt(h_r2[t]);
+                lambda[t] = h_lam[t];
+                if (resid) resid[t] = r;
+                if (r <= rtol) nconv++;
+            }
+            last_nwant = nwant;
+            have_result = true;
+            if (nconv >= kk) break;
+        }
+        if (!cycle_end) {
+            jc = mm;
+            continue;
+        }
+        if (restarts >= maxit || stuck == 1) break;
+        restarts++;
+
+        // ---- thick restart: the l wanted Ritz vectors and the residual block
+        const int l = std::min(l0, std::min(mm, mmax - b));
+        int tk = tm.begin();
+        launch_ritz_vectors(B.V, B.ldv, n, mm, B.S, mm, B.ord, 0, l, B.Vn, B.ldv, B.xn2, B.rs, st);
+        launch_scale_cols(n, l, B.Vn, B.ldv, B.xn2, st);
+        launch_block_copy(n, b, B.V + (size_t)mm * B.ldv, B.ldv, B.Vn + (size_t)l * B.ldv, B.ldv,
+                          st);
+        std::swap(B.V, B.Vn);
+        launch_block_set_diag(ldh, mmax, l, B.theta, B.ord, B.H, st);
+        tm.end(tk, &ms_ritz);
+        jc = l;
+    }
+    if (rc) return rc;
+    if (!have_result) return SPEIGS_ERR_INTERNAL;
+    *Xdev = B.X;
+    *ldx = B.ldv;
+    *nout = last_nwant;
+    if (int e = sync("block lanczos end")) return e;
+    info->nconv = nconv;
+    info->restarts = restarts;
+    info->nops = op.nvecs;
+    info->flag = (nconv >= kk) ? 0 : 1;
+    info->t_op += ms_op * 1e-3;
+    info->t_ortho += ms_ortho * 1e-3;
+    info->t_resid += ms_resid * 1e-3;
+    info->t_ritz += ms_ritz * 1e-3;
+    if (stats) {
+        stats->ms_op += ms_op; stats->ms_ortho += ms_ortho;
+        stats->ms_resid += ms_resid; stats->ms_ritz += ms_ritz;
+    }
+    return SPEIGS_OK;
+}
+
 // ----------------------------------------------------------- host CSR --
 int build_full_csr(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *Ax,
                    HostCSR *out) {
@@ -788,6 +1171,9 @@ struct speigs_plan_s {
     int32_t *d_rp = nullptr, *d_ci = nullptr;
     double *d_va = nullptr;
     spx::Factor mf;
+    bool banded = false;              // reported as the reference's banded route
+    bool lu = false;                  // indefinite route: the dense inverse below
+    double *d_ainv = nullptr;         // n x n, allocated on first use
     spx::RefineState refine;          // mixed precision only
     int64_t refine_reported = 0;      // corrections already reported
     int64_t last_refine = 0;          // corrections of the last solve
@@ -795,6 +1181,9 @@ struct speigs_plan_s {
     const double *ext_warm = nullptr; // start subspace (host, n x ext_warm_cols)
     int64_t ext_warm_cols = 0;
     int64_t last_warm = 0;            // start-subspace columns used by the last solve
+    int ext_block = 0;                // speigs_ext_opts.block
+    int last_block = 0;               // block size of the last solve (0: single vector)
+    int64_t last_block_solves = 0;    // its block solves (applications + corrections)
     double t_analyze = 0;
     std::vector<void *> owned;
 };
@@ -893,10 +1282,36 @@ int plan_from_csr(HostCSR &A, speigs_which which, const speigs_opts &o, double a
 // Numeric factorization with the reference's capped shift escalation
 // (src/speigs_core.c:938-970).  Returns 0, SPEIGS_ERR_FACTOR when A stays
 // indefinite, or another negative code.
+// The indefinite route's operator: A^{-1} formed on the device (the
+// reference's UMFPACK LU at sigma = 0, src/speigs_core.c:972-984).
+static int plan_dense_inverse(speigs_plan_s *p) {
+    cudaStream_t st = p->stream.s;
+    const int n = p->A.n;
+    if (n > kLuDenseMax) {
+        snprintf(g_err, sizeof g_err, "matrix is indefinite and its order %d exceeds the %d of "
+                 "the device's dense indefinite route", n, kLuDenseMax);
+        return SPEIGS_ERR_FACTOR;
+    }
+    if (!p->d_ainv) {
+        int rc = plan_alloc(p, (void **)&p->d_ainv, sizeof(double) * (size_t)n * n);
+        if (rc) return rc;
+    }
+    Arena ar(st);
+    double *rowbuf = ar.alloc<double>(n), *colbuf = ar.alloc<double>(n);
+    int *ipiv = ar.alloc<int>(n), *flags = ar.alloc<int>(2);
+    if (ar.failed) return SPEIGS_ERR_MEM;
+    launch_dense_inverse(n, p->d_rp, p->d_ci, p->d_va, p->anorm, p->d_ainv, rowbuf, colbuf, ipiv,
+                         flags, st);
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(e, "dense inverse");
+    return 0;
+}
+
 static int plan_factor(speigs_plan_s *p, EngineStats *stats) {
     cudaStream_t st = p->stream.s;
     const speigs_opts &o = p->opts;
     double delta = 0.0;
+    p->lu = false;
     // A pivot that is rounding noise on the scale of ||A||_1 is treated as
     // not positive, so an exactly singular PSD matrix takes the shift route
     // deterministically instead of by the sign of its last rounding error.
@@ -922,10 +1337,14 @@ static int plan_factor(speigs_plan_s *p, EngineStats *stats) {
     }
     if (fr < 0) return fr;
     if (fr == 1) {
-        // still indefinite: the reference switches to an LU here (:975-984),
-        // a route the device library does not provide
-        snprintf(g_err, sizeof g_err, "matrix is indefinite: LU route not available");
-        return SPEIGS_ERR_FACTOR;
+        // still indefinite: like the reference (:975-984), the Lanczos runs on
+        // A^{-1} at sigma = 0, the eigenvalues nearest zero
+        int rc = plan_dense_inverse(p);
+        if (rc) return rc;
+        p->lu = true;
+        p->shift = 0.0;
+        p->factored = true;
+        return 0;
     }
     p->shift = delta;
     p->factored = true;
@@ -977,6 +1396,7 @@ static int plan_solve(speigs_plan_s *p, int64_t k, double *lambda, double *V, do
     SpmvOperator spmv_op(dA);
     CholOperator chol_op(&p->mf);
     MixedCholOperator mixed_op(&p->mf, dA, 0.0, p->anorm, &p->refine);
+    DenseInvOperator lu_op(n, nullptr);
     Operator *op = &spmv_op;
     if (p->which == SPEIGS_LM) {
         info->path = SPEIGS_PATH_DIRECT;
@@ -986,13 +1406,16 @@ static int plan_solve(speigs_plan_s *p, int64_t k, double *lambda, double *V, do
         info->t_factor = wall() - tf;
         if (rc) return rc;
         mixed_op.shift = p->shift;
-        op = p->mf.mixed ? (Operator *)&mixed_op : (Operator *)&chol_op;
+        lu_op.M = p->d_ainv;
+        op = p->lu ? (Operator *)&lu_op
+                   : p->mf.mixed ? (Operator *)&mixed_op : (Operator *)&chol_op;
         info->shift = p->shift;
-        info->path = SPEIGS_PATH_SHIFTINV;
+        info->path = p->lu ? SPEIGS_PATH_LU : p->banded ? SPEIGS_PATH_BANDED
+                                                         : SPEIGS_PATH_SHIFTINV;
     }
     std::vector<double> lam_h(k, 0.0), res_h(k, 0.0);
     int rc = 0;
-    const size_t need = 2 * (size_t)k + 16;
+    const size_t need = 4 * (size_t)k + 16;
     double *pinbuf = pinned_scalars(need);
     if (!pinbuf) return SPEIGS_ERR_MEM;
     {
@@ -1012,18 +1435,68 @@ static int plan_solve(speigs_plan_s *p, int64_t k, double *lambda, double *V, do
             dwarm = dw;
         }
         int64_t wused = 0;
+        // block method ('sm'): explicit block size, or the start subspace's width
+        int bsz = 0;
+        if (p->which == SPEIGS_SM && !p->lu) {
+            if (p->ext_block > 0) bsz = std::min(p->ext_block, kBlockMaxB);
+            else if (p->ext_block == 0 && wcols > 0) bsz = (int)std::min<int64_t>(wcols, kBlockMaxB);
+            if (bsz > 0) {
+                // room for the basis: l + b <= mmax <= n - b (else the single-vector method)
+                const int64_t ncv_ref = p->opts.ncv ? p->opts.ncv : std::max<int64_t>(2 * k + 1, 20);
+                const int64_t l0 = std::min<int64_t>(k + 5, n);
+                int64_t mmax = std::min<int64_t>(std::max<int64_t>(ncv_ref, l0 + 3 * bsz), kBlockMaxM);
+                mmax = std::min<int64_t>(mmax, n - bsz);
+                if (mmax < l0 + bsz || mmax < k) bsz = 0;
+            }
+        }
+        p->last_block = bsz;
+        p->last_block_solves = 0;
+        if (bsz > 0) {
+            BlockRefineState brf;
+            if (p->mf.mixed) {
+                brf.ld = ((int64_t)n + 31) & ~(int64_t)31;
+                brf.R = ar.alloc<double>((size_t)brf.ld * bsz);
+                brf.D = ar.alloc<double>((size_t)brf.ld * bsz);
+                brf.part = ar.alloc<double>((size_t)3 * kBlockMaxB * ((n + 255) / 256));
+                brf.flag = ar.alloc<int>(1);
+                brf.count = ar.alloc<int>(1);
+                brf.counter = ar.alloc<unsigned>(1);
+                if (ar.failed) return SPEIGS_ERR_MEM;
+                cudaMemsetAsync(brf.count, 0, sizeof(int), st);
+                cudaMemsetAsync(brf.counter, 0, sizeof(unsigned), st);
+                brf.max_steps = p->refine.max_steps;
+                brf.tol = p->refine.tol;
+            }
+            BlockCholOperator bchol(&p->mf);
+            BlockMixedOperator bmixed(&p->mf, dA, p->shift, p->anorm, &brf);
+            BlockOperator &bop = p->mf.mixed ? (BlockOperator &)bmixed : (BlockOperator &)bchol;
+            rc = block_lanczos_device(bop, dA, n, k, bsz, p->opts, p->anorm, p->shift,
+                                      lam_h.data(), res_h.data(), &X, &ldx, &nout, info, stats,
+                                      ar, pinbuf, st, dwarm, wcols, &wused);
+            p->last_warm = wused;
+            p->last_ops = bop.nvecs;
+            int cnt = 0;
+            if (rc == 0 && p->mf.mixed) {
+                cudaMemcpyAsync(&cnt, brf.count, sizeof(int), cudaMemcpyDeviceToHost, st);
+                note_d2h(sizeof(int));
+                cudaStreamSynchronize(st);
+            }
+            p->last_refine = cnt;
+            p->last_block_solves = bop.napps + cnt;
+        } else {
         rc = lanczos_device(*op, dA, n, k, p->opts, p->anorm, lam_h.data(), res_h.data(), &X,
                             &ldx, &nout, info, stats, ar, pinbuf, st, dwarm, wcols, &wused);
         p->last_warm = wused;
         p->last_ops = op->nops;
-        if (rc == 0 && p->mf.mixed) {
+        }
+        if (rc == 0 && p->mf.mixed && bsz == 0 && !p->lu) {
             int cnt = 0;
             cudaMemcpyAsync(&cnt, p->refine.count, sizeof(int), cudaMemcpyDeviceToHost, st);
             note_d2h(sizeof(int));
             cudaStreamSynchronize(st);
             p->last_refine = cnt - p->refine_reported;
             p->refine_reported = cnt;
-        } else {
+        } else if (bsz == 0) {
             p->last_refine = 0;
         }
         if (rc == 0) {
@@ -1064,11 +1537,17 @@ static void fill_ext_info(const speigs_plan_s *p, speigs_ext_info *e) {
     e->refine_steps = p->last_refine;
     e->factor_solves = p->which == SPEIGS_SM ? p->last_ops + p->last_refine : 0;
     e->warm_cols = p->last_warm;
+    e->block = p->last_block;
+    e->block_solves = p->last_block_solves;
+    if (p->last_block > 0)
+        e->factor_solves = p->which == SPEIGS_SM ? p->last_ops + (int64_t)p->last_refine *
+                                                                     p->last_block : 0;
 }
 
 int device_krylov(HostCSR &A, int64_t k, speigs_which which, const speigs_opts &o,
                   double anorm, double *lambda, double *V, double *resid, speigs_info *info,
-                  EngineStats *stats, const speigs_ext_opts *ext, speigs_ext_info *einfo) {
+                  EngineStats *stats, const speigs_ext_opts *ext, speigs_ext_info *einfo,
+                  bool banded) {
     speigs_plan_s *p = nullptr;
     const double t0 = wall();
     int rc = plan_from_csr(A, which, o, anorm, ext, &p);
@@ -1076,6 +1555,8 @@ int device_krylov(HostCSR &A, int64_t k, speigs_which which, const speigs_opts &
     const double t_setup = wall() - t0 - p->t_analyze;
     p->ext_warm = ext ? ext->warm : nullptr;
     p->ext_warm_cols = ext ? ext->warm_cols : 0;
+    p->ext_block = ext ? ext->block : 0;
+    p->banded = banded;
     rc = plan_solve(p, k, lambda, V, resid, info, false, stats);
     fill_ext_info(p, einfo);
     const double t1 = wall();
@@ -1256,6 +1737,7 @@ int speigs_plan_create_ex(speigs_int n, const speigs_int *Ap, const speigs_int *
     p->Ai_copy.assign(Ai, Ai + Ap[n]);
     p->ext_warm = ext ? ext->warm : nullptr;
     p->ext_warm_cols = ext ? ext->warm_cols : 0;
+    p->ext_block = ext ? ext->block : 0;
     *plan = p;
     return SPEIGS_OK;
 }
@@ -1300,7 +1782,9 @@ int speigs_plan_apply_device(speigs_plan p, const double *x, double *y) {
             int rc = spx::plan_factor(p, nullptr);
             if (rc) return rc;
         }
-        if (p->mf.mixed) {
+        if (p->lu) {
+            spx::launch_dense_apply(p->A.n, p->d_ainv, x, y, st);
+        } else if (p->mf.mixed) {
             spx::DevA dA{p->A.n, p->d_rp, p->d_ci, p->d_va};
             spx::MixedCholOperator op(&p->mf, dA, p->shift, p->anorm, &p->refine);
             op.apply(x, y, st);
@@ -1309,10 +1793,66 @@ int speigs_plan_apply_device(speigs_plan p, const double *x, double *y) {
         }
     }
     int herr = 0;
-    if (p->which == SPEIGS_SM && p->mf.error_word())
+    if (p->which == SPEIGS_SM && !p->lu && p->mf.error_word())
         cudaMemcpyAsync(&herr, p->mf.error_word(), sizeof(int), cudaMemcpyDeviceToHost, st);
     cudaError_t e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return spx::cuda_fail(e, "apply");
+    if (herr) {
+        spx::set_last_error_text("solve failed: a dependency wait ran out");
+        return SPEIGS_ERR_INTERNAL;
+    }
+    return SPEIGS_OK;
+}
+
+int speigs_plan_apply_block_device(speigs_plan p, const double *x, int64_t ldx, double *y,
+                                   int64_t ldy, int nr) {
+    if (!p || !x || !y || nr < 1 || nr > spx::kBlockMaxB || ldx < p->A.n || ldy < p->A.n)
+        return SPEIGS_ERR_ARG;
+    cudaStream_t st = p->stream.s;
+    const int n = p->A.n;
+    int rc = 0;
+    if (p->which == SPEIGS_LM) {
+        for (int c = 0; c < nr; c++)
+            spx::launch_spmv(n, p->d_rp, p->d_ci, p->d_va, x + (size_t)c * ldx, y + (size_t)c * ldy,
+                             st);
+    } else {
+        if (!p->factored) {
+            rc = spx::plan_factor(p, nullptr);
+            if (rc) return rc;
+        }
+        if (p->lu) {
+            for (int c = 0; c < nr; c++)
+                spx::launch_dense_apply(n, p->d_ainv, x + (size_t)c * ldx, y + (size_t)c * ldy, st);
+        } else if (p->mf.mixed) {
+            spx::Arena ar(st);
+            spx::BlockRefineState brf;
+            brf.ld = ((int64_t)n + 31) & ~(int64_t)31;
+            brf.R = ar.alloc<double>((size_t)brf.ld * nr);
+            brf.D = ar.alloc<double>((size_t)brf.ld * nr);
+            brf.part = ar.alloc<double>((size_t)3 * spx::kBlockMaxB * ((n + 255) / 256));
+            brf.flag = ar.alloc<int>(1);
+            brf.count = ar.alloc<int>(1);
+            brf.counter = ar.alloc<unsigned>(1);
+            if (ar.failed) return SPEIGS_ERR_MEM;
+            cudaMemsetAsync(brf.count, 0, sizeof(int), st);
+            cudaMemsetAsync(brf.counter, 0, sizeof(unsigned), st);
+            brf.max_steps = p->refine.max_steps;
+            brf.tol = p->refine.tol;
+            spx::DevA dA{n, p->d_rp, p->d_ci, p->d_va};
+            spx::BlockMixedOperator op(&p->mf, dA, p->shift, p->anorm, &brf);
+            rc = op.apply(x, ldx, y, ldy, nr, st);
+            cudaError_t e = cudaStreamSynchronize(st);   // before the arena returns its memory
+            if (!rc && e != cudaSuccess) rc = spx::cuda_fail(e, "apply block");
+        } else {
+            rc = p->mf.solve_block(x, ldx, y, ldy, nr, st);
+        }
+        if (rc) return rc;
+    }
+    int herr = 0;
+    if (p->which == SPEIGS_SM && !p->lu && p->mf.error_word())
+        cudaMemcpyAsync(&herr, p->mf.error_word(), sizeof(int), cudaMemcpyDeviceToHost, st);
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return spx::cuda_fail(e, "apply block");
     if (herr) {
         spx::set_last_error_text("solve failed: a dependency wait ran out");
         return SPEIGS_ERR_INTERNAL;

@@ -46,10 +46,13 @@ struct EngineStats {
 // A is consumed (its host arrays are freed by the call).
 // ext (may be NULL) selects the operator precision; einfo (may be NULL)
 // receives the extension diagnostics.
+// banded: the input passed the reference's banded-route gate; the route is
+// reported as SPEIGS_PATH_BANDED (the band is factored by the supernodal
+// code under nested dissection, which cuts it into independent segments).
 int device_krylov(HostCSR &A, int64_t k, speigs_which which, const speigs_opts &o,
                   double anorm, double *lambda, double *V, double *resid, speigs_info *info,
                   EngineStats *stats, const speigs_ext_opts *ext = nullptr,
-                  speigs_ext_info *einfo = nullptr);
+                  speigs_ext_info *einfo = nullptr, bool banded = false);
 
 // Host set-up helpers shared by the C API entry points (driver.cpp).
 int    host_check_symmetry(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *Ax);

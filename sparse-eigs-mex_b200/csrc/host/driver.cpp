@@ -168,6 +168,56 @@ int64_t find_components(int64_t n, const int64_t *Ap, const int64_t *Ai, const d
     return nc;
 }
 
+// The reference's banded-route gate (src/speigs_core.c:865-893), decided on
+// the caller's CSC pattern: a reverse Cuthill-McKee order (breadth-first
+// levels from the lowest-degree unvisited vertex, each vertex's unvisited
+// neighbours appended in order of increasing column count, ties kept in
+// storage order, the whole order reversed), the bandwidth kd of A under it,
+// and the band's size and occupancy: kd <= band_max (512 when 0), (kd + 1) n
+// <= 2e7 cells and nnz / (n kd) >= 0.05.
+bool banded_gate(int64_t n, const int64_t *Ap, const int64_t *Ai, const speigs_opts &o) {
+    const int64_t bmax = o.band_max ? o.band_max : 512;
+    if (bmax <= 0) return false;
+    std::vector<int64_t> order;
+    order.reserve(n);
+    std::vector<char> seen(n, 0);
+    auto degree = [&](int64_t v) { return Ap[v + 1] - Ap[v]; };
+    std::vector<int64_t> fresh;
+    int64_t scan = 0;
+    while ((int64_t)order.size() < n) {
+        while (seen[scan]) scan++;
+        // the lowest-degree unvisited vertex at or after the first unvisited one
+        int64_t s = scan;
+        for (int64_t i = scan; i < n; i++)
+            if (!seen[i] && degree(i) < degree(s)) s = i;
+        seen[s] = 1;
+        size_t head = order.size();
+        order.push_back(s);
+        while (head < order.size()) {
+            const int64_t v = order[head++];
+            fresh.clear();
+            for (int64_t q = Ap[v]; q < Ap[v + 1]; q++) {
+                const int64_t w = Ai[q];
+                if (w < 0 || w >= n) return false;
+                if (!seen[w]) { seen[w] = 1; fresh.push_back(w); }
+            }
+            std::stable_sort(fresh.begin(), fresh.end(),
+                             [&](int64_t a, int64_t b) { return degree(a) < degree(b); });
+            order.insert(order.end(), fresh.begin(), fresh.end());
+        }
+    }
+    // position of each vertex in the reversed order
+    std::vector<int64_t> pos(n);
+    for (int64_t i = 0; i < n; i++) pos[order[n - 1 - i]] = i;
+    int64_t kd = 0;
+    for (int64_t c = 0; c < n; c++)
+        for (int64_t q = Ap[c]; q < Ap[c + 1]; q++)
+            kd = std::max<int64_t>(kd, std::llabs(pos[Ai[q]] - pos[c]));
+    const double cells = (double)(kd + 1) * (double)n;
+    const double occupancy = kd > 0 ? (double)Ap[n] / ((double)n * (double)kd) : 1.0;
+    return kd <= bmax && cells <= 2.0e7 && occupancy >= 0.05;
+}
+
 // ||A||_1 of the symmetric matrix of the upper triangle (cholmod_l_norm_sparse
 // with stype = 1, as the reference calls it at src/speigs_core.c:840).
 double norm1_upper(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *Ax) {
@@ -530,9 +580,13 @@ int speigs_impl(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *A
     if (rc) return rc;
     info->anorm = anorm;
     const double t_checks = wall() - tc;
+    // the reference's banded route ('sm'): the band is factored on the device
+    // by dissecting it into independent segments (the supernodal factor under
+    // nested dissection), with the same shift escalation
+    const bool banded = which == SPEIGS_SM && banded_gate(n, Ap, Ai, *opts);
     // factor + Lanczos on the device; results come back sorted by |lambda|
     rc = spx::device_krylov(A, k, which, *opts, anorm, lambda, V, resid, info, nullptr, ext,
-                            einfo);
+                            einfo, banded);
     einfo->t_checks = t_checks;
     return rc;
 }

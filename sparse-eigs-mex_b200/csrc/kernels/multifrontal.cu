@@ -1468,6 +1468,8 @@ __global__ void __launch_bounds__(kSThreads, 2) mf_solve_sf(SolveArgs a) {
     }
 }
 
+#include "mf_block_solve.cuh"
+
 static size_t solve_smem_bytes() {
     return std::max(sizeof(SolveShared), sizeof(WarpShared) * kSWarps);
 }
@@ -1524,9 +1526,11 @@ template <> void MultifrontalPlanT<Real>::release(cudaStream_t st) {
                     d_rowptr_, d_frontptr_, d_gptr_, d_uptr_, d_acolptr_, d_atpos_, d_asrc_,
                     d_tasks_, d_front_, d_G_, d_u_, d_yf_, d_x_, d_status_, d_meta_,
                     d_stask_, d_bundle_, d_cptr_, d_cidx_, d_chunks_, d_fpart_, d_bpart_,
-                    d_cnt_, d_sync_};
+                    d_cnt_, d_sync_, d_bin_, d_bout_, d_byf_, d_bx_, d_bu_, d_bfp_, d_bbp_};
     for (void *p : ptrs)
         if (p) cudaFreeAsync(p, st);
+    d_bin_ = d_bout_ = d_byf_ = d_bx_ = d_bu_ = d_bfp_ = d_bbp_ = nullptr;
+    bw_ = 0;
     d_perm_ = d_sfirst_ = d_rows_ = d_relmap_ = d_child_ptr_ = d_child_list_ = nullptr;
     d_cbnd_ = nullptr;
     d_cbnd_ptr_ = nullptr;
@@ -1944,6 +1948,8 @@ template <> int MultifrontalPlanT<Real>::init(const spx_symbolic &S, const int64
         rc = rc ? rc : dupload((SNodeH **)&d_meta_, meta.data(), meta.size(), st);
         rc = rc ? rc : dupload((STaskH **)&d_stask_, tasks_s.data(), tasks_s.size(), st);
         rc = rc ? rc : dupload(&d_bundle_, bundle.data(), bundle.size(), st);
+        fslots_ = fslots;
+        bslots_ = bslots;
         rc = rc ? rc : dmalloc(&d_fpart_, (size_t)fslots * kST, st);
         rc = rc ? rc : dmalloc(&d_bpart_, (size_t)bslots * kST, st);
         rc = rc ? rc : dmalloc(&d_cnt_, (size_t)(nfc_ + nbc_), st);
@@ -2145,6 +2151,100 @@ template <> void MultifrontalPlanT<Real>::solve(const double *b, double *x, cuda
     cudaMemsetAsync(d_sync_, 0, sizeof(int) * (sync_ints_ - 1), st);
     mf_solve_sf<<<solve_grid_, kSThreads, solve_smem_, st>>>(a);
     note_launch();
+}
+
+namespace {
+template <int NR>
+void launch_bsolve(const BSolveArgs &a, int n, int nr, const double *B, int64_t ldb, double *X,
+                   int64_t ldx, double *bin, const double *bout, int grid, size_t smem,
+                   cudaStream_t st) {
+    const int tb = (n + 31) / 32;
+    bs_to_rows<NR><<<tb, 256, 0, st>>>(n, nr, B, ldb, bin, a.skip);
+    mf_bsolve<NR><<<grid, kSThreads, smem, st>>>(a);
+    bs_from_rows<NR><<<tb, 256, 0, st>>>(n, nr, bout, X, ldx, a.skip);
+    note_launch(3);
+}
+
+template <int NR>
+int bsolve_config(int *grid, size_t *smem) {
+    *smem = bsolve_smem_bytes<NR>();
+    if (cudaFuncSetAttribute(mf_bsolve<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)*smem) != cudaSuccess) {
+        cudaGetLastError();
+        return SPEIGS_ERR_INTERNAL;
+    }
+    int dev = 0, nsm = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mf_bsolve<NR>, kSThreads, *smem);
+    if (per_sm <= 0 || nsm <= 0) return SPEIGS_ERR_INTERNAL;
+    *grid = nsm * std::min(per_sm, 4);
+    return 0;
+}
+}  // namespace
+
+template <> int MultifrontalPlanT<Real>::solve_block(const double *B, int64_t ldb, double *X,
+                                                     int64_t ldx, int nr, cudaStream_t st,
+                                                     const int *skip) {
+    if (nr < 1 || nr > 32 || !d_meta_) return SPEIGS_ERR_ARG;
+    const int w = nr <= 8 ? 8 : nr <= 16 ? 16 : 32;
+    if (w > bw_) {
+        // (re)allocate the block buffers for rows of w doubles
+        void *old[] = {d_bin_, d_bout_, d_byf_, d_bx_, d_bu_, d_bfp_, d_bbp_};
+        for (void *p : old)
+            if (p) cudaFreeAsync(p, st);
+        d_bin_ = d_bout_ = d_byf_ = d_bx_ = d_bu_ = d_bfp_ = d_bbp_ = nullptr;
+        bw_ = 0;
+        int rc = 0;
+        rc = rc ? rc : dmalloc(&d_bin_, (size_t)n_ * w, st);
+        rc = rc ? rc : dmalloc(&d_bout_, (size_t)n_ * w, st);
+        rc = rc ? rc : dmalloc(&d_byf_, (size_t)n_ * w, st);
+        rc = rc ? rc : dmalloc(&d_bx_, (size_t)n_ * w, st);
+        rc = rc ? rc : dmalloc(&d_bu_, (size_t)std::max<int64_t>(u_total_, 1) * w, st);
+        rc = rc ? rc : dmalloc(&d_bfp_, (size_t)std::max(fslots_, 1) * kST * w, st);
+        rc = rc ? rc : dmalloc(&d_bbp_, (size_t)std::max(bslots_, 1) * kST * w, st);
+        if (!rc) {
+            rc = w == 8 ? bsolve_config<8>(&bgrid_, &bsmem_)
+               : w == 16 ? bsolve_config<16>(&bgrid_, &bsmem_) : bsolve_config<32>(&bgrid_, &bsmem_);
+        }
+        if (rc) return rc;
+        bw_ = w;
+    }
+    BSolveArgs a;
+    a.meta = (const SNode *)d_meta_;
+    a.tasks = (const STask *)d_stask_;
+    a.ntasks = ntasks_;
+    a.ns = ns_;
+    a.bundle = d_bundle_;
+    a.perm = d_perm_;
+    a.rows = d_rows_;
+    a.cptr = d_cptr_;
+    a.cidx = d_cidx_;
+    a.G = d_G_;
+    a.u = d_bu_;
+    a.yf = d_byf_;
+    a.x = d_bx_;
+    a.fc_base = d_chunks_;
+    a.fc_n = d_chunks_ + nfc_;
+    a.bc_base = d_chunks_ + 2 * nfc_;
+    a.bc_n = d_chunks_ + 2 * nfc_ + nbc_;
+    a.fpart = d_bfp_;
+    a.bpart = d_bbp_;
+    a.fcnt = d_cnt_;
+    a.bcnt = d_cnt_ + nfc_;
+    a.sync = d_sync_;
+    a.b = d_bin_;
+    a.out = d_bout_;
+    a.skip = skip;
+    cudaMemsetAsync(d_sync_, 0, sizeof(int) * (sync_ints_ - 1), st);
+    // rows of bw_ doubles: a narrower block runs padded to the buffers' width
+    if (bw_ == 8)
+        launch_bsolve<8>(a, n_, nr, B, ldb, X, ldx, d_bin_, d_bout_, bgrid_, bsmem_, st);
+    else if (bw_ == 16)
+        launch_bsolve<16>(a, n_, nr, B, ldb, X, ldx, d_bin_, d_bout_, bgrid_, bsmem_, st);
+    else
+        launch_bsolve<32>(a, n_, nr, B, ldb, X, ldx, d_bin_, d_bout_, bgrid_, bsmem_, st);
+    return 0;
 }
 
 template <> int *MultifrontalPlanT<Real>::error_word() const { return d_sync_ ? d_sync_ + (sync_ints_ - 1) : nullptr; }

@@ -63,6 +63,16 @@ public:
     // does nothing (refinement steps that are no longer needed).
     void solve(const double *b, double *x, cudaStream_t st, const int *skip = nullptr);
 
+    // X = (A + shift I)^{-1} B for nr <= 32 right-hand sides at once: B and X
+    // are column-major n x nr device arrays in the original order (leading
+    // dimensions ldb, ldx).  One persistent launch runs the same task queue
+    // as solve() with every vector entry widened to nr columns, so the panel
+    // and the level structure are paid once for all columns.  `skip` as in
+    // solve().  Returns 0 or a negative code (device buffers for the block
+    // are allocated on first use).
+    int solve_block(const double *B, int64_t ldb, double *X, int64_t ldx, int nr,
+                    cudaStream_t st, const int *skip = nullptr);
+
     void release(cudaStream_t st);
 
     // device word set when a solve's dependency wait gave up (0 otherwise)
@@ -108,6 +118,14 @@ private:
     double *d_u_ = nullptr, *d_yf_ = nullptr, *d_x_ = nullptr;
     int *d_status_ = nullptr;
     double *d_params_ = nullptr;     // shift, pivot tolerance (read by the graph)
+    // block solve: rows of bw_ doubles (8, 16 or 32) for the right-hand
+    // sides, the result, yf, x, the update vectors and the chunk partials
+    int bw_ = 0;
+    int32_t fslots_ = 0, bslots_ = 0;
+    double *d_bin_ = nullptr, *d_bout_ = nullptr, *d_byf_ = nullptr, *d_bx_ = nullptr,
+           *d_bu_ = nullptr, *d_bfp_ = nullptr, *d_bbp_ = nullptr;
+    int bgrid_ = 0;
+    size_t bsmem_ = 0;
     cudaGraphExec_t fgraph_ = nullptr;
     bool use_side_ = false;                    // some front has >= 2 column blocks
     cudaStream_t fside_ = nullptr;             // second branch of the factor graph
@@ -130,6 +148,9 @@ using MultifrontalPlan32 = MultifrontalPlanT<float>;
                                                     cudaStream_t);                         \
     template <> void MultifrontalPlanT<R>::solve(const double *, double *, cudaStream_t,   \
                                                  const int *);                            \
+    template <> int MultifrontalPlanT<R>::solve_block(const double *, int64_t, double *,   \
+                                                      int64_t, int, cudaStream_t,         \
+                                                      const int *);                       \
     template <> void MultifrontalPlanT<R>::release(cudaStream_t);                          \
     template <> int *MultifrontalPlanT<R>::error_word() const;                             \
     template <> int64_t MultifrontalPlanT<R>::solve_bytes() const;                         \

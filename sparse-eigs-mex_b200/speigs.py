@@ -43,14 +43,14 @@ class Info(ctypes.Structure):
 class ExtOpts(ctypes.Structure):
     """speigs_ext_opts (include/speigs_b200.h): operator precision, start subspace."""
     _fields_ = [("precision", c_int), ("refine_max", c_int), ("refine_tol", c_double),
-                ("warm", c_void_p), ("warm_cols", c_int64)]
+                ("warm", c_void_p), ("warm_cols", c_int64), ("block", c_int)]
 
 
 class ExtInfo(ctypes.Structure):
     """speigs_ext_info (include/speigs_b200.h)."""
     _fields_ = [("precision", c_int), ("refine_steps", c_int64), ("factor_solves", c_int64),
-                ("warm_cols", c_int64), ("t_checks", c_double), ("t_setup", c_double),
-                ("t_release", c_double)]
+                ("warm_cols", c_int64), ("block", c_int), ("block_solves", c_int64),
+                ("t_checks", c_double), ("t_setup", c_double), ("t_release", c_double)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -76,6 +76,8 @@ _EXT_SIGNATURES = {
     "speigs_plan_solve_device": (c_int, [c_void_p, c_int64, c_void_p, c_void_p, c_void_p,
                                          POINTER(Info)]),
     "speigs_plan_apply_device": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "speigs_plan_apply_block_device": (c_int, [c_void_p, c_void_p, c_int64, c_void_p, c_int64,
+                                               c_int]),
     "speigs_plan_factor": (c_int, [c_void_p, _DP]),
     "speigs_plan_stream": (c_void_p, [c_void_p]),
     "speigs_plan_costs": (c_int, [c_void_p, _DP, _DP, _DP]),
@@ -297,6 +299,10 @@ class Plan:
 
     def apply_device(self, x_ptr, y_ptr):
         return self.lib.speigs_plan_apply_device(self.h, x_ptr, y_ptr)
+
+    def apply_block_device(self, x_ptr, ldx, y_ptr, ldy, nr):
+        """Y = Op X for nr <= 32 device columns (column-major, leading dims ldx, ldy)."""
+        return self.lib.speigs_plan_apply_block_device(self.h, x_ptr, ldx, y_ptr, ldy, nr)
 
     def factor(self):
         s = c_double()

@@ -86,8 +86,10 @@ def test_ref5_diagonal(pkg, lib):
     assert abs(abs(lam[0]) - 1.0) < 1e-12 and abs(abs(lam[3]) - 4.0) < 1e-12
 
 
-@pytest.mark.xfail(strict=True, reason="indefinite LU route is not on the device yet")
 def test_ref6_indefinite_lu(pkg, lib):
+    """A - cI with c between two eigenvalues (reference test_indefinite,
+    test/test_speigs.c:177-205): the indefinite route, converged, the k
+    eigenvalues nearest zero to 1e-7."""
     A = pkg.workloads.lap3d(12).tolil()
     ex = pkg.workloads.spectrum3d(12)
     mid = len(ex) // 2
@@ -95,8 +97,28 @@ def test_ref6_indefinite_lu(pkg, lib):
         mid += 1
     c = 0.5 * (ex[mid] + ex[mid + 1])
     A = (A - c * sp.identity(A.shape[0])).tocsc()
-    rc, lam, V, res, info = call(pkg, lib, A, 4, vectors=False)
-    assert rc == 0 and info["path"] == pkg.speigs.PATH_LU
+    k = 4
+    rc, lam, V, res, info = call(pkg, lib, A, k)
+    assert rc == 0 and info["path"] == pkg.speigs.PATH_LU and info["shift"] == 0.0
+    assert info["flag"] == 0
+    near = np.sort(np.abs(ex - c))[:k]
+    assert np.all(np.abs(np.abs(lam) - near) <= 1e-7 * np.maximum(1.0, near))
+    r = np.linalg.norm(A @ V - V * lam, axis=0)
+    assert r.max() <= 1e-8
+
+
+def test_ref7_singular_shift(pkg, lib):
+    """A - cI with c exactly an eigenvalue, maxit 40 (reference
+    test_pathological, test/test_speigs.c:207-227): returns cleanly, finds
+    the near-zero eigenvalue and reports partial convergence."""
+    A = pkg.workloads.lap3d(12)
+    ex = pkg.workloads.spectrum3d(12)
+    c = ex[len(ex) // 2]
+    A = (A - c * sp.identity(A.shape[0])).tocsc()
+    rc, lam, V, res, info = call(pkg, lib, A, 3, vectors=False, maxit=40)
+    assert rc == 0
+    assert abs(lam[0]) < 1e-6
+    assert info["flag"] == 1
 
 
 def test_ref8_blocks(pkg, lib):
@@ -123,10 +145,10 @@ def test_ref9_banded_1d(pkg, lib):
     assert np.all(np.abs(lam - ex) <= 1e-9 * np.maximum(1e-6, np.abs(ex)))
 
 
-@pytest.mark.xfail(strict=True, reason="the banded route is not on the device yet")
 def test_ref9_banded_route(pkg, lib):
     """The reference takes its banded route on the 1-D Laplacian
-    (test/test_speigs.c:289 asserts SPEIGS_PATH_BANDED)."""
+    (test/test_speigs.c:289 asserts SPEIGS_PATH_BANDED); so does the device
+    library, with the same gate (RCM bandwidth, band size and occupancy)."""
     A = pkg.workloads.lap1d(20000)
     rc, lam, V, res, info = call(pkg, lib, A, 4, vectors=False)
     assert rc == 0 and info["path"] == pkg.speigs.PATH_BANDED
@@ -243,3 +265,19 @@ def test_parity_varcoef_lm(pkg, lib, ref_lib):
     eigenvalues come in triples, whose discovery depends on rounding)."""
     A = pkg.workloads.varcoef3d(20, seed=5)
     _parity(pkg, lib, ref_lib, A, 6, 1)
+
+
+@pytest.mark.parametrize("N,band_max", [(40, 0), (40, 20), (60, 0)])
+def test_parity_banded_gate_lap2d(pkg, lib, ref_lib, N, band_max):
+    """2-D Laplacians whose RCM band passes or fails the reference's gate
+    (band_max 0 = the default 512; 20 rejects a 40-wide band): the same
+    route as the reference, and its eigenvalues."""
+    A = pkg.workloads.lap2d(N)
+    k = 6
+    rc, lam, V, res, info = call(pkg, lib, A, k, tol=1e-10, band_max=band_max)
+    rr, rlam, rV, rres, rinfo = call(pkg, ref_lib, A, k, tol=1e-10, band_max=band_max)
+    assert rc == 0 and rr == 0
+    assert info["path"] == rinfo["path"]
+    assert np.max(np.abs(lam - rlam) / np.abs(rlam)) <= 1e-12
+    ex = pkg.workloads.spectrum2d_extreme(N, k, False)
+    assert np.max(np.abs(lam - ex) / ex) <= 1e-12

@@ -8,11 +8,6 @@ The failures allowed here are named one by one, each with its reason:
 * [4] 'largest[3] vs analytic': the third copy of a triple eigenvalue is
   found by single-vector Lanczos only when rounding seeds it before
   convergence; the reference compiled here misses it too.
-* [6] and [7] (every check): the indefinite LU route is not on the device
-  yet; the library returns SPEIGS_ERR_FACTOR there.
-* [9] 'took the banded path': the banded route is not on the device yet;
-  the band is factored by the supernodal Cholesky and reported as
-  shift-invert (its eigenvalue checks must pass).
 Any other failing check fails this test.
 """
 import os
@@ -26,8 +21,8 @@ from conftest import ORACLE_DIR
 pytestmark = pytest.mark.gpu
 
 SUITE = os.path.join(ORACLE_DIR, "_ref", "test_speigs_b200")
-ALLOWED = {("[4]", "largest[3] vs analytic"), ("[9]", "took the banded path")}
-ALLOWED_SECTIONS = {"[6]", "[7]"}
+ALLOWED = {("[4]", "largest[3] vs analytic")}
+ALLOWED_SECTIONS = set()
 
 
 def _run_suite():

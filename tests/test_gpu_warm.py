@@ -1,30 +1,34 @@
-"""Start subspace for the thick-restart Lanczos (speigs_ext_opts.warm): the
-start vector is formed from an orthonormal basis of the subspace (plus a
-small share of the reference's random start).  The answer must not depend on
-the start (same eigenpairs as the random start, residual bound met); a start
-that already contains the wanted eigenvectors must need far fewer operator
-applications."""
+"""Start subspace for the thick-restart Lanczos (speigs_ext_opts.warm), in
+both of its uses: as the first block of the block method (block = 0, the
+default with a start subspace) and folded into the single-vector method's
+start vector (block = -1: the normalised sum of an orthonormal basis of the
+subspace plus a small share of the reference's random start).  The answer
+must not depend on the start (same eigenpairs as the random start, residual
+bound met); a start that already contains the wanted eigenvectors must need
+far fewer operator applications."""
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
 
 
-def _solve(pkg, lib, A, k, warm=None, mixed=False):
+def _solve(pkg, lib, A, k, warm=None, mixed=False, block=0):
     s = pkg.speigs
     o = s.default_opts(lib, tol=1e-10)
-    e = s.ext_opts(lib, precision=s.MIXED if mixed else s.FP64)
+    e = s.ext_opts(lib, precision=s.MIXED if mixed else s.FP64, block=block)
     return s.speigs_ex(A, k, s.SM, o, e, lib=lib, warm=warm)
 
 
-def test_exact_subspace_converges_at_once(lib, pkg):
+@pytest.mark.parametrize("block", [0, -1])
+def test_exact_subspace_converges_at_once(lib, pkg, block):
     A = pkg.workloads.varcoef3d(20, seed=9)
     k = 8
     rc, lam, V, res, info, ei = _solve(pkg, lib, A, k)
     assert rc == 0 and info["flag"] == 0 and ei["warm_cols"] == 0
     rng = np.random.default_rng(1)
     Y = V + 1e-9 * rng.standard_normal(V.shape)
-    rc2, lam2, V2, res2, info2, ei2 = _solve(pkg, lib, A, k, warm=Y)
+    rc2, lam2, V2, res2, info2, ei2 = _solve(pkg, lib, A, k, warm=Y, block=block)
+    assert ei2["block"] == (k if block == 0 else 0)
     assert rc2 == 0 and info2["flag"] == 0
     assert ei2["warm_cols"] == k
     assert info2["restarts"] <= 1
@@ -34,14 +38,14 @@ def test_exact_subspace_converges_at_once(lib, pkg):
     assert r.max() <= 1e-10 * info2["anorm"] * 1.0001
 
 
-@pytest.mark.parametrize("mixed", [False, True])
-def test_laplace_mode_start_same_answer(lib, pkg, mixed):
+@pytest.mark.parametrize("mixed,block", [(False, 0), (True, 0), (False, -1), (True, -1)])
+def test_laplace_mode_start_same_answer(lib, pkg, mixed, block):
     N, k = 16, 8
     w = pkg.workloads
     A = w.grf3d(N, seed=1001)
     rc, lam, V, res, info, _ = _solve(pkg, lib, A, k, mixed=mixed)
     Y = w.laplace_modes(N, k + 6)
-    rc2, lam2, V2, res2, info2, ei2 = _solve(pkg, lib, A, k, warm=Y, mixed=mixed)
+    rc2, lam2, V2, res2, info2, ei2 = _solve(pkg, lib, A, k, warm=Y, mixed=mixed, block=block)
     assert rc == 0 and rc2 == 0 and info2["flag"] == 0
     assert ei2["warm_cols"] == k + 6
     assert np.max(np.abs(lam2 - lam) / np.abs(lam)) <= 1e-10
@@ -49,12 +53,13 @@ def test_laplace_mode_start_same_answer(lib, pkg, mixed):
     assert r.max() <= 1e-10 * info2["anorm"] * 1.0001
 
 
-def test_dependent_columns_are_dropped(lib, pkg):
+@pytest.mark.parametrize("block", [0, -1])
+def test_dependent_columns_are_dropped(lib, pkg, block):
     A = pkg.workloads.lap3d(12)
     k = 4
     Y = pkg.workloads.laplace_modes(12, 6)
     Y = np.concatenate([Y, Y[:, :2] * 3.0, np.zeros((A.shape[0], 1))], axis=1)
-    rc, lam, V, res, info, ei = _solve(pkg, lib, A, k, warm=Y)
+    rc, lam, V, res, info, ei = _solve(pkg, lib, A, k, warm=Y, block=block)
     assert rc == 0 and info["flag"] == 0
     assert ei["warm_cols"] == 6
     ex = pkg.workloads.spectrum3d(12)[:k]
