@@ -20,9 +20,11 @@ namespace spx {
 
 // ------------------------------------------------------------------ SpMV --
 // One block per 128 consecutive rows.  When the block's nonzeros fit in
-// shared memory the products are formed with fully coalesced loads and each
-// thread then sums its own row from shared memory (CSR-stream); otherwise a
-// warp walks each row.
+// shared memory the products are formed with fully coalesced vector loads --
+// a pair of values (16 bytes) and a pair of column indices (8 bytes) per
+// thread and step, after at most one leading entry that puts the pairs on
+// their 16-byte boundary -- and each thread then sums its own row from
+// shared memory (CSR-stream); otherwise a warp walks each row.
 constexpr int kSpmvRows = 128;
 constexpr int kSpmvCap = 2048;
 
@@ -36,8 +38,21 @@ spmv_kernel(int n, const int32_t *__restrict__ rp, const int32_t *__restrict__ c
     const int p0 = rp[r0], p1 = rp[r1];
     const int cnt = p1 - p0;
     if (cnt <= kSpmvCap) {
-        for (int q = threadIdx.x; q < cnt; q += blockDim.x)
-            prod[q] = va[p0 + q] * __ldg(x + ci[p0 + q]);
+        // entries [p0, p1): an odd p0 is done alone, then aligned pairs, then
+        // an odd last entry alone
+        const int head = p0 & 1;
+        const int npair = (cnt - head) >> 1;
+        if (threadIdx.x == 0 && head && cnt > 0) prod[0] = va[p0] * __ldg(x + ci[p0]);
+        const double2 *va2 = reinterpret_cast<const double2 *>(va + p0 + head);
+        const int2 *ci2 = reinterpret_cast<const int2 *>(ci + p0 + head);
+        for (int t = threadIdx.x; t < npair; t += blockDim.x) {
+            const double2 v = va2[t];
+            const int2 c = ci2[t];
+            prod[head + 2 * t] = v.x * __ldg(x + c.x);
+            prod[head + 2 * t + 1] = v.y * __ldg(x + c.y);
+        }
+        const int last = head + 2 * npair;
+        if (threadIdx.x == 0 && last < cnt) prod[last] = va[p0 + last] * __ldg(x + ci[p0 + last]);
         __syncthreads();
         const int r = r0 + threadIdx.x;
         if (r < r1) {
