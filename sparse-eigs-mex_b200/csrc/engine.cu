@@ -1568,6 +1568,99 @@ int device_krylov(HostCSR &A, int64_t k, speigs_which which, const speigs_opts &
     return rc;
 }
 
+// -------------------------------------------------- Hermitian recovery --
+__global__ void times_i_kernel(int n, const double *w, double *dst) {
+    // dst = i w in the real embedding: [x; y] -> [-y; x]
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        dst[i] = -w[n + i];
+        dst[n + i] = w[i];
+    }
+}
+
+int device_hermitian_recover(int64_t n64, int64_t kk, int64_t k, const double *V2,
+                             const double *lam2, const double *res2, double *lambda, double *Vr,
+                             double *Vi, double *resid, int64_t *nacc_out) {
+    g_err[0] = 0;
+    if (2 * n64 > INT32_MAX) return SPEIGS_ERR_ARG;
+    const int n = (int)n64, n2 = 2 * n;
+    Stream stream;
+    if (stream.err != cudaSuccess) return cuda_fail(stream.err, "stream");
+    cudaStream_t st = stream.s;
+    int64_t nacc = 0;
+    std::vector<int64_t> src;   // candidate column behind each accepted vector
+    {
+        Arena ar(st);
+        const int64_t ldq = ((int64_t)n2 + 31) & ~(int64_t)31;
+        double *C = ar.alloc<double>((size_t)n2 * kk);           // the candidates
+        double *Q = ar.alloc<double>((size_t)ldq * 2 * k);       // accepted u, i u pairs
+        double *w = ar.alloc<double>(ldq);
+        double *h1 = ar.alloc<double>(2 * k + 1), *h2 = ar.alloc<double>(2 * k + 1);
+        double *nrm2 = ar.alloc<double>(4);
+        const int nblk = (n2 + 511) / 512 + 1;
+        ReduceScratch rs;
+        rs.part = ar.alloc<double>((size_t)nblk * (2 * k + 2));
+        rs.counter = ar.alloc<unsigned>(1);
+        rs.max_blocks = nblk;
+        rs.max_cols = (int)(2 * k + 2);
+        double *hn = pinned_scalars(16);
+        if (ar.failed || !hn) return SPEIGS_ERR_MEM;
+        cudaMemsetAsync(rs.counter, 0, sizeof(unsigned), st);
+        copy_async(C, V2, sizeof(double) * (size_t)n2 * kk, cudaMemcpyHostToDevice, st);
+        auto read_nrm = [&](double *out) -> int {
+            copy_async(hn, nrm2, sizeof(double), cudaMemcpyDeviceToHost, st);
+            cudaError_t e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) return cuda_fail(e, "hermitian recovery");
+            *out = std::sqrt(hn[0]);
+            return 0;
+        };
+        for (int64_t c = 0; c < kk && nacc < k; c++) {
+            // the candidate [a; b] as a unit complex vector a + i b
+            launch_copy(n2, C + (size_t)c * n2, w, st);
+            launch_ts_norm(n2, w, nrm2, rs, st);
+            double nr = 0.0;
+            if (int e = read_nrm(&nr)) return e;
+            if (!(nr > 0.0)) continue;
+            launch_scale_by_invnorm(n2, w, nrm2, w, st);
+            // complex Gram-Schmidt against the accepted u = real Gram-Schmidt
+            // against u and i u, twice
+            const int m = (int)(2 * nacc);
+            if (m > 0) {
+                launch_ts_dot(Q, ldq, n2, m, w, h1, nullptr, 0, rs, st);
+                launch_ts_update_dot(Q, ldq, n2, m, w, h1, h2, nullptr, 0, rs, st);
+                launch_ts_update_norm(Q, ldq, n2, m, w, h2, nrm2, rs, st);
+            } else {
+                launch_ts_norm(n2, w, nrm2, rs, st);
+            }
+            double wn = 0.0;
+            if (int e = read_nrm(&wn)) return e;
+            if (wn <= 0.1) continue;   // a complex multiple of an accepted vector
+            double *u = Q + (size_t)(2 * nacc) * ldq;
+            launch_scale_by_invnorm(n2, w, nrm2, u, st);
+            times_i_kernel<<<std::max(1, std::min(1024, (n + 255) / 256)), 256, 0, st>>>(
+                n, u, u + ldq);
+            note_launch();
+            src.push_back(c);
+            nacc++;
+        }
+        for (int64_t a = 0; a < nacc; a++) {
+            const double *u = Q + (size_t)(2 * a) * ldq;
+            if (Vr) copy_async(Vr + (size_t)a * n, u, sizeof(double) * n, cudaMemcpyDeviceToHost, st);
+            if (Vi) copy_async(Vi + (size_t)a * n, u + n, sizeof(double) * n,
+                               cudaMemcpyDeviceToHost, st);
+        }
+        cudaError_t e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return cuda_fail(e, "hermitian recovery");
+    }
+    for (int64_t a = 0; a < nacc; a++) {
+        lambda[a] = lam2[src[a]];
+        if (resid) resid[a] = res2[src[a]];
+    }
+    if (Vr) memset(Vr + (size_t)nacc * n, 0, sizeof(double) * (size_t)(k - nacc) * n);
+    if (Vi) memset(Vi + (size_t)nacc * n, 0, sizeof(double) * (size_t)(k - nacc) * n);
+    *nacc_out = nacc;
+    return SPEIGS_OK;
+}
+
 // ------------------------------------------------------------ diag path --
 __global__ void absbits_kernel(int n, const double *d, unsigned long long *key, int *idx) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {

@@ -71,6 +71,18 @@ int device_dense_path(const HostCSR &A, int64_t k, speigs_which which, double *l
 int  current_device();
 void use_device(int dev);
 
+// Complex eigenvectors from the real 2n x 2n embedding of a Hermitian
+// matrix: V2 (host, 2n x kk column-major) holds the embedded eigenvectors
+// in speigs() order; each candidate [a; b] is taken as a + i b, made
+// orthogonal on the device to the vectors already accepted (complex
+// Gram-Schmidt, twice) and kept when its norm stays above 0.1 -- the
+// candidates dropped are complex multiples of accepted ones.  Up to k
+// vectors are accepted: lambda/resid (host) from lam2/res2, Vr/Vi (host,
+// n x k; may be NULL) their real and imaginary parts, zero past *nacc.
+int device_hermitian_recover(int64_t n, int64_t kk, int64_t k, const double *V2,
+                             const double *lam2, const double *res2, double *lambda, double *Vr,
+                             double *Vi, double *resid, int64_t *nacc);
+
 // Thread-local text of the last CUDA failure seen by the engine.
 const char *last_cuda_error();
 

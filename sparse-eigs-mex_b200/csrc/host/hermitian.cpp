@@ -1,16 +1,63 @@
-// Complex Hermitian entry point through the real 2n x 2n embedding
-// [[R, -S], [S, R]] (reference speigs_z, src/speigs_core.c:660-768).  The
-// embedded real problem runs through speigs() on the device; this file builds
-// the embedding and recovers the complex eigenvectors, dropping the i-multiple
-// duplicates by complex Gram-Schmidt (the reference's :708-757).
-#include "../../../include/speigs.h"
+// Complex Hermitian entry point through the real embedding (reference
+// speigs_z, src/speigs_core.c:660-768).  For A = R + i S (R symmetric, S
+// skew-symmetric) the real 2n x 2n matrix E = [[R, -S], [S, R]] is
+// symmetric, and A (x + i y) = lambda (x + i y) exactly when E [x; y] =
+// lambda [x; y]; every eigenvalue of A appears twice in E, through [x; y]
+// and i (x + i y) = [-y; x].  The embedded problem runs through speigs() on
+// the device (every route: diagonal, dense, components, banded, Krylov), and
+// the complex eigenvectors are recovered on the device as well, the second
+// copy of each eigenvalue dropped by complex Gram-Schmidt
+// (spx::device_hermitian_recover).
+#include "../engine.h"
 
-#include <math.h>
 #include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
 #include <vector>
+
+namespace {
+
+// E in CSC with the numerically nonzero entries only: column j of E is
+// [R(:, j); S(:, j)] and column n + j is [-S(:, j); R(:, j)].  Each column's
+// length is counted first; then both halves of every column are written at
+// their offsets in one pass over the input.
+void embed(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *Axr, const double *Axi,
+           std::vector<int64_t> &Ep, std::vector<int64_t> &Ei, std::vector<double> &Ex) {
+    Ep.assign(2 * n + 1, 0);
+    std::vector<int64_t> nr(n), ns(n);
+    for (int64_t j = 0; j < n; j++) {
+        int64_t r = 0, s = 0;
+        for (int64_t q = Ap[j]; q < Ap[j + 1]; q++) {
+            r += Axr[q] != 0.0;
+            s += Axi[q] != 0.0;
+        }
+        nr[j] = r;
+        ns[j] = s;
+        Ep[j + 1] = r + s;        // column j
+        Ep[n + j + 1] = r + s;    // column n + j
+    }
+    for (int64_t c = 0; c < 2 * n; c++) Ep[c + 1] += Ep[c];
+    Ei.assign(std::max<int64_t>(Ep[2 * n], 1), 0);
+    Ex.assign(std::max<int64_t>(Ep[2 * n], 1), 0.0);
+    for (int64_t j = 0; j < n; j++) {
+        int64_t a = Ep[j], b = Ep[j] + nr[j];          // column j: R block, then S block
+        int64_t c = Ep[n + j], d = Ep[n + j] + ns[j];  // column n + j: -S block, then R block
+        for (int64_t q = Ap[j]; q < Ap[j + 1]; q++) {
+            const int64_t i = Ai[q];
+            if (Axr[q] != 0.0) {
+                Ei[a] = i;     Ex[a++] = Axr[q];
+                Ei[d] = n + i; Ex[d++] = Axr[q];
+            }
+            if (Axi[q] != 0.0) {
+                Ei[b] = n + i; Ex[b++] = Axi[q];
+                Ei[c] = i;     Ex[c++] = -Axi[q];
+            }
+        }
+    }
+}
+
+}  // namespace
 
 extern "C" int speigs_z(speigs_int n, const speigs_int *Ap, const speigs_int *Ai,
                         const double *Axr, const double *Axi, speigs_int k, speigs_which which,
@@ -20,72 +67,19 @@ extern "C" int speigs_z(speigs_int n, const speigs_int *Ap, const speigs_int *Ai
     speigs_info li;
     if (!info) info = &li;
     if (n <= 0 || k <= 0 || k > n || !Ap || !Ai || !Axr || !lambda) return SPEIGS_ERR_ARG;
-    const int64_t n2 = 2 * n, nnz = Ap[n];
-    int64_t nzR = 0, nzS = 0;
-    for (int64_t q = 0; q < nnz; q++) { nzR += (Axr[q] != 0.0); nzS += (Axi[q] != 0.0); }
-    const int64_t nz2 = 2 * (nzR + nzS);
-    std::vector<int64_t> Bp(n2 + 1), Bi(nz2 ? nz2 : 1);
-    std::vector<double> Bx(nz2 ? nz2 : 1);
-    int64_t t = 0;
-    for (int64_t j = 0; j < n; j++) {            // column j: [R; S]
-        Bp[j] = t;
-        for (int64_t q = Ap[j]; q < Ap[j + 1]; q++)
-            if (Axr[q] != 0.0) { Bi[t] = Ai[q]; Bx[t] = Axr[q]; t++; }
-        for (int64_t q = Ap[j]; q < Ap[j + 1]; q++)
-            if (Axi[q] != 0.0) { Bi[t] = n + Ai[q]; Bx[t] = Axi[q]; t++; }
-    }
-    for (int64_t j = 0; j < n; j++) {            // column n+j: [-S; R]
-        Bp[n + j] = t;
-        for (int64_t q = Ap[j]; q < Ap[j + 1]; q++)
-            if (Axi[q] != 0.0) { Bi[t] = Ai[q]; Bx[t] = -Axi[q]; t++; }
-        for (int64_t q = Ap[j]; q < Ap[j + 1]; q++)
-            if (Axr[q] != 0.0) { Bi[t] = n + Ai[q]; Bx[t] = Axr[q]; t++; }
-    }
-    Bp[n2] = t;
-    // every eigenvalue of A appears twice in the embedding
-    const int64_t kk = std::min<int64_t>(2 * k + 2, n2);
+    std::vector<int64_t> Ep, Ei;
+    std::vector<double> Ex;
+    embed(n, Ap, Ai, Axr, Axi, Ep, Ei, Ex);
+    // each wanted eigenvalue appears twice in the embedding: ask for 2k + 2
+    const int64_t n2 = 2 * n, kk = std::min<int64_t>(2 * k + 2, n2);
     std::vector<double> lam2(kk), res2(kk), V2((size_t)n2 * kk);
-    int rc = speigs(n2, Bp.data(), Bi.data(), Bx.data(), kk, which, opts, lam2.data(), V2.data(),
+    int rc = speigs(n2, Ep.data(), Ei.data(), Ex.data(), kk, which, opts, lam2.data(), V2.data(),
                     res2.data(), info);
     if (rc) return rc;
-    std::vector<double> ar((size_t)n * k, 0.0), ai((size_t)n * k, 0.0), wr(n), wi(n);
     int64_t nacc = 0;
-    for (int64_t c = 0; c < kk && nacc < k; c++) {
-        const double *a = V2.data() + (size_t)c * n2, *b = a + n;
-        double nr = 0.0;
-        for (int64_t i = 0; i < n; i++) nr += a[i] * a[i] + b[i] * b[i];
-        if (nr <= 0.0) continue;
-        nr = 1.0 / sqrt(nr);
-        for (int64_t i = 0; i < n; i++) { wr[i] = a[i] * nr; wi[i] = b[i] * nr; }
-        for (int pass = 0; pass < 2; pass++)
-            for (int64_t u = 0; u < nacc; u++) {
-                const double *ur = ar.data() + (size_t)u * n, *ui = ai.data() + (size_t)u * n;
-                double re = 0.0, im = 0.0;   // <u, w> = sum conj(u) w
-                for (int64_t i = 0; i < n; i++) {
-                    re += ur[i] * wr[i] + ui[i] * wi[i];
-                    im += ur[i] * wi[i] - ui[i] * wr[i];
-                }
-                for (int64_t i = 0; i < n; i++) {
-                    const double xr = ur[i], xi = ui[i];
-                    wr[i] -= re * xr - im * xi;
-                    wi[i] -= re * xi + im * xr;
-                }
-            }
-        double wn = 0.0;
-        for (int64_t i = 0; i < n; i++) wn += wr[i] * wr[i] + wi[i] * wi[i];
-        wn = sqrt(wn);
-        if (wn <= 0.1) continue;   // an i-multiple of an accepted vector
-        const double inv = 1.0 / wn;
-        for (int64_t i = 0; i < n; i++) {
-            ar[(size_t)nacc * n + i] = wr[i] * inv;
-            ai[(size_t)nacc * n + i] = wi[i] * inv;
-        }
-        lambda[nacc] = lam2[c];
-        if (resid) resid[nacc] = res2[c];
-        nacc++;
-    }
-    if (Vr) memcpy(Vr, ar.data(), (size_t)n * k * sizeof(double));
-    if (Vi) memcpy(Vi, ai.data(), (size_t)n * k * sizeof(double));
+    rc = spx::device_hermitian_recover(n, kk, k, V2.data(), lam2.data(), res2.data(), lambda, Vr,
+                                       Vi, resid, &nacc);
+    if (rc) return rc;
     info->nconv = nacc;
     if (nacc < k) info->flag = 1;
     return SPEIGS_OK;
