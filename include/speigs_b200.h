@@ -227,6 +227,24 @@ int speigs_b200_syev_small(int m, const double *H, double *theta, double *S, int
 int speigs_b200_syev_small_noalloc(int m, const double *H, double *theta, double *S, int *ord,
                                    int *status, void *stream);
 
+/* Factorization cache of speigs() / speigs_ex() (opt-in; off by default).
+ * With entries > 0 the device-resident plans -- the matrix, its symbolic
+ * analysis and its numeric factor -- of the last `entries` distinct
+ * operators that reached the Krylov route are kept, keyed by the matrix's
+ * contents (the symmetric matrix of its upper triangle, compared in full),
+ * the route, the factor options (ordering, shift0), the precision and the
+ * current device.  A later call on the same operator skips the analysis and
+ * the factorization (speigs_info t_analyze is then 0 and t_factor ~0); the
+ * Lanczos options (k, tol, ncv, maxit, seed) may differ between calls.  The
+ * kept plans hold device memory until they are evicted (least recently used
+ * first) or the cache is resized; entries = 0 releases them all.  Calls on
+ * other threads that want an entry in use build their own plan.  The
+ * reference documents this cache as a planned feature (docs/REQUIREMENTS.md);
+ * its speigs.h has no counterpart.  Returns SPEIGS_OK or SPEIGS_ERR_ARG. */
+int speigs_b200_factor_cache(int entries);
+/* Plans currently kept by the factorization cache. */
+int speigs_b200_factor_cache_size(void);
+
 /* Process-wide counts since the library was loaded: kernels this library
  * launched, and bytes it copied host->device and device->host. */
 void speigs_b200_counters(long long *launches, long long *h2d_bytes, long long *d2h_bytes);

@@ -1172,6 +1172,7 @@ struct speigs_plan_s {
     double *d_va = nullptr;
     spx::Factor mf;
     bool banded = false;              // reported as the reference's banded route
+    bool reuse_factor = false;        // factor cache hit: the numeric factor is current
     bool lu = false;                  // indefinite route: the dense inverse below
     double *d_ainv = nullptr;         // n x n, allocated on first use
     spx::RefineState refine;          // mixed precision only
@@ -1391,7 +1392,7 @@ static int plan_solve(speigs_plan_s *p, int64_t k, double *lambda, double *V, do
     if (k <= 0 || k > n) return SPEIGS_ERR_ARG;
     info->anorm = p->anorm;
     info->ncomp = 0;
-    info->t_analyze = p->t_analyze;
+    info->t_analyze = p->reuse_factor ? 0.0 : p->t_analyze;
     DevA dA{n, p->d_rp, p->d_ci, p->d_va};
     SpmvOperator spmv_op(dA);
     CholOperator chol_op(&p->mf);
@@ -1402,7 +1403,7 @@ static int plan_solve(speigs_plan_s *p, int64_t k, double *lambda, double *V, do
         info->path = SPEIGS_PATH_DIRECT;
     } else {
         const double tf = wall();
-        int rc = plan_factor(p, stats);
+        int rc = (p->reuse_factor && p->factored) ? 0 : plan_factor(p, stats);
         info->t_factor = wall() - tf;
         if (rc) return rc;
         mixed_op.shift = p->shift;
@@ -1544,28 +1545,187 @@ static void fill_ext_info(const speigs_plan_s *p, speigs_ext_info *e) {
                                                                      p->last_block : 0;
 }
 
+// ------------------------------------------------------ factor cache --
+// Opt-in, process-wide: the device plans (matrix, symbolic analysis, numeric
+// factor) of the last `capacity` distinct operators the Krylov route saw,
+// so a parameter sweep or a continuation loop over one matrix skips the
+// analysis and the factorization (the reference's planned cache keyed by
+// matrix contents).  The key is the full symmetric CSR built from the
+// caller's upper triangle, the route ('sm'/'lm'), the factor options
+// (ordering, shift0), the precision and the device; a 64-bit hash finds
+// candidates and the arrays are then compared in full.  An entry in use by
+// one call is not shared with a concurrent one (that call builds its own
+// plan).  Least recently used entries are released first.
+namespace {
+
+struct CacheEntry {
+    uint64_t hash = 0;
+    int dev = 0, which = 0, precision = 0, ordering = 0;
+    double shift0 = 0.0;
+    speigs_plan_s *plan = nullptr;
+    bool busy = false;
+    uint64_t last_use = 0;
+};
+
+struct FactorCache {
+    std::mutex mu;
+    int capacity = 0;
+    uint64_t clock = 0;
+    std::vector<CacheEntry> entries;
+};
+
+FactorCache &factor_cache() {
+    static FactorCache *c = new FactorCache;   // kept for the process's life
+    return *c;
+}
+
+uint64_t mix64(uint64_t h, uint64_t v) {
+    h ^= v + 0x9e3779b97f4a7c15ULL + (h << 6) + (h >> 2);
+    return h;
+}
+
+uint64_t csr_hash(const HostCSR &A) {
+    uint64_t h = mix64(0, (uint64_t)A.n);
+    const int64_t nnz = A.nnz();
+    for (int32_t i = 0; i <= A.n; i++) h = mix64(h, (uint64_t)A.rowptr[i]);
+    for (int64_t q = 0; q < nnz; q++) {
+        uint64_t bits;
+        memcpy(&bits, &A.val[q], sizeof bits);
+        h = mix64(mix64(h, (uint64_t)(uint32_t)A.col[q]), bits);
+    }
+    return h;
+}
+
+bool same_csr(const HostCSR &a, const HostCSR &b) {
+    if (a.n != b.n || a.nnz() != b.nnz()) return false;
+    const int64_t nnz = a.nnz();
+    return memcmp(a.rowptr, b.rowptr, sizeof(int64_t) * ((size_t)a.n + 1)) == 0 &&
+           memcmp(a.col, b.col, sizeof(int32_t) * (size_t)nnz) == 0 &&
+           memcmp(a.val, b.val, sizeof(double) * (size_t)nnz) == 0;
+}
+
+void evict_over_capacity(FactorCache &fc, std::vector<speigs_plan_s *> &drop) {
+    for (;;) {
+        int idle = 0;
+        for (auto &e : fc.entries) idle += !e.busy;
+        if ((int)fc.entries.size() <= fc.capacity || idle == 0) return;
+        size_t victim = fc.entries.size();
+        for (size_t i = 0; i < fc.entries.size(); i++)
+            if (!fc.entries[i].busy &&
+                (victim == fc.entries.size() || fc.entries[i].last_use < fc.entries[victim].last_use))
+                victim = i;
+        drop.push_back(fc.entries[victim].plan);
+        fc.entries.erase(fc.entries.begin() + (long)victim);
+    }
+}
+
+}  // namespace
+
 int device_krylov(HostCSR &A, int64_t k, speigs_which which, const speigs_opts &o,
                   double anorm, double *lambda, double *V, double *resid, speigs_info *info,
                   EngineStats *stats, const speigs_ext_opts *ext, speigs_ext_info *einfo,
                   bool banded) {
+    FactorCache &fc = factor_cache();
+    int cap = 0;
+    {
+        std::lock_guard<std::mutex> lk(fc.mu);
+        cap = fc.capacity;
+    }
+    const int precision = (which == SPEIGS_SM && ext && ext->precision == SPEIGS_B200_MIXED)
+                              ? SPEIGS_B200_MIXED : SPEIGS_B200_FP64;
+    const int dev = current_device();
+    uint64_t key = 0;
     speigs_plan_s *p = nullptr;
+    if (cap > 0) {
+        key = csr_hash(A);
+        std::lock_guard<std::mutex> lk(fc.mu);
+        for (auto &e : fc.entries)
+            if (!e.busy && e.hash == key && e.dev == dev && e.which == (int)which &&
+                e.precision == precision && e.ordering == o.ordering && e.shift0 == o.shift0 &&
+                same_csr(e.plan->A, A)) {
+                e.busy = true;
+                e.last_use = ++fc.clock;
+                p = e.plan;
+                break;
+            }
+    }
     const double t0 = wall();
-    int rc = plan_from_csr(A, which, o, anorm, ext, &p);
-    if (rc) return rc;
-    const double t_setup = wall() - t0 - p->t_analyze;
+    double t_setup = 0.0;
+    if (p) {
+        // a cache hit: the caller's copy of the matrix is not needed
+        free_csr(&A);
+        p->opts = o;
+        p->anorm = anorm;
+        p->reuse_factor = true;
+    } else {
+        int rc = plan_from_csr(A, which, o, anorm, ext, &p);
+        if (rc) return rc;
+        t_setup = wall() - t0 - p->t_analyze;
+    }
     p->ext_warm = ext ? ext->warm : nullptr;
     p->ext_warm_cols = ext ? ext->warm_cols : 0;
     p->ext_block = ext ? ext->block : 0;
     p->banded = banded;
-    rc = plan_solve(p, k, lambda, V, resid, info, false, stats);
+    int rc = plan_solve(p, k, lambda, V, resid, info, false, stats);
     fill_ext_info(p, einfo);
     const double t1 = wall();
-    speigs_plan_destroy(p);
+    std::vector<speigs_plan_s *> drop;
+    bool keep = false;
+    if (cap > 0 && rc == 0 && p->factored) {
+        std::lock_guard<std::mutex> lk(fc.mu);
+        p->reuse_factor = true;
+        bool found = false;
+        for (auto &e : fc.entries)
+            if (e.plan == p) { e.busy = false; e.last_use = ++fc.clock; found = true; }
+        if (!found) {
+            CacheEntry e;
+            e.hash = key;
+            e.dev = dev;
+            e.which = (int)which;
+            e.precision = precision;
+            e.ordering = o.ordering;
+            e.shift0 = o.shift0;
+            e.plan = p;
+            e.last_use = ++fc.clock;
+            fc.entries.push_back(e);
+        }
+        keep = true;
+        evict_over_capacity(fc, drop);
+    } else if (cap > 0) {
+        // a failed solve leaves no entry behind
+        std::lock_guard<std::mutex> lk(fc.mu);
+        for (size_t i = 0; i < fc.entries.size(); i++)
+            if (fc.entries[i].plan == p) {
+                fc.entries.erase(fc.entries.begin() + (long)i);
+                break;
+            }
+    }
+    if (!keep) speigs_plan_destroy(p);
+    for (speigs_plan_s *q : drop) speigs_plan_destroy(q);
     if (einfo) {
         einfo->t_setup = t_setup;
         einfo->t_release = wall() - t1;
     }
     return rc;
+}
+
+int factor_cache_configure(int entries) {
+    if (entries < 0) return SPEIGS_ERR_ARG;
+    FactorCache &fc = factor_cache();
+    std::vector<speigs_plan_s *> drop;
+    {
+        std::lock_guard<std::mutex> lk(fc.mu);
+        fc.capacity = entries;
+        evict_over_capacity(fc, drop);
+    }
+    for (speigs_plan_s *q : drop) speigs_plan_destroy(q);
+    return SPEIGS_OK;
+}
+
+int factor_cache_size() {
+    FactorCache &fc = factor_cache();
+    std::lock_guard<std::mutex> lk(fc.mu);
+    return (int)fc.entries.size();
 }
 
 // -------------------------------------------------- Hermitian recovery --
@@ -2027,6 +2187,10 @@ int speigs_b200_syev_small(int m, const double *H, double *theta, double *S, int
     if (!rc && hst[0] < 0) rc = SPEIGS_ERR_LAPACK;
     return rc;
 }
+
+int speigs_b200_factor_cache(int entries) { return spx::factor_cache_configure(entries); }
+
+int speigs_b200_factor_cache_size(void) { return spx::factor_cache_size(); }
 
 const char *speigs_b200_last_error(void) { return spx::last_cuda_error(); }
 

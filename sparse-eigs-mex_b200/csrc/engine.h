@@ -83,6 +83,10 @@ int device_hermitian_recover(int64_t n, int64_t kk, int64_t k, const double *V2,
                              const double *lam2, const double *res2, double *lambda, double *Vr,
                              double *Vi, double *resid, int64_t *nacc);
 
+// The factorization cache of the Krylov route (speigs_b200_factor_cache).
+int factor_cache_configure(int entries);
+int factor_cache_size();
+
 // Thread-local text of the last CUDA failure seen by the engine.
 const char *last_cuda_error();
 

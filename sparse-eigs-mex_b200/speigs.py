@@ -96,6 +96,8 @@ _EXT_SIGNATURES = {
     "speigs_b200_syev_small": (c_int, [c_int, _DP, _DP, _DP, POINTER(c_int)]),
     "speigs_b200_syev_small_noalloc": (c_int, [c_int, c_void_p, c_void_p, c_void_p, c_void_p,
                                                c_void_p, c_void_p]),
+    "speigs_b200_factor_cache": (c_int, [c_int]),
+    "speigs_b200_factor_cache_size": (c_int, []),
     "speigs_b200_last_error": (c_char_p, []),
     "speigs_b200_counters": (None, [POINTER(ctypes.c_longlong)] * 3),
 }
