@@ -14,6 +14,7 @@
 #include "kernels/multifrontal.cuh"
 #include "kernels/block_krylov.cuh"
 #include "kernels/dense_lu.cuh"
+#include "kernels/seg_lanczos.cuh"
 #include "counters.h"
 
 #include <cuda_runtime.h>
@@ -1726,6 +1727,252 @@ int factor_cache_size() {
     FactorCache &fc = factor_cache();
     std::lock_guard<std::mutex> lk(fc.mu);
     return (int)fc.entries.size();
+}
+
+// ---------------------------------------------------- batched Lanczos --
+// Many components in lockstep (speigs_batched).  A is the full CSR of the
+// components' block-diagonal matrix with component c on rows [off[c],
+// off[c+1]); one plan holds the whole forest: one analysis, one
+// factorization, and every operator application is one solve (or SpMV) for
+// all components.  The step pair (operator, segmented Gram-Schmidt step) is
+// captured once into a CUDA graph and replayed; the host reads the
+// per-component state once per restart cycle.
+int device_batched_krylov(HostCSR &A, int nseg, const int32_t *off_h, int64_t k,
+                          speigs_which which, const speigs_opts &o, const double *anorm_h,
+                          double *lam_out, double *res_out, double *X_out, int64_t *nconv_out,
+                          int64_t *nops_out, int64_t *restarts_out, int *flag_out,
+                          BatchedStats *bst) {
+    g_err[0] = 0;
+    const int n = A.n;
+    double amax = 1.0;
+    for (int c = 0; c < nseg; c++) amax = std::max(amax, anorm_h[c]);
+    // per-component basis size by the reference's rules
+    int ncv = 0;
+    std::vector<int> mh(nseg);
+    for (int c = 0; c < nseg; c++) {
+        const int64_t nc = off_h[c + 1] - off_h[c];
+        int64_t v = o.ncv ? o.ncv : std::max<int64_t>(2 * k + 1, 20);
+        if (v > nc) v = nc;
+        if (v <= k) v = std::min<int64_t>(nc, k + 1);
+        if (v < 2) v = std::min<int64_t>(nc, 2);
+        mh[c] = (int)v;
+        ncv = std::max(ncv, (int)v);
+    }
+    if (ncv > syev_small_smem_limit() || ncv > 128) { free_csr(&A); return 1; }
+    const std::vector<int> m0 = mh;
+    const int64_t maxit = o.maxit ? o.maxit : 300;
+    const double tol = o.tol > 0 ? o.tol : 1e-14;
+    const double t0 = wall();
+    speigs_plan_s *p = nullptr;
+    int rc = plan_from_csr(A, which, o, amax, nullptr, &p);
+    if (rc) return rc;
+    struct PlanGuard {
+        speigs_plan_s *p;
+        ~PlanGuard() { speigs_plan_destroy(p); }
+    } guard{p};
+    if (bst) bst->t_analyze = p->t_analyze;
+    cudaStream_t st = p->stream.s;
+    if (which == SPEIGS_SM) {
+        const double tf = wall();
+        rc = plan_factor(p, nullptr);
+        if (bst) bst->t_factor = wall() - tf;
+        if (rc) return rc == SPEIGS_ERR_FACTOR ? 1 : rc;
+        // a shifted or indefinite forest goes component by component (each
+        // component takes its own shift in the reference)
+        if (p->shift != 0.0 || p->lu) return 1;
+    }
+    const double ti = wall();
+    Arena ar(st);
+    SegArgs a;
+    a.nseg = nseg;
+    a.ncv = ncv;
+    a.k = (int)k;
+    a.l = (int)std::min<int64_t>(k + 5, ncv - 1);
+    a.ldv = ((int64_t)n + 31) & ~(int64_t)31;
+    int32_t *d_off = ar.alloc<int32_t>(nseg + 1);
+    a.off = d_off;
+    a.V = ar.alloc<double>((size_t)a.ldv * (ncv + 1));
+    a.Vn = ar.alloc<double>((size_t)a.ldv * (ncv + 1));
+    a.H = ar.alloc<double>((size_t)nseg * ncv * ncv);
+    a.theta = ar.alloc<double>((size_t)nseg * ncv);
+    a.S = ar.alloc<double>((size_t)nseg * ncv * ncv);
+    a.ord = ar.alloc<int>((size_t)nseg * ncv);
+    int *d_jst = ar.alloc<int>((size_t)2 * nseg);
+    a.j = ar.alloc<int>(nseg);
+    a.m = ar.alloc<int>(nseg);
+    a.ext = ar.alloc<int>(nseg);
+    a.live = ar.alloc<int>(nseg);
+    a.ops = ar.alloc<int>(nseg);
+    a.stop = ar.alloc<int>(nseg);
+    a.nconv = ar.alloc<int>(nseg);
+    a.seed = ar.alloc<uint64_t>(nseg);
+    double *d_bthr = ar.alloc<double>(nseg), *d_rtol = ar.alloc<double>(nseg);
+    a.bthr = d_bthr;
+    a.rtol = d_rtol;
+    a.x = ar.alloc<double>(a.ldv);
+    a.w = ar.alloc<double>(a.ldv);
+    a.X = ar.alloc<double>((size_t)a.ldv * k);
+    a.AX = ar.alloc<double>((size_t)a.ldv * k);
+    a.lam = ar.alloc<double>((size_t)nseg * k);
+    a.r2 = ar.alloc<double>((size_t)nseg * k);
+    a.err = ar.alloc<int>(1);
+    uint64_t *d_jt = ar.alloc<uint64_t>(64 * 64);
+    a.jt = d_jt;
+    if (ar.failed) return SPEIGS_ERR_MEM;
+    {
+        std::vector<double> bt(nseg), rt(nseg);
+        for (int c = 0; c < nseg; c++) {
+            bt[c] = 1e-13 * std::max(anorm_h[c], 1.0);
+            rt[c] = tol * std::max(anorm_h[c], 1.0);
+        }
+        copy_async(d_off, off_h, sizeof(int32_t) * (nseg + 1), cudaMemcpyHostToDevice, st);
+        copy_async(a.m, mh.data(), sizeof(int) * nseg, cudaMemcpyHostToDevice, st);
+        copy_async(d_bthr, bt.data(), sizeof(double) * nseg, cudaMemcpyHostToDevice, st);
+        copy_async(d_rtol, rt.data(), sizeof(double) * nseg, cudaMemcpyHostToDevice, st);
+        copy_async(d_jt, rng_jump_table(), sizeof(uint64_t) * 64 * 64, cudaMemcpyHostToDevice, st);
+        cudaMemsetAsync(a.err, 0, sizeof(int), st);
+        cudaMemsetAsync(a.X, 0, sizeof(double) * (size_t)a.ldv * k, st);
+        cudaMemsetAsync(a.x, 0, sizeof(double) * (size_t)a.ldv, st);
+        cudaError_t e = cudaStreamSynchronize(st);   // the host vectors die here
+        if (e != cudaSuccess) return cuda_fail(e, "batched set-up");
+    }
+    const uint64_t seed = o.seed ? o.seed : 88172645463325252ULL;
+    launch_seg_start(a, seed, st);
+
+    // one step for every component: w = Op x, then the segmented step
+    DevA dA{n, p->d_rp, p->d_ci, p->d_va};
+    auto issue_step = [&]() {
+        if (which == SPEIGS_SM) p->mf.solve(a.x, a.w, st);
+        else launch_spmv(n, dA.rp, dA.ci, dA.va, a.x, a.w, st);
+        launch_seg_step(a, st);
+    };
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    struct GraphGuard {
+        cudaGraph_t &g;
+        cudaGraphExec_t &x;
+        ~GraphGuard() {
+            if (x) cudaGraphExecDestroy(x);
+            if (g) cudaGraphDestroy(g);
+        }
+    } gg{graph, gexec};
+    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+        issue_step();
+        if (cudaStreamEndCapture(st, &graph) != cudaSuccess ||
+            cudaGraphInstantiate(&gexec, graph, 0) != cudaSuccess) {
+            cudaGetLastError();
+            gexec = nullptr;
+        }
+    } else {
+        cudaGetLastError();
+    }
+    const int *op_err = (which == SPEIGS_SM) ? p->mf.error_word() : nullptr;
+    std::vector<int> jh(nseg, 0), liveh(nseg, 1), nconvh(nseg, 0), jsth(2 * nseg);
+    std::vector<int64_t> resth(nseg, 0);
+    std::vector<double> lamh((size_t)nseg * k, 0.0), r2h((size_t)nseg * k, 0.0);
+    std::vector<double> lam_last((size_t)nseg * k, 0.0), r2_last((size_t)nseg * k, 0.0);
+    std::vector<int> nwant_last(nseg, 0);
+    int herr[2] = {0, 0};
+    auto sync_read = [&](const char *where) -> int {
+        copy_async(&herr[0], a.err, sizeof(int), cudaMemcpyDeviceToHost, st);
+        if (op_err) copy_async(&herr[1], op_err, sizeof(int), cudaMemcpyDeviceToHost, st);
+        cudaError_t e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return cuda_fail(e, where);
+        if (herr[0]) { set_last_error_text("a start vector has zero norm"); return SPEIGS_ERR_INTERNAL; }
+        if (herr[1]) {
+            set_last_error_text("operator application failed: a solve dependency wait ran out");
+            return SPEIGS_ERR_INTERNAL;
+        }
+        return 0;
+    };
+    int64_t restarts = 0, steps_total = 0;
+    for (;;) {
+        int nsteps = 0;
+        for (int c = 0; c < nseg; c++)
+            if (liveh[c]) nsteps = std::max(nsteps, mh[c] - jh[c]);
+        for (int sidx = 0; sidx < nsteps; sidx++) {
+            if (gexec) {
+                if (cudaGraphLaunch(gexec, st) != cudaSuccess)
+                    return cuda_fail(cudaGetLastError(), "batched step");
+                note_launch(2);
+            } else {
+                issue_step();
+            }
+        }
+        steps_total += nsteps;
+        // projected eigenproblems, Ritz vectors, true residuals of every live component
+        launch_syev_batched(nseg, ncv, a.m, a.H, ncv, (int64_t)ncv * ncv, a.theta, a.S, a.ord,
+                            d_jst, a.live, st);
+        launch_seg_ritz(a, st);
+        for (int64_t t = 0; t < k; t++)
+            launch_spmv(n, dA.rp, dA.ci, dA.va, a.X + (size_t)t * a.ldv, a.AX + (size_t)t * a.ldv,
+                        st);
+        launch_seg_resid(a, st);
+        copy_async(nconvh.data(), a.nconv, sizeof(int) * nseg, cudaMemcpyDeviceToHost, st);
+        copy_async(mh.data(), a.m, sizeof(int) * nseg, cudaMemcpyDeviceToHost, st);
+        copy_async(jsth.data(), d_jst, sizeof(int) * 2 * nseg, cudaMemcpyDeviceToHost, st);
+        copy_async(lamh.data(), a.lam, sizeof(double) * nseg * k, cudaMemcpyDeviceToHost, st);
+        copy_async(r2h.data(), a.r2, sizeof(double) * nseg * k, cudaMemcpyDeviceToHost, st);
+        if (int e = sync_read("batched check")) return e;
+        int nlive = 0;
+        for (int c = 0; c < nseg; c++) {
+            if (!liveh[c]) continue;
+            if (jsth[2 * c] < 0) return SPEIGS_ERR_LAPACK;
+            const int nw = (int)std::min<int64_t>(k, mh[c]);
+            nwant_last[c] = nw;
+            for (int t = 0; t < nw; t++) {
+                lam_last[(size_t)c * k + t] = lamh[(size_t)c * k + t];
+                r2_last[(size_t)c * k + t] = r2h[(size_t)c * k + t];
+            }
+            // the reference stops at convergence, at maxit, or when the basis
+            // ended early (m < ncv)
+            const bool done = nconvh[c] >= nw || restarts >= maxit || mh[c] < m0[c];
+            if (done) liveh[c] = 0;
+            else nlive++;
+        }
+        if (nlive == 0) break;
+        restarts++;
+        for (int c = 0; c < nseg; c++)
+            if (liveh[c]) resth[c]++;
+        copy_async(a.live, liveh.data(), sizeof(int) * nseg, cudaMemcpyHostToDevice, st);
+        launch_seg_restart(a, st);
+        copy_async(jh.data(), a.j, sizeof(int) * nseg, cudaMemcpyDeviceToHost, st);
+        copy_async(liveh.data(), a.live, sizeof(int) * nseg, cudaMemcpyDeviceToHost, st);
+        if (int e = sync_read("batched restart")) return e;
+        bool any = false;
+        for (int c = 0; c < nseg; c++) any |= liveh[c] != 0;
+        if (!any) break;
+    }
+    // results in Lanczos order, as the reference leaves them; the caller sorts
+    std::vector<int> opsh(nseg);
+    copy_async(opsh.data(), a.ops, sizeof(int) * nseg, cudaMemcpyDeviceToHost, st);
+    if (X_out)
+        for (int64_t t = 0; t < k; t++)
+            copy_async(X_out + (size_t)t * n, a.X + (size_t)t * a.ldv, sizeof(double) * n,
+                       cudaMemcpyDeviceToHost, st);
+    if (int e = sync_read("batched results")) return e;
+    for (int c = 0; c < nseg; c++) {
+        const int nw = nwant_last[c];
+        int conv = 0;
+        for (int t = 0; t < k; t++) {
+            const double r = t < nw ? std::sqrt(r2_last[(size_t)c * k + t]) : 0.0;
+            lam_out[(size_t)c * k + t] = t < nw ? lam_last[(size_t)c * k + t] : 0.0;
+            if (res_out) res_out[(size_t)c * k + t] = r;
+            if (t < nw && r <= tol * std::max(anorm_h[c], 1.0)) conv++;
+        }
+        nconv_out[c] = conv;
+        nops_out[c] = opsh[c];
+        restarts_out[c] = resth[c];
+        flag_out[c] = conv >= nw ? 0 : 1;
+    }
+    if (bst) {
+        bst->t_iter = wall() - ti;
+        bst->steps = steps_total;
+        bst->cycles = restarts + 1;
+        bst->graph = gexec != nullptr;
+        bst->t_total = wall() - t0;
+    }
+    return SPEIGS_OK;
 }
 
 // -------------------------------------------------- Hermitian recovery --

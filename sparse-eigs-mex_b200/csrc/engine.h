@@ -83,6 +83,24 @@ int device_hermitian_recover(int64_t n, int64_t kk, int64_t k, const double *V2,
                              const double *lam2, const double *res2, double *lambda, double *Vr,
                              double *Vi, double *resid, int64_t *nacc);
 
+// Many components in lockstep: A is the CSR of their block-diagonal matrix
+// with component c on rows [off[c], off[c+1]) (host, consumed); anorm[c] is
+// ||A_c||_1.  Per component c: lam_out/res_out[c*k .. c*k+k) in Lanczos
+// order (zero past min(k, its basis)), nconv/nops/restarts/flag; X_out (host,
+// n x k column-major, may be NULL) the Ritz vectors on each component's rows.
+// Returns 0, a negative code, or 1 when the forest needs a shift or the
+// indefinite route (solve those components one by one instead).
+struct BatchedStats {
+    double t_analyze = 0, t_factor = 0, t_iter = 0, t_total = 0;
+    int64_t steps = 0, cycles = 0;
+    bool graph = false;
+};
+int device_batched_krylov(HostCSR &A, int nseg, const int32_t *off, int64_t k,
+                          speigs_which which, const speigs_opts &o, const double *anorm,
+                          double *lam_out, double *res_out, double *X_out, int64_t *nconv_out,
+                          int64_t *nops_out, int64_t *restarts_out, int *flag_out,
+                          BatchedStats *bst);
+
 // The factorization cache of the Krylov route (speigs_b200_factor_cache).
 int factor_cache_configure(int entries);
 int factor_cache_size();

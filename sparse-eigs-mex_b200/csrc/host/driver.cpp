@@ -290,11 +290,18 @@ struct CompResult {
 int solve_components(const int64_t *Ap, const int64_t *Ai, const double *Ax,
                      const std::vector<int64_t> &comp, const CompSplit &sp, int64_t k,
                      speigs_which which, const speigs_opts *opts, const speigs_ext_opts *ext,
-                     bool want_vec, std::vector<CompResult> &out) {
-    const int64_t nc_all = sp.ncomp;
-    out.assign(nc_all, CompResult());
-    std::vector<int64_t> order(nc_all);
-    for (int64_t c = 0; c < nc_all; c++) order[c] = c;
+                     bool want_vec, std::vector<CompResult> &out,
+                     const std::vector<int64_t> *subset = nullptr) {
+    if ((int64_t)out.size() != sp.ncomp) out.assign(sp.ncomp, CompResult());
+    std::vector<int64_t> order;
+    if (subset) {
+        order = *subset;
+    } else {
+        order.resize(sp.ncomp);
+        for (int64_t c = 0; c < sp.ncomp; c++) order[c] = c;
+    }
+    const int64_t nc_all = (int64_t)order.size();
+    if (nc_all == 0) return 0;
     std::stable_sort(order.begin(), order.end(),
                      [&](int64_t a, int64_t b) { return sp.sz[a] > sp.sz[b]; });
     std::atomic<int> err{0};
@@ -332,6 +339,96 @@ int solve_components(const int64_t *Ap, const int64_t *Ai, const double *Ax,
     spx::run_pool(nc_all, nth, [dev] { spx::use_device(dev); }, solve_one,
                   [&] { return err.load() != 0; });
     return err.load();
+}
+
+// The components in `kry` (Krylov route, each connected and larger than the
+// dense gate) solved together by the segmented lockstep Lanczos: their rows
+// become contiguous segments, largest component first, of one
+// block-diagonal matrix whose full CSR is built from the upper triangle as
+// for a single call.  Results land in out[c] as solve_components leaves
+// them (sorted by |lambda|, vectors on the component's rows).  Returns 0, a
+// negative code, or 1 when these components must be solved one by one.
+int batched_krylov(const int64_t *Ap, const int64_t *Ai, const double *Ax,
+                   const std::vector<int64_t> &comp, const CompSplit &sp,
+                   std::vector<int64_t> kry, int64_t k, speigs_which which,
+                   const speigs_opts &o, bool want_vec, std::vector<CompResult> &out) {
+    std::stable_sort(kry.begin(), kry.end(),
+                     [&](int64_t a, int64_t b) { return sp.sz[a] > sp.sz[b]; });
+    const int nseg = (int)kry.size();
+    std::vector<int32_t> off(nseg + 1, 0);
+    for (int q = 0; q < nseg; q++) off[q + 1] = off[q] + (int32_t)sp.sz[kry[q]];
+    const int64_t ng = off[nseg];
+    // group CSC: segment q's column jl is the component's jl-th row (original order)
+    std::vector<int64_t> Gp(ng + 1, 0), Gi;
+    std::vector<double> Gx;
+    std::vector<double> anorm(nseg, 0.0), colsum;
+    for (int q = 0; q < nseg; q++) {
+        const int64_t c = kry[q], nc = sp.sz[c];
+        colsum.assign(nc, 0.0);
+        for (int64_t jl = 0; jl < nc; jl++) {
+            const int64_t g = off[q] + jl, gc = sp.gidx[sp.off[c] + jl];
+            Gp[g] = (int64_t)Gi.size();
+            for (int64_t e = Ap[gc]; e < Ap[gc + 1]; e++) {
+                const int64_t r = Ai[e];
+                if (comp[r] != c) continue;
+                const int64_t rl = sp.loc[r];
+                Gi.push_back(off[q] + rl);
+                Gx.push_back(Ax[e]);
+                // ||A_c||_1 of the symmetric matrix of the upper triangle
+                if (rl <= jl) {
+                    colsum[jl] += fabs(Ax[e]);
+                    if (rl != jl) colsum[rl] += fabs(Ax[e]);
+                }
+            }
+        }
+        double mx = 0.0;
+        for (double v : colsum) mx = std::max(mx, v);
+        anorm[q] = mx > 0 ? mx : 1.0;
+    }
+    Gp[ng] = (int64_t)Gi.size();
+    HostCSR A;
+    int rc = spx::build_full_csr(ng, Gp.data(), Gi.data(), Gx.data(), &A);
+    if (rc) return rc;
+    std::vector<double> lam((size_t)nseg * k), res((size_t)nseg * k);
+    std::vector<double> X(want_vec ? (size_t)ng * k : 0);
+    std::vector<int64_t> nconv(nseg), nops(nseg), rst(nseg);
+    std::vector<int> flag(nseg);
+    spx::BatchedStats bst;
+    rc = spx::device_batched_krylov(A, nseg, off.data(), k, which, o, anorm.data(), lam.data(),
+                                    res.data(), want_vec ? X.data() : nullptr, nconv.data(),
+                                    nops.data(), rst.data(), flag.data(), &bst);
+    if (rc) return rc;
+    for (int q = 0; q < nseg; q++) {
+        const int64_t c = kry[q], nc = sp.sz[c];
+        CompResult &R = out[c];
+        R.kc = std::min(k, nc);
+        // sort by |lambda| as speigs() does: ascending 'sm', descending 'lm'
+        std::vector<int64_t> idx(R.kc);
+        for (int64_t t = 0; t < R.kc; t++) idx[t] = t;
+        const double *lq = lam.data() + (size_t)q * k;
+        std::stable_sort(idx.begin(), idx.end(), [&](int64_t a, int64_t b) {
+            return which == SPEIGS_SM ? fabs(lq[a]) < fabs(lq[b]) : fabs(lq[a]) > fabs(lq[b]);
+        });
+        R.lam.assign(R.kc, 0.0);
+        R.res.assign(R.kc, 0.0);
+        if (want_vec) R.vec.assign((size_t)nc * R.kc, 0.0);
+        for (int64_t t = 0; t < R.kc; t++) {
+            R.lam[t] = lq[idx[t]];
+            R.res[t] = res[(size_t)q * k + idx[t]];
+            if (want_vec)
+                memcpy(R.vec.data() + (size_t)t * nc, X.data() + (size_t)idx[t] * ng + off[q],
+                       sizeof(double) * nc);
+        }
+        memset(&R.info, 0, sizeof R.info);
+        R.info.nconv = nconv[q];
+        R.info.nops = nops[q];
+        R.info.restarts = rst[q];
+        R.info.flag = flag[q];
+        R.info.anorm = anorm[q];
+        R.info.path = which == SPEIGS_SM ? SPEIGS_PATH_SHIFTINV : SPEIGS_PATH_DIRECT;
+        memset(&R.einfo, 0, sizeof R.einfo);
+    }
+    return 0;
 }
 
 // Solve every component separately and merge by |lambda| (reference
@@ -470,8 +567,25 @@ int speigs_batched(speigs_int n, const speigs_int *Ap, const speigs_int *Ai, con
     speigs_opts o2 = *opts;
     o2.check_sym = 0;
     o2.dense_max = 64;
-    std::vector<CompResult> cr;
-    int rc = solve_components(Ap, Ai, Ax, cv, sp, k, which, &o2, ext, V != nullptr, cr);
+    std::vector<CompResult> cr(ncomp);
+    // Components that take the Krylov route (larger than the dense gate) are
+    // solved together in lockstep by the segmented Lanczos; the others, and
+    // all of them when the forest needs a shift or an extension option asks
+    // for another operator, one per host thread.
+    std::vector<int64_t> kry, rest;
+    const bool seg_ok = !ext || (ext->precision == SPEIGS_B200_FP64 && !ext->warm && ext->block <= 0);
+    for (int64_t c = 0; c < ncomp; c++) {
+        const int64_t nc = sp.sz[c];
+        const bool dense = nc <= o2.dense_max || 4 * k > nc;
+        if (seg_ok && nc > 1 && !dense) kry.push_back(c);
+        else rest.push_back(c);
+    }
+    if (!kry.empty()) {
+        int rcs = batched_krylov(Ap, Ai, Ax, cv, sp, kry, k, which, o2, V != nullptr, cr);
+        if (rcs < 0) return rcs;
+        if (rcs == 1) rest.insert(rest.end(), kry.begin(), kry.end());
+    }
+    int rc = solve_components(Ap, Ai, Ax, cv, sp, k, which, &o2, ext, V != nullptr, cr, &rest);
     if (rc) return rc;
     memset(lambda, 0, sizeof(double) * (size_t)ncomp * k);
     if (resid) memset(resid, 0, sizeof(double) * (size_t)ncomp * k);

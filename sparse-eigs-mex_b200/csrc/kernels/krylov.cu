@@ -545,6 +545,8 @@ static const JumpTable &jump_table() {
     return T;
 }
 
+const uint64_t *rng_jump_table() { return &jump_table().col[0][0]; }
+
 uint64_t rng_advance(uint64_t seed, uint64_t steps) {
     const JumpTable &T = jump_table();
     for (int b = 0; b < 64; b++)
@@ -611,9 +613,8 @@ void launch_rand_vec(int n, uint64_t seed, double *v, cudaStream_t st) {
 // returns) and an index list by |theta| descending, stable among ties.
 constexpr int kJacThreads = 256;
 
-__global__ void __launch_bounds__(kJacThreads)
-jacobi_kernel(int m, const double *__restrict__ H, int ldh, double *theta, double *Sout,
-              int *ord, double *gwork, int *status, int use_smem) {
+__device__ void jacobi_body(int m, const double *__restrict__ H, int ldh, double *theta,
+                            double *Sout, int *ord, double *gwork, int *status, int use_smem) {
     extern __shared__ double sm[];
     const int me = (m + 1) & ~1;              // even size (a dummy index when m is odd)
     const int half = me / 2;
@@ -739,6 +740,26 @@ jacobi_kernel(int m, const double *__restrict__ H, int ldh, double *theta, doubl
     }
 }
 
+__global__ void __launch_bounds__(kJacThreads)
+jacobi_kernel(int m, const double *__restrict__ H, int ldh, double *theta, double *Sout,
+              int *ord, double *gwork, int *status, int use_smem) {
+    jacobi_body(m, H, ldh, theta, Sout, ord, gwork, status, use_smem);
+}
+
+// One problem per block: problem b (of order mvec[b] when mvec is given,
+// else m) reads H + b * strideH and writes theta, S (ld its order), ord and
+// status at b * m, b * m * m, b * m and b * 2; active[b] == 0 skips it.
+__global__ void __launch_bounds__(kJacThreads)
+jacobi_batched_kernel(int m, const int *mvec, const double *__restrict__ H, int ldh,
+                      int64_t strideH, double *theta, double *Sout, int *ord, int *status,
+                      const int *active) {
+    const int b = blockIdx.x;
+    if (active && !active[b]) return;
+    const int mb = mvec ? mvec[b] : m;
+    jacobi_body(mb, H + (size_t)b * strideH, ldh, theta + (size_t)b * m,
+                Sout + (size_t)b * m * m, ord + (size_t)b * m, nullptr, status + 2 * b, 1);
+}
+
 static size_t jac_small_bytes(int m) {
     size_t me = (size_t)((m + 1) & ~1);
     return sizeof(double) * (2 * me * me + me) + sizeof(int) * (me + 2);
@@ -760,6 +781,19 @@ void launch_syev_small(int m, const double *H, int ldh, double *theta, double *S
         cudaFuncSetAttribute(jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem);
     jacobi_kernel<<<1, kJacThreads, smem, st>>>(m, H, ldh, theta, S, ord, work, status, use_smem);
+    note_launch();
+}
+
+void launch_syev_batched(int nprob, int m, const int *mvec, const double *H, int ldh,
+                         int64_t strideH, double *theta, double *S, int *ord, int *status,
+                         const int *active, cudaStream_t st) {
+    if (nprob <= 0 || m <= 0) return;
+    const size_t smem = jac_small_bytes(m);
+    if (smem > 48 * 1024)
+        cudaFuncSetAttribute(jacobi_batched_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+    jacobi_batched_kernel<<<nprob, kJacThreads, smem, st>>>(m, mvec, H, ldh, strideH, theta, S,
+                                                            ord, status, active);
     note_launch();
 }
 

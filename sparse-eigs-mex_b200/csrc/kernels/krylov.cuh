@@ -58,6 +58,9 @@ void launch_rayleigh_resid(int n, int nvec, const double *X, int64_t ldx, const 
 void launch_rand_vec(int n, uint64_t seed, double *v, cudaStream_t st);
 // State after `steps` draws (host, exact jump-ahead).
 uint64_t rng_advance(uint64_t seed, uint64_t steps);
+// The jump table behind it (host, 64 x 64 words: entry [b][j] is M^(2^b) e_j
+// for the xorshift64* state update M), for kernels that jump on the device.
+const uint64_t *rng_jump_table();
 
 // Projected eigenproblem: symmetric m x m matrix H (column-major, ld = ldh)
 // -> theta[m] ascending, eigenvectors S (m x m, ld = m), and ord[m]: the
@@ -67,6 +70,14 @@ uint64_t rng_advance(uint64_t seed, uint64_t steps);
 void launch_syev_small(int m, const double *H, int ldh, double *theta, double *S, int *ord,
                        double *work, int *status, cudaStream_t st);
 int syev_small_smem_limit();
+// The same eigensolver on nprob problems at once, one block each: problem b
+// has order mvec[b] (or m when mvec is null; every order <= m <=
+// syev_small_smem_limit()), reads H + b * strideH (leading dimension ldh)
+// and writes theta[b*m ..], S[b*m*m ..] (ld its order), ord[b*m ..] and
+// status[2b]; problems with active[b] == 0 are skipped (active may be null).
+void launch_syev_batched(int nprob, int m, const int *mvec, const double *H, int ldh,
+                         int64_t strideH, double *theta, double *S, int *ord, int *status,
+                         const int *active, cudaStream_t st);
 // Same eigensolver, always keeping its two m x m matrices in the caller's
 // global workspace `work` (>= 2*m_even^2 doubles); shared memory holds only
 // the rotation parameters.

@@ -1,7 +1,9 @@
 """Batched components: k eigenpairs of every connected component
-(speigs_batched), checked per component against a dense CPU eigensolver, and
-the drop-in blocks route (which now solves the components concurrently)
-against the compiled reference."""
+(speigs_batched), checked per component against a dense CPU eigensolver; the
+components on the Krylov route go through the segmented lockstep Lanczos, and
+a forest that needs a shift falls back to one solve per component.  The
+drop-in blocks route (components solved concurrently, one per host thread)
+is checked against the compiled reference."""
 import numpy as np
 import pytest
 
@@ -67,3 +69,46 @@ def test_batched_rejects_bad_labels(lib, pkg):
     comp[0] = 5      # a label past ncomp - 1 leaves components empty
     rc, *_ = s.speigs_batched(A, 2, s.SM, comp=comp, lib=lib)
     assert rc == s.ERR_ARG
+
+
+def test_batched_singular_component_falls_back(lib, pkg):
+    """A singular PSD component (a Neumann Laplacian) needs its own shift, as
+    in the reference's per-component call: the answer is the per-component
+    one, zero eigenvalue included."""
+    s, w = pkg.speigs, pkg.workloads
+    A1, A2 = w.lap3d(7, dirichlet=False), w.lap3d(6)
+    A = w.block_diag(A1, A2)
+    k = 4
+    o = s.default_opts(lib, tol=1e-10)
+    rc, lam, V, res, nv, info = s.speigs_batched(A, k, s.SM, o, vectors=True, lib=lib)
+    assert rc == 0 and info["flag"] == 0 and info["ncomp"] == 2
+    ex1 = w.spectrum3d(7, dirichlet=False)[:k]
+    ex2 = w.spectrum3d(6)[:k]
+    assert abs(lam[0, 0]) <= 1e-9
+    assert np.all(np.abs(lam[0, 1:] - ex1[1:]) <= 1e-9 * ex1[1:])
+    assert np.all(np.abs(lam[1] - ex2) <= 1e-12 * ex2)
+
+
+def test_batched_matches_one_call_per_component(lib, pkg):
+    """The segmented lockstep Lanczos against the per-component drop-in
+    (speigs() on each component alone): the same eigenvalues to 1e-12 and
+    the residual bound on every component."""
+    s, w = pkg.speigs, pkg.workloads
+    A = w.rgg_blocks(4096, seed=4, first=24)
+    k = 4
+    o = s.default_opts(lib, tol=1e-10)
+    ncomp, comp = s.components(A, lib)
+    rc, lam, V, res, nv, info = s.speigs_batched(A, k, s.SM, o, comp=comp, vectors=True, lib=lib)
+    assert rc == 0 and info["flag"] == 0
+    Ad = A.tocsr()
+    for c in range(ncomp):
+        rows = np.flatnonzero(comp == c)
+        if len(rows) <= 64:
+            continue
+        Ac = Ad[rows][:, rows].tocsc()
+        r1, l1, V1, re1, i1 = s.speigs(Ac, k, s.SM, o, lib=lib)
+        assert r1 == 0
+        assert np.max(np.abs(lam[c] - l1) / np.abs(l1)) <= 1e-12
+        Vc = V[rows][:, :k]
+        r = np.linalg.norm(Ac @ Vc - Vc * lam[c], axis=0)
+        assert r.max() <= 1e-10 * max(i1["anorm"], 1.0) * 1.0001

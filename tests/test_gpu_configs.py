@@ -146,4 +146,5 @@ def test_c4_rgg_sample_batched(pkg, lib):
             Vc = V[rows][:, :kc]
             r = np.linalg.norm(Ac @ Vc - Vc * lam[c, :kc], axis=0)
             assert r.max() <= TOL * max(gc["anorm"], 1.0) * 1.0001
-    print(f"{ncomp} components, worst eigenvalue relative error {worst:.2e}")
+    print(f"{ncomp} components, worst eigenvalue relative error {worst:.2e}; total operator "
+          f"applications {info['nops']} (reference {sum(gc['nops'] for gc in g['components'])})")
