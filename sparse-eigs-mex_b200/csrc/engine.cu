@@ -771,8 +771,10 @@ static int lanczos_device(Operator &op, const DevA &A, int n, int64_t k, const s
 // random stream.  Convergence is decided as in the reference: true
 // residuals ||A x - lambda x|| <= tol max(||A||_1, 1) with lambda the
 // Rayleigh quotient of A, for the k Ritz vectors of largest |theta|.  The
-// residual of the block recurrence (cheap: a b x b Gram matrix) gates when
-// that test runs.
+// projected problem is solved at the end of each cycle (and once after the
+// first block of a start subspace); the residual of the block recurrence
+// (cheap: a b x b Gram matrix) decides whether the true-residual test runs
+// before the cycle's last check.
 namespace {
 
 struct BlockLanczosBufs {
@@ -960,6 +962,15 @@ static int block_lanczos_device(BlockOperator &op, const DevA &A, int n, int64_t
         if (stuck < 0) return stuck;
         tm.end(t1, &ms_ortho);
         const bool cycle_end = stuck == 1 || mm + b > mmax;
+        // The projected problem is solved where the reference solves it, at
+        // the end of a cycle, and also after the first block application of
+        // a start subspace: a proposal that already holds the wanted
+        // eigenvectors is then finished by one block solve.
+        const bool first_warm = (restarts == 0 && jc == 0 && pp > 0);
+        if (!cycle_end && !first_warm) {
+            jc = mm;
+            continue;
+        }
 
         // ---- Rayleigh-Ritz on H[0:mm, 0:mm]; the recurrence's residual
         // estimates gate the true-residual test
