@@ -139,15 +139,18 @@ def test_c4_rgg_sample_batched(pkg, lib):
         rl = np.array(gc["lam"])
         err = np.abs(lam[c, :kc] - rl) / np.abs(rl)
         worst = max(worst, float(err.max()))
+        rows = np.flatnonzero(comp == c)
+        Ac = Ad[rows][:, rows]
+        anorm_c = float(abs(Ac).sum(axis=0).max())
         # 1e-12 relative, down to the rounding floor of a Rayleigh quotient
-        # (16 eps ||A_c||_1): every block's smallest eigenvalue is 1e-3
-        floor = 16 * np.finfo(float).eps * max(gc.get("anorm", 1.0), 1.0)
+        # (16 eps ||A_c||_1): every block's smallest eigenvalue is 1e-3, and
+        # the reference solves components of up to 800 rows with the dense
+        # LAPACK eigensolver, whose backward error is also O(eps ||A_c||)
+        floor = 16 * np.finfo(float).eps * max(anorm_c, 1.0)
         assert np.all(np.abs(lam[c, :kc] - rl) <= 1e-12 * np.abs(rl) + floor), (c, lam[c, :kc], rl)
         if gc["n"] > 1:
-            rows = np.flatnonzero(comp == c)
-            Ac = Ad[rows][:, rows]
             Vc = V[rows][:, :kc]
             r = np.linalg.norm(Ac @ Vc - Vc * lam[c, :kc], axis=0)
-            assert r.max() <= TOL * max(gc["anorm"], 1.0) * 1.0001
+            assert r.max() <= TOL * max(anorm_c, 1.0) * 1.0001
     print(f"{ncomp} components, worst eigenvalue relative error {worst:.2e}; total operator "
           f"applications {info['nops']} (reference {sum(gc['nops'] for gc in g['components'])})")
