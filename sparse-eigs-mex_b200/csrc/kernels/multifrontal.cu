@@ -2187,7 +2187,8 @@ template <> int MultifrontalPlanT<Real>::solve_block(const double *B, int64_t ld
                                                      int64_t ldx, int nr, cudaStream_t st,
                                                      const int *skip) {
     if (nr < 1 || nr > 32 || !d_meta_) return SPEIGS_ERR_ARG;
-    const int w = nr <= 8 ? 8 : nr <= 16 ? 16 : 32;
+    const int w = (nr + 7) & ~7;          // 8, 16, 24 or 32 columns per row
+    const int q = w / 8 - 1;
     if (w > bw_) {
         // (re)allocate the block buffers for rows of w doubles
         void *old[] = {d_bin_, d_bout_, d_byf_, d_bx_, d_bu_, d_bfp_, d_bbp_};
@@ -2203,12 +2204,18 @@ template <> int MultifrontalPlanT<Real>::solve_block(const double *B, int64_t ld
         rc = rc ? rc : dmalloc(&d_bu_, (size_t)std::max<int64_t>(u_total_, 1) * w, st);
         rc = rc ? rc : dmalloc(&d_bfp_, (size_t)std::max(fslots_, 1) * kST * w, st);
         rc = rc ? rc : dmalloc(&d_bbp_, (size_t)std::max(bslots_, 1) * kST * w, st);
-        if (!rc) {
-            rc = w == 8 ? bsolve_config<8>(&bgrid_, &bsmem_)
-               : w == 16 ? bsolve_config<16>(&bgrid_, &bsmem_) : bsolve_config<32>(&bgrid_, &bsmem_);
-        }
         if (rc) return rc;
         bw_ = w;
+    }
+    if (!bgrid_[q]) {
+        const int rc = w == 8    ? bsolve_config<8>(&bgrid_[q], &bsmem_[q])
+                       : w == 16 ? bsolve_config<16>(&bgrid_[q], &bsmem_[q])
+                       : w == 24 ? bsolve_config<24>(&bgrid_[q], &bsmem_[q])
+                                 : bsolve_config<32>(&bgrid_[q], &bsmem_[q]);
+        if (rc) {
+            bgrid_[q] = 0;
+            return rc;
+        }
     }
     BSolveArgs a;
     a.meta = (const SNode *)d_meta_;
@@ -2237,13 +2244,14 @@ template <> int MultifrontalPlanT<Real>::solve_block(const double *B, int64_t ld
     a.out = d_bout_;
     a.skip = skip;
     cudaMemsetAsync(d_sync_, 0, sizeof(int) * (sync_ints_ - 1), st);
-    // rows of bw_ doubles: a narrower block runs padded to the buffers' width
-    if (bw_ == 8)
-        launch_bsolve<8>(a, n_, nr, B, ldb, X, ldx, d_bin_, d_bout_, bgrid_, bsmem_, st);
-    else if (bw_ == 16)
-        launch_bsolve<16>(a, n_, nr, B, ldb, X, ldx, d_bin_, d_bout_, bgrid_, bsmem_, st);
+    if (w == 8)
+        launch_bsolve<8>(a, n_, nr, B, ldb, X, ldx, d_bin_, d_bout_, bgrid_[q], bsmem_[q], st);
+    else if (w == 16)
+        launch_bsolve<16>(a, n_, nr, B, ldb, X, ldx, d_bin_, d_bout_, bgrid_[q], bsmem_[q], st);
+    else if (w == 24)
+        launch_bsolve<24>(a, n_, nr, B, ldb, X, ldx, d_bin_, d_bout_, bgrid_[q], bsmem_[q], st);
     else
-        launch_bsolve<32>(a, n_, nr, B, ldb, X, ldx, d_bin_, d_bout_, bgrid_, bsmem_, st);
+        launch_bsolve<32>(a, n_, nr, B, ldb, X, ldx, d_bin_, d_bout_, bgrid_[q], bsmem_[q], st);
     return 0;
 }
 

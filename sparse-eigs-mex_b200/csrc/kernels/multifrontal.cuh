@@ -118,14 +118,15 @@ private:
     double *d_u_ = nullptr, *d_yf_ = nullptr, *d_x_ = nullptr;
     int *d_status_ = nullptr;
     double *d_params_ = nullptr;     // shift, pivot tolerance (read by the graph)
-    // block solve: rows of bw_ doubles (8, 16 or 32) for the right-hand
-    // sides, the result, yf, x, the update vectors and the chunk partials
+    // block solve: buffers for rows of up to bw_ doubles (8, 16, 24 or 32)
+    // for the right-hand sides, the result, yf, x, the update vectors and
+    // the chunk partials; a solve of width NR <= bw_ uses them with stride NR
     int bw_ = 0;
     int32_t fslots_ = 0, bslots_ = 0;
     double *d_bin_ = nullptr, *d_bout_ = nullptr, *d_byf_ = nullptr, *d_bx_ = nullptr,
            *d_bu_ = nullptr, *d_bfp_ = nullptr, *d_bbp_ = nullptr;
-    int bgrid_ = 0;
-    size_t bsmem_ = 0;
+    int bgrid_[4] = {0, 0, 0, 0};          // per width NR = 8 (q + 1): grid, 0 = not set up
+    size_t bsmem_[4] = {0, 0, 0, 0};
     cudaGraphExec_t fgraph_ = nullptr;
     bool use_side_ = false;                    // some front has >= 2 column blocks
     cudaStream_t fside_ = nullptr;             // second branch of the factor graph

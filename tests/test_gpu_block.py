@@ -4,8 +4,9 @@ thick-restart Lanczos built on it (speigs_ext_opts.block).
 * A block solve of nr columns equals nr single solves column by column
   (1e-13 relative; the sums are ordered differently) and solves
   (A + shift I) X = B to a small backward error, for every block width the
-  kernel has (8, 16, 32 rows, narrower blocks padded) and for the FP32
-  factor with FP64 refinement.
+  kernel has (rows of 8, 16, 24 or 32 doubles, narrower blocks padded) and
+  for the FP32 factor with FP64 refinement; buffers sized for a wide block
+  serve narrower ones.
 * The block Lanczos returns the eigenpairs of the single-vector method
   (1e-12 relative in FP64, 1e-10 for the mixed form) with the residual bound
   met, for several block sizes, and uses every column of an exact start
@@ -53,6 +54,34 @@ def test_block_solve_matches_single_solves(pkg, lib, nr):
     assert np.max(np.linalg.norm(R, axis=0) /
                   (anorm * np.linalg.norm(Xb, axis=1) + np.linalg.norm(Bh[:, :n], axis=1))) <= 1e-14
     plan.close()
+
+
+def test_block_solve_narrower_after_wider(pkg, lib):
+    """Buffers sized for 32 columns serve later solves of 8 and 24 columns
+    (each at its own width) with the same results as on a fresh plan."""
+    torch = pytest.importorskip("torch")
+    A = pkg.workloads.varcoef3d(20, seed=4)
+    n = A.shape[0]
+    rng = np.random.default_rng(7)
+    Bh = rng.standard_normal((32, n))
+    B = torch.tensor(Bh, dtype=torch.float64, device="cuda")
+
+    def solve(plan, nr):
+        X = torch.zeros((nr, n), dtype=torch.float64, device="cuda")
+        assert plan.apply_block_device(B.data_ptr(), n, X.data_ptr(), n, nr) == 0
+        return X.cpu().numpy()
+
+    plan = _plan(pkg, lib, A)
+    assert plan.factor()[0] == 0
+    wide = solve(plan, 32)
+    narrow = {nr: solve(plan, nr) for nr in (8, 24, 5)}
+    plan.close()
+    for nr, Xn in narrow.items():
+        fresh = _plan(pkg, lib, A)
+        assert fresh.factor()[0] == 0
+        assert np.array_equal(Xn, solve(fresh, nr))
+        fresh.close()
+        assert np.max(np.abs(Xn - wide[:nr])) <= 1e-13 * np.max(np.abs(wide[:nr]))
 
 
 @pytest.mark.parametrize("nr", [3, 24])
