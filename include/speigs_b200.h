@@ -204,6 +204,16 @@ int speigs_b200_rand_vec(speigs_int n, uint64_t seed, double *v);
  * ascending, S[m*m] eigenvectors, ord[m] indices by |theta| descending. */
 int speigs_b200_syev_small(int m, const double *H, double *theta, double *S, int *ord);
 
+/* The same contract on a host core: Householder tridiagonalisation and the
+ * implicit symmetric QR iteration with Wilkinson shifts.  H has leading
+ * dimension ldh >= m; all buffers are host memory.  This is the solver the
+ * Lanczos loops of speigs() use for their projected problem (the reference
+ * calls LAPACK dsyev on the host there, src/speigs_core.c:180, :236).
+ * Returns 0, or -1 for bad arguments or when the iteration did not converge
+ * within 30 m steps. */
+int speigs_b200_syev_small_host(int m, const double *H, int ldh, double *theta, double *S,
+                                int *ord);
+
 /* Allocation-free variant of speigs_b200_syev_small.  No counterpart in the
  * reference interface.  For callers that cannot call cudaMalloc where they
  * need the solve -- code running under CUDA stream capture, real-time loops

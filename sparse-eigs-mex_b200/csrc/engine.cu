@@ -16,6 +16,7 @@
 #include "kernels/dense_lu.cuh"
 #include "kernels/seg_lanczos.cuh"
 #include "counters.h"
+#include "host/syev_host.h"
 
 #include <cuda_runtime.h>
 #include <cub/device/device_radix_sort.cuh>
@@ -66,6 +67,53 @@ static int cuda_fail(cudaError_t e, const char *where) {
     snprintf(g_err, sizeof g_err, "%s: %s", where, cudaGetErrorString(e));
     cudaGetLastError();
     return SPEIGS_ERR_INTERNAL;
+}
+
+// ---------------------------------------------- projected eigenproblem --
+// The Lanczos loops' projected problem (order m = the basis size) is solved on
+// the host, as the reference solves it with LAPACK: H is read back, solved by
+// syev_host, and theta, S, ord and the status word are written back in the
+// layout the device Jacobi (launch_syev_small) uses.  The pinned staging
+// buffers are reused from call to call: a call's first act is a synchronous
+// read-back on the same stream, after which the previous call's uploads have
+// completed.
+struct SyevStage {
+    double *buf = nullptr;
+    size_t cap = 0;
+    ~SyevStage() {
+        if (buf) cudaFreeHost(buf);   // an error at process exit is harmless
+    }
+};
+static int syev_projected(int m, const double *dH, int ldh, double *dtheta, double *dS, int *dord,
+                          int *dstat, cudaStream_t st) {
+    thread_local SyevStage sg;
+    const size_t need = 2 * (size_t)m * m + 2 * (size_t)m + 8;
+    if (sg.cap < need) {
+        double *nb = nullptr;
+        if (cudaMallocHost(&nb, sizeof(double) * need) != cudaSuccess) {
+            cudaGetLastError();
+            return SPEIGS_ERR_MEM;
+        }
+        if (sg.buf) cudaFreeHost(sg.buf);
+        sg.buf = nb;
+        sg.cap = need;
+    }
+    double *hH = sg.buf, *hS = hH + (size_t)m * m, *hth = hS + (size_t)m * m;
+    int *hord = reinterpret_cast<int *>(hth + m);
+    int *hst = reinterpret_cast<int *>(hth + 2 * m);
+    note_d2h((long long)sizeof(double) * m * m);
+    cudaMemcpy2DAsync(hH, sizeof(double) * m, dH, sizeof(double) * ldh, sizeof(double) * m, m,
+                      cudaMemcpyDeviceToHost, st);
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(e, "projected problem read-back");
+    const int steps = syev_host(m, hH, m, hth, hS, hord);
+    hst[0] = steps < 0 ? -1 : steps + 1;
+    hst[1] = 0;
+    copy_async(dtheta, hth, sizeof(double) * m, cudaMemcpyHostToDevice, st);
+    copy_async(dS, hS, sizeof(double) * m * m, cudaMemcpyHostToDevice, st);
+    copy_async(dord, hord, sizeof(int) * m, cudaMemcpyHostToDevice, st);
+    copy_async(dstat, hst, sizeof(int) * 2, cudaMemcpyHostToDevice, st);
+    return 0;
 }
 
 // ------------------------------------------------------------- resources --
@@ -373,8 +421,7 @@ struct LanczosBufs {
     int64_t ldv = 0;
     double *V = nullptr, *Vn = nullptr, *H = nullptr, *S = nullptr, *theta = nullptr,
            *thsave = nullptr, *w = nullptr, *X = nullptr, *AX = nullptr, *lam = nullptr,
-           *r2 = nullptr, *xn2 = nullptr, *h1 = nullptr, *h2 = nullptr, *nrm2 = nullptr,
-           *jwork = nullptr;
+           *r2 = nullptr, *xn2 = nullptr, *h1 = nullptr, *h2 = nullptr, *nrm2 = nullptr;
     int *ord = nullptr, *jstat = nullptr, *dflag = nullptr;
     ReduceScratch rs;
 };
@@ -447,8 +494,6 @@ static int lanczos_device(Operator &op, const DevA &A, int n, int64_t k, const s
     b.ord = ar.alloc<int>(ncv);
     b.jstat = ar.alloc<int>(2);
     b.dflag = ar.alloc<int>(1);
-    const int me = (int)((ncv + 1) & ~1);
-    b.jwork = ((int)ncv > syev_small_smem_limit()) ? ar.alloc<double>((size_t)2 * me * me) : nullptr;
     const int nblk = (n + 511) / 512 + 1;
     const int maxcols = (int)std::max<int64_t>(ncv + 1, b.kk) + 1;
     b.rs.part = ar.alloc<double>((size_t)nblk * maxcols);
@@ -630,7 +675,7 @@ static int lanczos_device(Operator &op, const DevA &A, int n, int64_t k, const s
         // ---- projected eigenproblem (reference :231-240)
         const int m = (int)ncv;
         int tr = tm.begin();
-        launch_syev_small(m, b.H, ldh, b.theta, b.S, b.ord, b.jwork, b.jstat, st);
+        if (int e = syev_projected(m, b.H, ldh, b.theta, b.S, b.ord, b.jstat, st)) return e;
 
         // ---- true residuals of the wanted Ritz pairs (reference :242-265)
         const int nwant = (int)std::min<int64_t>(k, m);
@@ -782,8 +827,7 @@ struct BlockLanczosBufs {
     int64_t ldv = 0;
     double *V = nullptr, *Vn = nullptr, *H = nullptr, *S = nullptr, *theta = nullptr,
            *hb = nullptr, *G = nullptr, *Gres = nullptr, *Rinv = nullptr, *est2 = nullptr,
-           *X = nullptr, *AX = nullptr, *lam = nullptr, *r2 = nullptr, *xn2 = nullptr,
-           *jwork = nullptr;
+           *X = nullptr, *AX = nullptr, *lam = nullptr, *r2 = nullptr, *xn2 = nullptr;
     int *ord = nullptr, *jstat = nullptr, *cstat = nullptr;
     ReduceScratch rs;
     BlockScratch bs;
@@ -833,8 +877,6 @@ static int block_lanczos_device(BlockOperator &op, const DevA &A, int n, int64_t
     B.ord = ar.alloc<int>(ldh);
     B.jstat = ar.alloc<int>(2);
     B.cstat = ar.alloc<int>(2);
-    const int me = (mmax + 1) & ~1;
-    B.jwork = (mmax > syev_small_smem_limit()) ? ar.alloc<double>((size_t)2 * me * me) : nullptr;
     const int nblk = (n + 511) / 512 + 1;
     const int maxc = std::max(cols, kk) + 1;
     B.rs.part = ar.alloc<double>((size_t)nblk * maxc);
@@ -976,7 +1018,7 @@ static int block_lanczos_device(BlockOperator &op, const DevA &A, int n, int64_t
         // estimates gate the true-residual test
         const int nwant = std::min(kk, mm);
         int tr = tm.begin();
-        launch_syev_small(mm, B.H, ldh, B.theta, B.S, B.ord, B.jwork, B.jstat, st);
+        if (int e = syev_projected(mm, B.H, ldh, B.theta, B.S, B.ord, B.jstat, st)) return e;
         launch_block_ritz_est(nwant, b, B.S, mm, jc, B.ord, B.Gres, b, B.est2, st);
         tm.end(tr, &ms_ritz);
         {
