@@ -37,6 +37,9 @@ typedef struct {
                                   host memory; NULL => the reference's random start   */
     speigs_int   warm_cols;
     int          block;        /* 'sm' Krylov method (see below); 0 => automatic        */
+    int          handoff;      /* speigs_batched: the lockstep loop hands its components
+                                  still iterating to the per-component executor once they
+                                  hold at most 1/handoff of the rows; 0 => 8, -1 => never */
 } speigs_ext_opts;
 
 /* speigs_ext_opts.block selects the Krylov method of the 'sm' route:

@@ -1794,9 +1794,10 @@ int device_batched_krylov(HostCSR &A, int nseg, const int32_t *off_h, int64_t k,
                           speigs_which which, const speigs_opts &o, const double *anorm_h,
                           double *lam_out, double *res_out, double *X_out, int64_t *nconv_out,
                           int64_t *nops_out, int64_t *restarts_out, int *flag_out,
-                          BatchedStats *bst) {
+                          BatchedStats *bst, int *handed, int handoff) {
     g_err[0] = 0;
     const int n = A.n;
+    if (handed) std::fill(handed, handed + nseg, 0);
     double amax = 1.0;
     for (int c = 0; c < nseg; c++) amax = std::max(amax, anorm_h[c]);
     // per-component basis size by the reference's rules
@@ -1984,6 +1985,20 @@ int device_batched_krylov(HostCSR &A, int nseg, const int32_t *off_h, int64_t k,
             else nlive++;
         }
         if (nlive == 0) break;
+        if (handed && handoff > 0) {
+            int64_t live_rows = 0;
+            for (int c = 0; c < nseg; c++)
+                if (liveh[c]) live_rows += off_h[c + 1] - off_h[c];
+            if ((int64_t)handoff * live_rows <= (int64_t)n) {
+                for (int c = 0; c < nseg; c++)
+                    if (liveh[c]) {
+                        handed[c] = 1;
+                        liveh[c] = 0;
+                    }
+                if (bst) bst->handed = nlive;
+                break;
+            }
+        }
         restarts++;
         for (int c = 0; c < nseg; c++)
             if (liveh[c]) resth[c]++;

@@ -90,16 +90,22 @@ int device_hermitian_recover(int64_t n, int64_t kk, int64_t k, const double *V2,
 // n x k column-major, may be NULL) the Ritz vectors on each component's rows.
 // Returns 0, a negative code, or 1 when the forest needs a shift or the
 // indefinite route (solve those components one by one instead).
+// handed (per segment, may be NULL): set to 1 for the components still
+// iterating when the lockstep loop stops early -- once the live components
+// hold at most 1/handoff of the forest's rows, every lockstep step would
+// still solve the whole forest for them, so they are handed back to be
+// solved one by one (their other outputs are then not set).  With handed
+// NULL or handoff <= 0 the loop runs every component to the end.
 struct BatchedStats {
     double t_analyze = 0, t_factor = 0, t_iter = 0, t_total = 0;
-    int64_t steps = 0, cycles = 0;
+    int64_t steps = 0, cycles = 0, handed = 0;
     bool graph = false;
 };
 int device_batched_krylov(HostCSR &A, int nseg, const int32_t *off, int64_t k,
                           speigs_which which, const speigs_opts &o, const double *anorm,
                           double *lam_out, double *res_out, double *X_out, int64_t *nconv_out,
                           int64_t *nops_out, int64_t *restarts_out, int *flag_out,
-                          BatchedStats *bst);
+                          BatchedStats *bst, int *handed = nullptr, int handoff = 0);
 
 // The factorization cache of the Krylov route (speigs_b200_factor_cache).
 int factor_cache_configure(int entries);

@@ -348,10 +348,13 @@ int solve_components(const int64_t *Ap, const int64_t *Ai, const double *Ax,
 // for a single call.  Results land in out[c] as solve_components leaves
 // them (sorted by |lambda|, vectors on the component's rows).  Returns 0, a
 // negative code, or 1 when these components must be solved one by one.
+// Components still iterating when few remain are appended to *handed_out,
+// to be solved one by one (the lockstep step solves the whole forest).
 int batched_krylov(const int64_t *Ap, const int64_t *Ai, const double *Ax,
                    const std::vector<int64_t> &comp, const CompSplit &sp,
                    std::vector<int64_t> kry, int64_t k, speigs_which which,
-                   const speigs_opts &o, bool want_vec, std::vector<CompResult> &out) {
+                   const speigs_opts &o, bool want_vec, std::vector<CompResult> &out,
+                   std::vector<int64_t> *handed_out, int handoff) {
     std::stable_sort(kry.begin(), kry.end(),
                      [&](int64_t a, int64_t b) { return sp.sz[a] > sp.sz[b]; });
     const int nseg = (int)kry.size();
@@ -394,12 +397,18 @@ int batched_krylov(const int64_t *Ap, const int64_t *Ai, const double *Ax,
     std::vector<int64_t> nconv(nseg), nops(nseg), rst(nseg);
     std::vector<int> flag(nseg);
     spx::BatchedStats bst;
+    std::vector<int> handed(nseg, 0);
     rc = spx::device_batched_krylov(A, nseg, off.data(), k, which, o, anorm.data(), lam.data(),
                                     res.data(), want_vec ? X.data() : nullptr, nconv.data(),
-                                    nops.data(), rst.data(), flag.data(), &bst);
+                                    nops.data(), rst.data(), flag.data(), &bst,
+                                    handed_out ? handed.data() : nullptr, handoff);
     if (rc) return rc;
     for (int q = 0; q < nseg; q++) {
         const int64_t c = kry[q], nc = sp.sz[c];
+        if (handed[q]) {
+            handed_out->push_back(c);
+            continue;
+        }
         CompResult &R = out[c];
         R.kc = std::min(k, nc);
         // sort by |lambda| as speigs() does: ascending 'sm', descending 'lm'
@@ -581,9 +590,13 @@ int speigs_batched(speigs_int n, const speigs_int *Ap, const speigs_int *Ai, con
         else rest.push_back(c);
     }
     if (!kry.empty()) {
-        int rcs = batched_krylov(Ap, Ai, Ax, cv, sp, kry, k, which, o2, V != nullptr, cr);
+        std::vector<int64_t> handed;
+        const int handoff = !ext || ext->handoff == 0 ? 8 : ext->handoff;
+        int rcs = batched_krylov(Ap, Ai, Ax, cv, sp, kry, k, which, o2, V != nullptr, cr, &handed,
+                                 handoff);
         if (rcs < 0) return rcs;
         if (rcs == 1) rest.insert(rest.end(), kry.begin(), kry.end());
+        else rest.insert(rest.end(), handed.begin(), handed.end());
     }
     int rc = solve_components(Ap, Ai, Ax, cv, sp, k, which, &o2, ext, V != nullptr, cr, &rest);
     if (rc) return rc;

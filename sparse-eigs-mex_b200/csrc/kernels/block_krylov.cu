@@ -15,53 +15,71 @@ namespace {
 
 constexpr int kTbThreads = 256;
 constexpr int kTbRows = 32;            // rows per staged chunk
+constexpr int kVS = kTbRows + 4;       // padded stride of staged columns / rows (36 doubles)
 
-// One row range per block: V^T W over the range into part[block], with the
-// chunk's rows of V (m columns) and W (b columns) staged in shared memory.
-// Thread t owns the outputs (i, j) with i = t % 64 + 64 s (s < 2) and
-// j = (t / 64) * 8 + q (q < 8): a warp reads 32 consecutive V columns of a
-// row (conflict-free) and one W entry (a broadcast).
+// m8n8k4 FP64 tensor-core product: lane = 4 gq + tq holds A[gq][tq],
+// B[tq][gq] and D[gq][2 tq .. 2 tq + 1]
+__device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(d[0]), "+d"(d[1]) : "d"(a), "d"(b));
+}
+
+// One row range per block: V^T W over the range into part[block] on the
+// tensor cores.  A 32-row chunk of V's m columns and W's b columns is staged
+// column by column (stride kVS, so the fragment reads of a half warp fall in
+// distinct banks); warp w owns the 8-row output tiles w and w + 8 of V^T W
+// and all of its 8-column tiles.
 __global__ void __launch_bounds__(kTbThreads) tsb_tn_part_kernel(
         const double *__restrict__ V, int64_t ldv, int n, int m, const double *__restrict__ W,
         int64_t ldw, int b, int rows_per_part, double *__restrict__ part) {
-    __shared__ double Vs[kTbRows][kBlockMaxM + 1];
-    __shared__ double Ws[kTbRows][kBlockMaxB];
-    const int t = threadIdx.x;
-    const int i0 = t & 63, jg = t >> 6;
-    double acc[2][8];
+    __shared__ double Cs[kBlockMaxM + kBlockMaxB][kVS];
+    const int t = threadIdx.x, lane = t & 31, wid = t >> 5, gq = lane >> 2, tq = lane & 3;
+    const int nmt = (m + 7) >> 3, nnt = (b + 7) >> 3;
+    double acc[2][4][2];
 #pragma unroll
     for (int s = 0; s < 2; s++)
 #pragma unroll
-        for (int q = 0; q < 8; q++) acc[s][q] = 0.0;
+        for (int q = 0; q < 4; q++) acc[s][q][0] = acc[s][q][1] = 0.0;
     const int rb = blockIdx.x * rows_per_part, re = min(n, rb + rows_per_part);
     for (int r0 = rb; r0 < re; r0 += kTbRows) {
         const int nr = min(kTbRows, re - r0);
-        for (int e = t; e < kTbRows * kBlockMaxM; e += kTbThreads) {
-            const int rr = e % kTbRows, c = e / kTbRows;
-            Vs[rr][c] = (rr < nr && c < m) ? V[(int64_t)(r0 + rr) + (int64_t)c * ldv] : 0.0;
-        }
-        for (int e = t; e < kTbRows * kBlockMaxB; e += kTbThreads) {
-            const int rr = e % kTbRows, c = e / kTbRows;
-            Ws[rr][c] = (rr < nr && c < b) ? W[(int64_t)(r0 + rr) + (int64_t)c * ldw] : 0.0;
+        for (int e = t; e < (m + b) * kTbRows; e += kTbThreads) {
+            const int c = e >> 5, rr = e & 31;
+            const double *src = c < m ? V + (int64_t)c * ldv : W + (int64_t)(c - m) * ldw;
+            Cs[c][rr] = rr < nr ? src[r0 + rr] : 0.0;
         }
         __syncthreads();
-#pragma unroll 4
-        for (int rr = 0; rr < kTbRows; rr++) {
-            const double v0 = Vs[rr][i0], v1 = Vs[rr][i0 + 64];
+#pragma unroll 2
+        for (int ks = 0; ks < kTbRows / 4; ks++) {
+            const int k = ks * 4 + tq;
+            double bf[4];
 #pragma unroll
-            for (int q = 0; q < 8; q++) {
-                const double w = Ws[rr][jg * 8 + q];
-                acc[0][q] += v0 * w;
-                acc[1][q] += v1 * w;
+            for (int q = 0; q < 4; q++) bf[q] = (q * 8 + gq < b) ? Cs[m + q * 8 + gq][k] : 0.0;
+#pragma unroll
+            for (int s = 0; s < 2; s++) {
+                const int mt = wid + 8 * s;
+                if (mt < nmt) {
+                    const double a = (mt * 8 + gq < m) ? Cs[mt * 8 + gq][k] : 0.0;
+#pragma unroll
+                    for (int q = 0; q < 4; q++)
+                        if (q < nnt) dmma884(acc[s][q], a, bf[q]);
+                }
             }
         }
         __syncthreads();
     }
     double *p = part + (size_t)blockIdx.x * (kBlockMaxM * kBlockMaxB);
 #pragma unroll
-    for (int s = 0; s < 2; s++)
+    for (int s = 0; s < 2; s++) {
+        const int mt = wid + 8 * s;
+        if (mt >= nmt) continue;
 #pragma unroll
-        for (int q = 0; q < 8; q++) p[(i0 + 64 * s) * kBlockMaxB + jg * 8 + q] = acc[s][q];
+        for (int q = 0; q < 4; q++)
+            if (q < nnt)
+#pragma unroll
+                for (int e = 0; e < 2; e++)
+                    p[(mt * 8 + gq) * kBlockMaxB + q * 8 + 2 * tq + e] = acc[s][q][e];
+    }
 }
 
 // H (=|+=) the sum of the parts, in part order; one thread per output.
@@ -77,31 +95,49 @@ __global__ void tsb_tn_reduce_kernel(int m, int b, int nparts, const double *__r
     *h = mode ? *h + acc : acc;
 }
 
-// W[row, 0:b] -= V[row, 0:m] H[0:m, 0:b]; one thread per row, H in shared
-// memory (read as broadcasts), the row's b sums in registers.
-template <int B>
-__global__ void __launch_bounds__(256) tsb_nn_sub_kernel(const double *__restrict__ V, int64_t ldv,
-                                                         int n, int m, const double *__restrict__ H,
-                                                         int ldh, double *W, int64_t ldw, int b) {
-    __shared__ double Hs[kBlockMaxM * B];
-    for (int e = threadIdx.x; e < m * B; e += blockDim.x) {
-        const int i = e / B, j = e % B;
-        Hs[e] = (j < b) ? H[i + (int64_t)j * ldh] : 0.0;
+// out[row, 0:b] = W[row, 0:b] - A[row, 0:K] Bm  (SUB), or A[row, 0:K] Bm,
+// on the tensor cores: warp w of a block holds 8 rows, Bm (K x b, leading
+// dimension ldb) is staged in shared memory with its rows padded to kVS.
+// The product overwrites W; with SUB false A may be W itself, since each
+// warp reads all of its rows' entries before it writes any.
+template <bool SUB>
+__global__ void __launch_bounds__(kTbThreads) tsb_rows_kernel(const double *A, int64_t lda, int n,
+                                                              int K, const double *Bm, int ldb,
+                                                              double *W, int64_t ldw, int b) {
+    __shared__ double Bs[kBlockMaxM][kVS];
+    const int nks = (K + 3) >> 2;
+    for (int e = threadIdx.x; e < nks * 4 * kVS; e += kTbThreads) {
+        const int k = e / kVS, j = e % kVS;
+        Bs[k][j] = (k < K && j < b) ? Bm[k + (int64_t)j * ldb] : 0.0;
     }
     __syncthreads();
-    const int row = blockIdx.x * blockDim.x + threadIdx.x;
-    if (row >= n) return;
-    double acc[B];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, gq = lane >> 2, tq = lane & 3;
+    const int r0 = blockIdx.x * (kTbThreads / 4) + wid * 8;
+    if (r0 >= n) return;
+    const int row = r0 + gq, nnt = (b + 7) >> 3;
+    double acc[4][2];
 #pragma unroll
-    for (int j = 0; j < B; j++) acc[j] = 0.0;
-    for (int i = 0; i < m; i++) {
-        const double v = V[(int64_t)row + (int64_t)i * ldv];
+    for (int q = 0; q < 4; q++) acc[q][0] = acc[q][1] = 0.0;
+#pragma unroll 4
+    for (int ks = 0; ks < nks; ks++) {
+        const int k = ks * 4 + tq;
+        const double a = (row < n && k < K) ? A[row + (int64_t)k * lda] : 0.0;
 #pragma unroll
-        for (int j = 0; j < B; j++) acc[j] += v * Hs[i * B + j];
+        for (int q = 0; q < 4; q++)
+            if (q < nnt) dmma884(acc[q], a, Bs[k][q * 8 + gq]);
     }
+    if (row >= n) return;
 #pragma unroll
-    for (int j = 0; j < B; j++)
-        if (j < b) W[(int64_t)row + (int64_t)j * ldw] -= acc[j];
+    for (int q = 0; q < 4; q++)
+        if (q < nnt)
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                const int j = q * 8 + 2 * tq + e;
+                if (j < b) {
+                    double *o = W + row + (int64_t)j * ldw;
+                    *o = SUB ? *o - acc[q][e] : acc[q][e];
+                }
+            }
 }
 
 // Cholesky of the column-scaled Gram matrix in one warp (lane j owns
@@ -168,27 +204,6 @@ __global__ void block_chol_kernel(int b, const double *G, int ldg, double *Rinv,
     if (j == 0) {
         status[0] = (int)dep;
         status[1] = dep ? 1 : 0;
-    }
-}
-
-__global__ void __launch_bounds__(256) tsb_right_mul_kernel(int n, int b, double *W, int64_t ldw,
-                                                            const double *__restrict__ Rinv) {
-    __shared__ double Rs[kBlockMaxB * kBlockMaxB];
-    for (int e = threadIdx.x; e < b * b; e += blockDim.x) Rs[e] = Rinv[e];
-    __syncthreads();
-    const int row = blockIdx.x * blockDim.x + threadIdx.x;
-    if (row >= n) return;
-    double w[kBlockMaxB];
-#pragma unroll
-    for (int j = 0; j < kBlockMaxB; j++) w[j] = (j < b) ? W[(int64_t)row + (int64_t)j * ldw] : 0.0;
-#pragma unroll
-    for (int c = 0; c < kBlockMaxB; c++) {
-        if (c >= b) break;
-        double s = 0.0;
-#pragma unroll
-        for (int j = 0; j < kBlockMaxB; j++)
-            if (j <= c) s += w[j] * Rs[j + c * b];
-        W[(int64_t)row + (int64_t)c * ldw] = s;
     }
 }
 
@@ -340,10 +355,9 @@ void launch_tsb_tn(const double *V, int64_t ldv, int n, int m, const double *W, 
 void launch_tsb_nn_sub(const double *V, int64_t ldv, int n, int m, const double *H, int ldh,
                        double *W, int64_t ldw, int b, cudaStream_t st) {
     if (m <= 0 || b <= 0) return;
-    const int nb = (n + 255) / 256;
-    if (b <= 8) tsb_nn_sub_kernel<8><<<nb, 256, 0, st>>>(V, ldv, n, m, H, ldh, W, ldw, b);
-    else if (b <= 16) tsb_nn_sub_kernel<16><<<nb, 256, 0, st>>>(V, ldv, n, m, H, ldh, W, ldw, b);
-    else tsb_nn_sub_kernel<32><<<nb, 256, 0, st>>>(V, ldv, n, m, H, ldh, W, ldw, b);
+    const int rows = kTbThreads / 4;
+    tsb_rows_kernel<true><<<(n + rows - 1) / rows, kTbThreads, 0, st>>>(V, ldv, n, m, H, ldh, W,
+                                                                        ldw, b);
     note_launch();
 }
 
@@ -355,7 +369,10 @@ void launch_block_chol(int b, const double *G, int ldg, double *Rinv, double abs
 
 void launch_tsb_right_mul(int n, int b, double *W, int64_t ldw, const double *Rinv,
                           cudaStream_t st) {
-    tsb_right_mul_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, b, W, ldw, Rinv);
+    if (b <= 0) return;
+    const int rows = kTbThreads / 4;
+    tsb_rows_kernel<false><<<(n + rows - 1) / rows, kTbThreads, 0, st>>>(W, ldw, n, b, Rinv, b, W,
+                                                                         ldw, b);
     note_launch();
 }
 

@@ -43,7 +43,8 @@ class Info(ctypes.Structure):
 class ExtOpts(ctypes.Structure):
     """speigs_ext_opts (include/speigs_b200.h): operator precision, start subspace."""
     _fields_ = [("precision", c_int), ("refine_max", c_int), ("refine_tol", c_double),
-                ("warm", c_void_p), ("warm_cols", c_int64), ("block", c_int)]
+                ("warm", c_void_p), ("warm_cols", c_int64), ("block", c_int),
+                ("handoff", c_int)]
 
 
 class ExtInfo(ctypes.Structure):

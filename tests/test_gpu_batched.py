@@ -6,6 +6,7 @@ drop-in blocks route (components solved concurrently, one per host thread)
 is checked against the compiled reference."""
 import numpy as np
 import pytest
+import scipy.sparse as sp
 
 pytestmark = pytest.mark.gpu
 
@@ -117,3 +118,40 @@ def test_batched_matches_one_call_per_component(lib, pkg):
         Vc = V[rows][:, :k]
         r = np.linalg.norm(Ac @ Vc - Vc * lam[c], axis=0)
         assert r.max() <= 1e-10 * max(i1["anorm"], 1.0) * 1.0001
+
+
+def test_batched_straggler_handed_off(lib, pkg):
+    """A forest of quickly converging components plus one slow one (a path
+    graph Laplacian + 1e-3 I, whose smallest eigenvalues are clustered to
+    1e-6 of each other): once the live components hold at most 1/8 of the
+    rows, the lockstep loop hands the straggler to the per-component
+    executor.  Every component must still agree with speigs() on it alone."""
+    s, w = pkg.speigs, pkg.workloads
+    n1 = 1500
+    path = sp.diags([-np.ones(n1 - 1), 2.0 * np.ones(n1) + 1e-3, -np.ones(n1 - 1)], [-1, 0, 1])
+    path = sp.csc_matrix(path)
+    path[0, 0] -= 1.0
+    path[n1 - 1, n1 - 1] -= 1.0
+    quick = w.rgg_blocks(4096, seed=4, first=40)
+    A = sp.block_diag([quick, path], format="csc")
+    A.sort_indices()
+    k = 4
+    o = s.default_opts(lib, tol=1e-10)
+    ncomp, comp = s.components(A, lib)
+    assert np.sum(comp == comp[-1]) * 8 <= A.shape[0]
+    rc, lam, V, res, nv, info = s.speigs_batched(A, k, s.SM, o, comp=comp, vectors=True, lib=lib)
+    assert rc == 0
+    Ad = A.tocsr()
+    for c in range(ncomp):
+        rows = np.flatnonzero(comp == c)
+        if len(rows) <= 64:
+            continue
+        Ac = Ad[rows][:, rows].tocsc()
+        r1, l1, V1, re1, i1 = s.speigs(Ac, k, s.SM, o, lib=lib)
+        assert r1 == 0
+        floor = 16 * np.finfo(float).eps * max(i1["anorm"], 1.0)
+        assert np.all(np.abs(lam[c] - l1) <= 1e-12 * np.abs(l1) + floor), c
+        Vc = V[rows][:, :k]
+        r = np.linalg.norm(Ac @ Vc - Vc * lam[c], axis=0)
+        if i1["flag"] == 0:
+            assert r.max() <= 1e-10 * max(i1["anorm"], 1.0) * 1.0001
