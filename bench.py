@@ -500,12 +500,15 @@ def run_batched(args, pkg, wl, rank=0, world=1, local=0):
         solve()
     ts = []
     c0 = s.counters(lib)
+    phases = []
     for _ in range(args.steps):
         if dist is not None:
             dist.barrier()
         t0 = time.perf_counter()
         _, out = solve()
         ts.append(tmax(time.perf_counter() - t0))
+        if out is not None:
+            phases.append(s.batched_stats(lib))
     c1 = s.counters(lib)
     launches = tmax((c1[0] - c0[0]) // args.steps)
     h2d = tmax((c1[1] - c0[1]) // args.steps)
@@ -576,6 +579,7 @@ def run_batched(args, pkg, wl, rank=0, world=1, local=0):
                 "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(launches),
         "step_s": [round(x, 4) for x in ts],
+        "phases_rank0": phases[-1] if phases else None,
     }
     print(json.dumps(line))
     return 0

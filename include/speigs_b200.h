@@ -107,6 +107,18 @@ int speigs_batched(speigs_int n, const speigs_int *Ap, const speigs_int *Ai, con
                    double *lambda, double *V, double *resid, speigs_int *nvals,
                    speigs_info *info);
 
+/* Phases of the calling thread's last speigs_batched call.  No counterpart in
+ * the reference interface.  times[9] (seconds): input checks and the
+ * component split; building the lockstep group's CSR; the group's symbolic
+ * analysis, numeric factorization and Lanczos iterations; the lockstep part
+ * in all; the components solved one by one (dense gate, singular forests,
+ * extension options, stragglers handed off); the whole call; the lockstep
+ * engine's own total.  counts[7]: components in the lockstep group,
+ * components solved one by one, stragglers handed off, lockstep steps,
+ * restart cycles, rows of the lockstep group, 1 if its step ran as a CUDA
+ * graph. */
+int speigs_b200_batched_stats(double *times, int64_t *counts);
+
 /* ---- learned warm start: the message-passing network -----------------------
  * h0 = tanh(W0 x + b0); h_l = tanh(W_l [h_{l-1}, A h_{l-1}] + b_l), l = 1..L;
  * Y = W_o h_L + b_o.  x: nfeat features per node (FP32), A: a sparse

@@ -876,7 +876,7 @@ static int block_lanczos_device(BlockOperator &op, const DevA &A, int n, int64_t
     B.xn2 = ar.alloc<double>(std::max(cols, kk));
     B.ord = ar.alloc<int>(ldh);
     B.jstat = ar.alloc<int>(2);
-    B.cstat = ar.alloc<int>(2);
+    B.cstat = ar.alloc<int>(4);
     const int nblk = (n + 511) / 512 + 1;
     const int maxc = std::max(cols, kk) + 1;
     B.rs.part = ar.alloc<double>((size_t)nblk * maxc);
@@ -938,9 +938,19 @@ static int block_lanczos_device(BlockOperator &op, const DevA &A, int n, int64_t
     // dependent are replaced by random vectors and the block is projected
     // again (up to three times).  *replaced gets the columns replaced in the
     // first test; returns 1 when the block stays dependent (no extension).
-    auto orthonormalise = [&](double *Wp, int m, unsigned *replaced, bool keep_gram) -> int {
+    // With spec, the dependency test is not read back: the first pass goes
+    // on as if no column were dependent, and the Cholesky kernel's sticky
+    // flag (cstat[2]) tells the caller later whether the step must be redone.
+    auto orthonormalise = [&](double *Wp, int m, unsigned *replaced, bool keep_gram,
+                              bool spec) -> int {
         unsigned first_mask = 0;
-        for (int att = 0;; att++) {
+        if (spec) {
+            launch_tsb_tn(Wp, B.ldv, n, b, Wp, B.ldv, b, B.G, b, 0, B.bs, st);
+            if (keep_gram)
+                cudaMemcpyAsync(B.Gres, B.G, sizeof(double) * b * b, cudaMemcpyDeviceToDevice, st);
+            launch_block_chol(b, B.G, b, B.Rinv, bthr, 1e-14, B.cstat, st);
+        }
+        for (int att = 0; !spec; att++) {
             launch_tsb_tn(Wp, B.ldv, n, b, Wp, B.ldv, b, B.G, b, 0, B.bs, st);
             if (keep_gram && att == 0)
                 cudaMemcpyAsync(B.Gres, B.G, sizeof(double) * b * b, cudaMemcpyDeviceToDevice, st);
@@ -976,7 +986,7 @@ static int block_lanczos_device(BlockOperator &op, const DevA &A, int n, int64_t
     }
     {
         unsigned rep = 0;
-        int e = orthonormalise(B.V, 0, &rep, false);
+        int e = orthonormalise(B.V, 0, &rep, false, false);
         if (e < 0) return e;
         if (e == 1) return SPEIGS_ERR_INTERNAL;
         int used = 0;
@@ -985,6 +995,22 @@ static int block_lanczos_device(BlockOperator &op, const DevA &A, int n, int64_t
     }
 
     int jc = 0, mm = 0;
+    // Cycles run speculatively (no host read per block step); the state a
+    // cycle starts from -- V[:, 0:jc + b] and H[:, 0:jc] -- is not written
+    // during the cycle, so a cycle in which a block lost rank is redone from
+    // it with the per-step test.
+    int *h_dep = h_stat + 6;
+    int jc_cycle = 0;
+    int64_t napps_cycle = 0, nvecs_cycle = 0;
+    bool spec_cycle = true;
+    auto start_cycle = [&]() {
+        jc_cycle = jc;
+        napps_cycle = op.napps;
+        nvecs_cycle = op.nvecs;
+        spec_cycle = true;
+        cudaMemsetAsync(B.cstat + 2, 0, sizeof(int), st);
+    };
+    start_cycle();
     int64_t restarts = 0, nconv = 0;
     int last_nwant = 0;
     int rc = SPEIGS_OK;
@@ -1000,7 +1026,7 @@ static int block_lanczos_device(BlockOperator &op, const DevA &A, int n, int64_t
         int t1 = tm.begin();
         cgs2(Wp, mm, B.H + (size_t)jc * ldh);
         unsigned rep = 0;
-        const int stuck = orthonormalise(Wp, mm, &rep, true);
+        const int stuck = orthonormalise(Wp, mm, &rep, true, spec_cycle);
         if (stuck < 0) return stuck;
         tm.end(t1, &ms_ortho);
         const bool cycle_end = stuck == 1 || mm + b > mmax;
@@ -1012,6 +1038,20 @@ static int block_lanczos_device(BlockOperator &op, const DevA &A, int n, int64_t
         if (!cycle_end && !first_warm) {
             jc = mm;
             continue;
+        }
+        if (spec_cycle) {
+            // a block that lost rank in this cycle: redo the cycle from its
+            // start with the dependency test read after every step
+            copy_async(h_dep, B.cstat + 2, sizeof(int), cudaMemcpyDeviceToHost, st);
+            if (int e = sync("block step check")) return e;
+            if (*h_dep) {
+                cudaMemsetAsync(B.cstat + 2, 0, sizeof(int), st);
+                op.napps = napps_cycle;
+                op.nvecs = nvecs_cycle;
+                jc = jc_cycle;
+                spec_cycle = false;
+                continue;
+            }
         }
 
         // ---- Rayleigh-Ritz on H[0:mm, 0:mm]; the recurrence's residual
@@ -1082,6 +1122,7 @@ static int block_lanczos_device(BlockOperator &op, const DevA &A, int n, int64_t
         launch_block_set_diag(ldh, mmax, l, B.theta, B.ord, B.H, st);
         tm.end(tk, &ms_ritz);
         jc = l;
+        start_cycle();
     }
     if (rc) return rc;
     if (!have_result) return SPEIGS_ERR_INTERNAL;

@@ -33,6 +33,14 @@ double wall() {
     return t.tv_sec + 1e-9 * t.tv_nsec;
 }
 
+// Phases of the calling thread's last speigs_batched (speigs_b200_batched_stats).
+struct BatchedCallStats {
+    double t_checks = 0, t_group = 0, t_seg = 0, t_rest = 0, t_total = 0;
+    int64_t nkry = 0, nrest = 0, kry_rows = 0;
+    spx::BatchedStats seg;
+};
+thread_local BatchedCallStats g_bstats;
+
 // Symmetry verdict of the reference's input check (src/speigs_core.c:363-401):
 // 1 when both triangles are stored and A equals its transpose entry for
 // entry (values within 1e-12 relative), 2 when only the upper triangle is
@@ -355,6 +363,7 @@ int batched_krylov(const int64_t *Ap, const int64_t *Ai, const double *Ax,
                    std::vector<int64_t> kry, int64_t k, speigs_which which,
                    const speigs_opts &o, bool want_vec, std::vector<CompResult> &out,
                    std::vector<int64_t> *handed_out, int handoff) {
+    const double t_group0 = wall();
     std::stable_sort(kry.begin(), kry.end(),
                      [&](int64_t a, int64_t b) { return sp.sz[a] > sp.sz[b]; });
     const int nseg = (int)kry.size();
@@ -396,7 +405,10 @@ int batched_krylov(const int64_t *Ap, const int64_t *Ai, const double *Ax,
     std::vector<double> X(want_vec ? (size_t)ng * k : 0);
     std::vector<int64_t> nconv(nseg), nops(nseg), rst(nseg);
     std::vector<int> flag(nseg);
-    spx::BatchedStats bst;
+    spx::BatchedStats &bst = g_bstats.seg;
+    bst = spx::BatchedStats();
+    g_bstats.kry_rows = ng;
+    g_bstats.t_group = wall() - t_group0;
     std::vector<int> handed(nseg, 0);
     rc = spx::device_batched_krylov(A, nseg, off.data(), k, which, o, anorm.data(), lam.data(),
                                     res.data(), want_vec ? X.data() : nullptr, nconv.data(),
@@ -558,6 +570,8 @@ int speigs_batched(speigs_int n, const speigs_int *Ap, const speigs_int *Ai, con
     speigs_info li;
     if (!info) info = &li;
     memset(info, 0, sizeof *info);
+    g_bstats = BatchedCallStats();
+    const double t0 = wall();
     if (n <= 0 || !Ap || !Ai || !Ax || !lambda || !comp || ncomp <= 0 || k <= 0)
         return SPEIGS_ERR_ARG;
     for (int64_t i = 0; i < n; i++)
@@ -589,7 +603,10 @@ int speigs_batched(speigs_int n, const speigs_int *Ap, const speigs_int *Ai, con
         if (seg_ok && nc > 1 && !dense) kry.push_back(c);
         else rest.push_back(c);
     }
+    g_bstats.t_checks = wall() - t0;
+    g_bstats.nkry = (int64_t)kry.size();
     if (!kry.empty()) {
+        const double ts = wall();
         std::vector<int64_t> handed;
         const int handoff = !ext || ext->handoff == 0 ? 8 : ext->handoff;
         int rcs = batched_krylov(Ap, Ai, Ax, cv, sp, kry, k, which, o2, V != nullptr, cr, &handed,
@@ -597,8 +614,12 @@ int speigs_batched(speigs_int n, const speigs_int *Ap, const speigs_int *Ai, con
         if (rcs < 0) return rcs;
         if (rcs == 1) rest.insert(rest.end(), kry.begin(), kry.end());
         else rest.insert(rest.end(), handed.begin(), handed.end());
+        g_bstats.t_seg = wall() - ts - g_bstats.t_group;
     }
+    g_bstats.nrest = (int64_t)rest.size();
+    const double tr = wall();
     int rc = solve_components(Ap, Ai, Ax, cv, sp, k, which, &o2, ext, V != nullptr, cr, &rest);
+    g_bstats.t_rest = wall() - tr;
     if (rc) return rc;
     memset(lambda, 0, sizeof(double) * (size_t)ncomp * k);
     if (resid) memset(resid, 0, sizeof(double) * (size_t)ncomp * k);
@@ -620,6 +641,7 @@ int speigs_batched(speigs_int n, const speigs_int *Ap, const speigs_int *Ai, con
     }
     info->ncomp = ncomp;
     info->path = SPEIGS_PATH_BLOCKS;
+    g_bstats.t_total = wall() - t0;
     return SPEIGS_OK;
 }
 
@@ -719,3 +741,15 @@ int speigs_impl(int64_t n, const int64_t *Ap, const int64_t *Ai, const double *A
 }
 
 }  // namespace
+
+int speigs_b200_batched_stats(double *times, int64_t *counts) {
+    if (!times || !counts) return SPEIGS_ERR_ARG;
+    const BatchedCallStats &b = g_bstats;
+    const double t[9] = {b.t_checks, b.t_group, b.seg.t_analyze, b.seg.t_factor, b.seg.t_iter,
+                         b.t_seg, b.t_rest, b.t_total, b.seg.t_total};
+    const int64_t c[7] = {b.nkry, b.nrest, b.seg.handed, b.seg.steps, b.seg.cycles, b.kry_rows,
+                          b.seg.graph ? 1 : 0};
+    memcpy(times, t, sizeof t);
+    memcpy(counts, c, sizeof c);
+    return SPEIGS_OK;
+}

@@ -82,17 +82,33 @@ __global__ void __launch_bounds__(kTbThreads) tsb_tn_part_kernel(
     }
 }
 
-// H (=|+=) the sum of the parts, in part order; one thread per output.
-__global__ void tsb_tn_reduce_kernel(int m, int b, int nparts, const double *__restrict__ part,
-                                     double *H, int ldh, int mode) {
-    const int o = blockIdx.x * blockDim.x + threadIdx.x;
-    if (o >= m * kBlockMaxB) return;
+// H (=|+=) the sum of the parts: a block per 32 consecutive outputs, warp s
+// adding parts s, s + 8, s + 16, ... of each output (coalesced rows of
+// part), then the 8 slice sums added in slice order -- a fixed order, so
+// the result repeats bit for bit.
+constexpr int kRedSlices = 8;
+__global__ void __launch_bounds__(32 * kRedSlices) tsb_tn_reduce_kernel(
+        int m, int b, int nparts, const double *__restrict__ part, double *H, int ldh, int mode) {
+    __shared__ double sl[kRedSlices][33];
+    const int lo = threadIdx.x & 31, sli = threadIdx.x >> 5;
+    const int o = blockIdx.x * 32 + lo;
+    const bool live = o < m * kBlockMaxB;
+    double acc = 0.0;
+    if (live) {
+#pragma unroll 4
+        for (int q = sli; q < nparts; q += kRedSlices)
+            acc += part[(size_t)q * (kBlockMaxM * kBlockMaxB) + o];
+    }
+    sl[sli][lo] = acc;
+    __syncthreads();
+    if (sli != 0 || !live) return;
     const int i = o / kBlockMaxB, j = o % kBlockMaxB;
     if (j >= b) return;
-    double acc = 0.0;
-    for (int q = 0; q < nparts; q++) acc += part[(size_t)q * (kBlockMaxM * kBlockMaxB) + o];
+    double t = 0.0;
+#pragma unroll
+    for (int q = 0; q < kRedSlices; q++) t += sl[q][lo];
     double *h = H + i + (int64_t)j * ldh;
-    *h = mode ? *h + acc : acc;
+    *h = mode ? *h + t : t;
 }
 
 // out[row, 0:b] = W[row, 0:b] - A[row, 0:K] Bm  (SUB), or A[row, 0:K] Bm,
@@ -204,6 +220,7 @@ __global__ void block_chol_kernel(int b, const double *G, int ldg, double *Rinv,
     if (j == 0) {
         status[0] = (int)dep;
         status[1] = dep ? 1 : 0;
+        if (dep) status[2] = 1;       // sticky until the caller clears it
     }
 }
 
@@ -348,7 +365,8 @@ void launch_tsb_tn(const double *V, int64_t ldv, int n, int m, const double *W, 
     const int np = (n + rows - 1) / rows;
     tsb_tn_part_kernel<<<np, kTbThreads, 0, st>>>(V, ldv, n, m, W, ldw, b, rows, bs.part);
     const int outs = m * kBlockMaxB;
-    tsb_tn_reduce_kernel<<<(outs + 255) / 256, 256, 0, st>>>(m, b, np, bs.part, H, ldh, mode);
+    tsb_tn_reduce_kernel<<<(outs + 31) / 32, 32 * kRedSlices, 0, st>>>(m, b, np, bs.part, H, ldh,
+                                                                       mode);
     note_launch(2);
 }
 

@@ -34,7 +34,8 @@ void launch_tsb_nn_sub(const double *V, int64_t ldv, int n, int m, const double 
 // bit mask of dependent columns: column j is dependent when its norm is
 // <= abs_floor or its scaled pivot is <= rel_floor; such a column gets a
 // unit pivot (it is replaced by the caller).  status[1] = 1 if any column
-// is dependent.  One warp.
+// is dependent, and then status[2] = 1 as well (status[2] is never cleared
+// here: it records a dependency over several calls).  One warp.
 void launch_block_chol(int b, const double *G, int ldg, double *Rinv, double abs_floor,
                        double rel_floor, int *status, cudaStream_t st);
 // W[:, 0:b] = W[:, 0:b] Rinv  (in place; Rinv upper triangular b x b, ld b)

@@ -242,6 +242,25 @@ def speigs_batched(A, k, which=SM, opts: Opts | None = None, ext: ExtOpts | None
     return rc, lam, (V.T.copy() if vectors else None), res, nv, info.as_dict()
 
 
+BATCHED_TIMES = ("t_checks", "t_group", "t_analyze", "t_factor", "t_iter", "t_lockstep",
+                 "t_one_by_one", "t_total", "t_engine")
+BATCHED_COUNTS = ("lockstep_components", "one_by_one_components", "handed_off", "steps",
+                  "cycles", "lockstep_rows", "graph")
+
+
+def batched_stats(lib=None) -> dict:
+    """speigs_b200_batched_stats(): phases of this thread's last speigs_batched."""
+    lib = lib or load()
+    t = np.zeros(len(BATCHED_TIMES))
+    c = np.zeros(len(BATCHED_COUNTS), dtype=np.int64)
+    rc = lib.speigs_b200_batched_stats(_p(t), _p(c, c_int64))
+    if rc:
+        raise RuntimeError(f"batched_stats: {errmsg(rc, lib)}")
+    out = {name: float(v) for name, v in zip(BATCHED_TIMES, t)}
+    out.update({name: int(v) for name, v in zip(BATCHED_COUNTS, c)})
+    return out
+
+
 def speigs_z(A_re, A_im, k, which=SM, opts: Opts | None = None, lib=None):
     """Complex Hermitian through the C ABI: A_re/A_im share one CSC pattern."""
     lib = lib or load()
