@@ -362,7 +362,7 @@ int batched_krylov(const int64_t *Ap, const int64_t *Ai, const double *Ax,
                    const std::vector<int64_t> &comp, const CompSplit &sp,
                    std::vector<int64_t> kry, int64_t k, speigs_which which,
                    const speigs_opts &o, bool want_vec, std::vector<CompResult> &out,
-                   std::vector<int64_t> *handed_out, int handoff) {
+                   std::vector<int64_t> *handed_out, int handoff, bool full_sorted) {
     const double t_group0 = wall();
     std::stable_sort(kry.begin(), kry.end(),
                      [&](int64_t a, int64_t b) { return sp.sz[a] > sp.sz[b]; });
@@ -370,22 +370,47 @@ int batched_krylov(const int64_t *Ap, const int64_t *Ai, const double *Ax,
     std::vector<int32_t> off(nseg + 1, 0);
     for (int q = 0; q < nseg; q++) off[q + 1] = off[q] + (int32_t)sp.sz[kry[q]];
     const int64_t ng = off[nseg];
-    // group CSC: segment q's column jl is the component's jl-th row (original order)
-    std::vector<int64_t> Gp(ng + 1, 0), Gi;
-    std::vector<double> Gx;
-    std::vector<double> anorm(nseg, 0.0), colsum;
-    for (int q = 0; q < nseg; q++) {
+    // group CSC: segment q's column jl is the component's jl-th row (original
+    // order).  Segments are independent: their column counts, entries and
+    // norms are built by a pool of host threads (largest segments first),
+    // with the offsets from a prefix sum in between.
+    std::vector<int64_t> Gp(ng + 1, 0);
+    std::vector<double> anorm(nseg, 0.0);
+    const int nth = (int)std::min<int64_t>(spx::host_threads(), nseg);
+    auto over_segments = [&](auto &&body) {
+        std::atomic<int> next{0};
+        auto worker = [&] {
+            for (int q; (q = next.fetch_add(1)) < nseg;) body(q);
+        };
+        std::vector<std::thread> th;
+        for (int t = 1; t < nth; t++) th.emplace_back(worker);
+        worker();
+        for (auto &t : th) t.join();
+    };
+    over_segments([&](int q) {
         const int64_t c = kry[q], nc = sp.sz[c];
-        colsum.assign(nc, 0.0);
+        for (int64_t jl = 0; jl < nc; jl++) {
+            const int64_t gc = sp.gidx[sp.off[c] + jl];
+            int64_t cnt = 0;
+            for (int64_t e = Ap[gc]; e < Ap[gc + 1]; e++) cnt += comp[Ai[e]] == c;
+            Gp[off[q] + jl + 1] = cnt;
+        }
+    });
+    for (int64_t g = 0; g < ng; g++) Gp[g + 1] += Gp[g];
+    std::vector<int64_t> Gi((size_t)Gp[ng]);
+    std::vector<double> Gx((size_t)Gp[ng]);
+    over_segments([&](int q) {
+        const int64_t c = kry[q], nc = sp.sz[c];
+        std::vector<double> colsum(nc, 0.0);
         for (int64_t jl = 0; jl < nc; jl++) {
             const int64_t g = off[q] + jl, gc = sp.gidx[sp.off[c] + jl];
-            Gp[g] = (int64_t)Gi.size();
+            int64_t d = Gp[g];
             for (int64_t e = Ap[gc]; e < Ap[gc + 1]; e++) {
                 const int64_t r = Ai[e];
                 if (comp[r] != c) continue;
                 const int64_t rl = sp.loc[r];
-                Gi.push_back(off[q] + rl);
-                Gx.push_back(Ax[e]);
+                Gi[d] = off[q] + rl;
+                Gx[d++] = Ax[e];
                 // ||A_c||_1 of the symmetric matrix of the upper triangle
                 if (rl <= jl) {
                     colsum[jl] += fabs(Ax[e]);
@@ -396,10 +421,12 @@ int batched_krylov(const int64_t *Ap, const int64_t *Ai, const double *Ax,
         double mx = 0.0;
         for (double v : colsum) mx = std::max(mx, v);
         anorm[q] = mx > 0 ? mx : 1.0;
-    }
-    Gp[ng] = (int64_t)Gi.size();
+    });
     HostCSR A;
-    int rc = spx::build_full_csr(ng, Gp.data(), Gi.data(), Gx.data(), &A);
+    // a full, sorted symmetric input keeps both properties in its diagonal
+    // blocks (each component's rows keep their order)
+    int rc = full_sorted ? spx::build_full_csr_sorted(ng, Gp.data(), Gi.data(), Gx.data(), &A)
+                         : spx::build_full_csr(ng, Gp.data(), Gi.data(), Gx.data(), &A);
     if (rc) return rc;
     std::vector<double> lam((size_t)nseg * k), res((size_t)nseg * k);
     std::vector<double> X(want_vec ? (size_t)ng * k : 0);
@@ -610,7 +637,7 @@ int speigs_batched(speigs_int n, const speigs_int *Ap, const speigs_int *Ai, con
         std::vector<int64_t> handed;
         const int handoff = !ext || ext->handoff == 0 ? 8 : ext->handoff;
         int rcs = batched_krylov(Ap, Ai, Ax, cv, sp, kry, k, which, o2, V != nullptr, cr, &handed,
-                                 handoff);
+                                 handoff, full_sorted);
         if (rcs < 0) return rcs;
         if (rcs == 1) rest.insert(rest.end(), kry.begin(), kry.end());
         else rest.insert(rest.end(), handed.begin(), handed.end());

@@ -186,12 +186,40 @@ struct NDState {
                 }
                 record(std::move(sp));
             }
-            int32_t at = lo;
+            // the pieces touch disjoint vertex sets: with spare threads they
+            // are ordered concurrently, largest first, each into its own
+            // range of perm (the result does not depend on the schedule)
+            std::vector<int32_t> at(pieces.size());
+            int32_t a0 = lo;
             for (size_t i = 0; i < pieces.size(); i++) {
-                int32_t sz = (int32_t)pieces[i].size();
-                order_region(std::move(pieces[i]), ids[i], at);
-                at += sz;
+                at[i] = a0;
+                a0 += (int32_t)pieces[i].size();
             }
+            const int avail = m >= kParallelMin && pieces.size() > 1
+                                  ? std::max(0, spare_threads.exchange(0)) : 0;
+            const int nw = (int)std::min<size_t>(pieces.size(), (size_t)avail + 1);
+            if (nw > 1) {
+                std::vector<int32_t> big(pieces.size());
+                for (size_t i = 0; i < pieces.size(); i++) big[i] = (int32_t)i;
+                std::stable_sort(big.begin(), big.end(), [&](int32_t x, int32_t y) {
+                    return pieces[x].size() > pieces[y].size();
+                });
+                std::atomic<size_t> nexti{0};
+                auto work = [&] {
+                    for (size_t q; (q = nexti.fetch_add(1)) < big.size();) {
+                        const int32_t i = big[q];
+                        order_region(std::move(pieces[i]), ids[i], at[i]);
+                    }
+                };
+                std::vector<std::thread> th;
+                for (int t = 1; t < nw; t++) th.emplace_back(work);
+                work();
+                for (auto &t : th) t.join();
+            } else {
+                for (size_t i = 0; i < pieces.size(); i++)
+                    order_region(std::move(pieces[i]), ids[i], at[i]);
+            }
+            spare_threads.fetch_add(avail);
             return;
         }
         for (int it = 0; it < 6; it++) {
@@ -435,19 +463,35 @@ extern "C" int spx_analyze(int32_t n, const int64_t *rowptr, const int32_t *col,
         {
             std::map<std::pair<int32_t, int32_t>, const NDState::Split *> split_of;
             for (const auto &sp : splits) split_of[{sp.lo, sp.m}] = &sp;
+            // threads beyond the caller's, shared by every level of the
+            // recursion: a split takes what it can use and gives it back
+            std::atomic<int> spare{(int)spx::host_threads() - 1};
+            auto take = [&](int want) {
+                int have = spare.load();
+                while (have > 0) {
+                    const int got = std::min(have, want);
+                    if (spare.compare_exchange_weak(have, have - got)) return got;
+                }
+                return 0;
+            };
             std::function<void(int32_t, int32_t)> tree_range = [&](int32_t lo, int32_t m) {
                 auto it = split_of.find({lo, m});
                 if (it == split_of.end()) { liu(lo, lo + m); return; }
                 const NDState::Split &sp = *it->second;
+                const int np = (int)sp.parts.size();
+                const int extra = np > 1 ? take(np - 1) : 0;
+                std::atomic<int> nextp{0};
+                auto work = [&] {
+                    for (int q; (q = nextp.fetch_add(1)) < np;)
+                        tree_range(sp.parts[q].first, sp.parts[q].second);
+                };
                 {
                     spx::TaskGroup g;
-                    for (size_t q = 1; q < sp.parts.size(); q++) {
-                        const auto pr = sp.parts[q];
-                        g.run([&tree_range, pr] { tree_range(pr.first, pr.second); });
-                    }
-                    if (!sp.parts.empty()) tree_range(sp.parts[0].first, sp.parts[0].second);
+                    for (int t = 0; t < extra; t++) g.run(work);
+                    work();
                     g.wait();
                 }
+                spare.fetch_add(extra);
                 int32_t end = lo;
                 for (const auto &pr : sp.parts) end = std::max(end, pr.first + pr.second);
                 liu(end, lo + m);
@@ -517,29 +561,57 @@ extern "C" int spx_analyze(int32_t n, const int64_t *rowptr, const int32_t *col,
         }
 
         // ---- 5. column counts (Gilbert, Ng and Peyton)
+        // In postorder every tree of the elimination forest is a contiguous
+        // range of columns ending at its root, and the algorithm reads and
+        // writes only entries of the tree it is in: ranges of whole trees
+        // are counted on separate threads.
         std::vector<int32_t> first(n, -1), maxfirst(n, -1), prevleaf(n, -1), ancestor(n);
-        std::vector<int64_t> delta(n, 0);
-        for (int32_t k = 0; k < n; k++) {
-            int32_t j = k;
-            delta[j] = (first[j] == -1) ? 1 : 0;
-            for (; j != -1 && first[j] == -1; j = par[j]) first[j] = k;
-        }
-        for (int32_t i = 0; i < n; i++) ancestor[i] = i;
-        for (int32_t j = 0; j < n; j++) {
-            if (par[j] != -1) delta[par[j]]--;
-            for (int64_t p = prp[j]; p < prp[j + 1]; p++) {
-                int32_t i = pci[p];
-                int jleaf;
-                int32_t q = gnp_leaf(i, j, first.data(), maxfirst.data(), prevleaf.data(),
-                                     ancestor.data(), &jleaf);
-                if (jleaf >= 1) delta[j]++;
-                if (jleaf == 2) delta[q]--;
+        std::vector<int64_t> delta(n, 0), cc(n, 0);
+        auto count_range = [&](int32_t c0, int32_t c1) {
+            for (int32_t k = c0; k < c1; k++) {
+                int32_t j = k;
+                delta[j] = (first[j] == -1) ? 1 : 0;
+                for (; j != -1 && first[j] == -1; j = par[j]) first[j] = k;
             }
-            if (par[j] != -1) ancestor[j] = par[j];
+            for (int32_t i = c0; i < c1; i++) ancestor[i] = i;
+            for (int32_t j = c0; j < c1; j++) {
+                if (par[j] != -1) delta[par[j]]--;
+                for (int64_t p = prp[j]; p < prp[j + 1]; p++) {
+                    int32_t i = pci[p];
+                    int jleaf;
+                    int32_t q = gnp_leaf(i, j, first.data(), maxfirst.data(), prevleaf.data(),
+                                         ancestor.data(), &jleaf);
+                    if (jleaf >= 1) delta[j]++;
+                    if (jleaf == 2) delta[q]--;
+                }
+                if (par[j] != -1) ancestor[j] = par[j];
+            }
+            for (int32_t j = c0; j < c1; j++) cc[j] = delta[j];
+            for (int32_t j = c0; j < c1; j++)
+                if (par[j] != -1) cc[par[j]] += cc[j];
+        };
+        {
+            // chunks of whole trees, about n / (4 threads) columns each
+            const int32_t want = std::max<int32_t>(kGrain, n / (int32_t)(4 * spx::host_threads()));
+            std::vector<std::pair<int32_t, int32_t>> chunks;
+            int32_t c0 = 0;
+            for (int32_t j = 0; j < n; j++)
+                if (par[j] == -1 && (j + 1 - c0 >= want || j == n - 1)) {
+                    chunks.push_back({c0, j + 1});
+                    c0 = j + 1;
+                }
+            if (c0 < n) chunks.push_back({c0, n});
+            std::atomic<size_t> nextc{0};
+            auto worker = [&] {
+                for (size_t q; (q = nextc.fetch_add(1)) < chunks.size();)
+                    count_range(chunks[q].first, chunks[q].second);
+            };
+            const unsigned nth = (unsigned)std::min<size_t>(spx::host_threads(), chunks.size());
+            spx::TaskGroup g(nth > 1);
+            for (unsigned t = 1; t < nth; t++) g.run(worker);
+            worker();
+            g.wait();
         }
-        std::vector<int64_t> cc(delta);
-        for (int32_t j = 0; j < n; j++)
-            if (par[j] != -1) cc[par[j]] += cc[j];
 
         // ---- 6. fundamental supernodes
         std::vector<int32_t> nchild(n, 0);
