@@ -36,6 +36,7 @@ PKG_DIR = os.path.join(ROOT, "sparse-eigs-mex_b200")
 REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libspeigs_ref.so")
 METRIC = "time to k eigenpairs @ resid 1e-10: mixed/learned vs plain FP64, same B200"
 TOL = 1e-10
+TUNE_SEED = 1000          # a training operator of the 48^3 GRF family (the tuner's input)
 
 
 def import_pkg():
@@ -262,19 +263,57 @@ def run_metric(args, pkg, wl, ctx):
         with torch.cuda.stream(stream):
             Yw.copy_(Y32.t())
 
-    forms_spec = [("fp64", s.FP64, False, -1), ("mixed", s.MIXED, False, -1)]
+    # ---- autotuning (before any timed region): the block size and basis
+    # size of the learned forms, chosen by pkg.tune on a TRAINING operator
+    # of the same family (seed 1000, one the network was trained on), with
+    # that operator's own proposal; the held-out operator is not seen
+    tuning = {}
+    if net is not None and not args.no_tune:
+        kap_t = w.grf_conductivity(N, TUNE_SEED)
+        A_t = w.grf3d(N, TUNE_SEED)
+        rp_t, ci_t, w_t = L.grid_graph(N, kap_t)
+        X_t = L.features(N, kap_t)
+        tt = [torch.from_numpy(a).to(dev) for a in (rp_t, ci_t, w_t, X_t)]
+        Y_t = torch.zeros((P, n), dtype=torch.float64, device=dev)
+        rc = net.forward_device(n, tt[0].data_ptr(), tt[1].data_ptr(), tt[2].data_ptr(),
+                                tt[3].data_ptr(), Y32.data_ptr(),
+                                torch.cuda.current_stream().cuda_stream)
+        if rc != 0:
+            raise RuntimeError(f"mpnn forward rc={rc}")
+        Y_t.copy_(Y32.t())
+        torch.cuda.synchronize()
+        cache = os.path.join(ROOT, "gpurun_out", "tune_cache.json") \
+            if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else None
+        t_tune = time.perf_counter()
+        for pname, prec in (("fp64", s.FP64), ("mixed", s.MIXED)):
+            e = pkg.tune.tune_operator(A_t, k, s.SM, prec, warm_ptr=Y_t.data_ptr(), warm_cols=P,
+                                       tol=TOL, blocks=(-1, 8, 16, 24), ncvs=(64, 96, 128),
+                                       reps=1, cache=cache, lib=lib)
+            tuning[pname] = e["best"]
+            tuning[pname + "_candidates"] = [
+                {kk: r.get(kk) for kk in ("block", "ncv", "ms", "ok", "block_solves")}
+                for r in e["results"]]
+        tuning["seconds"] = round(time.perf_counter() - t_tune, 2)
+        del Y_t, tt
+    fb, fn = (tuning["fp64"]["block"], tuning["fp64"]["ncv"]) if tuning else (0, 0)
+    mb, mn = (tuning["mixed"]["block"], tuning["mixed"]["ncv"]) if tuning else (0, 0)
+
+    forms_spec = [("fp64", s.FP64, False, -1, 0), ("mixed", s.MIXED, False, -1, 0)]
     if net is not None:
-        forms_spec += [("fp64+learned", s.FP64, True, 0), ("mixed+learned", s.MIXED, True, 0)]
-    forms_spec += [("fp64+block(random)", s.FP64, False, P),
-                   ("mixed+block(random)", s.MIXED, False, P)]
+        forms_spec += [("fp64+learned", s.FP64, True, fb, fn),
+                       ("mixed+learned", s.MIXED, True, mb, mn)]
+    forms_spec += [("fp64+block(random)", s.FP64, False, fb if fb > 0 else P, fn),
+                   ("mixed+block(random)", s.MIXED, False, mb if mb > 0 else P, mn)]
     target = "mixed+learned" if net is not None else "mixed"
+    form_params = {name: {"block": b, "ncv": c} for name, _, _, b, c in forms_spec}
     forms, keep = {}, {}
-    for name, prec, learned, block in forms_spec:
+    for name, prec, learned, block, ncv in forms_spec:
         ext = s.ext_opts(lib, precision=prec, block=block)
         if learned:
             ext.warm = Yw.data_ptr()
             ext.warm_cols = P
-        plan = s.Plan(A, s.SM, opts, lib=lib, ext=ext)
+        fopts = s.default_opts(lib, tol=TOL, ncv=ncv)
+        plan = s.Plan(A, s.SM, fopts, lib=lib, ext=ext)
         pstream = torch.cuda.ExternalStream(plan.stream(), device=dev)
         lam = torch.zeros(k, dtype=torch.float64, device=dev)
         V = torch.zeros((k, n), dtype=torch.float64, device=dev)
@@ -326,6 +365,7 @@ def run_metric(args, pkg, wl, ctx):
                        "step_ms": [round(x, 3) for x in step_ms],
                        "nops": int(info["nops"]), "restarts": int(info["restarts"]),
                        "flag": int(info["flag"]), "block": int(ei["block"]),
+                       "ncv_opt": int(ncv),
                        "block_solves": int(ei["block_solves"]),
                        "refine_steps": int(ei["refine_steps"]), "warm_cols": int(ei["warm_cols"]),
                        "max_resid_over_anorm": float(r.max() / info["anorm"]),
@@ -344,8 +384,10 @@ def run_metric(args, pkg, wl, ctx):
             Yp = L.propose(net, N, kap)
             extra_h2d = rowptr.nbytes + col.nbytes + wts.nbytes + X.nbytes
             extra_d2h = Yp.nbytes // 2          # float32 on the device, widened on the host
-            ext = s.ext_opts(lib, precision=prec)
-            rc, *_ = s.speigs_ex(A, k, s.SM, opts, ext, vectors=True, lib=lib, warm=Yp)
+            fp = form_params[name]
+            ext = s.ext_opts(lib, precision=prec, block=fp["block"])
+            eopts = s.default_opts(lib, tol=TOL, ncv=fp["ncv"])
+            rc, *_ = s.speigs_ex(A, k, s.SM, eopts, ext, vectors=True, lib=lib, warm=Yp)
         else:
             ext = s.ext_opts(lib, precision=prec, block=-1)
             rc, *_ = s.speigs_ex(A, k, s.SM, opts, ext, vectors=True, lib=lib)
@@ -431,6 +473,10 @@ def run_metric(args, pkg, wl, ctx):
             "config": {"workload": wl["desc"], "n": int(n), "nnz": int(nnz), "k": k, "tol": TOL,
                        "form": target + (" (block thick-restart Lanczos, first block = the "
                                          "network's %d-column proposal)" % P if net else ""),
+                       "form_params": form_params,
+                       "tuning": tuning or None,
+                       "tuning_operator": f"48^3 GRF seed {TUNE_SEED} (a training operator)"
+                                          if tuning else None,
                        "checkpoint": os.path.relpath(L.CHECKPOINT, ROOT) if have_net else None,
                        "parallelism": f"replicas x{ctx['world']}",
                        "l2": "256 MiB buffer written between timed steps",
@@ -593,6 +639,9 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="grf48")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="learned forms with the automatic block method instead of the block "
+                         "and basis sizes the tuner picks on a training operator")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="operator of the timed line: plain FP64 factor, or FP32 factor on the "
                          "tensor cores with FP64 refinement")
