@@ -491,6 +491,70 @@ def run_metric(args, pkg, wl, ctx):
     return 0
 
 
+def run_one_form(args, pkg, wl, ctx):
+    """One form of the 48^3 GRF metric alone, for profiling launch lists and
+    single kernels: --form NAME (fp64, mixed, fp64+learned, mixed+learned,
+    fp64+block, mixed+block) with --block / --ncv, W warm-up and K timed
+    solves on a resident plan.  Prints one JSON line with the per-solve
+    device times and phases; no CPU baseline, no end-to-end leg."""
+    import torch
+    s, w, L = pkg.speigs, pkg.workloads, pkg.learned
+    lib, dev = ctx["lib"], ctx["dev"]
+    N, seed = 48, 3200
+    A = wl["build"]()
+    n, k = A.shape[0], wl["k"]
+    name = args.form
+    prec = s.MIXED if name.startswith("mixed") else s.FP64
+    learned = "learned" in name
+    block = -1 if "+" not in name else args.block
+    ext = s.ext_opts(lib, precision=prec, block=block)
+    Yw = None
+    if learned:
+        net = L.WarmStartNet.load(L.CHECKPOINT, lib=lib)
+        kap = w.grf_conductivity(N, seed)
+        rowptr, col, wts = L.grid_graph(N, kap)
+        tt = [torch.from_numpy(a).to(dev) for a in (rowptr, col, wts, L.features(N, kap))]
+        Y32 = torch.empty((n, net.nout), dtype=torch.float32, device=dev)
+        rc = net.forward_device(n, tt[0].data_ptr(), tt[1].data_ptr(), tt[2].data_ptr(),
+                                tt[3].data_ptr(), Y32.data_ptr(),
+                                torch.cuda.current_stream().cuda_stream)
+        if rc != 0:
+            raise RuntimeError(f"mpnn forward rc={rc}")
+        Yw = Y32.t().contiguous().to(torch.float64)
+        ext.warm = Yw.data_ptr()
+        ext.warm_cols = net.nout
+    opts = s.default_opts(lib, tol=TOL, ncv=args.ncv if "+" in name else 0)
+    plan = s.Plan(A, s.SM, opts, lib=lib, ext=ext)
+    st = torch.cuda.ExternalStream(plan.stream(), device=dev)
+    lam = torch.zeros(k, dtype=torch.float64, device=dev)
+    V = torch.zeros((k, n), dtype=torch.float64, device=dev)
+    res = torch.zeros(k, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    ms, info = [], None
+    for it in range(args.warmup + args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        rc, info = plan.solve_device(k, lam.data_ptr(), V.data_ptr(), res.data_ptr())
+        e1.record(st)
+        e1.synchronize()
+        if rc != 0:
+            raise RuntimeError(f"{name}: rc={rc} {s.last_error(lib)}")
+        if it >= args.warmup:
+            ms.append(e0.elapsed_time(e1))
+    ei = plan.ext_info()
+    plan.close()
+    print(json.dumps({"form": name, "block": block, "ncv": opts.ncv, "step_ms": ms,
+                      "nops": int(info["nops"]), "restarts": int(info["restarts"]),
+                      "flag": int(info["flag"]), "block_solves": int(ei["block_solves"]),
+                      "refine_steps": int(ei["refine_steps"]),
+                      "phases_ms": {kk: round(info[kk] * 1e3, 3) for kk in
+                                    ("t_factor", "t_op", "t_ortho", "t_resid", "t_ritz")}}))
+    return 0
+
+
 def run_batched(args, pkg, wl, rank=0, world=1, local=0):
     """k eigenpairs of every component through speigs_batched -- the
     components on the Krylov route solved together by the segmented lockstep
@@ -639,6 +703,11 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="grf48")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--form", default=None,
+                    help="time this form of the 48^3 GRF metric alone (profiling): fp64, mixed, "
+                         "fp64+learned, mixed+learned, fp64+block, mixed+block")
+    ap.add_argument("--block", type=int, default=8, help="block size of --form's block forms")
+    ap.add_argument("--ncv", type=int, default=96, help="basis size of --form's block forms")
     ap.add_argument("--no-tune", action="store_true",
                     help="learned forms with the automatic block method instead of the block "
                          "and basis sizes the tuner picks on a training operator")
@@ -683,7 +752,7 @@ def main():
                 dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ctx = {"lib": lib, "dev": dev, "rank": rank, "world": world, "barrier": barrier,
                "max": tmax}
-        rc = run_metric(args, pkg, wl, ctx)
+        rc = run_one_form(args, pkg, wl, ctx) if args.form else run_metric(args, pkg, wl, ctx)
         if world > 1:
             dist.destroy_process_group()
         return rc

@@ -32,7 +32,8 @@ extern "C" {
 typedef struct {
     int          precision;    /* SPEIGS_B200_FP64 (default) or SPEIGS_B200_MIXED     */
     int          refine_max;   /* corrections per solve (mixed); 0 => 10               */
-    double       refine_tol;   /* backward-error target (mixed); 0 => 1e-14            */
+    double       refine_tol;   /* backward-error target (mixed); 0 => 1e-2 tol, within
+                                  [1e-14, 1e-12]                                        */
     const double *warm;        /* optional start subspace, n x warm_cols, column-major,
                                   host memory; NULL => the reference's random start   */
     speigs_int   warm_cols;

@@ -1271,6 +1271,7 @@ struct speigs_plan_s {
     bool lu = false;                  // indefinite route: the dense inverse below
     double *d_ainv = nullptr;         // n x n, allocated on first use
     spx::RefineState refine;          // mixed precision only
+    double refine_tol_user = 0;       // speigs_ext_opts.refine_tol (0: from opts.tol)
     int64_t refine_reported = 0;      // corrections already reported
     int64_t last_refine = 0;          // corrections of the last solve
     int64_t last_ops = 0;             // operator applications of the last solve
@@ -1328,7 +1329,7 @@ int plan_from_csr(HostCSR &A, speigs_which which, const speigs_opts &o, double a
     p->anorm = anorm;
     p->mf.mixed = (which == SPEIGS_SM && ext && ext->precision == SPEIGS_B200_MIXED);
     if (ext && ext->refine_max > 0) p->refine.max_steps = ext->refine_max;
-    if (ext && ext->refine_tol > 0) p->refine.tol = ext->refine_tol;
+    if (ext && ext->refine_tol > 0) p->refine_tol_user = ext->refine_tol;
     if (p->stream.err != cudaSuccess) { int rc = cuda_fail(p->stream.err, "stream"); speigs_plan_destroy(p); return rc; }
     cudaStream_t st = p->stream.s;
     const int n = p->A.n;
@@ -1489,6 +1490,14 @@ static int plan_solve(speigs_plan_s *p, int64_t k, double *lambda, double *V, do
     info->ncomp = 0;
     info->t_analyze = p->reuse_factor ? 0.0 : p->t_analyze;
     DevA dA{n, p->d_rp, p->d_ci, p->d_va};
+    // the refinement's backward-error target: the caller's, else two orders
+    // below the Lanczos tolerance, within [1e-14, 1e-12] -- a solve refined
+    // that far perturbs the operator by less than the residual test admits
+    {
+        const double t = p->opts.tol > 0 ? p->opts.tol : 1e-14;
+        p->refine.tol = p->refine_tol_user > 0 ? p->refine_tol_user
+                                               : std::min(1e-12, std::max(1e-14, 1e-2 * t));
+    }
     SpmvOperator spmv_op(dA);
     CholOperator chol_op(&p->mf);
     MixedCholOperator mixed_op(&p->mf, dA, 0.0, p->anorm, &p->refine);
