@@ -407,38 +407,44 @@ def run_metric(args, pkg, wl, ctx):
         e2e[name] = {"value": statistics.mean(ts), "unit": "s", "h2d_bytes_per_step": int(h2d),
                      "d2h_bytes_per_step": int(d2h), "steps_s": [round(x, 4) for x in ts]}
 
-    # ---- roofline of the dominant kernel of the timed form: its operator
-    # application (block solve with the FP32 panels, and the FP64 block
-    # residuals and corrections of the refinement), bytes from the plan's
-    # figures, time = the device time of the applications inside the timed
-    # solves (CUDA events on the plan's stream)
+    # ---- roofline of the dominant kernel of the timed form.  For a block
+    # form that is the block solve mf_bsolve (FP32 panels in the mixed
+    # form): algorithmic bytes of one launch (the plan's solve-pair bytes
+    # with rows of b values) over its average device time, measured by the
+    # library with CUDA events around every block solve of the timed solve
+    # (t_block_solve over the solves that ran; corrections that returned at
+    # once on the device add a few microseconds each).  For the
+    # single-vector forms it is the solve pair mf_solve_sf, timed the same
+    # way through the operator phase.
     kt = keep[target]
     ei, info = kt["ei"], kt["info"]
     bsz = max(1, int(ei["block"]))
-    apps = max(1, int(ei["block_solves"]) - int(ei["refine_steps"])) if bsz > 1 else max(1, int(info["nops"]))
-    corr = int(ei["refine_steps"])
     if bsz > 1:
-        bs_bytes = block_solve_bytes(kt["costs"]["op_bytes"], n, bsz)
-        res_bytes = 12.0 * nnz + 4.0 * n + 24.0 * n * bsz
-        total = (apps + corr) * (bs_bytes + res_bytes) + corr * 24.0 * n * bsz
+        launches = max(1, int(ei["block_solves"]))
+        per_launch = block_solve_bytes(kt["costs"]["op_bytes"], n, bsz)
+        avg_s = float(ei["t_block_solve"]) / launches
+        kname = f"mf_bsolve<{(bsz + 7) // 8 * 8}>"
     else:
-        total = info["nops"] * kt["costs"]["op_bytes"]
-    achieved = total / kt["t_op"] / 1e9 if kt["t_op"] > 0 else None
+        launches = max(1, int(info["nops"]) + int(ei["refine_steps"]))
+        per_launch = kt["costs"]["op_bytes"]
+        avg_s = kt["t_op"] / launches
+        kname = "mf_solve_sf"
+    achieved = per_launch / avg_s / 1e9 if avg_s > 0 else None
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         try:
-            traffic = json.load(open(tpath)).get(f"grf48:{target}")
+            traffic = json.load(open(tpath)).get(f"grf48:{target}:{kname}")
         except Exception:
             traffic = None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                "kernel": "refined block application: mf_bsolve (FP32 panels, %d columns) + "
-                          "FP64 block residuals and corrections" % bsz if target.startswith("mixed")
-                          else "block shift-invert solve",
-                "bytes_per_solve": total,
-                "op_time_s": kt["t_op"], "block_applications": apps, "corrections": corr,
+                "kernel": kname + (" (FP32 panels, %d right-hand sides)" % bsz
+                                   if target.startswith("mixed") and bsz > 1 else ""),
+                "bytes_per_launch": per_launch, "avg_launch_s": avg_s, "launches": launches,
                 "peak_source": peak_kind}
+    if bsz > 1:
+        roofline["queued_solves"] = int(ei["block_solve_calls"])
 
     # ---- the reference's CPU solver on the same operator (rank 0, N=1)
     cpu, check = None, {}
@@ -545,8 +551,10 @@ def run_one_form(args, pkg, wl, ctx):
         if it >= args.warmup:
             ms.append(e0.elapsed_time(e1))
     ei = plan.ext_info()
+    costs = plan.costs()
     plan.close()
     print(json.dumps({"form": name, "block": block, "ncv": opts.ncv, "step_ms": ms,
+                      "costs": costs,
                       "nops": int(info["nops"]), "restarts": int(info["restarts"]),
                       "flag": int(info["flag"]), "block_solves": int(ei["block_solves"]),
                       "refine_steps": int(ei["refine_steps"]),

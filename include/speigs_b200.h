@@ -68,6 +68,11 @@ typedef struct {
      * t_factor / t_iter: input checks and the CSR build, plan set-up (device
      * buffers, uploads), copy-out and release */
     double       t_checks, t_setup, t_release;
+    /* block method: device time (s) of the block solves (their layout
+     * conversions included) and the number queued, corrections that returned
+     * at once on the device included */
+    double       t_block_solve;
+    speigs_int   block_solve_calls;
 } speigs_ext_info;
 
 /* Fill *e with the defaults (FP64, no start subspace). */

@@ -355,7 +355,26 @@ struct BlockOperator {
     virtual int apply(const double *V, int64_t ldv, double *W, int64_t ldw, int b,
                       cudaStream_t st) = 0;
     virtual const int *error_word() const { return nullptr; }
+    // A device word set when an application fell short of its accuracy
+    // target with the work queued for it (the caller redoes that work with
+    // set_full(true)); nullptr when every application is complete.
+    virtual int *short_word() const { return nullptr; }
+    virtual void set_full(bool) {}
     int64_t napps = 0, nvecs = 0;
+    // optional: device time of the block solves (layout conversions
+    // included), accumulated into *ms_solve by tm
+    PhaseTimer *tm = nullptr;
+    double *ms_solve = nullptr;
+    double ms_solve_acc = 0;
+    int64_t solve_calls = 0;
+    int timed_solve(Factor *plan, const double *B, int64_t ldb, double *X, int64_t ldx, int nr,
+                    cudaStream_t st, const int *skip = nullptr) {
+        solve_calls++;
+        const int t = tm ? tm->begin() : -1;
+        const int rc = plan->solve_block(B, ldb, X, ldx, nr, st, skip);
+        if (tm) tm->end(t, ms_solve);
+        return rc;
+    }
 };
 
 struct BlockCholOperator : BlockOperator {
@@ -365,7 +384,7 @@ struct BlockCholOperator : BlockOperator {
               cudaStream_t st) override {
         napps++;
         nvecs += b;
-        return plan->solve_block(V, ldv, W, ldw, b, st);
+        return timed_solve(plan, V, ldv, W, ldw, b, st);
     }
     const int *error_word() const override { return plan->error_word(); }
 };
@@ -375,10 +394,16 @@ struct BlockRefineState {
     double *R = nullptr, *D = nullptr, *part = nullptr;
     int64_t ld = 0;
     int *flag = nullptr, *count = nullptr;
+    int *short_word = nullptr;   // set when a solve was left unconverged within `budget`
     unsigned *counter = nullptr;
     int max_steps = 10;
+    int budget = 0;              // corrections queued per solve (0: max_steps)
     double tol = 1e-14;
 };
+
+__global__ void flag_if_unset_kernel(const int *flag, int *word) {
+    if (!*(volatile const int *)flag) *word = 1;
+}
 
 // Mixed precision on a block: X = M^{-1} B with the FP32 factor, then
 // R = B - (A + shift I) X and X += M^{-1} R until every column passes the
@@ -396,21 +421,34 @@ struct BlockMixedOperator : BlockOperator {
               cudaStream_t st) override {
         napps++;
         nvecs += b;
-        int rc = plan->solve_block(V, ldv, W, ldw, b, st);
+        int rc = timed_solve(plan, V, ldv, W, ldw, b, st);
         if (rc) return rc;
         cudaMemsetAsync(rf->flag, 0, sizeof(int), st);
-        for (int it = 0; it <= rf->max_steps; it++) {
+        // With a budget, only that many corrections are queued (the rest of
+        // max_steps would return at once on the device flag but still cost
+        // their launches); a solve still unconverged after them sets
+        // short_word, and the caller redoes its work with the full loop.
+        const int steps = (rf->budget > 0 && rf->short_word && !full)
+                              ? std::min(rf->budget, rf->max_steps) : rf->max_steps;
+        for (int it = 0; it <= steps; it++) {
             launch_block_refine_residual(A.n, A.rp, A.ci, A.va, shift, V, ldv, W, ldw, rf->R,
                                          rf->ld, b, rf->tol, anorm, rf->flag, rf->count,
                                          rf->part, rf->counter, st);
-            if (it == rf->max_steps) break;
-            rc = plan->solve_block(rf->R, rf->ld, rf->D, rf->ld, b, st, rf->flag);
+            if (it == steps) break;
+            rc = timed_solve(plan, rf->R, rf->ld, rf->D, rf->ld, b, st, rf->flag);
             if (rc) return rc;
             launch_block_axpy_unless(A.n, b, W, ldw, rf->D, rf->ld, rf->flag, st);
+        }
+        if (steps < rf->max_steps) {
+            flag_if_unset_kernel<<<1, 1, 0, st>>>(rf->flag, rf->short_word);
+            note_launch();
         }
         return 0;
     }
     const int *error_word() const override { return plan->error_word(); }
+    int *short_word() const override { return rf->budget > 0 ? rf->short_word : nullptr; }
+    void set_full(bool f) override { full = f; }
+    bool full = false;
 };
 
 // ------------------------------------------------------------- Lanczos --
@@ -900,6 +938,14 @@ static int block_lanczos_device(BlockOperator &op, const DevA &A, int n, int64_t
 
     PhaseTimer tm(st);
     double ms_op = 0, ms_ortho = 0, ms_resid = 0, ms_ritz = 0;
+    // the operator times its block solves with this loop's timer (resolved
+    // at each sync) until the loop returns
+    struct TimerLink {
+        BlockOperator &o;
+        ~TimerLink() { o.tm = nullptr; }
+    } tlink{op};
+    op.tm = &tm;
+    op.ms_solve = &op.ms_solve_acc;
     auto sync = [&](const char *where) -> int {
         if (op_err) copy_async(h_operr, op_err, sizeof(int), cudaMemcpyDeviceToHost, st);
         cudaError_t e = cudaStreamSynchronize(st);
@@ -1008,6 +1054,7 @@ static int block_lanczos_device(BlockOperator &op, const DevA &A, int n, int64_t
         napps_cycle = op.napps;
         nvecs_cycle = op.nvecs;
         spec_cycle = true;
+        op.set_full(false);
         cudaMemsetAsync(B.cstat + 2, 0, sizeof(int), st);
     };
     start_cycle();
@@ -1039,17 +1086,24 @@ static int block_lanczos_device(BlockOperator &op, const DevA &A, int n, int64_t
             jc = mm;
             continue;
         }
-        if (spec_cycle) {
-            // a block that lost rank in this cycle: redo the cycle from its
-            // start with the dependency test read after every step
+        if (spec_cycle || op.short_word()) {
+            // a block that lost rank in this cycle, or an application that
+            // fell short of its accuracy: redo the cycle from its start, with
+            // the dependency test read after every step and the full
+            // refinement loop
             copy_async(h_dep, B.cstat + 2, sizeof(int), cudaMemcpyDeviceToHost, st);
+            h_dep[1] = 0;
+            if (op.short_word())
+                copy_async(h_dep + 1, op.short_word(), sizeof(int), cudaMemcpyDeviceToHost, st);
             if (int e = sync("block step check")) return e;
-            if (*h_dep) {
+            if ((spec_cycle && h_dep[0]) || h_dep[1]) {
                 cudaMemsetAsync(B.cstat + 2, 0, sizeof(int), st);
+                if (op.short_word()) cudaMemsetAsync(op.short_word(), 0, sizeof(int), st);
                 op.napps = napps_cycle;
                 op.nvecs = nvecs_cycle;
                 jc = jc_cycle;
                 spec_cycle = false;
+                op.set_full(true);
                 continue;
             }
         }
@@ -1281,6 +1335,9 @@ struct speigs_plan_s {
     int ext_block = 0;                // speigs_ext_opts.block
     int last_block = 0;               // block size of the last solve (0: single vector)
     int64_t last_block_solves = 0;    // its block solves (applications + corrections)
+    double last_t_block_solve = 0;    // device time of its block solves (s)
+    int64_t last_block_solve_calls = 0;   // block solves queued (corrections skipped on
+                                          // the device included)
     double t_analyze = 0;
     std::vector<void *> owned;
 };
@@ -1565,12 +1622,17 @@ static int plan_solve(speigs_plan_s *p, int64_t k, double *lambda, double *V, do
                 brf.part = ar.alloc<double>((size_t)3 * kBlockMaxB * ((n + 255) / 256));
                 brf.flag = ar.alloc<int>(1);
                 brf.count = ar.alloc<int>(1);
+                brf.short_word = ar.alloc<int>(1);
                 brf.counter = ar.alloc<unsigned>(1);
                 if (ar.failed) return SPEIGS_ERR_MEM;
                 cudaMemsetAsync(brf.count, 0, sizeof(int), st);
+                cudaMemsetAsync(brf.short_word, 0, sizeof(int), st);
                 cudaMemsetAsync(brf.counter, 0, sizeof(unsigned), st);
                 brf.max_steps = p->refine.max_steps;
                 brf.tol = p->refine.tol;
+                // two corrections are queued per block solve; a cycle in which
+                // one fell short is redone with the full loop
+                brf.budget = 2;
             }
             BlockCholOperator bchol(&p->mf);
             BlockMixedOperator bmixed(&p->mf, dA, p->shift, p->anorm, &brf);
@@ -1588,6 +1650,8 @@ static int plan_solve(speigs_plan_s *p, int64_t k, double *lambda, double *V, do
             }
             p->last_refine = cnt;
             p->last_block_solves = bop.napps + cnt;
+            p->last_t_block_solve = bop.ms_solve_acc * 1e-3;
+            p->last_block_solve_calls = bop.solve_calls;
         } else {
         rc = lanczos_device(*op, dA, n, k, p->opts, p->anorm, lam_h.data(), res_h.data(), &X,
                             &ldx, &nout, info, stats, ar, pinbuf, st, dwarm, wcols, &wused);
@@ -1644,6 +1708,8 @@ static void fill_ext_info(const speigs_plan_s *p, speigs_ext_info *e) {
     e->warm_cols = p->last_warm;
     e->block = p->last_block;
     e->block_solves = p->last_block_solves;
+    e->t_block_solve = p->last_t_block_solve;
+    e->block_solve_calls = p->last_block_solve_calls;
     if (p->last_block > 0)
         e->factor_solves = p->which == SPEIGS_SM ? p->last_ops + (int64_t)p->last_refine *
                                                                      p->last_block : 0;

@@ -29,24 +29,52 @@ __device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
 // column by column (stride kVS, so the fragment reads of a half warp fall in
 // distinct banks); warp w owns the 8-row output tiles w and w + 8 of V^T W
 // and all of its 8-column tiles.
+__device__ __forceinline__ void cp_async8z(double *dst, const double *src, bool valid) {
+    const unsigned saddr = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(saddr), "l"(src),
+                 "r"(valid ? 8 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 __global__ void __launch_bounds__(kTbThreads) tsb_tn_part_kernel(
         const double *__restrict__ V, int64_t ldv, int n, int m, const double *__restrict__ W,
         int64_t ldw, int b, int rows_per_part, double *__restrict__ part) {
-    __shared__ double Cs[kBlockMaxM + kBlockMaxB][kVS];
+    // two chunk buffers of (m + b) staged columns: the copies of chunk i+1
+    // (cp.async, 8 bytes each, zero-filled past the range) are in flight
+    // while chunk i is multiplied
+    extern __shared__ double dsm[];
     const int t = threadIdx.x, lane = t & 31, wid = t >> 5, gq = lane >> 2, tq = lane & 3;
-    const int nmt = (m + 7) >> 3, nnt = (b + 7) >> 3;
+    const int nmt = (m + 7) >> 3, nnt = (b + 7) >> 3, ncol = m + b;
     double acc[2][4][2];
 #pragma unroll
     for (int s = 0; s < 2; s++)
 #pragma unroll
         for (int q = 0; q < 4; q++) acc[s][q][0] = acc[s][q][1] = 0.0;
     const int rb = blockIdx.x * rows_per_part, re = min(n, rb + rows_per_part);
-    for (int r0 = rb; r0 < re; r0 += kTbRows) {
+    auto stage = [&](double *Cs, int r0) {
         const int nr = min(kTbRows, re - r0);
-        for (int e = t; e < (m + b) * kTbRows; e += kTbThreads) {
+        for (int e = t; e < ncol * kTbRows; e += kTbThreads) {
             const int c = e >> 5, rr = e & 31;
-            const double *src = c < m ? V + (int64_t)c * ldv : W + (int64_t)(c - m) * ldw;
-            Cs[c][rr] = rr < nr ? src[r0 + rr] : 0.0;
+            const double *src = (c < m ? V + (int64_t)c * ldv : W + (int64_t)(c - m) * ldw) + r0;
+            cp_async8z(Cs + c * kVS + rr, src + (rr < nr ? rr : 0), rr < nr);
+        }
+        cp_async_commit();
+    };
+    if (rb < re) stage(dsm, rb);
+    int buf = 0;
+    for (int r0 = rb; r0 < re; r0 += kTbRows) {
+        const double *Cs = dsm + buf * ncol * kVS;
+        if (r0 + kTbRows < re) {
+            stage(dsm + (buf ^ 1) * ncol * kVS, r0 + kTbRows);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
         }
         __syncthreads();
 #pragma unroll 2
@@ -54,12 +82,12 @@ __global__ void __launch_bounds__(kTbThreads) tsb_tn_part_kernel(
             const int k = ks * 4 + tq;
             double bf[4];
 #pragma unroll
-            for (int q = 0; q < 4; q++) bf[q] = (q * 8 + gq < b) ? Cs[m + q * 8 + gq][k] : 0.0;
+            for (int q = 0; q < 4; q++) bf[q] = (q * 8 + gq < b) ? Cs[(m + q * 8 + gq) * kVS + k] : 0.0;
 #pragma unroll
             for (int s = 0; s < 2; s++) {
                 const int mt = wid + 8 * s;
                 if (mt < nmt) {
-                    const double a = (mt * 8 + gq < m) ? Cs[mt * 8 + gq][k] : 0.0;
+                    const double a = (mt * 8 + gq < m) ? Cs[(mt * 8 + gq) * kVS + k] : 0.0;
 #pragma unroll
                     for (int q = 0; q < 4; q++)
                         if (q < nnt) dmma884(acc[s][q], a, bf[q]);
@@ -67,6 +95,7 @@ __global__ void __launch_bounds__(kTbThreads) tsb_tn_part_kernel(
             }
         }
         __syncthreads();
+        buf ^= 1;
     }
     double *p = part + (size_t)blockIdx.x * (kBlockMaxM * kBlockMaxB);
 #pragma unroll
@@ -134,13 +163,23 @@ __global__ void __launch_bounds__(kTbThreads) tsb_rows_kernel(const double *A, i
     double acc[4][2];
 #pragma unroll
     for (int q = 0; q < 4; q++) acc[q][0] = acc[q][1] = 0.0;
-#pragma unroll 4
-    for (int ks = 0; ks < nks; ks++) {
-        const int k = ks * 4 + tq;
-        const double a = (row < n && k < K) ? A[row + (int64_t)k * lda] : 0.0;
+    // eight steps' A entries are loaded before they are used, so eight
+    // loads per lane are in flight
+    for (int ks0 = 0; ks0 < nks; ks0 += 8) {
+        double a[8];
 #pragma unroll
-        for (int q = 0; q < 4; q++)
-            if (q < nnt) dmma884(acc[q], a, Bs[k][q * 8 + gq]);
+        for (int u = 0; u < 8; u++) {
+            const int k = (ks0 + u) * 4 + tq;
+            a[u] = (row < n && k < K) ? A[row + (int64_t)k * lda] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            if (ks0 + u >= nks) break;
+            const int k = (ks0 + u) * 4 + tq;
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                if (q < nnt) dmma884(acc[q], a[u], Bs[k][q * 8 + gq]);
+        }
     }
     if (row >= n) return;
 #pragma unroll
@@ -363,7 +402,14 @@ void launch_tsb_tn(const double *V, int64_t ldv, int n, int m, const double *W, 
     int rows = (n + nparts - 1) / nparts;
     rows = (rows + kTbRows - 1) / kTbRows * kTbRows;
     const int np = (n + rows - 1) / rows;
-    tsb_tn_part_kernel<<<np, kTbThreads, 0, st>>>(V, ldv, n, m, W, ldw, b, rows, bs.part);
+    const size_t smem = sizeof(double) * 2 * (size_t)(m + b) * kVS;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(tsb_tn_part_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(sizeof(double) * 2 * (kBlockMaxM + kBlockMaxB) * kVS));
+        attr = true;
+    }
+    tsb_tn_part_kernel<<<np, kTbThreads, smem, st>>>(V, ldv, n, m, W, ldw, b, rows, bs.part);
     const int outs = m * kBlockMaxB;
     tsb_tn_reduce_kernel<<<(outs + 31) / 32, 32 * kRedSlices, 0, st>>>(m, b, np, bs.part, H, ldh,
                                                                        mode);

@@ -51,7 +51,8 @@ class ExtInfo(ctypes.Structure):
     """speigs_ext_info (include/speigs_b200.h)."""
     _fields_ = [("precision", c_int), ("refine_steps", c_int64), ("factor_solves", c_int64),
                 ("warm_cols", c_int64), ("block", c_int), ("block_solves", c_int64),
-                ("t_checks", c_double), ("t_setup", c_double), ("t_release", c_double)]
+                ("t_checks", c_double), ("t_setup", c_double), ("t_release", c_double),
+                ("t_block_solve", c_double), ("block_solve_calls", c_int64)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
