@@ -945,7 +945,9 @@ def main():
         line = {
             "metric": METRIC, "value": ms * 1e-3, "unit": "s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else
+                     "f32 factor panels, f64 refinement / recurrence / Ritz",
             "data": "synthetic",
             "config": {"workload": wl["desc"], "n": int(n), "nnz": int(A.nnz), "k": k, "tol": TOL,
                        "precision": "plain FP64" if args.precision == "fp64" else

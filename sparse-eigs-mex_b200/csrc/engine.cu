@@ -1022,12 +1022,59 @@ static int block_lanczos_device(BlockOperator &op, const DevA &A, int n, int64_t
         return 0;
     };
 
-    // ---- start block: the proposal's columns, completed with random ones
+    // ---- start block: the proposal's columns, completed with random ones.
+    // A proposal wider than the block is first reduced to its b best
+    // directions: the Rayleigh-Ritz vectors of A on span(Y) whose Ritz values
+    // lie nearest the wanted end (smallest |theta + shift|), formed from the
+    // orthonormalised proposal (b SpMV columns at a time would do too; one
+    // SpMV per column is cheap beside a block solve).
     if (warm_used) *warm_used = 0;
-    const int pp = (int)std::min<int64_t>(Y ? p : 0, b);
-    for (int c = 0; c < b; c++) {
+    const double *Ysrc = Y;
+    int64_t psrc = Y ? p : 0;
+    bool compressed = false;
+    if (Y && p > b && p <= kBlockMaxB) {
+        const int q = (int)p;
+        double *Yp = ar.alloc<double>((size_t)B.ldv * q), *AY = ar.alloc<double>((size_t)B.ldv * q);
+        double *G32 = ar.alloc<double>((size_t)q * q), *R32 = ar.alloc<double>((size_t)q * q);
+        double *Hq = ar.alloc<double>((size_t)q * q), *Sq = ar.alloc<double>((size_t)q * b);
+        int *cst = ar.alloc<int>(4);
+        if (ar.failed) return SPEIGS_ERR_MEM;
+        for (int c = 0; c < q; c++) launch_copy(n, Y + (size_t)c * n, Yp + (size_t)c * B.ldv, st);
+        for (int pass = 0; pass < 2; pass++) {
+            launch_tsb_tn(Yp, B.ldv, n, q, Yp, B.ldv, q, G32, q, 0, B.bs, st);
+            launch_block_chol(q, G32, q, R32, bthr, 1e-14, cst, st);
+            launch_tsb_right_mul(n, q, Yp, B.ldv, R32, st);
+        }
+        for (int c = 0; c < q; c++)
+            launch_spmv(A.n, A.rp, A.ci, A.va, Yp + (size_t)c * B.ldv, AY + (size_t)c * B.ldv, st);
+        launch_tsb_tn(Yp, B.ldv, n, q, AY, B.ldv, q, Hq, q, 0, B.bs, st);
+        std::vector<double> hH((size_t)q * q), th(q), hS((size_t)q * q), sel((size_t)q * b);
+        std::vector<int> ordv(q);
+        int hst[4] = {0, 0, 0, 0};
+        copy_async(hst, cst, sizeof(int) * 2, cudaMemcpyDeviceToHost, st);
+        copy_async(hH.data(), Hq, sizeof(double) * q * q, cudaMemcpyDeviceToHost, st);
+        if (int e = sync("start subspace")) return e;
+        if (!hst[1] && syev_host(q, hH.data(), q, th.data(), hS.data(), ordv.data()) >= 0) {
+            std::vector<int> idx(q);
+            for (int i = 0; i < q; i++) idx[i] = i;
+            std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) {
+                return std::fabs(th[x] + shift) < std::fabs(th[y] + shift);
+            });
+            for (int c = 0; c < b; c++)
+                std::memcpy(sel.data() + (size_t)c * q, hS.data() + (size_t)idx[c] * q,
+                            sizeof(double) * q);
+            copy_async(Sq, sel.data(), sizeof(double) * q * b, cudaMemcpyHostToDevice, st);
+            // V[:, 0:b] = Yp * S_sel (the product reads Yp only)
+            launch_tsb_right_mul_into(n, q, Yp, B.ldv, Sq, q, B.V, B.ldv, b, st);
+            if (int e = sync("start subspace")) return e;      // the host vectors die here
+            compressed = true;
+            psrc = b;
+        }
+    }
+    const int pp = (int)std::min<int64_t>(psrc, b);
+    for (int c = 0; c < b && !compressed; c++) {
         double *dst = B.V + (size_t)c * B.ldv;
-        if (c < pp) launch_copy(n, Y + (size_t)c * n, dst, st);
+        if (c < pp) launch_copy(n, Ysrc + (size_t)c * n, dst, st);
         else rand_col(dst);
     }
     {

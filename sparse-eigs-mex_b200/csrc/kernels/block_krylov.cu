@@ -440,6 +440,15 @@ void launch_tsb_right_mul(int n, int b, double *W, int64_t ldw, const double *Ri
     note_launch();
 }
 
+void launch_tsb_right_mul_into(int n, int K, const double *X, int64_t ldx, const double *S,
+                               int lds, double *W, int64_t ldw, int b, cudaStream_t st) {
+    if (b <= 0 || K <= 0) return;
+    const int rows = kTbThreads / 4;
+    tsb_rows_kernel<false><<<(n + rows - 1) / rows, kTbThreads, 0, st>>>(X, ldx, n, K, S, lds, W,
+                                                                         ldw, b);
+    note_launch();
+}
+
 void launch_block_refine_residual(int n, const int32_t *rowptr, const int32_t *col,
                                   const double *val, double shift, const double *B, int64_t ldb,
                                   const double *Y, int64_t ldy, double *R, int64_t ldr, int b,

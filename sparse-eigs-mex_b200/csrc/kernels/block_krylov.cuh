@@ -41,6 +41,10 @@ void launch_block_chol(int b, const double *G, int ldg, double *Rinv, double abs
 // W[:, 0:b] = W[:, 0:b] Rinv  (in place; Rinv upper triangular b x b, ld b)
 void launch_tsb_right_mul(int n, int b, double *W, int64_t ldw, const double *Rinv,
                           cudaStream_t st);
+// W[:, 0:b] = X[:, 0:K] S  (S: K x b, leading dimension lds; K <= kBlockMaxM; W and X
+// distinct)
+void launch_tsb_right_mul_into(int n, int K, const double *X, int64_t ldx, const double *S,
+                               int lds, double *W, int64_t ldw, int b, cudaStream_t st);
 
 // FP64 refinement residual of a block solve:
 //   R = B - (A + shift I) Y   (columns 0..b-1), and *flag <- 1 once every

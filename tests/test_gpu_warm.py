@@ -64,3 +64,26 @@ def test_dependent_columns_are_dropped(lib, pkg, block):
     assert ei["warm_cols"] == 6
     ex = pkg.workloads.spectrum3d(12)[:k]
     assert np.max(np.abs(lam - ex) / ex) <= 1e-10
+
+
+def test_wide_start_subspace_reduced_to_its_best_block(lib, pkg):
+    """A start subspace wider than the block is reduced to the block's width
+    by Rayleigh-Ritz with A: given the 8 wanted eigenvectors hidden among 16
+    unwanted ones (the wanted ones last), blocks of 8 start from the wanted
+    directions and finish in one restart cycle, where the first 8 columns
+    alone would start from unwanted ones."""
+    A = pkg.workloads.varcoef3d(20, seed=9)
+    k = 8
+    rc, lam, V, res, info, ei = _solve(pkg, lib, A, 24)
+    assert rc == 0 and info["flag"] == 0
+    order = np.argsort(np.abs(lam))
+    rng = np.random.default_rng(3)
+    Y = V[:, order[::-1]] + 1e-9 * rng.standard_normal(V.shape)      # wanted columns last
+    rc0, lam0, *_ = _solve(pkg, lib, A, k)
+    rc2, lam2, V2, res2, info2, ei2 = _solve(pkg, lib, A, k, warm=Y, block=8)
+    assert rc0 == 0 and rc2 == 0 and info2["flag"] == 0
+    assert ei2["block"] == 8 and ei2["warm_cols"] == 8
+    assert info2["restarts"] <= 1
+    assert np.max(np.abs(lam2 - lam0) / np.abs(lam0)) <= 1e-10
+    r = np.linalg.norm(A @ V2 - V2 * lam2, axis=0)
+    assert r.max() <= 1e-10 * info2["anorm"] * 1.0001
