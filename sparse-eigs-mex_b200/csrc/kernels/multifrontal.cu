@@ -1845,6 +1845,18 @@ template <> int MultifrontalPlanT<Real>::init(const spx_symbolic &S, const int64
                 meta[s2].bwd_expect = fwd_done_count(s2);
             }
         }
+        // The small supernodes of a level are bundled by decreasing work (rows
+        // per lane, then pivots): a bundle's warps then finish together, and
+        // the longest bundles are dequeued first.  Supernodes of one level do
+        // not depend on each other, and each is computed the same way in any
+        // bundle, so the results do not change.
+        auto sort_by_work = [&](std::vector<int32_t> &v) {
+            std::stable_sort(v.begin(), v.end(), [&](int32_t x, int32_t y2) {
+                const int qx = (meta[x].r + 31) / 32, qy = (meta[y2].r + 31) / 32;
+                if (qx != qy) return qx > qy;
+                return meta[x].c > meta[y2].c;
+            });
+        };
         for (int l = 0; l < S.nlevels; l++) {
             for (int32_t q = S.level_ptr[l]; q < S.level_ptr[l + 1]; q++) {
                 const int s2 = S.level_sup[q];
@@ -1869,6 +1881,7 @@ template <> int MultifrontalPlanT<Real>::init(const spx_symbolic &S, const int64
                 if (tiny_leaf(s2)) ti.push_back(s2);
                 else if (small(meta[s2].r, meta[s2].c)) sm.push_back(s2);
             }
+            sort_by_work(sm);
             for (size_t b0 = 0; b0 < sm.size(); b0 += kSWarps) {
                 const int nb = (int)std::min<size_t>(kSWarps, sm.size() - b0);
                 tasks_s.push_back({ST_FWD_BUNDLE, 0, 0, 0, 0, (int)bundle.size(), nb, 0});
@@ -1903,6 +1916,7 @@ template <> int MultifrontalPlanT<Real>::init(const spx_symbolic &S, const int64
                 if (tiny_leaf(s2)) ti.push_back(s2);
                 else if (small(meta[s2].r, meta[s2].c)) sm.push_back(s2);
             }
+            sort_by_work(sm);
             for (size_t b0 = 0; b0 < sm.size(); b0 += kSWarps) {
                 const int nb = (int)std::min<size_t>(kSWarps, sm.size() - b0);
                 tasks_s.push_back({ST_BWD_BUNDLE, 0, 0, 0, 0, (int)bundle.size(), nb, 0});

@@ -52,31 +52,35 @@ def _bind(lib):
 def grid_graph(N: int, kap: np.ndarray):
     """Normalised adjacency of the N^3 finite-volume operator: w_ij = t_ij /
     sqrt(s_i s_j), t the face transmissibilities, s_i = sum_j t_ij.  Returns
-    (rowptr int32, col int32, w float32), rows in the operator's order."""
+    (rowptr int32, col int32, w float32), rows in the operator's order.
+
+    Built straight in CSR order: node i = (z, y, x) has the neighbours
+    i - N^2, i - N, i - 1, i + 1, i + N, i + N^2 (ascending), each present when
+    it lies in the grid."""
     n = N ** 3
-    idx = np.arange(n).reshape(N, N, N)
-    rows, cols, vals = [], [], []
+    kap = np.asarray(kap, dtype=np.float64).reshape(N, N, N)
+    T = np.zeros((N, N, N, 6))                  # face transmissibility per neighbour slot
     for ax in range(3):
         a = [slice(None)] * 3
         b = [slice(None)] * 3
         a[ax] = slice(0, N - 1)
         b[ax] = slice(1, N)
         ka, kb = kap[tuple(a)], kap[tuple(b)]
-        t = (2.0 * ka * kb / (ka + kb)).ravel()
-        ia, ib = idx[tuple(a)].ravel(), idx[tuple(b)].ravel()
-        rows += [ia, ib]
-        cols += [ib, ia]
-        vals += [t, t]
-    r = np.concatenate(rows)
-    c = np.concatenate(cols)
-    v = np.concatenate(vals)
-    s = np.bincount(r, weights=v, minlength=n)
-    v = v / np.sqrt(s[r] * s[c])
-    order = np.lexsort((c, r))
-    r, c, v = r[order], c[order], v[order]
+        t = 2.0 * ka * kb / (ka + kb)
+        # axis 0 has stride N^2, axis 2 stride 1: slot ax is the lower
+        # neighbour along ax (seen from the upper cell), slot 5 - ax the upper
+        # one (seen from the lower cell)
+        T[tuple(b) + (ax,)] = t
+        T[tuple(a) + (5 - ax,)] = t
+    T = T.reshape(n, 6)
+    present = T > 0.0
+    step = np.array([-N * N, -N, -1, 1, N, N * N], dtype=np.int64)
+    cols = np.arange(n, dtype=np.int64)[:, None] + step[None, :]
+    s = T.sum(axis=1)
+    W = T / np.sqrt(s[:, None] * s[np.where(present, cols, 0)])
     rowptr = np.zeros(n + 1, dtype=np.int32)
-    np.cumsum(np.bincount(r, minlength=n), out=rowptr[1:])
-    return rowptr, c.astype(np.int32), v.astype(np.float32)
+    np.cumsum(present.sum(axis=1), out=rowptr[1:])
+    return rowptr, cols[present].astype(np.int32), W[present].astype(np.float32)
 
 
 _MODES: dict = {}
