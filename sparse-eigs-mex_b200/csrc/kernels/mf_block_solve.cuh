@@ -32,6 +32,8 @@ struct BSolveArgs {
     double *fpart, *bpart;               // per strip slot: kST rows of NR
     int *fcnt, *bcnt;
     int *sync;                           // as SolveArgs::sync
+    const STask *wtasks;                 // as SolveArgs::wtasks
+    int nfw, nbw;
     const double *b;                     // n rows of NR, original order
     double *out;                         // n rows of NR, original order
     const int *skip;
@@ -481,6 +483,27 @@ SPX_DEV void bbwd_tile(const BSolveArgs &a, int s, int J, int S, int chunk, BSha
     __syncthreads();
 }
 
+// Warp tasks of one phase (as solve_warp_tasks): a small supernode, or up to
+// 32 tiny leaves solved one after another by the warp.
+template <int NR>
+SPX_DEV void bsolve_warp_tasks(const BSolveArgs &a, const STask *tq, int nt, int *ctr,
+                               BWarpShared<NR> &w) {
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        int t = 0;
+        if (lane == 0) t = atomicAdd(ctr, 1);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= nt) break;
+        const STask tk = tq[t];
+        const bool fwd = tk.a.x == ST_FWD_BUNDLE || tk.a.x == ST_FWD_THREADS;
+        for (int q = 0; q < tk.b.z; q++) {
+            if (fwd) bfwd_warp<NR>(a, a.bundle[tk.b.y + q], w);
+            else bbwd_warp<NR>(a, a.bundle[tk.b.y + q], w);
+        }
+        __syncwarp();
+    }
+}
+
 template <int NR>
 __global__ void __launch_bounds__(kSThreads, 2) mf_bsolve(BSolveArgs a) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -492,7 +515,9 @@ __global__ void __launch_bounds__(kSThreads, 2) mf_bsolve(BSolveArgs a) {
     BWarpShared<NR> &ws = reinterpret_cast<BWarpShared<NR> *>(smem_raw)[wid];
     uint32_t phase = 0;
     if (threadIdx.x == 0) mbar_init(&s_bar);
+    bsolve_warp_tasks<NR>(a, a.wtasks, a.nfw, a.sync + 1 + a.ns, ws);
     __syncthreads();
+    fence_proxy_async();
     for (;;) {
         if (threadIdx.x == 0) s_task = atomicAdd(a.sync, 1);
         __syncthreads();
@@ -525,6 +550,7 @@ __global__ void __launch_bounds__(kSThreads, 2) mf_bsolve(BSolveArgs a) {
         // proxy in the next one
         fence_proxy_async();
     }
+    bsolve_warp_tasks<NR>(a, a.wtasks + a.nfw, a.nbw, a.sync + 1 + 4 * a.ns, ws);
 }
 
 template <int NR>

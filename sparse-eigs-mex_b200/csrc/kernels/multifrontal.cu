@@ -908,8 +908,11 @@ struct SolveArgs {
     const int32_t *fc_base, *fc_n, *bc_base, *bc_n;
     double *fpart, *bpart;
     int *fcnt, *bcnt;
-    int *sync;          // queue | forward arrivals per parent [ns] | (unused) [ns] |
-                        // backward arrivals [ns] | root forward arrivals [ns] | [ns] | err
+    int *sync;          // block queue | forward arrivals per parent [ns] | forward warp
+                        // queue, then unused [ns] | backward arrivals [ns] | root forward
+                        // arrivals [ns] | backward warp queue, then unused [ns] | err
+    const STask *wtasks;    // warp tasks: nfw forward, then nbw backward
+    int nfw, nbw;
     const double *b;
     double *out;
     const int *skip;    // when set and nonzero: nothing to do
@@ -1423,6 +1426,32 @@ SPX_DEV void bwd_tile(const SolveArgs &a, int s, int J, int S, int chunk, SolveS
     __syncthreads();
 }
 
+// Warp tasks of one phase: each warp takes the next task from the phase's
+// own counter.  A task is one small supernode (ST_*_BUNDLE with one entry)
+// or up to 32 tiny leaves, one per lane (ST_*_THREADS).
+SPX_DEV void solve_warp_tasks(const SolveArgs &a, const STask *tq, int nt, int *ctr,
+                              WarpShared &w) {
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        int t = 0;
+        if (lane == 0) t = atomicAdd(ctr, 1);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= nt) break;
+        const STask tk = tq[t];
+        switch (tk.a.x) {
+            case ST_FWD_BUNDLE: fwd_warp(a, a.bundle[tk.b.y], w); break;
+            case ST_BWD_BUNDLE: bwd_warp(a, a.bundle[tk.b.y]); break;
+            case ST_FWD_THREADS:
+                if (lane < tk.b.z) fwd_thread(a, a.bundle[tk.b.y + lane]);
+                break;
+            default:
+                if (lane < tk.b.z) bwd_thread(a, a.bundle[tk.b.y + lane]);
+                break;
+        }
+        __syncwarp();
+    }
+}
+
 __global__ void __launch_bounds__(kSThreads, 2) mf_solve_sf(SolveArgs a) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ int s_task, s_flag;
@@ -1433,7 +1462,10 @@ __global__ void __launch_bounds__(kSThreads, 2) mf_solve_sf(SolveArgs a) {
     const int wid = threadIdx.x >> 5;
     uint32_t phase = 0;
     if (threadIdx.x == 0) mbar_init(&s_bar);
+    // forward warp tasks (the small subtrees), every warp on its own
+    solve_warp_tasks(a, a.wtasks, a.nfw, a.sync + 1 + a.ns, ws[wid]);
     __syncthreads();
+    fence_proxy_async();
     for (;;) {
         if (threadIdx.x == 0) s_task = atomicAdd(a.sync, 1);
         __syncthreads();
@@ -1466,6 +1498,8 @@ __global__ void __launch_bounds__(kSThreads, 2) mf_solve_sf(SolveArgs a) {
         // proxy in the next one
         fence_proxy_async();
     }
+    // backward warp tasks
+    solve_warp_tasks(a, a.wtasks + a.nfw, a.nbw, a.sync + 1 + 4 * a.ns, ws[wid]);
 }
 
 #include "mf_block_solve.cuh"
@@ -1857,6 +1891,46 @@ template <> int MultifrontalPlanT<Real>::init(const spx_symbolic &S, const int64
                 return meta[x].c > meta[y2].c;
             });
         };
+        // Warp tasks: a small supernode whose whole subtree is small is solved
+        // by one warp that dequeues it on its own (a tiny leaf by one lane of
+        // a warp, 32 to a task), in a phase before (forward) or after
+        // (backward) the block tasks.  A warp task then never waits for a
+        // block task in the forward pass, and no block task waits for a warp
+        // task of the backward pass, so neither phase can stall the other.
+        std::vector<char> warpable(ns, 0);
+        for (int l = 0; l < S.nlevels; l++)
+            for (int32_t q = S.level_ptr[l]; q < S.level_ptr[l + 1]; q++) {
+                const int s2 = S.level_sup[q];
+                bool ok = small(meta[s2].r, meta[s2].c);
+                for (int32_t e = S.child_ptr[s2]; ok && e < S.child_ptr[s2 + 1]; e++)
+                    ok = warpable[S.child_list[e]] != 0;
+                warpable[s2] = ok;
+            }
+        std::vector<STaskH> wtasks_f, wtasks_b;
+        auto emit_warp_level = [&](int l, bool fwd) {
+            std::vector<int32_t> sm, ti;
+            for (int32_t q = S.level_ptr[l]; q < S.level_ptr[l + 1]; q++) {
+                const int s2 = S.level_sup[q];
+                if (!warpable[s2]) continue;
+                if (tiny_leaf(s2)) ti.push_back(s2);
+                else sm.push_back(s2);
+            }
+            sort_by_work(sm);
+            std::vector<STaskH> &out = fwd ? wtasks_f : wtasks_b;
+            for (int32_t s2 : sm) {
+                out.push_back({fwd ? ST_FWD_BUNDLE : ST_BWD_BUNDLE, 0, 0, 0, 0,
+                               (int)bundle.size(), 1, 0});
+                bundle.push_back(s2);
+            }
+            for (size_t b0 = 0; b0 < ti.size(); b0 += 32) {
+                const int nb = (int)std::min<size_t>(32, ti.size() - b0);
+                out.push_back({fwd ? ST_FWD_THREADS : ST_BWD_THREADS, 0, 0, 0, 0,
+                               (int)bundle.size(), nb, 0});
+                bundle.insert(bundle.end(), ti.begin() + b0, ti.begin() + b0 + nb);
+            }
+        };
+        for (int l = 0; l < S.nlevels; l++) emit_warp_level(l, true);
+        for (int l = S.nlevels - 1; l >= 0; l--) emit_warp_level(l, false);
         for (int l = 0; l < S.nlevels; l++) {
             for (int32_t q = S.level_ptr[l]; q < S.level_ptr[l + 1]; q++) {
                 const int s2 = S.level_sup[q];
@@ -1878,6 +1952,7 @@ template <> int MultifrontalPlanT<Real>::init(const spx_symbolic &S, const int64
             std::vector<int32_t> sm, ti;
             for (int32_t q = S.level_ptr[l]; q < S.level_ptr[l + 1]; q++) {
                 const int s2 = S.level_sup[q];
+                if (warpable[s2]) continue;
                 if (tiny_leaf(s2)) ti.push_back(s2);
                 else if (small(meta[s2].r, meta[s2].c)) sm.push_back(s2);
             }
@@ -1913,6 +1988,7 @@ template <> int MultifrontalPlanT<Real>::init(const spx_symbolic &S, const int64
             std::vector<int32_t> sm, ti;
             for (int32_t q = S.level_ptr[l]; q < S.level_ptr[l + 1]; q++) {
                 const int s2 = S.level_sup[q];
+                if (warpable[s2]) continue;
                 if (tiny_leaf(s2)) ti.push_back(s2);
                 else if (small(meta[s2].r, meta[s2].c)) sm.push_back(s2);
             }
@@ -1929,6 +2005,10 @@ template <> int MultifrontalPlanT<Real>::init(const spx_symbolic &S, const int64
             }
         }
         ntasks_ = (int)tasks_s.size();
+        nfw_ = (int)wtasks_f.size();
+        nbw_ = (int)wtasks_b.size();
+        tasks_s.insert(tasks_s.end(), wtasks_f.begin(), wtasks_f.end());
+        tasks_s.insert(tasks_s.end(), wtasks_b.begin(), wtasks_b.end());
         side.wait();
         int rc = 0;
         rc = rc ? rc : dupload(&d_cbnd_, cbnd.data(), cbnd.size(), st);
@@ -2138,6 +2218,9 @@ template <> void MultifrontalPlanT<Real>::solve(const double *b, double *x, cuda
     a.meta = (const SNode *)d_meta_;
     a.tasks = (const STask *)d_stask_;
     a.ntasks = ntasks_;
+    a.wtasks = a.tasks + ntasks_;
+    a.nfw = nfw_;
+    a.nbw = nbw_;
     a.ns = ns_;
     a.bundle = d_bundle_;
     a.perm = d_perm_;
@@ -2235,6 +2318,9 @@ template <> int MultifrontalPlanT<Real>::solve_block(const double *B, int64_t ld
     a.meta = (const SNode *)d_meta_;
     a.tasks = (const STask *)d_stask_;
     a.ntasks = ntasks_;
+    a.wtasks = a.tasks + ntasks_;
+    a.nfw = nfw_;
+    a.nbw = nbw_;
     a.ns = ns_;
     a.bundle = d_bundle_;
     a.perm = d_perm_;

@@ -108,7 +108,8 @@ private:
     double *d_fpart_ = nullptr, *d_bpart_ = nullptr;
     int *d_cnt_ = nullptr, *d_sync_ = nullptr;
     int32_t nfc_ = 0, nbc_ = 0;
-    int ntasks_ = 0;
+    int ntasks_ = 0;                 // block tasks of the solve queue
+    int nfw_ = 0, nbw_ = 0;          // warp tasks after them: forward, then backward
     size_t sync_ints_ = 0;
     int solve_grid_ = 0;
     size_t solve_smem_ = 0;
