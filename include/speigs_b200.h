@@ -140,6 +140,14 @@ typedef struct speigs_mpnn_s *speigs_mpnn;
 int  speigs_b200_mpnn_create(int nfeat, int hidden, int layers, int nout, uint64_t seed,
                              speigs_mpnn *net);
 void speigs_b200_mpnn_destroy(speigs_mpnn net);
+/* Kernels of the forward pass's dense layers: on = 1 (the default) runs the
+ * BF16 layers whose shapes fit (inputs 16..128 wide in multiples of 16,
+ * at most 64 outputs, 16-byte aligned rows) on the tensor cores (tcgen05,
+ * FP32 accumulation in TMEM), on = 0 runs every layer on the FP32-FMA
+ * kernels; on < 0 only queries.  Returns the previous setting, or
+ * SPEIGS_ERR_ARG for a null network.  The two differ only in the order of
+ * the FP32 sums. */
+int  speigs_b200_mpnn_tensor_cores(speigs_mpnn net, int on);
 /* FP32 weights to (set = 0) or from (set = 1) host memory; host == NULL
  * reports the count in *count. */
 int  speigs_b200_mpnn_params(speigs_mpnn net, float *host, int64_t *count, int set);

@@ -1632,8 +1632,9 @@ static int plan_solve(speigs_plan_s *p, int64_t k, double *lambda, double *V, do
         const double *X = nullptr;
         int64_t ldx = 0;
         int nout = 0;
-        const double ti = wall();
-        // start subspace (host, n x ext_warm_cols) to the device
+        // start subspace (host, n x ext_warm_cols) to the device; like the
+        // matrix, it is input staging, so the iteration clock starts once it
+        // has landed
         const double *dwarm = nullptr;
         const int64_t wcols = p->ext_warm ? std::min<int64_t>(p->ext_warm_cols, 64) : 0;
         if (wcols > 0) {
@@ -1641,8 +1642,10 @@ static int plan_solve(speigs_plan_s *p, int64_t k, double *lambda, double *V, do
             if (ar.failed) return SPEIGS_ERR_MEM;
             copy_async(dw, p->ext_warm, sizeof(double) * (size_t)n * wcols,
                        on_device ? cudaMemcpyDefault : cudaMemcpyHostToDevice, st);
+            if (cudaError_t e = cudaStreamSynchronize(st)) return cuda_fail(e, "start subspace upload");
             dwarm = dw;
         }
+        const double ti = wall();
         int64_t wused = 0;
         // block method ('sm'): explicit block size, or the start subspace's width
         int bsz = 0;

@@ -156,6 +156,172 @@ dense_bwd_kernel(int n, int K1, const T1 *__restrict__ X1, int K2, const bf16 *_
     }
 }
 
+// ---- dense layer forward on the tensor cores (tcgen05, TMEM accumulator)
+// out[i, o] = act(b[o] + sum_k W[o, k] x[i, k]) as dense_fwd_kernel, for BF16
+// inputs x = [X1[i, 0:K1], X2[i, 0:K2]] (K1, K2 multiples of 8, K = K1 + K2 a
+// multiple of 16, at most 128) and N <= 64 outputs.  One block of 4 warps
+// takes 128 rows:
+//   * the rows (A, 128 x K) and W (B, NP x K, NP = N rounded up to 16, rows
+//     >= N zero) are staged in shared memory in the K-major layout without
+//     swizzle that tcgen05 descriptors address: 8-row x 16-byte core
+//     matrices, the K chunks of one 8-row group 128 bytes apart (leading
+//     byte offset), 8-row groups K/8 x 128 bytes apart (stride byte offset);
+//   * one thread issues K/16 tcgen05.mma kind::f16 (M = 128, N = NP, K = 16,
+//     BF16 operands, FP32 accumulation) into NP columns of TMEM and commits
+//     them to an mbarrier;
+//   * each warp reads its 32 TMEM lanes -- lane = row -- with tcgen05.ld and
+//     applies bias and activation; a thread stores its row in 16-byte pieces.
+// The mbarrier wait is bounded: when it runs out, *err is set, the block
+// waits (bounded) once more for its MMAs, frees its TMEM and stores nothing.
+constexpr int kTcRows = 128;
+constexpr int kTcThreads = 128;
+constexpr long kTcSpin = 1L << 22;
+
+SPX_DEV uint32_t sh_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// shared-memory matrix descriptor: start address, leading and stride byte
+// offsets (16-byte units), descriptor version 1, no swizzle
+SPX_DEV uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)(lbo >> 4) << 16) |
+           ((uint64_t)(sbo >> 4) << 32) | (1ull << 46);
+}
+// instruction descriptor of kind::f16: FP32 D (bits 4-5 = 1), BF16 A and B
+// (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at bit 24
+constexpr uint32_t umma_idesc_bf16(int nn) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(nn >> 3) << 17) |
+           ((uint32_t)(kTcRows >> 4) << 24);
+}
+SPX_DEV bool tc_bar_test(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                 " selp.u32 %0, 1, 0, p;\n}" : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
+    return ok != 0;
+}
+SPX_DEV float tc_act(float v, int act) { return act ? tanhf(v) : v; }
+
+template <class TO>
+__global__ void __launch_bounds__(kTcThreads)
+dense_fwd_tc_kernel(int n, int K1, const bf16 *__restrict__ X1, int K2, const bf16 *__restrict__ X2,
+                    int N, int NP, const bf16 *__restrict__ W, const float *__restrict__ b, int act,
+                    TO *__restrict__ out, volatile int *err) {
+    extern __shared__ __align__(1024) unsigned char tc_sm[];
+    __shared__ uint32_t s_tmem;
+    __shared__ __align__(8) unsigned long long s_bar;
+    const int K = K1 + K2, KC = K >> 3, KC1 = K1 >> 3;
+    const uint32_t sbo = (uint32_t)KC * 128u;
+    unsigned char *sA = tc_sm, *sB = tc_sm + (size_t)kTcRows * K * 2;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t ncols = NP <= 32 ? 32u : 64u;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(sh_addr(&s_tmem)), "r"(ncols) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (threadIdx.x == 32) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(sh_addr(&s_bar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    const int row0 = blockIdx.x * kTcRows;
+    // A: 128 rows x KC chunks; consecutive threads take the 8 rows of a core
+    // matrix, then the next chunk (512 contiguous bytes a warp)
+    for (int idx = threadIdx.x; idx < kTcRows * KC; idx += kTcThreads) {
+        const int r0 = idx & 7, c = (idx >> 3) % KC, r1 = (idx >> 3) / KC;
+        const int i = row0 + r1 * 8 + r0;
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        if (i < n)
+            v = c < KC1 ? *reinterpret_cast<const uint4 *>(X1 + (size_t)i * K1 + c * 8)
+                        : *reinterpret_cast<const uint4 *>(X2 + (size_t)i * K2 + (c - KC1) * 8);
+        *reinterpret_cast<uint4 *>(sA + r0 * 16 + r1 * sbo + c * 128) = v;
+    }
+    // B: NP rows of W (rows >= N zero)
+    for (int idx = threadIdx.x; idx < NP * KC; idx += kTcThreads) {
+        const int r0 = idx & 7, c = (idx >> 3) % KC, r1 = (idx >> 3) / KC;
+        const int o = r1 * 8 + r0;
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        if (o < N) v = *reinterpret_cast<const uint4 *>(W + (size_t)o * K + c * 8);
+        *reinterpret_cast<uint4 *>(sB + r0 * 16 + r1 * sbo + c * 128) = v;
+    }
+    // the generic-proxy stores above become visible to the tensor core's reads
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = s_tmem;
+    const uint32_t bar = sh_addr(&s_bar);
+    if (threadIdx.x == 0) {
+        const uint32_t idesc = umma_idesc_bf16(NP);
+        const uint32_t a0 = sh_addr(sA), b0 = sh_addr(sB);
+        for (int j = 0; j < (K >> 4); j++) {
+            const uint64_t da = umma_desc(a0 + 256u * j, 128u, sbo);
+            const uint64_t db = umma_desc(b0 + 256u * j, 128u, sbo);
+            const uint32_t acc = j > 0 ? 1u : 0u;
+            asm volatile(
+                "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}"
+                ::"r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc) : "memory");
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                     ::"r"(bar) : "memory");
+    }
+    bool done = false;
+    for (long it = 0; it < kTcSpin && !done; it++) done = tc_bar_test(bar, 0);
+    if (!done) {
+        *err = 1;
+        for (long it = 0; it < kTcSpin && !done; it++) done = tc_bar_test(bar, 0);
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const int ok = __syncthreads_and(done ? 1 : 0);
+    if (ok) {
+        const int i = row0 + warp * 32 + lane;
+        TO *orow = out + (size_t)i * N;
+        for (int c0 = 0; c0 < NP; c0 += 16) {
+            uint32_t r[16];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,"
+                "%12,%13,%14,%15}, [%16];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+                  "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+                  "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (i >= n) continue;
+            if constexpr (std::is_same<TO, bf16>::value) {
+                // 8 outputs per 16-byte store (N is a multiple of 8)
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const int o0 = c0 + 8 * h;
+                    if (o0 >= N) break;
+                    __align__(16) bf16 v[8];
+#pragma unroll
+                    for (int e = 0; e < 8; e++)
+                        v[e] = __float2bfloat16(tc_act(__uint_as_float(r[8 * h + e]) + b[o0 + e], act));
+                    *reinterpret_cast<uint4 *>(orow + o0) = *reinterpret_cast<const uint4 *>(v);
+                }
+            } else {
+                // 4 outputs per 16-byte store (N is a multiple of 4)
+#pragma unroll
+                for (int h = 0; h < 4; h++) {
+                    const int o0 = c0 + 4 * h;
+                    if (o0 >= N) break;
+                    float4 v;
+                    v.x = tc_act(__uint_as_float(r[4 * h + 0]) + b[o0 + 0], act);
+                    v.y = tc_act(__uint_as_float(r[4 * h + 1]) + b[o0 + 1], act);
+                    v.z = tc_act(__uint_as_float(r[4 * h + 2]) + b[o0 + 2], act);
+                    v.w = tc_act(__uint_as_float(r[4 * h + 3]) + b[o0 + 3], act);
+                    *reinterpret_cast<float4 *>(orow + o0) = v;
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols)
+                     : "memory");
+}
+
+size_t tc_smem(int K, int NP) { return (size_t)(kTcRows + NP) * K * sizeof(bf16); }
+
 // ---- loss: G = Y^T Y (P x P), B = Y^T U (P x k), FP64 sums
 __global__ void __launch_bounds__(kThreads)
 gram_kernel(int n, int P, const float *__restrict__ Y, int k, const float *__restrict__ U,
@@ -298,10 +464,17 @@ struct speigs_mpnn_s {
     double *G = nullptr, *B = nullptr, *loss = nullptr;
     float *C = nullptr;
     int kcap = 0;
+    // dense layers of the forward pass on the tensor cores (tcgen05) where
+    // their shapes allow it; 0 selects the FP32-FMA kernels throughout
+    int tensor_cores = 1;
+    // set by a tensor-core wait that ran out; mapped page-locked memory, so
+    // the host reads it without synchronising the stream
+    int *err_h = nullptr, *err_d = nullptr;
     ~speigs_mpnn_s() {
         void *ptrs[] = {p, g, m, v, pb, Hs, Ms, Y, dY, dH, dH2, dM, G, B, loss, C};
         for (void *q : ptrs)
             if (q) cudaFree(q);
+        if (err_h) cudaFreeHost(err_h);
     }
     int layer_in(int l) const { return l == 0 ? F : (l <= L ? 2 * H : H); }
     int layer_out(int l) const { return l <= L ? H : P; }
@@ -345,6 +518,34 @@ void set_smem_limits() {
     cudaFuncSetAttribute(dense_bwd_kernel<float, bf16>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
     cudaFuncSetAttribute(dense_bwd_kernel<bf16, bf16>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
     cudaFuncSetAttribute(dense_bwd_kernel<bf16, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    cudaFuncSetAttribute(dense_fwd_tc_kernel<bf16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)tc_smem(128, 64));
+    cudaFuncSetAttribute(dense_fwd_tc_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)tc_smem(128, 64));
+}
+
+bool aligned16(const void *q) { return ((uintptr_t)q & 15u) == 0; }
+
+// out = act(b + [X1, X2] W^T) for BF16 X1/X2 (node-major, K1 and K2 wide):
+// the tensor-core kernel when the network allows it and the shapes and
+// addresses fit its 16-byte pieces, else the FP32-FMA kernel
+template <class TO>
+void dense_fwd(const speigs_mpnn_s *net, int n, int K1, const bf16 *X1, int K2, const bf16 *X2,
+               int N, const bf16 *W, const float *b, int act, TO *out, cudaStream_t st) {
+    const int K = K1 + K2;
+    const int vec = 16 / (int)sizeof(TO);
+    const bool tc = net->tensor_cores && K1 % 8 == 0 && K2 % 8 == 0 && K % 16 == 0 && K <= 128 &&
+                    N <= 64 && N % vec == 0 && aligned16(X1) && (K2 == 0 || aligned16(X2)) &&
+                    aligned16(W) && aligned16(out);
+    if (tc) {
+        const int NP = (N + 15) & ~15;
+        dense_fwd_tc_kernel<TO><<<(n + kTcRows - 1) / kTcRows, kTcThreads, tc_smem(K, NP), st>>>(
+            n, K1, X1, K2, X2, N, NP, W, b, act, out, net->err_d);
+    } else {
+        dense_fwd_kernel<bf16, TO><<<(n + kRows - 1) / kRows, kThreads, dense_smem(K, N, false), st>>>(
+            n, K1, X1, K2, X2, N, W, b, act, out);
+    }
+    spx::note_launch();
 }
 
 // forward pass keeping the activations; Y (FP32) in net->Y
@@ -361,14 +562,12 @@ void forward(speigs_mpnn_s *net, int n, const int32_t *rp, const int32_t *ci, co
         bf16 *Hp = net->Hs + (size_t)(l - 1) * n * H, *Hn = net->Hs + (size_t)l * n * H;
         bf16 *Ml = net->Ms + (size_t)(l - 1) * n * H;
         spmm_kernel<bf16, bf16><<<sb, 256, 0, st>>>(n, H, rp, ci, w, Hp, Ml, 0);
-        dense_fwd_kernel<bf16, bf16><<<nb, kThreads, dense_smem(2 * H, H, false), st>>>(
-            n, H, Hp, H, Ml, H, net->pb + net->woff[l], net->p + net->boff[l], 1, Hn);
-        spx::note_launch(2);
+        spx::note_launch();
+        dense_fwd<bf16>(net, n, H, Hp, H, Ml, H, net->pb + net->woff[l], net->p + net->boff[l], 1,
+                        Hn, st);
     }
-    dense_fwd_kernel<bf16, float><<<nb, kThreads, dense_smem(H, net->P, false), st>>>(
-        n, H, net->Hs + (size_t)L * n * H, 0, nullptr, net->P, net->pb + net->woff[L + 1],
-        net->p + net->boff[L + 1], 0, net->Y);
-    spx::note_launch();
+    dense_fwd<float>(net, n, H, net->Hs + (size_t)L * n * H, 0, nullptr, net->P,
+                     net->pb + net->woff[L + 1], net->p + net->boff[L + 1], 0, net->Y, st);
 }
 
 }  // namespace
@@ -419,6 +618,13 @@ int speigs_b200_mpnn_create(int nfeat, int hidden, int layers, int nout, uint64_
     cudaMemset(net->g, 0, sizeof(float) * off);
     to_bf16_kernel<<<64, 256>>>(off, net->p, net->pb);
     spx::note_launch();
+    if (cudaHostAlloc((void **)&net->err_h, sizeof(int), cudaHostAllocMapped) != cudaSuccess ||
+        cudaHostGetDevicePointer((void **)&net->err_d, net->err_h, 0) != cudaSuccess) {
+        cudaGetLastError();
+        delete net;
+        return SPEIGS_ERR_MEM;
+    }
+    *net->err_h = 0;
     set_smem_limits();
     if (cudaDeviceSynchronize() != cudaSuccess) { cudaGetLastError(); delete net; return SPEIGS_ERR_INTERNAL; }
     *out = net;
@@ -426,6 +632,13 @@ int speigs_b200_mpnn_create(int nfeat, int hidden, int layers, int nout, uint64_
 }
 
 void speigs_b200_mpnn_destroy(speigs_mpnn net) { delete net; }
+
+int speigs_b200_mpnn_tensor_cores(speigs_mpnn net, int on) {
+    if (!net) return SPEIGS_ERR_ARG;
+    const int was = net->tensor_cores;
+    if (on >= 0) net->tensor_cores = on ? 1 : 0;
+    return was;
+}
 
 int speigs_b200_mpnn_params(speigs_mpnn net, float *host, int64_t *count, int set) {
     if (!net || !count) return SPEIGS_ERR_ARG;
@@ -452,6 +665,10 @@ int speigs_b200_mpnn_forward(speigs_mpnn net, int64_t n, const int32_t *rowptr, 
                              const float *w, const float *X, float *Y, void *stream) {
     if (!net || n <= 0 || n > INT32_MAX || !rowptr || !col || !w || !X || !Y) return SPEIGS_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
+    if (*(volatile int *)net->err_h) {
+        spx::set_last_error_text("mpnn: a tensor-core wait of an earlier call ran out");
+        return SPEIGS_ERR_INTERNAL;
+    }
     if (net->reserve(n, 1)) return SPEIGS_ERR_MEM;
     forward(net, (int)n, rowptr, col, w, X, st);
     cudaMemcpyAsync(Y, net->Y, sizeof(float) * (size_t)n * net->P, cudaMemcpyDeviceToDevice, st);
@@ -514,6 +731,10 @@ int speigs_b200_mpnn_train_step(speigs_mpnn net, int64_t n, const int32_t *rowpt
     cudaMemcpyAsync(&hl, net->loss, sizeof(double), cudaMemcpyDeviceToHost, st);
     cudaError_t e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) { spx::set_last_error_text(cudaGetErrorString(e)); return SPEIGS_ERR_INTERNAL; }
+    if (*(volatile int *)net->err_h) {
+        spx::set_last_error_text("mpnn: a tensor-core wait ran out");
+        return SPEIGS_ERR_INTERNAL;
+    }
     if (loss) *loss = hl;
     return SPEIGS_OK;
 }

@@ -35,6 +35,7 @@ def _bind(lib):
         "speigs_b200_mpnn_create": (c_int, [c_int, c_int, c_int, c_int, c_uint64,
                                             POINTER(c_void_p)]),
         "speigs_b200_mpnn_destroy": (None, [c_void_p]),
+        "speigs_b200_mpnn_tensor_cores": (c_int, [c_void_p, c_int]),
         "speigs_b200_mpnn_params": (c_int, [c_void_p, c_void_p, POINTER(c_int64), c_int]),
         "speigs_b200_mpnn_grads": (c_int, [c_void_p, c_void_p]),
         "speigs_b200_mpnn_forward": (c_int, [c_void_p, c_int64, c_void_p, c_void_p, c_void_p,
@@ -130,6 +131,12 @@ class WarmStartNet:
         g = np.zeros(self.nparam, dtype=np.float32)
         self.lib.speigs_b200_mpnn_grads(self.h, g.ctypes.data)
         return g
+
+    def tensor_cores(self, on: int = -1) -> int:
+        """Select the dense-layer kernels of the forward pass (1: tcgen05
+        where the shapes fit, 0: FP32 FMA; -1: query); returns the previous
+        setting."""
+        return int(self.lib.speigs_b200_mpnn_tensor_cores(self.h, on))
 
     def forward_device(self, n, rowptr, col, w, X, Y, stream=0):
         """All arguments are device pointers (ints)."""

@@ -64,3 +64,29 @@ def test_training_reduces_loss(pkg):
     for _ in range(60):
         last = net.train_step_device(*args, 3e-3, 0)
     assert last < 0.8 * first, (first, last)
+
+
+@pytest.mark.parametrize("N,P", [(48, 24), (7, 8), (6, 6)])
+def test_tensor_core_layers_match_fma_layers(pkg, N, P):
+    """The dense layers on the tensor cores (tcgen05, FP32 accumulation in
+    TMEM) against the FP32-FMA kernels on the same BF16 operands: the
+    48^3 proposal workload (hidden and output layers on the tensor cores),
+    a ragged last tile (343 rows) and an output width the tensor-core
+    kernel does not take (6: that layer stays on FMA).  The two differ in
+    the order of the FP32 sums only, so BF16 activations agree except for
+    an occasional last-bit flip."""
+    torch, net, t, A, X, U, n, dims, k = _device_case(pkg, N=N, P=P)
+    Y = {}
+    for on in (0, 1):
+        net.tensor_cores(on)
+        Y[on] = torch.empty((n, P), dtype=torch.float32, device="cuda")
+        torch.cuda.synchronize()
+        rc = net.forward_device(n, t["rp"].data_ptr(), t["ci"].data_ptr(), t["w"].data_ptr(),
+                                t["X"].data_ptr(), Y[on].data_ptr(), 0)
+        assert rc == 0
+    torch.cuda.synchronize()
+    assert net.tensor_cores(-1) == 1
+    a, b = Y[1].double().cpu().numpy(), Y[0].double().cpu().numpy()
+    assert np.all(np.isfinite(a))
+    err = np.linalg.norm(a - b) / np.linalg.norm(b)
+    assert err < 1e-2, err
