@@ -243,6 +243,19 @@ int speigs_b200_syev_small(int m, const double *H, double *theta, double *S, int
 int speigs_b200_syev_small_host(int m, const double *H, int ldh, double *theta, double *S,
                                 int *ord);
 
+/* The same contract with eigenvectors for the nvec leading entries of ord
+ * only (the other columns of S are set to zero): Householder reduction of
+ * the lower triangle, the implicit QR on the eigenvalues alone (theta agrees
+ * with speigs_b200_syev_small_host's to rounding), inverse iteration on the
+ * tridiagonal with
+ * Gram-Schmidt inside clusters of close eigenvalues, and the reflectors
+ * applied to the vectors -- LAPACK dsyevx's method, O(m^2) per vector.  The
+ * block Lanczos method solves its projected problem with it (its restart
+ * and residual test read only the wanted Ritz vectors).  nvec >= m solves
+ * fully.  Returns 0, or -1 for bad arguments or no convergence. */
+int speigs_b200_syev_select_host(int m, const double *H, int ldh, int nvec, double *theta,
+                                 double *S, int *ord);
+
 /* Allocation-free variant of speigs_b200_syev_small.  No counterpart in the
  * reference interface.  For callers that cannot call cudaMalloc where they
  * need the solve -- code running under CUDA stream capture, real-time loops

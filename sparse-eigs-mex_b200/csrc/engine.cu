@@ -85,7 +85,7 @@ struct SyevStage {
     }
 };
 static int syev_projected(int m, const double *dH, int ldh, double *dtheta, double *dS, int *dord,
-                          int *dstat, cudaStream_t st) {
+                          int *dstat, cudaStream_t st, int nvec = -1) {
     thread_local SyevStage sg;
     const size_t need = 2 * (size_t)m * m + 2 * (size_t)m + 8;
     if (sg.cap < need) {
@@ -106,7 +106,10 @@ static int syev_projected(int m, const double *dH, int ldh, double *dtheta, doub
                       cudaMemcpyDeviceToHost, st);
     cudaError_t e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return cuda_fail(e, "projected problem read-back");
-    const int steps = syev_host(m, hH, m, hth, hS, hord);
+    // nvec >= 0: eigenvectors only for the nvec wanted Ritz values (the
+    // rest of S is zero); the eigenvalues are those of the full solver
+    const int steps = (nvec >= 0 && nvec < m) ? syev_host_select(m, hH, m, nvec, hth, hS, hord)
+                                              : syev_host(m, hH, m, hth, hS, hord);
     hst[0] = steps < 0 ? -1 : steps + 1;
     hst[1] = 0;
     copy_async(dtheta, hth, sizeof(double) * m, cudaMemcpyHostToDevice, st);
@@ -1159,7 +1162,11 @@ static int block_lanczos_device(BlockOperator &op, const DevA &A, int n, int64_t
         // estimates gate the true-residual test
         const int nwant = std::min(kk, mm);
         int tr = tm.begin();
-        if (int e = syev_projected(mm, B.H, ldh, B.theta, B.S, B.ord, B.jstat, st)) return e;
+        // the Ritz vectors read later are the nwant wanted ones and the l
+        // kept at a restart
+        if (int e = syev_projected(mm, B.H, ldh, B.theta, B.S, B.ord, B.jstat, st,
+                                   std::max(nwant, std::min(l0, mm))))
+            return e;
         launch_block_ritz_est(nwant, b, B.S, mm, jc, B.ord, B.Gres, b, B.est2, st);
         tm.end(tr, &ms_ritz);
         {
