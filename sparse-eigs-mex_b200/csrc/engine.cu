@@ -971,14 +971,10 @@ static int block_lanczos_device(BlockOperator &op, const DevA &A, int n, int64_t
     auto cgs2 = [&](double *Wp, int m, double *hcol) {
         if (m <= 0) return;
         double *V = B.V;
-        if (hcol) {
-            launch_tsb_tn(V, B.ldv, n, m, Wp, B.ldv, b, hcol, ldh, 0, B.bs, st);
-            launch_tsb_nn_sub(V, B.ldv, n, m, hcol, ldh, Wp, B.ldv, b, st);
-        } else {
-            launch_tsb_tn(V, B.ldv, n, m, Wp, B.ldv, b, B.hb, ldh, 0, B.bs, st);
-            launch_tsb_nn_sub(V, B.ldv, n, m, B.hb, ldh, Wp, B.ldv, b, st);
-        }
-        launch_tsb_tn(V, B.ldv, n, m, Wp, B.ldv, b, B.hb, ldh, 0, B.bs, st);
+        // pass 1's update and pass 2's product share one sweep over V
+        double *h1 = hcol ? hcol : B.hb;
+        launch_tsb_tn(V, B.ldv, n, m, Wp, B.ldv, b, h1, ldh, 0, B.bs, st);
+        launch_tsb_sub_tn(V, B.ldv, n, m, h1, ldh, Wp, B.ldv, b, B.hb, ldh, 0, B.bs, st);
         launch_tsb_nn_sub(V, B.ldv, n, m, B.hb, ldh, Wp, B.ldv, b, st);
         if (hcol) launch_block_axpy_unless(m, b, hcol, ldh, B.hb, ldh, nullptr, st);
     };

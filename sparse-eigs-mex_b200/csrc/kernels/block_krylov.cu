@@ -111,6 +111,109 @@ __global__ void __launch_bounds__(kTbThreads) tsb_tn_part_kernel(
     }
 }
 
+// The first Gram-Schmidt pass's update and the second pass's product in one
+// sweep over V: for each staged 32-row chunk, W[chunk] -= V[chunk] H1 (the
+// arithmetic of tsb_rows_kernel<true>: the same fragments, k in the same
+// order), the new rows written to W and into the staged chunk, then
+// V[chunk]^T W[chunk] accumulated as tsb_tn_part_kernel does -- so the parts,
+// and with them the reduced coefficients, are bit for bit those of the two
+// separate kernels, for one read of V instead of two.  H1 (m x b, leading
+// dimension ldh1) is staged with rows of b + 4 doubles.
+__global__ void __launch_bounds__(kTbThreads) tsb_sub_tn_part_kernel(
+        const double *__restrict__ V, int64_t ldv, int n, int m, const double *__restrict__ H1,
+        int ldh1, double *__restrict__ W, int64_t ldw, int b, int rows_per_part,
+        double *__restrict__ part) {
+    extern __shared__ double dsm[];
+    const int t = threadIdx.x, lane = t & 31, wid = t >> 5, gq = lane >> 2, tq = lane & 3;
+    const int nmt = (m + 7) >> 3, nnt = (b + 7) >> 3, ncol = m + b;
+    const int nks = (m + 3) >> 2, sbs = nnt * 8 + 4;
+    double *Bs = dsm + 2 * ncol * kVS;                   // H1: nks * 4 rows of sbs
+    for (int e = t; e < nks * 4 * sbs; e += kTbThreads) {
+        const int k = e / sbs, j = e % sbs;
+        Bs[e] = (k < m && j < b) ? H1[k + (int64_t)j * ldh1] : 0.0;
+    }
+    double acc[2][4][2];
+#pragma unroll
+    for (int s = 0; s < 2; s++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) acc[s][q][0] = acc[s][q][1] = 0.0;
+    const int rb = blockIdx.x * rows_per_part, re = min(n, rb + rows_per_part);
+    auto stage = [&](double *Cs, int r0) {
+        const int nr = min(kTbRows, re - r0);
+        for (int e = t; e < ncol * kTbRows; e += kTbThreads) {
+            const int c = e >> 5, rr = e & 31;
+            const double *src = (c < m ? V + (int64_t)c * ldv : W + (int64_t)(c - m) * ldw) + r0;
+            cp_async8z(Cs + c * kVS + rr, src + (rr < nr ? rr : 0), rr < nr);
+        }
+        cp_async_commit();
+    };
+    if (rb < re) stage(dsm, rb);
+    int buf = 0;
+    for (int r0 = rb; r0 < re; r0 += kTbRows) {
+        double *Cs = dsm + buf * ncol * kVS;
+        if (r0 + kTbRows < re) {
+            stage(dsm + (buf ^ 1) * ncol * kVS, r0 + kTbRows);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        // W[chunk] -= V[chunk] H1: output tile ti = (8-row tile ti % 4,
+        // 8-column tile ti / 4), tiles taken by the warps in turn
+        for (int ti = wid; ti < 4 * nnt; ti += kTbThreads / 32) {
+            const int rt = ti & 3, q = ti >> 2;
+            double d[2] = {0.0, 0.0};
+            for (int ks = 0; ks < nks; ks++) {
+                const int k = ks * 4 + tq;
+                dmma884(d, k < m ? Cs[k * kVS + rt * 8 + gq] : 0.0, Bs[k * sbs + q * 8 + gq]);
+            }
+            const int rr = rt * 8 + gq;
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                const int j = q * 8 + 2 * tq + e;
+                if (j < b) {
+                    double *cw = Cs + (m + j) * kVS + rr;
+                    const double v = *cw - d[e];
+                    *cw = v;
+                    if (r0 + rr < re) W[r0 + rr + (int64_t)j * ldw] = v;
+                }
+            }
+        }
+        __syncthreads();
+#pragma unroll 2
+        for (int ks = 0; ks < kTbRows / 4; ks++) {
+            const int k = ks * 4 + tq;
+            double bf[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) bf[q] = (q * 8 + gq < b) ? Cs[(m + q * 8 + gq) * kVS + k] : 0.0;
+#pragma unroll
+            for (int s = 0; s < 2; s++) {
+                const int mt = wid + 8 * s;
+                if (mt < nmt) {
+                    const double a = (mt * 8 + gq < m) ? Cs[(mt * 8 + gq) * kVS + k] : 0.0;
+#pragma unroll
+                    for (int q = 0; q < 4; q++)
+                        if (q < nnt) dmma884(acc[s][q], a, bf[q]);
+                }
+            }
+        }
+        __syncthreads();
+        buf ^= 1;
+    }
+    double *p = part + (size_t)blockIdx.x * (kBlockMaxM * kBlockMaxB);
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+        const int mt = wid + 8 * s;
+        if (mt >= nmt) continue;
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+            if (q < nnt)
+#pragma unroll
+                for (int e = 0; e < 2; e++)
+                    p[(mt * 8 + gq) * kBlockMaxB + q * 8 + 2 * tq + e] = acc[s][q][e];
+    }
+}
+
 // H (=|+=) the sum of the parts: a block per 32 consecutive outputs, warp s
 // adding parts s, s + 8, s + 16, ... of each output (coalesced rows of
 // part), then the 8 slice sums added in slice order -- a fixed order, so
@@ -412,6 +515,31 @@ void launch_tsb_tn(const double *V, int64_t ldv, int n, int m, const double *W, 
     tsb_tn_part_kernel<<<np, kTbThreads, smem, st>>>(V, ldv, n, m, W, ldw, b, rows, bs.part);
     const int outs = m * kBlockMaxB;
     tsb_tn_reduce_kernel<<<(outs + 31) / 32, 32 * kRedSlices, 0, st>>>(m, b, np, bs.part, H, ldh,
+                                                                       mode);
+    note_launch(2);
+}
+
+void launch_tsb_sub_tn(const double *V, int64_t ldv, int n, int m, const double *H1, int ldh1,
+                       double *W, int64_t ldw, int b, double *H2, int ldh2, int mode,
+                       const BlockScratch &bs, cudaStream_t st) {
+    if (m <= 0 || b <= 0) return;
+    const int nparts = std::min(tsb_parts(n), bs.max_parts);
+    int rows = (n + nparts - 1) / nparts;
+    rows = (rows + kTbRows - 1) / kTbRows * kTbRows;
+    const int np = (n + rows - 1) / rows;
+    const int nnt = (b + 7) >> 3, nks = (m + 3) >> 2;
+    const size_t smem = sizeof(double) * (2 * (size_t)(m + b) * kVS + (size_t)nks * 4 * (nnt * 8 + 4));
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(tsb_sub_tn_part_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(sizeof(double) * (2 * (kBlockMaxM + kBlockMaxB) * kVS +
+                                                     kBlockMaxM * (kBlockMaxB + 4))));
+        attr = true;
+    }
+    tsb_sub_tn_part_kernel<<<np, kTbThreads, smem, st>>>(V, ldv, n, m, H1, ldh1, W, ldw, b, rows,
+                                                         bs.part);
+    const int outs = m * kBlockMaxB;
+    tsb_tn_reduce_kernel<<<(outs + 31) / 32, 32 * kRedSlices, 0, st>>>(m, b, np, bs.part, H2, ldh2,
                                                                        mode);
     note_launch(2);
 }

@@ -29,6 +29,12 @@ void launch_tsb_tn(const double *V, int64_t ldv, int n, int m, const double *W, 
 // W[:, 0:b] -= V[:, 0:m] H[0:m, 0:b]
 void launch_tsb_nn_sub(const double *V, int64_t ldv, int n, int m, const double *H, int ldh,
                        double *W, int64_t ldw, int b, cudaStream_t st);
+// W[:, 0:b] -= V[:, 0:m] H1, then H2[0:m, 0:b] = V^T W (mode 0) or += (mode
+// 1), in one sweep over V; the results equal, bit for bit, those of
+// launch_tsb_nn_sub followed by launch_tsb_tn.  H2 may be H1.
+void launch_tsb_sub_tn(const double *V, int64_t ldv, int n, int m, const double *H1, int ldh1,
+                       double *W, int64_t ldw, int b, double *H2, int ldh2, int mode,
+                       const BlockScratch &bs, cudaStream_t st);
 // Gram matrix G (b x b) of a block -> Rinv (b x b, upper triangular) with
 // G = R^T R, by a Cholesky of the column-scaled G.  status[0] receives a
 // bit mask of dependent columns: column j is dependent when its norm is
