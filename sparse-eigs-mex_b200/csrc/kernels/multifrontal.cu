@@ -107,28 +107,66 @@ mf_assemble(const int4 *__restrict__ tasks, Sym y, Real *__restrict__ F,
     tile_range<T>(f, I, ra, rb);
     tile_range<T>(f, J, ca, cb);
     const int h = rb - ra, w = cb - ca;
+    // The children's geometry is read by one thread per child, a batch of
+    // kFThreads children at a time, and the children that touch this tile
+    // are listed in child order; only those are added, one after another
+    // (a parent entry can receive several children's terms, and the fixed
+    // order keeps the sums reproducible).
+    __shared__ int s_ch[kFThreads], s_ia[kFThreads], s_ja[kFThreads], s_hw[kFThreads];
+    __shared__ int s_cnt;
     for (int t = threadIdx.x; t < T * T; t += blockDim.x) S[t & (T - 1)][t >> 5] = 0.0;
-    __syncthreads();
-    for (int q = y.child_ptr[s]; q < y.child_ptr[s + 1]; q++) {
-        const int ch = y.child_list[q];
-        const int rch = (int)(y.rowptr[ch + 1] - y.rowptr[ch]);
-        const int cch = y.sfirst[ch + 1] - y.sfirst[ch];
-        const int nb = rch - cch;
-        const int32_t *rm = y.relmap + y.rowptr[ch] + cch;
-        const int32_t *bd = y.cbnd + y.cbnd_ptr[ch];
-        const int ia = bd[I], ib = bd[I + 1], ja = bd[J], jb = bd[J + 1];
-        const int hi = ib - ia, wj = jb - ja;
-        (void)nb;
-        if (hi > 0 && wj > 0) {
-            const Real *U = F + y.frontptr[ch];
-            for (int t = threadIdx.x; t < hi * wj; t += blockDim.x) {
-                const int i = ia + t % hi, j = ja + t / hi;
+    const int q0 = y.child_ptr[s], q1 = y.child_ptr[s + 1];
+    for (int qb = q0; qb < q1; qb += kFThreads) {
+        if (threadIdx.x == 0) s_cnt = 0;
+        __syncthreads();
+        const int q = qb + (int)threadIdx.x;
+        int ch = -1, ia = 0, ja = 0, hi = 0, wj = 0;
+        if (q < q1) {
+            ch = y.child_list[q];
+            const int32_t *bd = y.cbnd + y.cbnd_ptr[ch];
+            ia = bd[I];
+            hi = bd[I + 1] - ia;
+            ja = bd[J];
+            wj = bd[J + 1] - ja;
+        }
+        const bool live = hi > 0 && wj > 0;
+        // order-preserving compaction: warp ballots, then the warps' counts
+        const unsigned bal = __ballot_sync(0xffffffffu, live);
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        __shared__ int s_wcnt[kFThreads / 32];
+        if (lane == 0) s_wcnt[wid] = __popc(bal);
+        __syncthreads();
+        if (live) {
+            int pos = __popc(bal & ((1u << lane) - 1u));
+            for (int w2 = 0; w2 < wid; w2++) pos += s_wcnt[w2];
+            s_ch[pos] = ch;
+            s_ia[pos] = ia;
+            s_ja[pos] = ja;
+            s_hw[pos] = hi | (wj << 16);
+        }
+        if (threadIdx.x == 0) {
+            int tot = 0;
+            for (int w2 = 0; w2 < kFThreads / 32; w2++) tot += s_wcnt[w2];
+            s_cnt = tot;
+        }
+        __syncthreads();
+        const int cnt = s_cnt;
+        for (int e = 0; e < cnt; e++) {
+            const int c2 = s_ch[e], ia2 = s_ia[e], ja2 = s_ja[e];
+            const int hi2 = s_hw[e] & 0xffff, wj2 = s_hw[e] >> 16;
+            const int rch = (int)(y.rowptr[c2 + 1] - y.rowptr[c2]);
+            const int cch = y.sfirst[c2 + 1] - y.sfirst[c2];
+            const int32_t *rm = y.relmap + y.rowptr[c2] + cch;
+            const Real *U = F + y.frontptr[c2];
+            for (int t = threadIdx.x; t < hi2 * wj2; t += blockDim.x) {
+                const int i = ia2 + t % hi2, j = ja2 + t / hi2;
                 if (i >= j)
                     S[rm[i] - ra][rm[j] - ca] += U[(int64_t)(cch + i) + (int64_t)(cch + j) * rch];
             }
+            __syncthreads();
         }
-        __syncthreads();
     }
+    __syncthreads();
     if (J < f.nkb) {
         if (threadIdx.x < w) {
             const int jj = ca + threadIdx.x;
