@@ -263,6 +263,29 @@ def run_metric(args, pkg, wl, ctx):
         with torch.cuda.stream(stream):
             Yw.copy_(Y32.t())
 
+    # the proposal's forward pass alone (CUDA events, median of 20 after 3
+    # warm-up runs), with the dense layers on the tensor cores (the default)
+    # and on the FP32-FMA kernels, before any timed region
+    proposal_ms = None
+    if net is not None:
+        proposal_ms = {}
+        pst = torch.cuda.current_stream()
+        for label, on in (("fma_dense_layers", 0), ("tensor_core_dense_layers", 1)):
+            net.tensor_cores(on)
+            for _ in range(3):
+                propose_device(pst)
+            tms = []
+            for _ in range(20):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(pst)
+                propose_device(pst)
+                e1.record(pst)
+                e1.synchronize()
+                tms.append(e0.elapsed_time(e1))
+            proposal_ms[label] = round(statistics.median(tms), 4)
+        net.tensor_cores(1)
+
     # ---- autotuning (before any timed region): the block size and basis
     # size of the learned forms, chosen by pkg.tune on a TRAINING operator
     # of the same family (seed 1000, one the network was trained on), with
@@ -489,7 +512,8 @@ def run_metric(args, pkg, wl, ctx):
                        "value_scope": "numeric factor + proposal on the device + Lanczos, "
                                       "matrix and analysis resident"},
             "ratio_target_over_fp64": tv / forms["fp64"]["value_s"],
-            "forms": forms, "check": check, "roofline": roofline, "cpu_baseline": cpu,
+            "forms": forms, "proposal_ms": proposal_ms, "check": check, "roofline": roofline,
+            "cpu_baseline": cpu,
             "e2e": e2e[target], "e2e_fp64": e2e["fp64"],
             "gpu_launches": int(keep[target]["launches"]), "clocks": keep[target]["clocks"],
         }
