@@ -266,6 +266,110 @@ SPX_DEV void bbwd_leaves(const BSolveArgs &a, int boff, int bn, BWarpShared<NR> 
     for (int li = threadIdx.x >> 5; li < bn; li += kSWarps) bbwd_warp<NR>(a, a.bundle[boff + li], w);
 }
 
+// ---- tiny leaves eight to a warp: lanes 4 g .. 4 g + 3 take one leaf (live
+// when the leaf exists), lane tq columns 2 tq, 2 tq + 1 of every 8-column
+// chunk, with plain FP64 multiply-adds (a leaf's G is at most kTinyR x
+// kTinyC).  Forward: [yf(pivots); -u] = G b(pivots) -- a leaf has no
+// children to wait for.
+template <int NR>
+SPX_DEV void bfwd_leaf_group(const BSolveArgs &a, int s, bool live) {
+    constexpr int NCH = NR / 8;
+    int *const fcd = a.sync + 1, *const fchk = fcd + 3 * a.ns;
+    const int tq = threadIdx.x & 3;
+    int parent = -1;
+    if (live) {
+        const SNode m = a.meta[s];
+        const int first = m.a.x, c = m.a.y, r = m.a.z, ldg = m.a.w;
+        parent = m.b.x;
+        const Real *Gs = a.G + m.p.x;
+        int pr[kTinyC];
+#pragma unroll
+        for (int j = 0; j < kTinyC; j++) pr[j] = j < c ? a.perm[first + j] : 0;
+#pragma unroll 1
+        for (int ch = 0; ch < NCH; ch++) {
+            const int col = 8 * ch + 2 * tq;
+            double2 f[kTinyC];
+#pragma unroll
+            for (int j = 0; j < kTinyC; j++)
+                f[j] = j < c ? __ldg(reinterpret_cast<const double2 *>(a.b + (int64_t)pr[j] * NR + col))
+                             : make_double2(0.0, 0.0);
+#pragma unroll 2
+            for (int i = 0; i < r; i++) {
+                {
+                    double x0 = 0.0, x1 = 0.0;
+#pragma unroll
+                    for (int j = 0; j < kTinyC; j++)
+                        if (j < c) {
+                            const double g = ldg_panel(Gs + (int64_t)i + (int64_t)j * ldg);
+                            x0 += g * f[j].x;
+                            x1 += g * f[j].y;
+                        }
+                    if (i < c) st2(a.yf + (int64_t)(first + i) * NR + col, x0, x1);
+                    else st2(a.u + (m.uptr + (i - c)) * NR + col, -x0, -x1);
+                }
+            }
+        }
+    }
+    __syncwarp();
+    if (live && tq == 0) add_release(parent >= 0 ? fcd + parent : fchk + s, 1);
+}
+
+// Backward: x(pivots) = G^T [yf(pivots); -x(rows below)] once the parent's
+// backward has completed.
+template <int NR>
+SPX_DEV void bbwd_leaf_group(const BSolveArgs &a, int s, bool live) {
+    constexpr int NCH = NR / 8;
+    int *const bdone = a.sync + 1 + 2 * a.ns, *const fchk = bdone + a.ns,
+              *const err = a.sync + 1 + 5 * a.ns;
+    const int tq = threadIdx.x & 3;
+    SNode m{};
+    if (live) {
+        m = a.meta[s];
+        if (tq == 0) wait_at_least(m.b.x >= 0 ? bdone + m.b.x : fchk + s, m.bwd_expect, err);
+    }
+    __syncwarp();
+    if (live) {
+        const int first = m.a.x, c = m.a.y, r = m.a.z, ldg = m.a.w;
+        const int32_t *rows = a.rows + m.p.y;
+        const Real *Gs = a.G + m.p.x;
+#pragma unroll 1
+        for (int ch = 0; ch < NCH; ch++) {
+            const int col = 8 * ch + 2 * tq;
+            double2 acc[kTinyC];
+#pragma unroll
+            for (int j = 0; j < kTinyC; j++) acc[j] = make_double2(0.0, 0.0);
+#pragma unroll 2
+            for (int i = 0; i < r; i++) {
+                {
+                    double2 v;
+                    if (i < c) {
+                        v = ldcg2(a.yf + (int64_t)(first + i) * NR + col);
+                    } else {
+                        v = ldcg2(a.x + (int64_t)rows[i] * NR + col);
+                        v.x = -v.x;
+                        v.y = -v.y;
+                    }
+#pragma unroll
+                    for (int j = 0; j < kTinyC; j++)
+                        if (j < c) {
+                            const double g = ldg_panel(Gs + (int64_t)i + (int64_t)j * ldg);
+                            acc[j].x += g * v.x;
+                            acc[j].y += g * v.y;
+                        }
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < kTinyC; j++)
+                if (j < c) {
+                    st2(a.x + (int64_t)(first + j) * NR + col, acc[j].x, acc[j].y);
+                    st2(a.out + (int64_t)a.perm[first + j] * NR + col, acc[j].x, acc[j].y);
+                }
+        }
+    }
+    __syncwarp();
+    if (live && tq == 0) add_release(bdone + s, 1);
+}
+
 
 // ---- forward, rows [64 I, 64 I + 64) x a 128-column strip S of a large
 // supernode's panel: (64 x 128) x (128 x NR) on the tensor cores, warp w
@@ -496,9 +600,20 @@ SPX_DEV void bsolve_warp_tasks(const BSolveArgs &a, const STask *tq, int nt, int
         if (t >= nt) break;
         const STask tk = tq[t];
         const bool fwd = tk.a.x == ST_FWD_BUNDLE || tk.a.x == ST_FWD_THREADS;
-        for (int q = 0; q < tk.b.z; q++) {
-            if (fwd) bfwd_warp<NR>(a, a.bundle[tk.b.y + q], w);
-            else bbwd_warp<NR>(a, a.bundle[tk.b.y + q], w);
+        if (tk.a.x == ST_FWD_THREADS || tk.a.x == ST_BWD_THREADS) {
+            // tiny leaves: eight at a time, four lanes each
+            const int g = lane >> 2;
+            for (int p = 0; p < tk.b.z; p += 8) {
+                const bool live = p + g < tk.b.z;
+                const int s = live ? a.bundle[tk.b.y + p + g] : 0;
+                if (fwd) bfwd_leaf_group<NR>(a, s, live);
+                else bbwd_leaf_group<NR>(a, s, live);
+            }
+        } else {
+            for (int q = 0; q < tk.b.z; q++) {
+                if (fwd) bfwd_warp<NR>(a, a.bundle[tk.b.y + q], w);
+                else bbwd_warp<NR>(a, a.bundle[tk.b.y + q], w);
+            }
         }
         __syncwarp();
     }
