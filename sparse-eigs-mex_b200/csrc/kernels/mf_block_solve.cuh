@@ -392,12 +392,36 @@ SPX_DEV void bfwd_tile(const BSolveArgs &a, int s, int I, int S, int chunk, BSha
     const int t = threadIdx.x;
     // the strip's right-hand-side rows, read before the wait
     double2 bv[PP];
+    // and the children's gather lists of those rows -- their bounds and first
+    // two entries -- so that after the wait only the update rows are read
+    int qb[PP], qe[PP], q0i[PP], q1i[PP];
 #pragma unroll
     for (int p = 0; p < PP; p++) {
         const int e = t + kSThreads * p, jj = e / H, h = e % H;
         bv[p] = (jj < jn) ? __ldg(reinterpret_cast<const double2 *>(a.b) +
                                   (int64_t)a.perm[first + j0 + jj] * H + h)
                           : make_double2(0.0, 0.0);
+        qb[p] = qe[p] = q0i[p] = q1i[p] = 0;
+        if (jj < jn && nchild > 0) {
+            const int64_t g = g0 + j0 + jj;
+            qb[p] = a.cptr[g];
+            qe[p] = a.cptr[g + 1];
+            if (qb[p] < qe[p]) q0i[p] = a.cidx[qb[p]];
+            if (qb[p] + 1 < qe[p]) q1i[p] = a.cidx[qb[p] + 1];
+        }
+    }
+    // the same for this lane's row of the update part, which the block that
+    // completes the row chunk gathers
+    int ub = 0, ue = 0, u0i = 0, u1i = 0;
+    {
+        const int ur = i0 + (t >> 5) * 8 + ((t & 31) >> 2);
+        if (nchild > 0 && ur >= c && ur < r) {
+            const int64_t g = g0 + ur;
+            ub = a.cptr[g];
+            ue = a.cptr[g + 1];
+            if (ub < ue) u0i = a.cidx[ub];
+            if (ub + 1 < ue) u1i = a.cidx[ub + 1];
+        }
     }
     if (nchild > 0 && t == 0) wait_at_least(fcd + s, expect, err);
     __syncthreads();
@@ -406,10 +430,9 @@ SPX_DEV void bfwd_tile(const BSolveArgs &a, int s, int I, int S, int chunk, BSha
         const int e = t + kSThreads * p, jj = e / H, h = e % H;
         double2 v = bv[p];
         if (jj < jn && nchild > 0) {
-            const int64_t g = g0 + j0 + jj;
-            const int e1 = a.cptr[g + 1];
-            for (int q = a.cptr[g]; q < e1; q++) {
-                const double2 u = ldcg2(a.u + (int64_t)a.cidx[q] * NR + 2 * h);
+            for (int q = qb[p]; q < qe[p]; q++) {
+                const int ci = q == qb[p] ? q0i[p] : (q == qb[p] + 1 ? q1i[p] : a.cidx[q]);
+                const double2 u = ldcg2(a.u + (int64_t)ci * NR + 2 * h);
                 v.x += u.x;
                 v.y += u.y;
             }
@@ -465,10 +488,9 @@ SPX_DEV void bfwd_tile(const BSolveArgs &a, int s, int I, int S, int chunk, BSha
 #pragma unroll
                 for (int ch = 0; ch < NCH; ch++) add[ch] = make_double2(0.0, 0.0);
                 if (nchild > 0) {
-                    const int64_t g = g0 + ii;
-                    const int e1 = a.cptr[g + 1];
-                    for (int q = a.cptr[g]; q < e1; q++) {
-                        const double *src = a.u + (int64_t)a.cidx[q] * NR + 2 * tq;
+                    for (int q = ub; q < ue; q++) {
+                        const int ci = q == ub ? u0i : (q == ub + 1 ? u1i : a.cidx[q]);
+                        const double *src = a.u + (int64_t)ci * NR + 2 * tq;
 #pragma unroll
                         for (int ch = 0; ch < NCH; ch++) {
                             const double2 u = ldcg2(src + 8 * ch);
