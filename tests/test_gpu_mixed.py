@@ -78,3 +78,33 @@ def test_mixed_singular_takes_shift(lib, pkg):
     rc, shift = P.factor()
     assert rc == 0 and shift > 0.0
     P.close()
+
+
+@pytest.mark.parametrize("case", ["lap40", "var24", "dense333"])
+def test_fp32_factor_is_fp32_accurate(lib, pkg, case):
+    """One solve with the FP32 factor alone (refine_tol = 1 accepts it
+    without a correction): its backward error is at the FP32 level.  The
+    trailing updates take three TF32 products (hi.hi + hi.lo + lo.hi) on the
+    tensor cores; with the head alone the factor would carry TF32 errors
+    (~1e-3), far above this bound."""
+    torch = pytest.importorskip("torch")
+    import scipy.sparse as sp
+    w = pkg.workloads
+    if case == "dense333":
+        rng = np.random.default_rng(7)
+        B = rng.standard_normal((333, 333))
+        A = sp.csc_matrix(B @ B.T / 333 + np.eye(333))
+    else:
+        A = {"lap40": lambda: w.lap3d(40), "var24": lambda: w.varcoef3d(24, seed=24)}[case]()
+    P = _mixed_plan(pkg, lib, A, refine_tol=1.0)
+    rc, shift = P.factor()
+    assert rc == 0 and shift == 0.0
+    b = torch.randn(A.shape[0], dtype=torch.float64, device="cuda")
+    x = torch.empty_like(b)
+    torch.cuda.synchronize()
+    assert P.apply_device(b.data_ptr(), x.data_ptr()) == 0
+    bh, xh = b.cpu().numpy(), x.cpu().numpy()
+    anorm = abs(A).sum(axis=0).max()
+    be = np.linalg.norm(bh - A @ xh) / (anorm * np.linalg.norm(xh) + np.linalg.norm(bh))
+    assert be < 1e-5, be
+    P.close()
