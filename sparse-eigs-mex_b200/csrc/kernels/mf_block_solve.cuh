@@ -4,9 +4,10 @@
 // Included by multifrontal.cu inside its anonymous namespace: it runs the
 // task queue of mf_solve_sf (same tasks, same per-supernode metadata, same
 // dependency counters and chunk partial sums) with every vector entry of the
-// single solve widened to a row of NR doubles, stored row-major with stride
-// NR: the right-hand sides and the result in the original order, the
-// intermediate yf, x and update vectors u in factor order.  A task's
+// single solve widened to a row of NR doubles: the intermediate yf, x and
+// update vectors u are stored row-major with stride NR in factor order; the
+// right-hand sides are read from, and the results written to, the caller's
+// column-major arrays in the original order.  A task's
 // product (rows x pivots) x (pivots x 1) becomes (rows x pivots) x
 // (pivots x NR), so the panel G is read once for all NR columns and the
 // level structure -- which bounds the single solve -- is paid once.
@@ -34,8 +35,15 @@ struct BSolveArgs {
     int *sync;                           // as SolveArgs::sync
     const STask *wtasks;                 // as SolveArgs::wtasks
     int nfw, nbw;
-    const double *b;                     // n rows of NR, original order
-    double *out;                         // n rows of NR, original order
+    // the caller's right-hand sides and results: nr columns, column-major,
+    // original order (columns nr .. NR-1 read as zero and are not written);
+    // every read of bc is in a forward task and every write of xc in a
+    // backward task, which starts after the whole forward pass, so xc may
+    // be bc
+    const double *bc;
+    double *xc;
+    int64_t ldb, ldx;
+    int nr;
     const int *skip;
 };
 
@@ -63,6 +71,15 @@ struct BWarpShared {                     // one warp task
 SPX_DEV double2 ldcg2(const double *p) { return __ldcg(reinterpret_cast<const double2 *>(p)); }
 SPX_DEV void st2(double *p, double a, double b) { *reinterpret_cast<double2 *>(p) = make_double2(a, b); }
 SPX_DEV double ldg_panel(const Real *p) { return (double)__ldg(p); }
+// right-hand-side columns col, col + 1 of original row `row`
+SPX_DEV double2 brhs2(const BSolveArgs &a, int64_t row, int col) {
+    return make_double2(col < a.nr ? __ldg(a.bc + (int64_t)col * a.ldb + row) : 0.0,
+                        col + 1 < a.nr ? __ldg(a.bc + (int64_t)(col + 1) * a.ldb + row) : 0.0);
+}
+// result column col of original row `row`
+SPX_DEV void bout1(const BSolveArgs &a, int64_t row, int col, double v) {
+    if (col < a.nr) a.xc[(int64_t)col * a.ldx + row] = v;
+}
 
 SPX_DEV void bstage_list(const BSolveArgs &a, int64_t g, int *idx, int *n, int *e0) {
     const int b0 = a.cptr[g], b1 = a.cptr[g + 1];
@@ -98,9 +115,7 @@ SPX_DEV void bfwd_warp(const BSolveArgs &a, int s, BWarpShared<NR> &w) {
 #pragma unroll
     for (int p = 0; p < PP; p++) {
         const int e = lane + 32 * p, j = e / H, h = e % H;
-        bv[p] = (j < c) ? __ldg(reinterpret_cast<const double2 *>(a.b) +
-                                (int64_t)a.perm[first + j] * H + h)
-                        : make_double2(0.0, 0.0);
+        bv[p] = (j < c) ? brhs2(a, a.perm[first + j], 2 * h) : make_double2(0.0, 0.0);
     }
     if (nchild > 0)
         for (int i = lane; i < r; i += 32) bstage_list(a, g0 + i, w.idx[i], &w.cnt[i], &w.e0[i]);
@@ -242,12 +257,11 @@ SPX_DEV void bbwd_warp(const BSolveArgs &a, int s, BWarpShared<NR> &w) {
         const int j = (q >> 1) * 8 + 2 * tq + (q & 1);
         if (j >= c) continue;
         double *xr = a.x + (int64_t)(first + j) * NR + gq;
-        double *orow = a.out + (int64_t)pv[q] * NR + gq;
 #pragma unroll
         for (int ch = 0; ch < NCH; ch++) {
             const double v = d[ch][q >> 1][q & 1];
             xr[8 * ch] = v;
-            orow[8 * ch] = v;
+            bout1(a, pv[q], 8 * ch + gq, v);
         }
     }
     __syncwarp();
@@ -291,8 +305,7 @@ SPX_DEV void bfwd_leaf_group(const BSolveArgs &a, int s, bool live) {
             double2 f[kTinyC];
 #pragma unroll
             for (int j = 0; j < kTinyC; j++)
-                f[j] = j < c ? __ldg(reinterpret_cast<const double2 *>(a.b + (int64_t)pr[j] * NR + col))
-                             : make_double2(0.0, 0.0);
+                f[j] = j < c ? brhs2(a, pr[j], col) : make_double2(0.0, 0.0);
 #pragma unroll 2
             for (int i = 0; i < r; i++) {
                 {
@@ -362,7 +375,9 @@ SPX_DEV void bbwd_leaf_group(const BSolveArgs &a, int s, bool live) {
             for (int j = 0; j < kTinyC; j++)
                 if (j < c) {
                     st2(a.x + (int64_t)(first + j) * NR + col, acc[j].x, acc[j].y);
-                    st2(a.out + (int64_t)a.perm[first + j] * NR + col, acc[j].x, acc[j].y);
+                    const int pj = a.perm[first + j];
+                    bout1(a, pj, col, acc[j].x);
+                    bout1(a, pj, col + 1, acc[j].y);
                 }
         }
     }
@@ -398,9 +413,7 @@ SPX_DEV void bfwd_tile(const BSolveArgs &a, int s, int I, int S, int chunk, BSha
 #pragma unroll
     for (int p = 0; p < PP; p++) {
         const int e = t + kSThreads * p, jj = e / H, h = e % H;
-        bv[p] = (jj < jn) ? __ldg(reinterpret_cast<const double2 *>(a.b) +
-                                  (int64_t)a.perm[first + j0 + jj] * H + h)
-                          : make_double2(0.0, 0.0);
+        bv[p] = (jj < jn) ? brhs2(a, a.perm[first + j0 + jj], 2 * h) : make_double2(0.0, 0.0);
         qb[p] = qe[p] = q0i[p] = q1i[p] = 0;
         if (jj < jn && nchild > 0) {
             const int64_t g = g0 + j0 + jj;
@@ -588,7 +601,7 @@ SPX_DEV void bbwd_tile(const BSolveArgs &a, int s, int J, int S, int chunk, BSha
         for (int e = 0; e < 2; e++) {
             const int jj = wid * 8 + 2 * tq + e;
             if (jj >= jn) continue;
-            const int64_t orow = (int64_t)a.perm[first + j0 + jj] * NR;
+            const int64_t orow = a.perm[first + j0 + jj];
 #pragma unroll
             for (int ch = 0; ch < NCH; ch++) {
                 double rr = d[ch][e];
@@ -599,7 +612,7 @@ SPX_DEV void bbwd_tile(const BSolveArgs &a, int s, int J, int S, int chunk, BSha
                     for (int q = 0; q < nt; q++) rr += __ldcg(p0 + (int64_t)q * kST * NR);
                 }
                 a.x[(int64_t)(first + j0 + jj) * NR + 8 * ch + gq] = rr;
-                a.out[orow + 8 * ch + gq] = rr;
+                bout1(a, orow, 8 * ch + gq, rr);
             }
         }
         __syncthreads();
@@ -694,42 +707,4 @@ template <int NR>
 constexpr size_t bsolve_smem_bytes() {
     return sizeof(BShared<NR>) > sizeof(BWarpShared<NR>) * kSWarps
                ? sizeof(BShared<NR>) : sizeof(BWarpShared<NR>) * kSWarps;
-}
-
-// Column-major n x nr (leading dimension ld) <-> row-major n x NR (stride
-// NR, columns nr..NR-1 zero on the way in).  A block of 256 threads moves 32
-// rows through shared memory so both sides are read and written in
-// contiguous runs.
-template <int NR>
-__global__ void __launch_bounds__(256) bs_to_rows(int n, int nr, const double *B, int64_t ld,
-                                                  double *R, const int *skip) {
-    __shared__ double tile[32][NR + 1];
-    if (skip && *(volatile const int *)skip) return;
-    const int r0 = blockIdx.x * 32;
-    for (int e = threadIdx.x; e < 32 * NR; e += blockDim.x) {
-        const int i = e % 32, c = e / 32;     // consecutive threads: consecutive rows
-        tile[i][c] = (r0 + i < n && c < nr) ? B[(int64_t)(r0 + i) + (int64_t)c * ld] : 0.0;
-    }
-    __syncthreads();
-    for (int e = threadIdx.x; e < 32 * NR; e += blockDim.x) {
-        const int i = e / NR, c = e % NR;     // consecutive threads: one row's columns
-        if (r0 + i < n) R[(int64_t)(r0 + i) * NR + c] = tile[i][c];
-    }
-}
-
-template <int NR>
-__global__ void __launch_bounds__(256) bs_from_rows(int n, int nr, const double *R, double *X,
-                                                    int64_t ld, const int *skip) {
-    __shared__ double tile[32][NR + 1];
-    if (skip && *(volatile const int *)skip) return;
-    const int r0 = blockIdx.x * 32;
-    for (int e = threadIdx.x; e < 32 * NR; e += blockDim.x) {
-        const int i = e / NR, c = e % NR;
-        tile[i][c] = (r0 + i < n) ? R[(int64_t)(r0 + i) * NR + c] : 0.0;
-    }
-    __syncthreads();
-    for (int e = threadIdx.x; e < 32 * NR; e += blockDim.x) {
-        const int i = e % 32, c = e / 32;
-        if (r0 + i < n && c < nr) X[(int64_t)(r0 + i) + (int64_t)c * ld] = tile[i][c];
-    }
 }

@@ -1598,10 +1598,10 @@ template <> void MultifrontalPlanT<Real>::release(cudaStream_t st) {
                     d_rowptr_, d_frontptr_, d_gptr_, d_uptr_, d_acolptr_, d_atpos_, d_asrc_,
                     d_tasks_, d_front_, d_G_, d_u_, d_yf_, d_x_, d_status_, d_meta_,
                     d_stask_, d_bundle_, d_cptr_, d_cidx_, d_chunks_, d_fpart_, d_bpart_,
-                    d_cnt_, d_sync_, d_bin_, d_bout_, d_byf_, d_bx_, d_bu_, d_bfp_, d_bbp_};
+                    d_cnt_, d_sync_, d_byf_, d_bx_, d_bu_, d_bfp_, d_bbp_};
     for (void *p : ptrs)
         if (p) cudaFreeAsync(p, st);
-    d_bin_ = d_bout_ = d_byf_ = d_bx_ = d_bu_ = d_bfp_ = d_bbp_ = nullptr;
+    d_byf_ = d_bx_ = d_bu_ = d_bfp_ = d_bbp_ = nullptr;
     bw_ = 0;
     d_perm_ = d_sfirst_ = d_rows_ = d_relmap_ = d_child_ptr_ = d_child_list_ = nullptr;
     d_cbnd_ = nullptr;
@@ -2290,14 +2290,9 @@ template <> void MultifrontalPlanT<Real>::solve(const double *b, double *x, cuda
 
 namespace {
 template <int NR>
-void launch_bsolve(const BSolveArgs &a, int n, int nr, const double *B, int64_t ldb, double *X,
-                   int64_t ldx, double *bin, const double *bout, int grid, size_t smem,
-                   cudaStream_t st) {
-    const int tb = (n + 31) / 32;
-    bs_to_rows<NR><<<tb, 256, 0, st>>>(n, nr, B, ldb, bin, a.skip);
+void launch_bsolve(const BSolveArgs &a, int grid, size_t smem, cudaStream_t st) {
     mf_bsolve<NR><<<grid, kSThreads, smem, st>>>(a);
-    bs_from_rows<NR><<<tb, 256, 0, st>>>(n, nr, bout, X, ldx, a.skip);
-    note_launch(3);
+    note_launch();
 }
 
 template <int NR>
@@ -2326,14 +2321,12 @@ template <> int MultifrontalPlanT<Real>::solve_block(const double *B, int64_t ld
     const int q = w / 8 - 1;
     if (w > bw_) {
         // (re)allocate the block buffers for rows of w doubles
-        void *old[] = {d_bin_, d_bout_, d_byf_, d_bx_, d_bu_, d_bfp_, d_bbp_};
+        void *old[] = {d_byf_, d_bx_, d_bu_, d_bfp_, d_bbp_};
         for (void *p : old)
             if (p) cudaFreeAsync(p, st);
-        d_bin_ = d_bout_ = d_byf_ = d_bx_ = d_bu_ = d_bfp_ = d_bbp_ = nullptr;
+        d_byf_ = d_bx_ = d_bu_ = d_bfp_ = d_bbp_ = nullptr;
         bw_ = 0;
         int rc = 0;
-        rc = rc ? rc : dmalloc(&d_bin_, (size_t)n_ * w, st);
-        rc = rc ? rc : dmalloc(&d_bout_, (size_t)n_ * w, st);
         rc = rc ? rc : dmalloc(&d_byf_, (size_t)n_ * w, st);
         rc = rc ? rc : dmalloc(&d_bx_, (size_t)n_ * w, st);
         rc = rc ? rc : dmalloc(&d_bu_, (size_t)std::max<int64_t>(u_total_, 1) * w, st);
@@ -2378,18 +2371,21 @@ template <> int MultifrontalPlanT<Real>::solve_block(const double *B, int64_t ld
     a.fcnt = d_cnt_;
     a.bcnt = d_cnt_ + nfc_;
     a.sync = d_sync_;
-    a.b = d_bin_;
-    a.out = d_bout_;
+    a.bc = B;
+    a.xc = X;
+    a.ldb = ldb;
+    a.ldx = ldx;
+    a.nr = nr;
     a.skip = skip;
     cudaMemsetAsync(d_sync_, 0, sizeof(int) * (sync_ints_ - 1), st);
     if (w == 8)
-        launch_bsolve<8>(a, n_, nr, B, ldb, X, ldx, d_bin_, d_bout_, bgrid_[q], bsmem_[q], st);
+        launch_bsolve<8>(a, bgrid_[q], bsmem_[q], st);
     else if (w == 16)
-        launch_bsolve<16>(a, n_, nr, B, ldb, X, ldx, d_bin_, d_bout_, bgrid_[q], bsmem_[q], st);
+        launch_bsolve<16>(a, bgrid_[q], bsmem_[q], st);
     else if (w == 24)
-        launch_bsolve<24>(a, n_, nr, B, ldb, X, ldx, d_bin_, d_bout_, bgrid_[q], bsmem_[q], st);
+        launch_bsolve<24>(a, bgrid_[q], bsmem_[q], st);
     else
-        launch_bsolve<32>(a, n_, nr, B, ldb, X, ldx, d_bin_, d_bout_, bgrid_[q], bsmem_[q], st);
+        launch_bsolve<32>(a, bgrid_[q], bsmem_[q], st);
     return 0;
 }
 

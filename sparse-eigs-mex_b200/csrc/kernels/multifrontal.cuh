@@ -124,7 +124,7 @@ private:
     // the chunk partials; a solve of width NR <= bw_ uses them with stride NR
     int bw_ = 0;
     int32_t fslots_ = 0, bslots_ = 0;
-    double *d_bin_ = nullptr, *d_bout_ = nullptr, *d_byf_ = nullptr, *d_bx_ = nullptr,
+    double *d_byf_ = nullptr, *d_bx_ = nullptr,
            *d_bu_ = nullptr, *d_bfp_ = nullptr, *d_bbp_ = nullptr;
     int bgrid_[4] = {0, 0, 0, 0};          // per width NR = 8 (q + 1): grid, 0 = not set up
     size_t bsmem_[4] = {0, 0, 0, 0};
