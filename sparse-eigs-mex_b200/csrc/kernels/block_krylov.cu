@@ -429,13 +429,29 @@ __global__ void __launch_bounds__(kRefRows) block_refine_residual_kernel(
     __syncthreads();
     if (!am_last) return;
     __threadfence();
-    // fixed-order sums per column: thread c takes column c
+    // fixed-order sums: each of the 3 b sums is split over g threads (thread
+    // k of the sum takes blocks k, k + g, ...), and the g partial sums are
+    // added in thread order -- the same order in every run
+    __shared__ double red[kRefRows];
+    const int nv = 3 * b, g = kRefRows / nv;
+    {
+        const int v = threadIdx.x % nv, k = threadIdx.x / nv;
+        double t = 0.0;
+        if (k < g) {
+#pragma unroll 4
+            for (int bk = k; bk < (int)gridDim.x; bk += g)
+                t += __ldcg(part + (size_t)bk * (3 * BW) + v);
+        }
+        red[threadIdx.x] = t;
+    }
+    __syncthreads();
     bool ok = true;
-    for (int c = threadIdx.x; c < b; c += blockDim.x) {
+    if ((int)threadIdx.x < b) {
+        const int c = threadIdx.x;
         double t[3] = {0.0, 0.0, 0.0};
-        for (int bk = 0; bk < (int)gridDim.x; bk++)
-            for (int q = 0; q < 3; q++)
-                t[q] += ((volatile double *)part)[(size_t)bk * (3 * BW) + 3 * c + q];
+        for (int k = 0; k < g; k++)
+#pragma unroll
+            for (int q = 0; q < 3; q++) t[q] += red[k * nv + 3 * c + q];
         if (!(sqrt(t[0]) <= tol * (anorm * sqrt(t[1]) + sqrt(t[2])))) ok = false;
     }
     ok = __syncthreads_and(ok);
@@ -582,6 +598,7 @@ void launch_block_refine_residual(int n, const int32_t *rowptr, const int32_t *c
                                   const double *Y, int64_t ldy, double *R, int64_t ldr, int b,
                                   double tol, double anorm, int *flag, int *count, double *part,
                                   unsigned *counter, cudaStream_t st) {
+    if (b <= 0) return;
     const int grid = (n + kRefRows - 1) / kRefRows;
 #define SPX_REFINE(BW)                                                                        \
     block_refine_residual_kernel<BW><<<grid, kRefRows, 0, st>>>(n, rowptr, col, val, shift, B, \
