@@ -272,9 +272,9 @@ struct Factor {
         else f64.solve(b, x, st, skip);
     }
     int solve_block(const double *B, int64_t ldb, double *X, int64_t ldx, int nr, cudaStream_t st,
-                    const int *skip = nullptr) {
-        return mixed ? f32.solve_block(B, ldb, X, ldx, nr, st, skip)
-                     : f64.solve_block(B, ldb, X, ldx, nr, st, skip);
+                    const int *skip = nullptr, bool accumulate = false) {
+        return mixed ? f32.solve_block(B, ldb, X, ldx, nr, st, skip, accumulate)
+                     : f64.solve_block(B, ldb, X, ldx, nr, st, skip, accumulate);
     }
     int *error_word() const { return mixed ? f32.error_word() : f64.error_word(); }
     double factor_flops() const { return mixed ? f32.factor_flops() : f64.factor_flops(); }
@@ -371,10 +371,10 @@ struct BlockOperator {
     double ms_solve_acc = 0;
     int64_t solve_calls = 0;
     int timed_solve(Factor *plan, const double *B, int64_t ldb, double *X, int64_t ldx, int nr,
-                    cudaStream_t st, const int *skip = nullptr) {
+                    cudaStream_t st, const int *skip = nullptr, bool accumulate = false) {
         solve_calls++;
         const int t = tm ? tm->begin() : -1;
-        const int rc = plan->solve_block(B, ldb, X, ldx, nr, st, skip);
+        const int rc = plan->solve_block(B, ldb, X, ldx, nr, st, skip, accumulate);
         if (tm) tm->end(t, ms_solve);
         return rc;
     }
@@ -394,7 +394,7 @@ struct BlockCholOperator : BlockOperator {
 
 // Device state of the FP64 refinement of a mixed-precision block solve.
 struct BlockRefineState {
-    double *R = nullptr, *D = nullptr, *part = nullptr;
+    double *R = nullptr, *part = nullptr;
     int64_t ld = 0;
     int *flag = nullptr, *count = nullptr;
     int *short_word = nullptr;   // set when a solve was left unconverged within `budget`
@@ -409,10 +409,11 @@ __global__ void flag_if_unset_kernel(const int *flag, int *word) {
 }
 
 // Mixed precision on a block: X = M^{-1} B with the FP32 factor, then
-// R = B - (A + shift I) X and X += M^{-1} R until every column passes the
-// backward-error test or max_steps corrections were made.  As for one
-// vector, the whole loop is queued; once the flag is set, the remaining
-// solves and updates return at once on the device.
+// R = B - (A + shift I) X and X += M^{-1} R (the correction solve adds its
+// result into X) until every column passes the backward-error test or
+// max_steps corrections were made.  As for one vector, the whole loop is
+// queued; once the flag is set, the remaining solves return at once on the
+// device.
 struct BlockMixedOperator : BlockOperator {
     Factor *plan;
     DevA A;
@@ -438,9 +439,8 @@ struct BlockMixedOperator : BlockOperator {
                                          rf->ld, b, rf->tol, anorm, rf->flag, rf->count,
                                          rf->part, rf->counter, st);
             if (it == steps) break;
-            rc = timed_solve(plan, rf->R, rf->ld, rf->D, rf->ld, b, st, rf->flag);
+            rc = timed_solve(plan, rf->R, rf->ld, W, ldw, b, st, rf->flag, true);
             if (rc) return rc;
-            launch_block_axpy_unless(A.n, b, W, ldw, rf->D, rf->ld, rf->flag, st);
         }
         if (steps < rf->max_steps) {
             flag_if_unset_kernel<<<1, 1, 0, st>>>(rf->flag, rf->short_word);
@@ -1671,7 +1671,6 @@ static int plan_solve(speigs_plan_s *p, int64_t k, double *lambda, double *V, do
             if (p->mf.mixed) {
                 brf.ld = ((int64_t)n + 31) & ~(int64_t)31;
                 brf.R = ar.alloc<double>((size_t)brf.ld * bsz);
-                brf.D = ar.alloc<double>((size_t)brf.ld * bsz);
                 brf.part = ar.alloc<double>((size_t)3 * kBlockMaxB * ((n + 255) / 256));
                 brf.flag = ar.alloc<int>(1);
                 brf.count = ar.alloc<int>(1);
@@ -2565,7 +2564,6 @@ int speigs_plan_apply_block_device(speigs_plan p, const double *x, int64_t ldx, 
             spx::BlockRefineState brf;
             brf.ld = ((int64_t)n + 31) & ~(int64_t)31;
             brf.R = ar.alloc<double>((size_t)brf.ld * nr);
-            brf.D = ar.alloc<double>((size_t)brf.ld * nr);
             brf.part = ar.alloc<double>((size_t)3 * spx::kBlockMaxB * ((n + 255) / 256));
             brf.flag = ar.alloc<int>(1);
             brf.count = ar.alloc<int>(1);

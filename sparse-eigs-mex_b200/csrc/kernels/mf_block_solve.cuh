@@ -44,6 +44,7 @@ struct BSolveArgs {
     double *xc;
     int64_t ldb, ldx;
     int nr;
+    int accumulate;                      // xc += the solution (else xc = it)
     const int *skip;
 };
 
@@ -78,7 +79,10 @@ SPX_DEV double2 brhs2(const BSolveArgs &a, int64_t row, int col) {
 }
 // result column col of original row `row`
 SPX_DEV void bout1(const BSolveArgs &a, int64_t row, int col, double v) {
-    if (col < a.nr) a.xc[(int64_t)col * a.ldx + row] = v;
+    if (col < a.nr) {
+        double *o = a.xc + (int64_t)col * a.ldx + row;
+        *o = a.accumulate ? *o + v : v;
+    }
 }
 
 SPX_DEV void bstage_list(const BSolveArgs &a, int64_t g, int *idx, int *n, int *e0) {

@@ -2315,7 +2315,7 @@ int bsolve_config(int *grid, size_t *smem) {
 
 template <> int MultifrontalPlanT<Real>::solve_block(const double *B, int64_t ldb, double *X,
                                                      int64_t ldx, int nr, cudaStream_t st,
-                                                     const int *skip) {
+                                                     const int *skip, bool accumulate) {
     if (nr < 1 || nr > 32 || !d_meta_) return SPEIGS_ERR_ARG;
     const int w = (nr + 7) & ~7;          // 8, 16, 24 or 32 columns per row
     const int q = w / 8 - 1;
@@ -2376,6 +2376,7 @@ template <> int MultifrontalPlanT<Real>::solve_block(const double *B, int64_t ld
     a.ldb = ldb;
     a.ldx = ldx;
     a.nr = nr;
+    a.accumulate = accumulate ? 1 : 0;
     a.skip = skip;
     cudaMemsetAsync(d_sync_, 0, sizeof(int) * (sync_ints_ - 1), st);
     if (w == 8)

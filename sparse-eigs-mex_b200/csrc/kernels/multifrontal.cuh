@@ -68,10 +68,11 @@ public:
     // dimensions ldb, ldx).  One persistent launch runs the same task queue
     // as solve() with every vector entry widened to nr columns, so the panel
     // and the level structure are paid once for all columns.  `skip` as in
-    // solve().  Returns 0 or a negative code (device buffers for the block
-    // are allocated on first use).
+    // solve(); with `accumulate`, X += the solution instead of X = it.
+    // Returns 0 or a negative code (device buffers for the block are
+    // allocated on first use).
     int solve_block(const double *B, int64_t ldb, double *X, int64_t ldx, int nr,
-                    cudaStream_t st, const int *skip = nullptr);
+                    cudaStream_t st, const int *skip = nullptr, bool accumulate = false);
 
     void release(cudaStream_t st);
 
@@ -152,7 +153,7 @@ using MultifrontalPlan32 = MultifrontalPlanT<float>;
                                                  const int *);                            \
     template <> int MultifrontalPlanT<R>::solve_block(const double *, int64_t, double *,   \
                                                       int64_t, int, cudaStream_t,         \
-                                                      const int *);                       \
+                                                      const int *, bool);                 \
     template <> void MultifrontalPlanT<R>::release(cudaStream_t);                          \
     template <> int *MultifrontalPlanT<R>::error_word() const;                             \
     template <> int64_t MultifrontalPlanT<R>::solve_bytes() const;                         \
