@@ -967,16 +967,21 @@ static int block_lanczos_device(BlockOperator &op, const DevA &A, int n, int64_t
         seed = rng_advance(seed, (uint64_t)n);
     };
     // W (b columns at Wp) <- (I - V V^T) W twice against V[:, 0:m]; with
-    // hcol, the two passes' coefficients are summed into H[0:m, hcol..]
-    auto cgs2 = [&](double *Wp, int m, double *hcol) {
-        if (m <= 0) return;
+    // hcol, the two passes' coefficients are summed into H[0:m, hcol..];
+    // with gram, the Gram matrix W^T W of the result is left in B.G.
+    // Returns whether it was (m > 0).
+    auto cgs2 = [&](double *Wp, int m, double *hcol, bool gram) -> bool {
+        if (m <= 0) return false;
         double *V = B.V;
-        // pass 1's update and pass 2's product share one sweep over V
+        // pass 1's update and pass 2's product share one sweep over V, and
+        // pass 2's update the sweep that forms the Gram matrix
         double *h1 = hcol ? hcol : B.hb;
         launch_tsb_tn(V, B.ldv, n, m, Wp, B.ldv, b, h1, ldh, 0, B.bs, st);
         launch_tsb_sub_tn(V, B.ldv, n, m, h1, ldh, Wp, B.ldv, b, B.hb, ldh, 0, B.bs, st);
-        launch_tsb_nn_sub(V, B.ldv, n, m, B.hb, ldh, Wp, B.ldv, b, st);
+        if (gram) launch_tsb_sub_gram(V, B.ldv, n, m, B.hb, ldh, Wp, B.ldv, b, B.G, B.bs, st);
+        else launch_tsb_nn_sub(V, B.ldv, n, m, B.hb, ldh, Wp, B.ldv, b, st);
         if (hcol) launch_block_axpy_unless(m, b, hcol, ldh, B.hb, ldh, nullptr, st);
+        return gram;
     };
     // Orthonormalise the block at Wp against V[:, 0:m] (already projected
     // out) and within itself by two Cholesky QR passes.  Columns found
@@ -986,17 +991,19 @@ static int block_lanczos_device(BlockOperator &op, const DevA &A, int n, int64_t
     // With spec, the dependency test is not read back: the first pass goes
     // on as if no column were dependent, and the Cholesky kernel's sticky
     // flag (cstat[2]) tells the caller later whether the step must be redone.
+    // gram_ready: B.G already holds W^T W (left there by cgs2).
     auto orthonormalise = [&](double *Wp, int m, unsigned *replaced, bool keep_gram,
-                              bool spec) -> int {
+                              bool spec, bool gram_ready = false) -> int {
         unsigned first_mask = 0;
         if (spec) {
-            launch_tsb_tn(Wp, B.ldv, n, b, Wp, B.ldv, b, B.G, b, 0, B.bs, st);
+            if (!gram_ready) launch_tsb_tn(Wp, B.ldv, n, b, Wp, B.ldv, b, B.G, b, 0, B.bs, st);
             if (keep_gram)
                 cudaMemcpyAsync(B.Gres, B.G, sizeof(double) * b * b, cudaMemcpyDeviceToDevice, st);
             launch_block_chol(b, B.G, b, B.Rinv, bthr, 1e-14, B.cstat, st);
         }
         for (int att = 0; !spec; att++) {
-            launch_tsb_tn(Wp, B.ldv, n, b, Wp, B.ldv, b, B.G, b, 0, B.bs, st);
+            if (!(gram_ready && att == 0))
+                launch_tsb_tn(Wp, B.ldv, n, b, Wp, B.ldv, b, B.G, b, 0, B.bs, st);
             if (keep_gram && att == 0)
                 cudaMemcpyAsync(B.Gres, B.G, sizeof(double) * b * b, cudaMemcpyDeviceToDevice, st);
             launch_block_chol(b, B.G, b, B.Rinv, bthr, 1e-14, B.cstat, st);
@@ -1011,10 +1018,10 @@ static int block_lanczos_device(BlockOperator &op, const DevA &A, int n, int64_t
             }
             for (int c = 0; c < b; c++)
                 if ((mask >> c) & 1u) rand_col(Wp + (size_t)c * B.ldv);
-            cgs2(Wp, m, nullptr);
+            cgs2(Wp, m, nullptr, false);
         }
-        launch_tsb_right_mul(n, b, Wp, B.ldv, B.Rinv, st);
-        launch_tsb_tn(Wp, B.ldv, n, b, Wp, B.ldv, b, B.G, b, 0, B.bs, st);
+        // the first Cholesky QR step and the second step's Gram matrix
+        launch_tsb_mul_gram(n, b, Wp, B.ldv, B.Rinv, B.G, B.bs, st);
         launch_block_chol(b, B.G, b, B.Rinv, 0.0, 0.0, B.cstat, st);
         launch_tsb_right_mul(n, b, Wp, B.ldv, B.Rinv, st);
         if (replaced) *replaced = first_mask;
@@ -1117,9 +1124,9 @@ static int block_lanczos_device(BlockOperator &op, const DevA &A, int n, int64_t
         tm.end(t0, &ms_op);
         mm = jc + b;
         int t1 = tm.begin();
-        cgs2(Wp, mm, B.H + (size_t)jc * ldh);
+        const bool gram = cgs2(Wp, mm, B.H + (size_t)jc * ldh, true);
         unsigned rep = 0;
-        const int stuck = orthonormalise(Wp, mm, &rep, true, spec_cycle);
+        const int stuck = orthonormalise(Wp, mm, &rep, true, spec_cycle, gram);
         if (stuck < 0) return stuck;
         tm.end(t1, &ms_ortho);
         const bool cycle_end = stuck == 1 || mm + b > mmax;

@@ -111,26 +111,39 @@ __global__ void __launch_bounds__(kTbThreads) tsb_tn_part_kernel(
     }
 }
 
-// The first Gram-Schmidt pass's update and the second pass's product in one
-// sweep over V: for each staged 32-row chunk, W[chunk] -= V[chunk] H1 (the
-// arithmetic of tsb_rows_kernel<true>: the same fragments, k in the same
-// order), the new rows written to W and into the staged chunk, then
-// V[chunk]^T W[chunk] accumulated as tsb_tn_part_kernel does -- so the parts,
-// and with them the reduced coefficients, are bit for bit those of the two
-// separate kernels, for one read of V instead of two.  H1 (m x b, leading
-// dimension ldh1) is staged with rows of b + 4 doubles.
-__global__ void __launch_bounds__(kTbThreads) tsb_sub_tn_part_kernel(
+// Fused passes over the staged 32-row chunks of one row range, each
+// first updating W and then accumulating a product of the updated chunk
+// into part[block] exactly as tsb_tn_part_kernel does:
+//   kSubTn:   W -= V H1, then V^T W  (the first Gram-Schmidt pass's update
+//             and the second pass's product: one read of V for both);
+//   kSubGram: W -= V H1, then W^T W  (the second pass's update and the
+//             Gram matrix of the Cholesky QR);
+//   kMulGram: W = W H1 (H1 = R^{-1}, b x b), then W^T W (a Cholesky QR
+//             step and the Gram matrix of the next one).
+// The update uses the fragments and the k order of tsb_rows_kernel and the
+// product those of tsb_tn_part_kernel, so the results are bit for bit those
+// of the separate kernels.  H1 (K x b, leading dimension ldh1; K = m, or b
+// for kMulGram) is staged with rows of b + 4 doubles.
+enum { kSubTn = 0, kSubGram = 1, kMulGram = 2 };
+
+template <int MODE>
+__global__ void __launch_bounds__(kTbThreads) tsb_fused_part_kernel(
         const double *__restrict__ V, int64_t ldv, int n, int m, const double *__restrict__ H1,
         int ldh1, double *__restrict__ W, int64_t ldw, int b, int rows_per_part,
         double *__restrict__ part) {
     extern __shared__ double dsm[];
     const int t = threadIdx.x, lane = t & 31, wid = t >> 5, gq = lane >> 2, tq = lane & 3;
-    const int nmt = (m + 7) >> 3, nnt = (b + 7) >> 3, ncol = m + b;
-    const int nks = (m + 3) >> 2, sbs = nnt * 8 + 4;
+    if (MODE == kMulGram) m = 0;                          // no V: the chunk is W alone
+    const int nnt = (b + 7) >> 3, ncol = m + b;
+    const int K = MODE == kMulGram ? b : m;               // inner size of the update
+    const int nks = (K + 3) >> 2, sbs = nnt * 8 + 4;
+    // the product's A side: V (kSubTn) or the updated W
+    const int pa = MODE == kSubTn ? 0 : m, pm = MODE == kSubTn ? m : b;
+    const int nmt = (pm + 7) >> 3;
     double *Bs = dsm + 2 * ncol * kVS;                   // H1: nks * 4 rows of sbs
     for (int e = t; e < nks * 4 * sbs; e += kTbThreads) {
         const int k = e / sbs, j = e % sbs;
-        Bs[e] = (k < m && j < b) ? H1[k + (int64_t)j * ldh1] : 0.0;
+        Bs[e] = (k < K && j < b) ? H1[k + (int64_t)j * ldh1] : 0.0;
     }
     double acc[2][4][2];
 #pragma unroll
@@ -158,22 +171,36 @@ __global__ void __launch_bounds__(kTbThreads) tsb_sub_tn_part_kernel(
             cp_async_wait<0>();
         }
         __syncthreads();
-        // W[chunk] -= V[chunk] H1: output tile ti = (8-row tile ti % 4,
-        // 8-column tile ti / 4), tiles taken by the warps in turn
-        for (int ti = wid; ti < 4 * nnt; ti += kTbThreads / 32) {
-            const int rt = ti & 3, q = ti >> 2;
-            double d[2] = {0.0, 0.0};
-            for (int ks = 0; ks < nks; ks++) {
-                const int k = ks * 4 + tq;
-                dmma884(d, k < m ? Cs[k * kVS + rt * 8 + gq] : 0.0, Bs[k * sbs + q * 8 + gq]);
+        // the update of W[chunk]: output tile ti = (8-row tile ti % 4,
+        // 8-column tile ti / 4), tiles taken by the warps in turn; the A
+        // side is staged column k (of V, or of W itself for kMulGram, whose
+        // products all finish before any of them is written)
+        double dv[2][2];
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const int ti = wid + u * (kTbThreads / 32);
+            dv[u][0] = dv[u][1] = 0.0;
+            if (ti < 4 * nnt) {
+                const int rt = ti & 3, q = ti >> 2;
+                for (int ks = 0; ks < nks; ks++) {
+                    const int k = ks * 4 + tq;
+                    const double av = k < K ? Cs[k * kVS + rt * 8 + gq] : 0.0;
+                    dmma884(dv[u], av, Bs[k * sbs + q * 8 + gq]);
+                }
             }
-            const int rr = rt * 8 + gq;
+        }
+        if (MODE == kMulGram) __syncthreads();
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const int ti = wid + u * (kTbThreads / 32);
+            if (ti >= 4 * nnt) continue;
+            const int rt = ti & 3, q = ti >> 2, rr = rt * 8 + gq;
 #pragma unroll
             for (int e = 0; e < 2; e++) {
                 const int j = q * 8 + 2 * tq + e;
                 if (j < b) {
                     double *cw = Cs + (m + j) * kVS + rr;
-                    const double v = *cw - d[e];
+                    const double v = MODE == kMulGram ? dv[u][e] : *cw - dv[u][e];
                     *cw = v;
                     if (r0 + rr < re) W[r0 + rr + (int64_t)j * ldw] = v;
                 }
@@ -190,7 +217,7 @@ __global__ void __launch_bounds__(kTbThreads) tsb_sub_tn_part_kernel(
             for (int s = 0; s < 2; s++) {
                 const int mt = wid + 8 * s;
                 if (mt < nmt) {
-                    const double a = (mt * 8 + gq < m) ? Cs[(mt * 8 + gq) * kVS + k] : 0.0;
+                    const double a = (mt * 8 + gq < pm) ? Cs[(pa + mt * 8 + gq) * kVS + k] : 0.0;
 #pragma unroll
                     for (int q = 0; q < 4; q++)
                         if (q < nnt) dmma884(acc[s][q], a, bf[q]);
@@ -535,29 +562,56 @@ void launch_tsb_tn(const double *V, int64_t ldv, int n, int m, const double *W, 
     note_launch(2);
 }
 
-void launch_tsb_sub_tn(const double *V, int64_t ldv, int n, int m, const double *H1, int ldh1,
-                       double *W, int64_t ldw, int b, double *H2, int ldh2, int mode,
-                       const BlockScratch &bs, cudaStream_t st) {
-    if (m <= 0 || b <= 0) return;
+namespace {
+// one fused pass (tsb_fused_part_kernel<MODE>) and the reduction of its
+// parts into H2 (pm x b, leading dimension ldh2)
+template <int MODE>
+void launch_fused(const double *V, int64_t ldv, int n, int m, const double *H1, int ldh1,
+                  double *W, int64_t ldw, int b, double *H2, int ldh2, int mode,
+                  const BlockScratch &bs, cudaStream_t st) {
     const int nparts = std::min(tsb_parts(n), bs.max_parts);
     int rows = (n + nparts - 1) / nparts;
     rows = (rows + kTbRows - 1) / kTbRows * kTbRows;
     const int np = (n + rows - 1) / rows;
-    const int nnt = (b + 7) >> 3, nks = (m + 3) >> 2;
-    const size_t smem = sizeof(double) * (2 * (size_t)(m + b) * kVS + (size_t)nks * 4 * (nnt * 8 + 4));
+    const int mm = MODE == kMulGram ? 0 : m, K = MODE == kMulGram ? b : m;
+    const int nnt = (b + 7) >> 3, nks = (K + 3) >> 2;
+    const size_t smem =
+        sizeof(double) * (2 * (size_t)(mm + b) * kVS + (size_t)nks * 4 * (nnt * 8 + 4));
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(tsb_sub_tn_part_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(tsb_fused_part_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(sizeof(double) * (2 * (kBlockMaxM + kBlockMaxB) * kVS +
                                                      kBlockMaxM * (kBlockMaxB + 4))));
         attr = true;
     }
-    tsb_sub_tn_part_kernel<<<np, kTbThreads, smem, st>>>(V, ldv, n, m, H1, ldh1, W, ldw, b, rows,
-                                                         bs.part);
-    const int outs = m * kBlockMaxB;
-    tsb_tn_reduce_kernel<<<(outs + 31) / 32, 32 * kRedSlices, 0, st>>>(m, b, np, bs.part, H2, ldh2,
+    tsb_fused_part_kernel<MODE><<<np, kTbThreads, smem, st>>>(V, ldv, n, mm, H1, ldh1, W, ldw, b,
+                                                               rows, bs.part);
+    const int pm = MODE == kSubTn ? m : b;
+    const int outs = pm * kBlockMaxB;
+    tsb_tn_reduce_kernel<<<(outs + 31) / 32, 32 * kRedSlices, 0, st>>>(pm, b, np, bs.part, H2, ldh2,
                                                                        mode);
     note_launch(2);
+}
+}  // namespace
+
+void launch_tsb_sub_tn(const double *V, int64_t ldv, int n, int m, const double *H1, int ldh1,
+                       double *W, int64_t ldw, int b, double *H2, int ldh2, int mode,
+                       const BlockScratch &bs, cudaStream_t st) {
+    if (m <= 0 || b <= 0) return;
+    launch_fused<kSubTn>(V, ldv, n, m, H1, ldh1, W, ldw, b, H2, ldh2, mode, bs, st);
+}
+
+void launch_tsb_sub_gram(const double *V, int64_t ldv, int n, int m, const double *H1, int ldh1,
+                         double *W, int64_t ldw, int b, double *G, const BlockScratch &bs,
+                         cudaStream_t st) {
+    if (m <= 0 || b <= 0) return;
+    launch_fused<kSubGram>(V, ldv, n, m, H1, ldh1, W, ldw, b, G, b, 0, bs, st);
+}
+
+void launch_tsb_mul_gram(int n, int b, double *W, int64_t ldw, const double *Rinv, double *G,
+                         const BlockScratch &bs, cudaStream_t st) {
+    if (b <= 0) return;
+    launch_fused<kMulGram>(nullptr, 0, n, 0, Rinv, b, W, ldw, b, G, b, 0, bs, st);
 }
 
 void launch_tsb_nn_sub(const double *V, int64_t ldv, int n, int m, const double *H, int ldh,

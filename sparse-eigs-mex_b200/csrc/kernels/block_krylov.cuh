@@ -35,6 +35,15 @@ void launch_tsb_nn_sub(const double *V, int64_t ldv, int n, int m, const double 
 void launch_tsb_sub_tn(const double *V, int64_t ldv, int n, int m, const double *H1, int ldh1,
                        double *W, int64_t ldw, int b, double *H2, int ldh2, int mode,
                        const BlockScratch &bs, cudaStream_t st);
+// W[:, 0:b] -= V[:, 0:m] H1, then G = W^T W (b x b, leading dimension b),
+// in one sweep; bit for bit launch_tsb_nn_sub followed by launch_tsb_tn(W, W).
+void launch_tsb_sub_gram(const double *V, int64_t ldv, int n, int m, const double *H1, int ldh1,
+                         double *W, int64_t ldw, int b, double *G, const BlockScratch &bs,
+                         cudaStream_t st);
+// W[:, 0:b] = W Rinv (Rinv b x b, leading dimension b), then G = W^T W, in one
+// sweep; bit for bit launch_tsb_right_mul followed by launch_tsb_tn(W, W).
+void launch_tsb_mul_gram(int n, int b, double *W, int64_t ldw, const double *Rinv, double *G,
+                         const BlockScratch &bs, cudaStream_t st);
 // Gram matrix G (b x b) of a block -> Rinv (b x b, upper triangular) with
 // G = R^T R, by a Cholesky of the column-scaled G.  status[0] receives a
 // bit mask of dependent columns: column j is dependent when its norm is
