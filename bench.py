@@ -404,13 +404,17 @@ def run_metric(args, pkg, wl, ctx):
         t0 = time.perf_counter()
         extra_h2d = extra_d2h = 0
         if learned:
-            Yp = L.propose(net, N, kap)
+            # the proposal stays on the device: its graph and features go up,
+            # the network runs, and speigs_ex takes the device subspace
+            Yd = L.propose(net, N, kap, on_device=True)
             extra_h2d = rowptr.nbytes + col.nbytes + wts.nbytes + X.nbytes
-            extra_d2h = Yp.nbytes // 2          # float32 on the device, widened on the host
             fp = form_params[name]
             ext = s.ext_opts(lib, precision=prec, block=fp["block"])
+            ext.warm = Yd.data_ptr()
+            ext.warm_cols = Yd.shape[0]
             eopts = s.default_opts(lib, tol=TOL, ncv=fp["ncv"])
-            rc, *_ = s.speigs_ex(A, k, s.SM, eopts, ext, vectors=True, lib=lib, warm=Yp)
+            rc, *_ = s.speigs_ex(A, k, s.SM, eopts, ext, vectors=True, lib=lib)
+            del Yd
         else:
             ext = s.ext_opts(lib, precision=prec, block=-1)
             rc, *_ = s.speigs_ex(A, k, s.SM, opts, ext, vectors=True, lib=lib)

@@ -35,7 +35,8 @@ typedef struct {
     double       refine_tol;   /* backward-error target (mixed); 0 => 1e-2 tol, within
                                   [1e-14, 1e-12]                                        */
     const double *warm;        /* optional start subspace, n x warm_cols, column-major,
-                                  host memory; NULL => the reference's random start   */
+                                  host or device memory (on the calling thread's
+                                  device); NULL => the reference's random start       */
     speigs_int   warm_cols;
     int          block;        /* 'sm' Krylov method (see below); 0 => automatic        */
     int          handoff;      /* speigs_batched: the lockstep loop hands its components

@@ -1650,8 +1650,15 @@ static int plan_solve(speigs_plan_s *p, int64_t k, double *lambda, double *V, do
         if (wcols > 0) {
             double *dw = ar.alloc<double>((size_t)n * wcols);
             if (ar.failed) return SPEIGS_ERR_MEM;
-            copy_async(dw, p->ext_warm, sizeof(double) * (size_t)n * wcols,
-                       on_device ? cudaMemcpyDefault : cudaMemcpyHostToDevice, st);
+            // the subspace may be host or device memory (a proposal computed
+            // on the device need not go through the host)
+            cudaMemcpyKind kind = on_device ? cudaMemcpyDefault : cudaMemcpyHostToDevice;
+            cudaPointerAttributes pa{};
+            if (cudaPointerGetAttributes(&pa, p->ext_warm) == cudaSuccess &&
+                (pa.type == cudaMemoryTypeDevice || pa.type == cudaMemoryTypeManaged))
+                kind = cudaMemcpyDeviceToDevice;
+            cudaGetLastError();
+            copy_async(dw, p->ext_warm, sizeof(double) * (size_t)n * wcols, kind, st);
             if (cudaError_t e = cudaStreamSynchronize(st)) return cuda_fail(e, "start subspace upload");
             dwarm = dw;
         }

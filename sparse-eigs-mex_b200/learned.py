@@ -174,8 +174,10 @@ class WarmStartNet:
             pass
 
 
-def propose(net: WarmStartNet, N: int, kap: np.ndarray) -> np.ndarray:
-    """The network's proposal for one operator: n x nout float64 (host)."""
+def propose(net: WarmStartNet, N: int, kap: np.ndarray, on_device: bool = False):
+    """The network's proposal for one operator: n x nout float64 (host), or
+    with on_device a CUDA tensor of shape (nout, n) -- column-major n x nout,
+    usable directly as speigs_ext_opts.warm."""
     import torch
     rowptr, col, w = grid_graph(N, kap)
     X = features(N, kap)
@@ -191,5 +193,10 @@ def propose(net: WarmStartNet, N: int, kap: np.ndarray) -> np.ndarray:
                             t_Y.data_ptr(), 0)
     if rc != 0:
         raise RuntimeError(f"mpnn_forward rc={rc}")
+    if on_device:
+        Y = t_Y.t().double().contiguous()
+        # the solver reads it on its own stream
+        torch.cuda.synchronize()
+        return Y
     torch.cuda.synchronize()
     return t_Y.double().cpu().numpy()

@@ -87,3 +87,31 @@ def test_wide_start_subspace_reduced_to_its_best_block(lib, pkg):
     assert np.max(np.abs(lam2 - lam0) / np.abs(lam0)) <= 1e-10
     r = np.linalg.norm(A @ V2 - V2 * lam2, axis=0)
     assert r.max() <= 1e-10 * info2["anorm"] * 1.0001
+
+
+def test_device_subspace_equals_host_subspace(lib, pkg):
+    """speigs_ext_opts.warm may point to device memory (a proposal computed
+    on the GPU): the eigenpairs are bit for bit those of the same subspace
+    given from host memory, and its bytes are not counted as host-to-device
+    traffic."""
+    torch = pytest.importorskip("torch")
+    s = pkg.speigs
+    A = pkg.workloads.varcoef3d(18, seed=4)
+    n, k, p = A.shape[0], 6, 8
+    rng = np.random.default_rng(3)
+    Y = np.asfortranarray(rng.standard_normal((n, p)))
+    o = s.default_opts(lib, tol=1e-10)
+    c0 = s.counters(lib)
+    rc, lam, V, res, info, ei = s.speigs_ex(A, k, s.SM, o, s.ext_opts(lib, block=8), lib=lib,
+                                            warm=Y)
+    c1 = s.counters(lib)
+    Yd = torch.from_numpy(np.ascontiguousarray(Y.T)).cuda()      # (p, n): column-major n x p
+    torch.cuda.synchronize()
+    e = s.ext_opts(lib, block=8)
+    e.warm = Yd.data_ptr()
+    e.warm_cols = p
+    rc2, lam2, V2, res2, info2, ei2 = s.speigs_ex(A, k, s.SM, o, e, lib=lib)
+    c2 = s.counters(lib)
+    assert rc == 0 and rc2 == 0 and ei2["warm_cols"] == ei["warm_cols"] == p
+    assert np.array_equal(lam, lam2) and np.array_equal(V, V2)
+    assert (c1[1] - c0[1]) - (c2[1] - c1[1]) == Y.nbytes
