@@ -245,17 +245,24 @@ def run_metric(args, pkg, wl, ctx):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     peak, peak_kind = measured_peaks()
 
-    # the proposal's inputs on the device (the learned forms read them there)
-    rowptr, col, wts = L.grid_graph(N, kap)
+    # the proposal's inputs on the device (the learned forms read them
+    # there): the conductivities and the node features; the network's graph
+    # is built from the conductivities on the device in every step
     X = L.features(N, kap)
-    t_rp = torch.from_numpy(rowptr).to(dev)
-    t_ci = torch.from_numpy(col).to(dev)
-    t_w = torch.from_numpy(wts).to(dev)
+    t_kap = torch.from_numpy(np.ascontiguousarray(kap, dtype=np.float64).ravel()).to(dev)
+    gnnz = 6 * N * N * (N - 1)
+    t_rp = torch.empty(n + 1, dtype=torch.int32, device=dev)
+    t_ci = torch.empty(gnnz, dtype=torch.int32, device=dev)
+    t_w = torch.empty(gnnz, dtype=torch.float32, device=dev)
     t_X = torch.from_numpy(X).to(dev)
     Y32 = torch.empty((n, P), dtype=torch.float32, device=dev)
     Yw = torch.zeros((P, n), dtype=torch.float64, device=dev)      # column-major n x P
 
     def propose_device(stream):
+        rc = net.grid_graph_device(N, t_kap.data_ptr(), t_rp.data_ptr(), t_ci.data_ptr(),
+                                   t_w.data_ptr(), stream.cuda_stream)
+        if rc != 0:
+            raise RuntimeError(f"mpnn grid graph rc={rc}")
         rc = net.forward_device(n, t_rp.data_ptr(), t_ci.data_ptr(), t_w.data_ptr(),
                                 t_X.data_ptr(), Y32.data_ptr(), stream.cuda_stream)
         if rc != 0:
@@ -407,7 +414,7 @@ def run_metric(args, pkg, wl, ctx):
             # the proposal stays on the device: its graph and features go up,
             # the network runs, and speigs_ex takes the device subspace
             Yd = L.propose(net, N, kap, on_device=True)
-            extra_h2d = rowptr.nbytes + col.nbytes + wts.nbytes + X.nbytes
+            extra_h2d = kap.nbytes + X.nbytes
             fp = form_params[name]
             ext = s.ext_opts(lib, precision=prec, block=fp["block"])
             ext.warm = Yd.data_ptr()

@@ -149,6 +149,15 @@ void speigs_b200_mpnn_destroy(speigs_mpnn net);
  * SPEIGS_ERR_ARG for a null network.  The two differ only in the order of
  * the FP32 sums. */
 int  speigs_b200_mpnn_tensor_cores(speigs_mpnn net, int on);
+/* The network's input graph for an N x N x N finite-volume grid, built on
+ * the device: the normalised adjacency w_ij = t_ij / sqrt(s_i s_j) of the
+ * operator with face transmissibilities t = 2 k_a k_b / (k_a + k_b) from the
+ * cell conductivities kap (N^3 doubles, index (a0 N + a1) N + a2), s_i the
+ * sum of node i's t.  Rows in node order, neighbours ascending; rowptr has
+ * N^3 + 1 entries, col and w room for 6 N^2 (N - 1).  All pointers are
+ * device memory; queued on `stream`.  Returns 0 or a negative code. */
+int  speigs_b200_mpnn_grid_graph(speigs_mpnn net, int N, const double *kap, int32_t *rowptr,
+                                 int32_t *col, float *w, void *stream);
 /* FP32 weights to (set = 0) or from (set = 1) host memory; host == NULL
  * reports the count in *count. */
 int  speigs_b200_mpnn_params(speigs_mpnn net, float *host, int64_t *count, int set);

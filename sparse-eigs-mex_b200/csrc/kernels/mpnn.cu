@@ -16,6 +16,7 @@
 #include "../counters.h"
 #include "../../../include/speigs_b200.h"
 
+#include <cub/device/device_scan.cuh>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -322,6 +323,63 @@ dense_fwd_tc_kernel(int n, int K1, const bf16 *__restrict__ X1, int K2, const bf
 
 size_t tc_smem(int K, int NP) { return (size_t)(kTcRows + NP) * K * sizeof(bf16); }
 
+// ---- the network's input graph on the device ---------------------------
+// The normalised adjacency of the N^3 finite-volume operator from the cell
+// conductivities kap (node i = (a0 N + a1) N + a2): the neighbours of i are
+// i - N^2, i - N, i - 1, i + 1, i + N, i + N^2 (slots 0..5, ascending) where
+// they lie in the grid; a face between a lower cell a and an upper cell b
+// has t = 2 k_a k_b / (k_a + k_b); s_i = t_0 + ... + t_5 in slot order
+// (absent slots 0); w_ij = t_ij / sqrt(s_i s_j) rounded to FP32.  These are
+// the operations, in the same order, of the host construction, so the CSR
+// is the same to the bit.
+__global__ void grid_faces_kernel(int N, const double *__restrict__ kap, double *__restrict__ T,
+                                  double *__restrict__ s, int32_t *__restrict__ deg) {
+    const int64_t n = (int64_t)N * N * N;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int a0 = (int)(i / ((int64_t)N * N)), a1 = (int)((i / N) % N), a2 = (int)(i % N);
+    const int64_t step[6] = {-(int64_t)N * N, -(int64_t)N, -1, 1, N, (int64_t)N * N};
+    const bool in[6] = {a0 > 0, a1 > 0, a2 > 0, a2 < N - 1, a1 < N - 1, a0 < N - 1};
+    const double ki = kap[i];
+    double acc = 0.0;
+    int d = 0;
+#pragma unroll
+    for (int j = 0; j < 6; j++) {
+        double t = 0.0;
+        if (in[j]) {
+            const double kj = kap[i + step[j]];
+            // slots 0-2: the neighbour is the lower cell; 3-5: this cell is
+            t = j < 3 ? 2.0 * kj * ki / (kj + ki) : 2.0 * ki * kj / (ki + kj);
+        }
+        T[i * 6 + j] = t;
+        acc += t;
+        d += t > 0.0;
+    }
+    s[i] = acc;
+    deg[i] = d;
+}
+
+__global__ void grid_fill_kernel(int N, const double *__restrict__ T, const double *__restrict__ s,
+                                 const int32_t *__restrict__ rowptr, int32_t *__restrict__ col,
+                                 float *__restrict__ w) {
+    const int64_t n = (int64_t)N * N * N;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t step[6] = {-(int64_t)N * N, -(int64_t)N, -1, 1, N, (int64_t)N * N};
+    int32_t q = rowptr[i];
+    const double si = s[i];
+#pragma unroll
+    for (int j = 0; j < 6; j++) {
+        const double t = T[i * 6 + j];
+        if (t > 0.0) {
+            const int64_t c = i + step[j];
+            col[q] = (int32_t)c;
+            w[q] = (float)(t / sqrt(si * s[c]));
+            q++;
+        }
+    }
+}
+
 // ---- loss: G = Y^T Y (P x P), B = Y^T U (P x k), FP64 sums
 __global__ void __launch_bounds__(kThreads)
 gram_kernel(int n, int P, const float *__restrict__ Y, int k, const float *__restrict__ U,
@@ -470,8 +528,16 @@ struct speigs_mpnn_s {
     // set by a tensor-core wait that ran out; mapped page-locked memory, so
     // the host reads it without synchronising the stream
     int *err_h = nullptr, *err_d = nullptr;
+    // scratch of the device grid graph: face values (6 a node), node sums,
+    // degrees and the scan's temporary storage
+    double *gT = nullptr, *gs = nullptr;
+    int32_t *gdeg = nullptr;
+    void *gscan = nullptr;
+    size_t gscan_bytes = 0;
+    int64_t gcap = 0;
     ~speigs_mpnn_s() {
-        void *ptrs[] = {p, g, m, v, pb, Hs, Ms, Y, dY, dH, dH2, dM, G, B, loss, C};
+        void *ptrs[] = {p, g, m, v, pb, Hs, Ms, Y, dY, dH, dH2, dM, G, B, loss, C, gT, gs, gdeg,
+                        gscan};
         for (void *q : ptrs)
             if (q) cudaFree(q);
         if (err_h) cudaFreeHost(err_h);
@@ -632,6 +698,37 @@ int speigs_b200_mpnn_create(int nfeat, int hidden, int layers, int nout, uint64_
 }
 
 void speigs_b200_mpnn_destroy(speigs_mpnn net) { delete net; }
+
+int speigs_b200_mpnn_grid_graph(speigs_mpnn net, int N, const double *kap, int32_t *rowptr,
+                                int32_t *col, float *w, void *stream) {
+    if (!net || N < 1 || (int64_t)N * N * N > INT32_MAX / 6 || !kap || !rowptr || !col || !w)
+        return SPEIGS_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    const int64_t n = (int64_t)N * N * N;
+    if (n > net->gcap) {
+        void *old[] = {net->gT, net->gs, net->gdeg, net->gscan};
+        for (void *q : old)
+            if (q) cudaFree(q);
+        net->gT = dalloc<double>((size_t)n * 6);
+        net->gs = dalloc<double>((size_t)n);
+        net->gdeg = dalloc<int32_t>((size_t)n);
+        net->gscan_bytes = 0;
+        cub::DeviceScan::InclusiveSum(nullptr, net->gscan_bytes, net->gdeg, rowptr + 1, (int)n, st);
+        net->gscan = net->gscan_bytes ? (void *)dalloc<unsigned char>(net->gscan_bytes) : nullptr;
+        net->gcap = (net->gT && net->gs && net->gdeg && (net->gscan || !net->gscan_bytes)) ? n : 0;
+        if (!net->gcap) return SPEIGS_ERR_MEM;
+    }
+    const int tb = 256, nb = (int)((n + tb - 1) / tb);
+    grid_faces_kernel<<<nb, tb, 0, st>>>(N, kap, net->gT, net->gs, net->gdeg);
+    cudaMemsetAsync(rowptr, 0, sizeof(int32_t), st);
+    size_t tmp = net->gscan_bytes;
+    cub::DeviceScan::InclusiveSum(net->gscan, tmp, net->gdeg, rowptr + 1, (int)n, st);
+    grid_fill_kernel<<<nb, tb, 0, st>>>(N, net->gT, net->gs, rowptr, col, w);
+    spx::note_launch(3);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) { spx::set_last_error_text(cudaGetErrorString(e)); return SPEIGS_ERR_INTERNAL; }
+    return SPEIGS_OK;
+}
 
 int speigs_b200_mpnn_tensor_cores(speigs_mpnn net, int on) {
     if (!net) return SPEIGS_ERR_ARG;

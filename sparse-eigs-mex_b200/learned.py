@@ -36,6 +36,8 @@ def _bind(lib):
                                             POINTER(c_void_p)]),
         "speigs_b200_mpnn_destroy": (None, [c_void_p]),
         "speigs_b200_mpnn_tensor_cores": (c_int, [c_void_p, c_int]),
+        "speigs_b200_mpnn_grid_graph": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p,
+                                                c_void_p, c_void_p]),
         "speigs_b200_mpnn_params": (c_int, [c_void_p, c_void_p, POINTER(c_int64), c_int]),
         "speigs_b200_mpnn_grads": (c_int, [c_void_p, c_void_p]),
         "speigs_b200_mpnn_forward": (c_int, [c_void_p, c_int64, c_void_p, c_void_p, c_void_p,
@@ -138,6 +140,12 @@ class WarmStartNet:
         setting."""
         return int(self.lib.speigs_b200_mpnn_tensor_cores(self.h, on))
 
+    def grid_graph_device(self, N, kap, rowptr, col, w, stream=0):
+        """grid_graph on the device: kap (N^3 float64), rowptr (N^3 + 1 int32),
+        col (int32) and w (float32) with room for 6 N^2 (N - 1) entries, all
+        device pointers.  The CSR is grid_graph's to the bit."""
+        return self.lib.speigs_b200_mpnn_grid_graph(self.h, N, kap, rowptr, col, w, stream)
+
     def forward_device(self, n, rowptr, col, w, X, Y, stream=0):
         """All arguments are device pointers (ints)."""
         return self.lib.speigs_b200_mpnn_forward(self.h, n, rowptr, col, w, X, Y, stream)
@@ -179,16 +187,22 @@ def propose(net: WarmStartNet, N: int, kap: np.ndarray, on_device: bool = False)
     with on_device a CUDA tensor of shape (nout, n) -- column-major n x nout,
     usable directly as speigs_ext_opts.warm."""
     import torch
-    rowptr, col, w = grid_graph(N, kap)
     X = features(N, kap)
     dev = torch.device("cuda")
-    t_rp = torch.from_numpy(rowptr).to(dev)
-    t_ci = torch.from_numpy(col).to(dev)
-    t_w = torch.from_numpy(w).to(dev)
-    t_X = torch.from_numpy(X).to(dev)
     n = N ** 3
+    # the graph is built on the device from the conductivities
+    t_kap = torch.from_numpy(np.ascontiguousarray(kap, dtype=np.float64).ravel()).to(dev)
+    t_rp = torch.empty(n + 1, dtype=torch.int32, device=dev)
+    nnz = 6 * N * N * max(N - 1, 0)
+    t_ci = torch.empty(max(nnz, 1), dtype=torch.int32, device=dev)
+    t_w = torch.empty(max(nnz, 1), dtype=torch.float32, device=dev)
+    t_X = torch.from_numpy(X).to(dev)
     t_Y = torch.empty((n, net.nout), dtype=torch.float32, device=dev)
     torch.cuda.synchronize()
+    rc = net.grid_graph_device(N, t_kap.data_ptr(), t_rp.data_ptr(), t_ci.data_ptr(),
+                               t_w.data_ptr(), 0)
+    if rc != 0:
+        raise RuntimeError(f"mpnn_grid_graph rc={rc}")
     rc = net.forward_device(n, t_rp.data_ptr(), t_ci.data_ptr(), t_w.data_ptr(), t_X.data_ptr(),
                             t_Y.data_ptr(), 0)
     if rc != 0:

@@ -90,3 +90,28 @@ def test_tensor_core_layers_match_fma_layers(pkg, N, P):
     assert np.all(np.isfinite(a))
     err = np.linalg.norm(a - b) / np.linalg.norm(b)
     assert err < 1e-2, err
+
+
+@pytest.mark.parametrize("N", [1, 2, 6, 48])
+def test_device_grid_graph_is_host_grid_graph(pkg, N):
+    """The network's input graph built on the device from the conductivities
+    equals the host construction bit for bit (row pointers, columns and
+    FP32 weights), including the smallest grids."""
+    torch = pytest.importorskip("torch")
+    L = pkg.learned
+    rng = np.random.default_rng(N)
+    kap = np.exp(rng.standard_normal((N, N, N)))
+    rp, ci, w = L.grid_graph(N, kap)
+    net = L.WarmStartNet(nout=8, layers=1, seed=3)
+    n, nnz = N ** 3, 6 * N * N * (N - 1)
+    t_kap = torch.from_numpy(kap.ravel()).cuda()
+    t_rp = torch.empty(n + 1, dtype=torch.int32, device="cuda")
+    t_ci = torch.empty(max(nnz, 1), dtype=torch.int32, device="cuda")
+    t_w = torch.empty(max(nnz, 1), dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    assert net.grid_graph_device(N, t_kap.data_ptr(), t_rp.data_ptr(), t_ci.data_ptr(),
+                                 t_w.data_ptr(), 0) == 0
+    torch.cuda.synchronize()
+    assert np.array_equal(t_rp.cpu().numpy(), rp) and rp[-1] == nnz
+    assert np.array_equal(t_ci.cpu().numpy()[:nnz], ci)
+    assert np.array_equal(t_w.cpu().numpy()[:nnz], w)
