@@ -80,7 +80,8 @@ def grid_graph(N: int, kap: np.ndarray):
     step = np.array([-N * N, -N, -1, 1, N, N * N], dtype=np.int64)
     cols = np.arange(n, dtype=np.int64)[:, None] + step[None, :]
     s = T.sum(axis=1)
-    W = T / np.sqrt(s[:, None] * s[np.where(present, cols, 0)])
+    with np.errstate(invalid="ignore", divide="ignore"):    # absent slots are dropped below
+        W = T / np.sqrt(s[:, None] * s[np.where(present, cols, 0)])
     rowptr = np.zeros(n + 1, dtype=np.int32)
     np.cumsum(present.sum(axis=1), out=rowptr[1:])
     return rowptr, cols[present].astype(np.int32), W[present].astype(np.float32)
