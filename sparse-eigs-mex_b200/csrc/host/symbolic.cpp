@@ -344,7 +344,11 @@ int order_nd(int32_t n, const int64_t *rowptr, const int32_t *col, int32_t *perm
         Graph g{n, rowptr, col};
         NDState st(g, perm);
         const unsigned hw = std::thread::hardware_concurrency();
-        st.spare_threads = (int)std::min(hw > 1 ? hw - 1 : 0u, 31u);
+        // helper threads for the halves of a split: more than the cores, so
+        // that a large half never waits behind its sibling's whole subtree
+        // because every helper was taken at the moment of its split (the
+        // ordering itself does not depend on the schedule)
+        st.spare_threads = (int)std::min(hw > 1 ? 4 * hw : 0u, 64u);
         std::vector<int32_t> all(n);
         for (int32_t i = 0; i < n; i++) all[i] = i;
         st.order_region(std::move(all), 0, 0);
