@@ -696,11 +696,14 @@ SPX_DEV void mma_tf32(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
 
-// F_IJ -= L_Ik L_Jk^T on FP32 tiles: warp tile 32 x 32 = 2 x 4 fragments
+// F_IJ -= L_Ik L_Jk^T on FP32 tiles: warp tile 32 x 32 = 2 x 4 fragments.
+// The output tile is staged in Cs with the operands, so the subtraction does
+// not wait on global loads after the products.
 SPX_DEV void update_tile_f32(float *Fs, int ld, int ra, int h, int ca, int w, int ka, int kw,
-                             float *As, float *Bs) {
+                             float *As, float *Bs, float *Cs) {
     ftile_load_f32(As, Fs, ld, ra, h, ka, kw);
     ftile_load_f32(Bs, Fs, ld, ca, w, ka, kw);
+    ftile_load_f32(Cs, Fs, ld, ra, h, ca, w);
     asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
     __syncthreads();
     const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
@@ -746,7 +749,8 @@ SPX_DEV void update_tile_f32(float *Fs, int ld, int ra, int h, int ca, int w, in
 #pragma unroll
             for (int e = 0; e < 4; e++) {
                 const int m = m0 + 16 * i + g + 8 * (e >> 1), n = n0 + 8 * j + 2 * t + (e & 1);
-                if (m < h && n < w) Fs[(int64_t)(ra + m) + (int64_t)(ca + n) * ld] -= acc[i][j][e];
+                if (m < h && n < w)
+                    Fs[(int64_t)(ra + m) + (int64_t)(ca + n) * ld] = Cs[n * FLDF + m] - acc[i][j][e];
             }
 }
 
@@ -765,8 +769,8 @@ mf_update64(const int4 *__restrict__ tasks, Sym y, Real *__restrict__ F, const i
     const int h = rb - ra, w = cb - ca, kw = kz - ka;
     Real *Fs = F + f.fptr;
     if constexpr (std::is_same<Real, float>::value) {
-        float *As = reinterpret_cast<float *>(fsm), *Bs = As + FT * FLDF;
-        update_tile_f32(reinterpret_cast<float *>(Fs), f.r, ra, h, ca, w, ka, kw, As, Bs);
+        float *As = reinterpret_cast<float *>(fsm), *Bs = As + FT * FLDF, *Cs = Bs + FT * FLDF;
+        update_tile_f32(reinterpret_cast<float *>(Fs), f.r, ra, h, ca, w, ka, kw, As, Bs, Cs);
     } else {
         // the output tile is staged with the operands, so the subtraction
         // does not wait on global loads after the products
