@@ -325,7 +325,7 @@ SPX_DEV void dmma(double &d0, double &d1, double a, double b) {
                  : "+d"(d0), "+d"(d1) : "d"(a), "d"(b));
 }
 
-// Tile loads go through cp.async (8 bytes per element, zero-filled outside
+// Tile loads go through cp.async (one element per copy, zero-filled outside
 // the h x w block), so all of a thread's 32 element copies are in flight at
 // once; cp_wait() completes them and makes them visible to the block.
 SPX_DEV void cp_async8(double *dst, const double *src, bool valid) {
@@ -343,12 +343,65 @@ SPX_DEV void cp_wait_all_but_last() {
     asm volatile("cp.async.wait_group 1;" ::: "memory");
     __syncthreads();
 }
-// one element of a tile: an asynchronous copy for FP64 storage, a load and
-// widening conversion for FP32 storage (zero when !valid)
+SPX_DEV void cp_async4(float *dst, const float *src, bool valid) {
+    const unsigned saddr = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(saddr), "l"(src),
+                 "r"(valid ? 4 : 0) : "memory");
+}
+// FP32 storage: element (i, j) of a tile is copied asynchronously (4 bytes)
+// to a 64 x 65 float staging area at the top of the tile's own storage,
+// float offset kStageOff + j * FST + i, and the tile is widened in place
+// once the copies are complete (tile_widen).  The staging area starts above
+// the FP64 columns 0 .. 31, so only the second half of the widening has to
+// wait until every staged float has been read.
+constexpr int FST = 65;
+constexpr int kStageOff = 2 * kFTileDoubles - FT * FST;
+static_assert(kStageOff * 4 >= 32 * FLD * 8, "staging area overlaps the first 32 columns");
+
+// one element of a tile (zero when !valid)
 template <class MT>
-SPX_DEV void elem_copy(double *dst, const MT *src, bool valid) {
-    if constexpr (std::is_same<MT, double>::value) cp_async8(dst, src, valid);
-    else *dst = valid ? (double)*src : 0.0;
+SPX_DEV void elem_copy(double *s, int i, int j, const MT *src, bool valid) {
+    if constexpr (std::is_same<MT, double>::value) cp_async8(s + j * FLD + i, src, valid);
+    else cp_async4(reinterpret_cast<float *>(s) + kStageOff + j * FST + i, src, valid);
+}
+
+// Widen a staged FP32 tile to FP64 in place (a no-op for FP64 storage).  The
+// block's copies must be complete and visible (cp_wait); the caller
+// synchronises the block again before the tile is read.
+template <class MT>
+SPX_DEV void tile_widen(double *s) {
+    if constexpr (!std::is_same<MT, double>::value) {
+        constexpr int kPer = FT * FT / kGThreads, kHalf = kPer / 2;
+        const float *f = reinterpret_cast<const float *>(s) + kStageOff;
+        float hi[kHalf];
+#pragma unroll
+        for (int q = 0; q < kHalf; q++) {
+            const int t = threadIdx.x + (q + kHalf) * kGThreads;
+            hi[q] = f[(t >> 6) * FST + (t & (FT - 1))];
+        }
+#pragma unroll
+        for (int q = 0; q < kHalf; q++) {
+            const int t = threadIdx.x + q * kGThreads;
+            s[(t >> 6) * FLD + (t & (FT - 1))] = (double)f[(t >> 6) * FST + (t & (FT - 1))];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < kHalf; q++) {
+            const int t = threadIdx.x + (q + kHalf) * kGThreads;
+            s[(t >> 6) * FLD + (t & (FT - 1))] = (double)hi[q];
+        }
+    }
+}
+
+// complete the block's tile copies and make the tiles a (and b) readable
+template <class MT>
+SPX_DEV void tiles_ready(double *a, double *b = nullptr) {
+    cp_wait();
+    if constexpr (!std::is_same<MT, double>::value) {
+        tile_widen<MT>(a);
+        if (b) tile_widen<MT>(b);
+        __syncthreads();
+    }
 }
 
 // s(i, j) = M(ra + i, ca + j) for i < h, j < w; zero elsewhere in the tile
@@ -359,7 +412,7 @@ SPX_DEV void ftile_load(double *s, const MT *M, int64_t ld, int ra, int h, int c
         const int t = threadIdx.x + q * kGThreads;
         const int i = t & (FT - 1), j = t >> 6;
         const bool v = (i < h && j < w);
-        elem_copy(s + j * FLD + i, v ? M + (int64_t)(ra + i) + (int64_t)(ca + j) * ld : M, v);
+        elem_copy(s, i, j, v ? M + (int64_t)(ra + i) + (int64_t)(ca + j) * ld : M, v);
     }
 }
 // s(i, j) = M(ca + j, ra + i): the transpose of the stored block
@@ -370,7 +423,7 @@ SPX_DEV void ftile_load_t(double *s, const MT *M, int64_t ld, int ra, int h, int
         const int t = threadIdx.x + q * kGThreads;
         const int j = t & (FT - 1), i = t >> 6;
         const bool v = (i < h && j < w);
-        elem_copy(s + j * FLD + i, v ? M + (int64_t)(ca + j) + (int64_t)(ra + i) * ld : M, v);
+        elem_copy(s, i, j, v ? M + (int64_t)(ca + j) + (int64_t)(ra + i) * ld : M, v);
     }
 }
 // lower triangle of the w x w block at (a, a); zero elsewhere
@@ -381,7 +434,7 @@ SPX_DEV void ftile_load_lower(double *s, const MT *M, int64_t ld, int a, int w) 
         const int t = threadIdx.x + q * kGThreads;
         const int i = t & (FT - 1), j = t >> 6;
         const bool v = (i < w && j <= i);
-        elem_copy(s + j * FLD + i, v ? M + (int64_t)(a + i) + (int64_t)(a + j) * ld : M, v);
+        elem_copy(s, i, j, v ? M + (int64_t)(a + i) + (int64_t)(a + j) * ld : M, v);
     }
 }
 
@@ -605,7 +658,7 @@ mf_diag64(const int4 *__restrict__ tasks, Sym y, Real *__restrict__ F, Real *__r
     tile_range<FT>(f, kb, ka, kz);
     const int w = kz - ka;
     ftile_load_lower(Ds, F + f.fptr, f.r, ka, w);
-    cp_wait();
+    tiles_ready<Real>(Ds);
     chol_inv_rec<64>(Ds, Ls, Xs, Ts, w, params[1], status, f.first + ka, true);
     Real *Gs = G + f.gptr;
     for (int t = threadIdx.x; t < FT * FT; t += blockDim.x) {
@@ -645,6 +698,11 @@ mf_rows64(const int4 *__restrict__ tasks, Sym y, Real *__restrict__ F,
         if (I + 1 < I0 + nI) load_tile(spare, I + 1);
         cp_commit();
         cp_wait_all_but_last();      // inv(L_kk) and tile I are in
+        if constexpr (!std::is_same<Real, double>::value) {
+            if (I == I0) tile_widen<Real>(Xs);
+            tile_widen<Real>(cur);
+            __syncthreads();
+        }
         int ra, rb;
         tile_range<FT>(f, I, ra, rb);
         const int h = rb - ra;
@@ -665,11 +723,6 @@ mf_rows64(const int4 *__restrict__ tasks, Sym y, Real *__restrict__ F,
 // fragment reads).
 constexpr int FLDF = 72;
 
-SPX_DEV void cp_async4(float *dst, const float *src, bool valid) {
-    const unsigned saddr = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(saddr), "l"(src),
-                 "r"(valid ? 4 : 0) : "memory");
-}
 SPX_DEV void ftile_load_f32(float *s, const float *M, int64_t ld, int ra, int h, int ca, int w) {
 #pragma unroll 8
     for (int q = 0; q < FT * FT / kGThreads; q++) {
@@ -816,7 +869,7 @@ mf_inv_t64(const int4 *__restrict__ tasks, Sym y, Real *__restrict__ F,
         const int kw = kz - ka;
         ftile_load(As, Fs, f.r, ra, h, ka, kw);      // L_ik
         ftile_load(Bs, Gs, f.ldg, ka, kw, ca, w);    // X_kj
-        cp_wait();
+        tiles_ready<Real>(As, Bs);
         warp_mma<false>(acc, As, Bs, (kw + 3) & ~3, h, w);
         __syncthreads();
     }
@@ -848,7 +901,7 @@ mf_inv_x64(const int4 *__restrict__ tasks, Sym y, const Real *__restrict__ F,
         const int kw = kz - ka;
         ftile_load(As, Gs, f.ldg, ra, h, ka, kw);    // X_ik
         ftile_load_t(Bs, Fs, f.r, ka, kw, ca, w);    // T_kj, stored transposed at tile (j, k)
-        cp_wait();
+        tiles_ready<Real>(As, Bs);
         warp_mma<false>(acc, As, Bs, (kw + 3) & ~3, h, w);
         __syncthreads();
     }
@@ -879,7 +932,7 @@ mf_wmul64(const int4 *__restrict__ tasks, Sym y, const Real *__restrict__ F,
         const int kw = kz - ka;
         ftile_load(As, Fs, f.r, ra, h, ka, kw);
         ftile_load(Bs, Gs, f.ldg, ka, kw, ca, w);
-        cp_wait();
+        tiles_ready<Real>(As, Bs);
         warp_mma<false>(acc, As, Bs, (kw + 3) & ~3, h, w);
         __syncthreads();
     }
