@@ -115,9 +115,23 @@ class ClockSampler:
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
+    def _wait_line(self, timeout):
+        t0 = time.time()
+        while not self.lines and time.time() - t0 < timeout and self.proc.poll() is None:
+            time.sleep(0.005)
+
+    def ready(self, timeout=5.0):
+        """Wait until nvidia-smi reports, then drop what it sampled before the
+        timed region (a short region would otherwise see no sample at all)."""
+        if self.proc:
+            self._wait_line(timeout)
+            self.lines.clear()
+
     def stop(self, gpu_index=None):
         if not self.proc:
             return None
+        # a region shorter than the sampling interval: take the next sample
+        self._wait_line(0.5)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -364,6 +378,7 @@ def run_metric(args, pkg, wl, ctx):
         sampler = ClockSampler()
         if is_target:
             sampler.start()
+            sampler.ready()
         ctx["barrier"]()
         torch.cuda.synchronize()
         l0 = s.counters(lib)[0]
@@ -830,6 +845,7 @@ def main():
         sampler = ClockSampler()
         if with_clocks:
             sampler.start()
+            sampler.ready()
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
